@@ -1,0 +1,197 @@
+/*
+ * pdhg_b200.h -- C-ABI of the B200-native PDHG LP engine (libpdhg_b200.so).
+ *
+ * Drop-in for the reference's PDHG engine, sov::Pdhg::solve
+ * (AtharvPhutela/sovereign-solver: include/sovereign/pdhg.hpp:155-172,
+ * src/l1/pdhg.cpp:218-502). The reference has no FFI of its own; this is the
+ * plain-C surface its C++ call sites (apps/sovereign_cli.cpp:196-236,
+ * src/l1/race.cpp:123-129, src/l1/crossover.cpp:192-237) would bind. Only POD
+ * types cross it, no exception crosses it, and every entry returns a
+ * pdhg_error code that mirrors sov::Status (include/sovereign/status.hpp:25-34).
+ *
+ * Units and sense: everything that crosses the ABI is in the ORIGINAL problem's
+ * units and objective sense, exactly like sov::PdhgResult. Scaling (Ruiz +
+ * Pock-Chambolle, src/l1/scaling.cpp:155-205) happens inside the engine.
+ *
+ * Threading: a context is not thread-safe, like sov::Backend (one per thread,
+ * src/l1/race.cpp:126). pdhg_solve is synchronous on the caller's thread; the
+ * checkpoint callback runs on that thread.
+ */
+#ifndef PDHG_B200_H
+#define PDHG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDHG_B200_ABI_VERSION 1
+
+/* Return codes: the order and meaning of sov::Status (status.hpp:25-34). */
+typedef enum {
+    PDHG_OK = 0,
+    PDHG_ERR_UNSUPPORTED = 1,
+    PDHG_ERR_NOT_IMPLEMENTED = 2,
+    PDHG_ERR_INVALID_ARGUMENT = 3,
+    PDHG_ERR_DIMENSION_MISMATCH = 4,
+    PDHG_ERR_OUT_OF_MEMORY = 5,
+    PDHG_ERR_BACKEND = 6, /* the CUDA runtime reported a failure */
+    PDHG_ERR_NUMERICAL_FAILURE = 7
+} pdhg_error;
+
+/* Solve outcomes: sov::PdhgStatus (include/sovereign/pdhg.hpp:74-81). */
+typedef enum {
+    PDHG_STATUS_OPTIMAL = 0,
+    PDHG_STATUS_ITERATION_LIMIT = 1,
+    PDHG_STATUS_TIME_LIMIT = 2,
+    PDHG_STATUS_NUMERICAL_FAILURE = 3,
+    PDHG_STATUS_NOT_SOLVED = 4,
+    PDHG_STATUS_CANCELLED = 5
+} pdhg_status;
+
+/* Arithmetic of the iteration kernels. */
+typedef enum {
+    /* FP64, each sum accumulated in the reference's own order with no fused
+     * multiply-add: iterates, restarts, statuses and results are bit-identical
+     * to the reference's Host backend (src/l0/backend_host.cpp). */
+    PDHG_PREC_FP64_EXACT = 0,
+    /* FP32 matrix values and iterates in the per-iteration kernels; FP64 for
+     * the KKT residuals, the restart decision, the objective and the result. */
+    PDHG_PREC_MIXED = 1,
+    /* FP64 everywhere, warp-parallel sums (not in the reference's order). */
+    PDHG_PREC_FP64 = 2
+} pdhg_precision;
+
+typedef void (*pdhg_checkpoint_fn)(void* user, long long iteration, const double* x_original,
+                                   const double* y_original, double original_residual);
+
+/* sov::PdhgOptions (pdhg.hpp:85-134) + sov::ScalingOptions (scaling.hpp:296-310)
+ * + engine extensions. pdhg_default_options() gives the reference defaults
+ * with every extension off. */
+typedef struct pdhg_options {
+    double tolerance;                   /* 1e-4 */
+    long long max_iterations;           /* 1000000 */
+    double time_limit_seconds;          /* 0 = none */
+    long long restart_check_period;     /* 40 */
+    double restart_sufficient_decrease; /* 0.5 */
+    double step_size_safety;            /* 0.9 */
+    int power_iterations;               /* 30 */
+    int verbose;                        /* restart lines on stderr, as pdhg.cpp:405-407 */
+    /* Ruiz + Pock-Chambolle (scaling.hpp:296-310) */
+    int ruiz_iterations;          /* 8 */
+    double ruiz_tolerance;        /* 1e-2 */
+    double pock_chambolle_alpha;  /* 1.0 */
+    int apply_ruiz;               /* 1 */
+    int apply_pock_chambolle;     /* 1 */
+    /* extensions (off = reference behaviour) */
+    int precision;           /* pdhg_precision; default PDHG_PREC_FP64_EXACT */
+    int termination_rule;    /* 0 = reference absolute residual (pdhg.cpp:383);
+                                1 = relative KKT: max(primal/(1+|b|inf), dual/(1+|c|inf), gap) */
+    long long polish_iterations; /* MIXED only: FP64 iterations allowed after the FP32
+                                    phase stalls (no 2% gain in 25 checks); -1 = the rest
+                                    of max_iterations, 0 = never leave FP32 */
+    int restart_rule;        /* 0 = reference (pdhg.cpp:391-408); 1 = adaptive: restart to
+                                the better of average/current on sufficient (0.2x) or
+                                necessary (0.8x, no progress) decay or when the average
+                                spans 36% of all iterations. 1 needs MIXED or FP64. */
+    int primal_weight_update; /* 0 = reference tau = sigma (pdhg.cpp:263-265); 1 = primal
+                                weight omega (tau = eta/omega, sigma = eta*omega) starts at
+                                |c|/|b| and moves to sqrt(omega |dy|/|dx|) at each restart */
+    const double* x0;        /* optional warm start, original units (n); NULL = proj(0) */
+    const double* y0;        /* optional warm start, original units and sense (m); NULL = 0 */
+    pdhg_checkpoint_fn checkpoint; /* pdhg.hpp:121-134; NULL = none */
+    void* checkpoint_user;
+    const volatile int* cancel_flag; /* CancellationToken (cancellation.hpp:23-30); NULL = none */
+    int trace_iters;         /* record scaled-space x, y after each of the first trace_iters */
+    double* trace_x;         /* iterations: trace_iters * n, host (test support) */
+    double* trace_y;         /* trace_iters * m, host */
+} pdhg_options;
+
+/* sov::PdhgResult (pdhg.hpp:136-153) minus the vectors, which pdhg_solve
+ * writes into caller-owned buffers. */
+typedef struct pdhg_info {
+    int status;                    /* pdhg_status */
+    double objective;
+    double primal_infeasibility;
+    double dual_infeasibility;
+    double duality_gap;
+    long long iterations;
+    long long restarts;
+    double seconds;
+    double operator_norm_estimate;
+    int has_point;                 /* 0 where the reference returns empty vectors */
+    char message[256];
+    /* engine extensions */
+    double relative_kkt;           /* the relative-KKT value of the reported point */
+    long long fp64_iterations;     /* iterations run by FP64 kernels (MIXED: the polish) */
+    long long kernel_launches;     /* engine kernels launched by this solve */
+    double device_seconds;         /* iteration-loop time measured with CUDA events */
+} pdhg_info;
+
+typedef struct pdhg_ctx pdhg_ctx;
+
+int pdhg_abi_version(void);
+void pdhg_default_options(pdhg_options* options);
+const char* pdhg_status_string(int status);      /* to_string(PdhgStatus), pdhg.cpp:17-27 */
+const char* pdhg_error_string(int error);        /* to_string(Status), status.hpp:36-48 */
+
+/* One context per device and thread (replaces make_backend, backend.hpp:172-184). */
+int pdhg_create(int device, pdhg_ctx** out);
+int pdhg_destroy(pdhg_ctx* ctx);
+/* Text of the last error on this context ("" if none). */
+const char* pdhg_last_error(const pdhg_ctx* ctx);
+/* The cudaStream_t every kernel of this context is launched on (for callers
+ * that time or order work against it); NULL for a NULL context. */
+void* pdhg_stream(const pdhg_ctx* ctx);
+
+/* Hands the engine an LP (host buffers, copied). Replaces the Problem handed to
+ * Pdhg::solve plus DeviceCsr::upload (src/l0/backend.cpp:154-188): validation,
+ * scaling, the device CSR of A and the device-built CSR of A^T happen here.
+ * An invalid problem is NOT an error here: like the reference (pdhg.cpp:223-228)
+ * pdhg_solve then reports PDHG_STATUS_NUMERICAL_FAILURE "invalid problem: ...".
+ * Sizes that do not fit int32 indices return PDHG_ERR_INVALID_ARGUMENT. */
+int pdhg_load_problem(pdhg_ctx* ctx, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_idx, const double* values, const double* c,
+                      double obj_const, int maximize, const double* col_lo,
+                      const double* col_hi, const double* row_lo, const double* row_hi);
+
+/* Pdhg::solve (pdhg.cpp:218-502) on the loaded problem. x (n), y (m) and rc (n)
+ * are caller-owned HOST buffers in original units (any may be NULL); they are
+ * written only when info->has_point is set. */
+int pdhg_solve(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* info, double* x,
+               double* y, double* rc);
+
+/* Per-kernel timing of the iteration kernels on the loaded problem (CUDA events
+ * on the engine's stream around each launch, after `warmup` untimed iterations).
+ * Runs `iterations` iterations from the state the last pdhg_solve left. */
+typedef struct pdhg_kernel_stats {
+    int count;                   /* kernels reported */
+    char name[8][32];
+    double avg_ms[8];            /* mean launch duration */
+    double bytes[8];             /* algorithmic bytes per launch */
+    int launches[8];
+} pdhg_kernel_stats;
+int pdhg_profile_kernels(pdhg_ctx* ctx, int precision, int warmup, int iterations,
+                         pdhg_kernel_stats* out);
+
+/* Backend primitives on the engine's kernels (FP64 exact order), host buffers:
+ * y := alpha*op(A)*x + beta*y (Backend::spmv / spmv_transpose, backend.hpp:120-126;
+ * beta == 0 overwrites y, backend_host.cpp:420-422) and x := clamp(x, lo, hi)
+ * with NULL = unbounded side (Backend::project_box, backend.hpp:131). */
+int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
+                  const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                  double alpha, const double* x, double beta, double* y);
+int pdhg_project_box(int device, int32_t n, const double* lo, const double* hi, double* x);
+
+/* Scaling::equilibrate(CsrMatrix) (src/l1/scaling.cpp:19-104) as the engine
+ * computes it (host FP64, reference order). */
+int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
+                 const int32_t* col_idx, const double* values, const pdhg_options* options,
+                 double* row_scale, double* col_scale);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDHG_B200_H */

@@ -1,0 +1,307 @@
+"""ctypes face of the checkers -- TEST INFRASTRUCTURE ONLY.
+
+Loads ``oracle/liborc_pdhg.so`` (the C restatement, pdhg_oracle.c) and, when
+present, ``oracle/_ref/libsovref.so`` (the reference PDHG path compiled from the
+reference sources by oracle/Makefile). Only the tests, ``__graft_entry__.smoke``
+and ``bench.py``'s CPU-baseline leg import this module; the engine never does.
+
+Every entry takes any object with the ``Problem`` attributes (m, n, row_ptr,
+col_idx, val, c, col_lo, col_hi, row_lo, row_hi, obj_const, maximize).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORC_SO = os.path.join(HERE, "liborc_pdhg.so")
+REF_SO = os.path.join(HERE, "_ref", "libsovref.so")
+
+STATUS = ["optimal", "iteration_limit", "time_limit", "numerical_failure", "not_solved",
+          "cancelled"]
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+CHECKPOINT_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_longlong, _dp, _dp, C.c_double)
+
+
+class OrcProblem(C.Structure):
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64),
+                ("row_ptr", _ip), ("col_idx", _ip), ("val", _dp), ("c", _dp),
+                ("obj_const", C.c_double), ("maximize", C.c_int),
+                ("col_lo", _dp), ("col_hi", _dp), ("row_lo", _dp), ("row_hi", _dp)]
+
+
+class OrcOptions(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_longlong),
+                ("time_limit_seconds", C.c_double), ("restart_check_period", C.c_longlong),
+                ("restart_sufficient_decrease", C.c_double), ("step_size_safety", C.c_double),
+                ("power_iterations", C.c_int), ("verbose", C.c_int),
+                ("ruiz_iterations", C.c_int), ("ruiz_tolerance", C.c_double),
+                ("pock_chambolle_alpha", C.c_double), ("apply_ruiz", C.c_int),
+                ("apply_pock_chambolle", C.c_int), ("termination_rule", C.c_int),
+                ("trace_iters", C.c_int), ("trace_x", _dp), ("trace_y", _dp),
+                ("checkpoint", CHECKPOINT_FN), ("checkpoint_user", C.c_void_p),
+                ("cancel_flag", C.POINTER(C.c_int)), ("iter_times", _dp),
+                ("iter_times_cap", C.c_longlong), ("restart_rule", C.c_int),
+                ("primal_weight_update", C.c_int)]
+
+
+class OrcInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("objective", C.c_double),
+                ("primal_infeasibility", C.c_double), ("dual_infeasibility", C.c_double),
+                ("duality_gap", C.c_double), ("iterations", C.c_longlong),
+                ("restarts", C.c_longlong), ("seconds", C.c_double),
+                ("operator_norm_estimate", C.c_double), ("has_point", C.c_int),
+                ("message", C.c_char * 256)]
+
+
+@dataclass
+class Result:
+    status: str
+    objective: float
+    primal: np.ndarray | None
+    dual: np.ndarray | None
+    reduced_costs: np.ndarray | None
+    primal_infeasibility: float
+    dual_infeasibility: float
+    duality_gap: float
+    iterations: int
+    restarts: int
+    seconds: float
+    operator_norm_estimate: float
+    message: str
+    trace_x: np.ndarray | None = None
+    trace_y: np.ndarray | None = None
+    checkpoints: list = field(default_factory=list)
+    loop_seconds: float = 0.0
+    loop_iterations: int = 0
+
+
+_libs: dict = {}
+
+
+def _lib(path: str) -> C.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"checker library not built: {path} (run make -C oracle)")
+        lib = C.CDLL(path)
+        _libs[path] = lib
+    return _libs[path]
+
+
+def orc_lib() -> C.CDLL:
+    lib = _lib(ORC_SO)
+    lib.orc_pdhg_solve.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcOptions),
+                                   C.POINTER(OrcInfo), _dp, _dp, _dp]
+    lib.orc_default_options.argtypes = [C.POINTER(OrcOptions)]
+    lib.orc_scaling.argtypes = [C.c_int32, C.c_int32, _ip, _ip, _dp, C.POINTER(OrcOptions),
+                                _dp, _dp]
+    lib.orc_spmv.argtypes = [C.c_int32, _ip, _ip, _dp, C.c_double, _dp, C.c_double, _dp]
+    lib.orc_spmv_transpose.argtypes = [C.c_int32, C.c_int32, _ip, _ip, _dp, C.c_double, _dp,
+                                       C.c_double, _dp]
+    lib.orc_project_box.argtypes = [C.c_int32, _dp, _dp, _dp]
+    lib.orc_pairwise_dot.argtypes = [_dp, _dp, C.c_int64]
+    lib.orc_pairwise_dot.restype = C.c_double
+    lib.orc_operator_norm.argtypes = [C.c_int32, C.c_int32, _ip, _ip, _dp, C.c_int]
+    lib.orc_operator_norm.restype = C.c_double
+    return lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib() -> C.CDLL:
+    lib = _lib(REF_SO)
+    lib.ref_pdhg_solve.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcOptions),
+                                   C.POINTER(OrcInfo), _dp, _dp, _dp, _dp]
+    lib.ref_scaling.argtypes = [C.c_int32, C.c_int32, C.c_int64, _ip, _ip, _dp,
+                                C.POINTER(OrcOptions), _dp, _dp]
+    lib.ref_backend_spmv.argtypes = [C.c_int, C.c_int32, C.c_int32, C.c_int64, _ip, _ip, _dp,
+                                     C.c_double, _dp, C.c_double, _dp]
+    lib.ref_read_model_string.argtypes = [C.c_char_p, C.c_int]
+    lib.ref_read_model_string.restype = C.c_void_p
+    lib.ref_model_shape.argtypes = [C.c_void_p, _ip, _ip, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int), _dp]
+    lib.ref_model_arrays.argtypes = [C.c_void_p, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp]
+    lib.ref_model_free.argtypes = [C.c_void_p]
+    return lib
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+def _problem(p, keep: list) -> OrcProblem:
+    arrs = {}
+    for f in ("row_ptr", "col_idx"):
+        arrs[f] = np.ascontiguousarray(getattr(p, f), dtype=np.int32)
+    for f in ("val", "c", "col_lo", "col_hi", "row_lo", "row_hi"):
+        a = np.ascontiguousarray(getattr(p, f), dtype=np.float64)
+        arrs[f] = a if a.size else np.zeros(1)
+    if arrs["col_idx"].size == 0:
+        arrs["col_idx"] = np.zeros(1, dtype=np.int32)
+    keep.append(arrs)
+    return OrcProblem(int(p.m), int(p.n), int(np.asarray(p.row_ptr)[-1]), _i(arrs["row_ptr"]),
+                      _i(arrs["col_idx"]), _d(arrs["val"]), _d(arrs["c"]), float(p.obj_const),
+                      int(bool(p.maximize)), _d(arrs["col_lo"]), _d(arrs["col_hi"]),
+                      _d(arrs["row_lo"]), _d(arrs["row_hi"]))
+
+
+def make_options(**kw) -> OrcOptions:
+    o = OrcOptions()
+    orc_lib().orc_default_options(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+def _solve(which: str, p, trace_iters: int = 0, checkpoints: bool = False,
+           cancel: bool = False, iter_times: np.ndarray | None = None, **kw) -> Result:
+    keep: list = []
+    prob = _problem(p, keep)
+    o = make_options(**kw)
+    if iter_times is not None:
+        o.iter_times = _d(iter_times)
+        o.iter_times_cap = int(iter_times.size)
+    tx = ty = None
+    if trace_iters > 0:
+        tx = np.zeros((trace_iters, max(p.n, 1)))
+        ty = np.zeros((trace_iters, max(p.m, 1)))
+        o.trace_iters = trace_iters
+        o.trace_x = _d(tx)
+        o.trace_y = _d(ty)
+    cps: list = []
+    if checkpoints:
+        def cb(_user, it, xp, yp, res):
+            x = np.ctypeslib.as_array(xp, shape=(p.n,)).copy() if p.n else np.zeros(0)
+            y = np.ctypeslib.as_array(yp, shape=(p.m,)).copy() if p.m else np.zeros(0)
+            cps.append((int(it), x, y, float(res)))
+        cfn = CHECKPOINT_FN(cb)
+        keep.append(cfn)
+        o.checkpoint = cfn
+    flag = C.c_int(1 if cancel else 0)
+    if cancel:
+        o.cancel_flag = C.pointer(flag)
+    info = OrcInfo()
+    x = np.zeros(max(p.n, 1))
+    y = np.zeros(max(p.m, 1))
+    rc = np.zeros(max(p.n, 1))
+    loop = np.zeros(2)
+    if which == "oracle":
+        orc_lib().orc_pdhg_solve(C.byref(prob), C.byref(o), C.byref(info), _d(x), _d(y), _d(rc))
+    else:
+        rcode = ref_lib().ref_pdhg_solve(C.byref(prob), C.byref(o), C.byref(info), _d(x), _d(y),
+                                         _d(rc), _d(loop))
+        if rcode != 0:
+            raise RuntimeError(info.message.decode())
+    hp = bool(info.has_point)
+    return Result(
+        status=STATUS[info.status], objective=info.objective,
+        primal=x[: p.n].copy() if hp else None, dual=y[: p.m].copy() if hp else None,
+        reduced_costs=rc[: p.n].copy() if hp else None,
+        primal_infeasibility=info.primal_infeasibility,
+        dual_infeasibility=info.dual_infeasibility, duality_gap=info.duality_gap,
+        iterations=info.iterations, restarts=info.restarts, seconds=info.seconds,
+        operator_norm_estimate=info.operator_norm_estimate, message=info.message.decode(),
+        trace_x=None if tx is None else tx[:, : p.n], trace_y=None if ty is None else ty[:, : p.m],
+        checkpoints=cps, loop_seconds=float(loop[0]), loop_iterations=int(loop[1]))
+
+
+def oracle_solve(p, **kw) -> Result:
+    """The C restatement of ``Pdhg::solve`` (src/l1/pdhg.cpp:218-502)."""
+    return _solve("oracle", p, **kw)
+
+
+def reference_solve(p, **kw) -> Result:
+    """The reference's own ``sov::Pdhg::solve`` on its Host backend."""
+    return _solve("reference", p, **kw)
+
+
+def oracle_scaling(p, **kw):
+    rs = np.zeros(max(p.m, 1))
+    cs = np.zeros(max(p.n, 1))
+    keep: list = []
+    prob = _problem(p, keep)
+    o = make_options(**kw)
+    orc_lib().orc_scaling(prob.m, prob.n, prob.row_ptr, prob.col_idx, prob.val, C.byref(o),
+                          _d(rs), _d(cs))
+    return rs[: p.m], cs[: p.n]
+
+
+def reference_scaling(p, **kw):
+    rs = np.zeros(max(p.m, 1))
+    cs = np.zeros(max(p.n, 1))
+    keep: list = []
+    prob = _problem(p, keep)
+    o = make_options(**kw)
+    if ref_lib().ref_scaling(prob.m, prob.n, prob.nnz, prob.row_ptr, prob.col_idx, prob.val,
+                             C.byref(o), _d(rs), _d(cs)) != 0:
+        raise RuntimeError("reference scaling failed")
+    return rs[: p.m], cs[: p.n]
+
+
+def oracle_spmv(p, alpha, x, beta, y, transpose=False):
+    keep: list = []
+    prob = _problem(p, keep)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.array(y, dtype=np.float64)
+    if transpose:
+        orc_lib().orc_spmv_transpose(prob.m, prob.n, prob.row_ptr, prob.col_idx, prob.val,
+                                     alpha, _d(x), beta, _d(y))
+    else:
+        orc_lib().orc_spmv(prob.m, prob.row_ptr, prob.col_idx, prob.val, alpha, _d(x), beta,
+                           _d(y))
+    return y
+
+
+def reference_spmv(p, alpha, x, beta, y, transpose=False):
+    keep: list = []
+    prob = _problem(p, keep)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.array(y, dtype=np.float64)
+    if ref_lib().ref_backend_spmv(int(transpose), prob.m, prob.n, prob.nnz, prob.row_ptr,
+                                  prob.col_idx, prob.val, alpha, _d(x), beta, _d(y)) != 0:
+        raise RuntimeError("reference spmv failed")
+    return y
+
+
+def oracle_operator_norm(p, iterations=30) -> float:
+    keep: list = []
+    prob = _problem(p, keep)
+    return orc_lib().orc_operator_norm(prob.m, prob.n, prob.row_ptr, prob.col_idx, prob.val,
+                                       iterations)
+
+
+def reference_read_model(text: str, is_mps: bool = False) -> dict:
+    """read_lp_string / read_mps_string (include/sovereign/io.hpp:57-64) -> CSR arrays."""
+    lib = ref_lib()
+    h = lib.ref_read_model_string(text.encode(), int(is_mps))
+    if not h:
+        raise ValueError("reference reader rejected the model")
+    m, n, nnz, mx, oc = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int(), C.c_double()
+    lib.ref_model_shape(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(oc))
+    rp = np.zeros(m.value + 1, dtype=np.int32)
+    ci = np.zeros(max(nnz.value, 1), dtype=np.int32)
+    va = np.zeros(max(nnz.value, 1))
+    c = np.zeros(max(n.value, 1))
+    cl = np.zeros(max(n.value, 1))
+    ch = np.zeros(max(n.value, 1))
+    rl = np.zeros(max(m.value, 1))
+    rh = np.zeros(max(m.value, 1))
+    lib.ref_model_arrays(h, _i(rp), _i(ci), _d(va), _d(c), _d(cl), _d(ch), _d(rl), _d(rh))
+    lib.ref_model_free(h)
+    k, nn, mm = nnz.value, n.value, m.value
+    return {"m": mm, "n": nn, "row_ptr": rp, "col_idx": ci[:k], "val": va[:k], "c": c[:nn],
+            "col_lo": cl[:nn], "col_hi": ch[:nn], "row_lo": rl[:mm], "row_hi": rh[:mm],
+            "obj_const": oc.value, "maximize": bool(mx.value)}

@@ -1,0 +1,12 @@
+"""B200-native PDHG LP engine (drop-in for sovereign-solver's ``Pdhg::solve``).
+
+The engine is ``libpdhg_b200.so`` (CUDA kernels + C-ABI, include/pdhg_b200.h).
+This package holds its Python face (``pdhg``), the LP container (``problem``)
+and the seeded workload generators (``lpgen``).
+"""
+from .problem import INF, Problem  # noqa: F401
+from . import lpgen  # noqa: F401
+from .pdhg import (  # noqa: F401
+    CancellationToken, Engine, Pdhg, PdhgError, PdhgOptions, PdhgResult, csr_spmv, project_box,
+    scaling,
+)

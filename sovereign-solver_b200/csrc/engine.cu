@@ -1,0 +1,1289 @@
+// engine.cu -- host orchestration of the PDHG engine and the C-ABI
+// (include/pdhg_b200.h).
+//
+// pdhg_solve follows Pdhg::solve (src/l1/pdhg.cpp:218-502) step for step:
+// validation, scaling, step size from the power iteration, the iteration loop
+// with a check every restart_check_period iterations, and the final result.
+// What changes is where the work runs: every iteration and every check is a
+// device kernel; the host only enqueues. One check period (period x 2 fused
+// iteration kernels + the check kernels) is captured once as a CUDA graph and
+// launched repeatedly; the device decides convergence, restarts and failure
+// and every later kernel returns at once after a stop, so the host can keep
+// several periods in flight and only waits on an event ring. Time limit and
+// cancellation reach the device through a host-mapped mailbox that the check
+// reads (granularity: one check period, where the reference polls every
+// iteration, pdhg.cpp:288-293).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/pdhg_b200.h"
+#include "engine.cuh"
+#include "host_prep.hpp"
+
+namespace pdhg {
+
+namespace {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+constexpr int kLookahead = 4;
+constexpr int kStopSwitchPrecision = 100;  // internal stop code: FP32 phase stalled
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p != nullptr) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        if (count == n && p != nullptr) return cudaSuccess;
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count);
+    }
+};
+
+struct MatDev {
+    int32_t rows = 0, cols = 0;
+    int64_t nnz = 0;
+    DBuf<int32_t> rp, ci, long_rows;
+    DBuf<double> v64;
+    DBuf<float> v32;
+    int32_t n_long = 0, n_short = 0;
+    int vw = 1;
+    DevCsr view() const {
+        DevCsr d;
+        d.rows = rows;
+        d.cols = cols;
+        d.nnz = nnz;
+        d.rp = rp.p;
+        d.ci = ci.p;
+        d.v64 = v64.p;
+        d.v32 = v32.p;
+        d.long_rows = long_rows.p;
+        d.n_long = n_long;
+        d.n_short = n_short;
+        d.vw = vw;
+        return d;
+    }
+};
+
+// Everything a captured check-period graph bakes into its kernel parameters.
+struct GraphSig {
+    int prec = -1;
+    long long period = 0;
+    int cand = 0;
+    double tol = 0, bt = 0, dec = 0;
+    int rule = 0, restart_rule = 0, pw = 0;
+    long long gen = -1;
+    bool operator==(const GraphSig& o) const {
+        return prec == o.prec && period == o.period && cand == o.cand && tol == o.tol &&
+               bt == o.bt && dec == o.dec && rule == o.rule && restart_rule == o.restart_rule &&
+               pw == o.pw && gen == o.gen;
+    }
+};
+
+}  // namespace
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long gen = 0;  // bumps on every load / rescale
+
+    bool loaded = false, valid = false;
+    std::string why;
+    HostLp lp;
+    ScalingParams sp;
+    bool scaled = false;
+    std::vector<double> rs, cs;
+    double bnorm = 0, cnorm = 0;        // relative-KKT norms, original space (inf-norms)
+    double cnorm2_s = 0, bnorm2_s = 0;  // initial primal weight |c|_2 / |b|_2, scaled space
+
+    MatDev Ao, ATo, As, ATs;
+    DBuf<double> c_o, lo_o, hi_o, rlo_o, rhi_o, c_s, lo_s, hi_s, rlo_s, rhi_s, rs_d, cs_d;
+    DBuf<float> c32, lo32, hi32, rlo32, rhi32;
+
+    bool have_opnorm = false;
+    int opnorm_iters = -1;
+    double opnorm = 0;
+
+    DBuf<double> x64, xbar64, s64, y64, xsum, ysum;
+    DBuf<float> x32, xbar32, s32, y32, psx, psy;
+    DBuf<double> act_avg, cand_xo, cand_yo, part, bx, by, xo, yo, rc, trow, tcol;
+    DBuf<double> pw_u, pw_v, pw_w, pw_part, pw_out, x0s, y0s;
+    DBuf<double> x_last, y_last;  // restart points (primal-weight update)
+    DBuf<DevState> st;
+    Mailbox* mail = nullptr;
+    Mailbox* mail_dev = nullptr;
+
+    cudaGraphExec_t graph = nullptr;
+    GraphSig graph_sig;
+    long long launches = 0;
+
+    ~Ctx() {
+        if (graph != nullptr) cudaGraphExecDestroy(graph);
+        if (mail != nullptr) cudaFreeHost(mail);
+        if (stream != nullptr) cudaStreamDestroy(stream);
+    }
+
+    DevProblem problem() const {
+        DevProblem P;
+        P.m = lp.m;
+        P.n = lp.n;
+        P.obj_sign = lp.maximize ? -1.0 : 1.0;
+        P.obj_const = lp.obj_const;
+        P.c = c_s.p;
+        P.lo = lo_s.p;
+        P.hi = hi_s.p;
+        P.rlo = rlo_s.p;
+        P.rhi = rhi_s.p;
+        P.c_o = c_o.p;
+        P.lo_o = lo_o.p;
+        P.hi_o = hi_o.p;
+        P.rlo_o = rlo_o.p;
+        P.rhi_o = rhi_o.p;
+        P.rs = rs_d.p;
+        P.cs = cs_d.p;
+        P.c32 = c32.p;
+        P.lo32 = lo32.p;
+        P.hi32 = hi32.p;
+        P.rlo32 = rlo32.p;
+        P.rhi32 = rhi32.p;
+        P.bnorm = bnorm;
+        P.cnorm = cnorm;
+        return P;
+    }
+};
+
+}  // namespace pdhg
+
+struct pdhg_ctx {
+    pdhg::Ctx c;
+};
+
+namespace pdhg {
+namespace {
+
+int fail(Ctx& c, cudaError_t e, const char* what) {
+    c.err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PDHG_ERR_OUT_OF_MEMORY : PDHG_ERR_BACKEND;
+}
+
+#define CK(expr)                                               \
+    do {                                                       \
+        cudaError_t e_ = (expr);                               \
+        if (e_ != cudaSuccess) return fail(c, e_, #expr);      \
+    } while (0)
+
+template <class T>
+cudaError_t upload(DBuf<T>& d, const T* h, size_t n, cudaStream_t s) {
+    cudaError_t e = d.alloc(n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(d.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+}
+
+template <class T>
+cudaError_t upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+    return upload(d, h.data(), h.size(), s);
+}
+
+cudaError_t to_float(DBuf<float>& d, const DBuf<double>& src, cudaStream_t s) {
+    cudaError_t e = d.alloc(src.n);
+    if (e != cudaSuccess) return e;
+    launch_to_float(src.p, d.p, static_cast<int64_t>(src.n), s);
+    return cudaGetLastError();
+}
+
+// CSR + transpose on the device, with row binning of both.
+int upload_matrix(Ctx& c, const HostCsr& A, MatDev& M, MatDev& MT, bool want_f32) {
+    cudaStream_t s = c.stream;
+    M.rows = A.rows;
+    M.cols = A.cols;
+    M.nnz = A.nnz();
+    CK(upload(M.rp, A.rp, s));
+    CK(upload(M.ci, A.ci, s));
+    CK(upload(M.v64, A.v, s));
+    MT.rows = A.cols;
+    MT.cols = A.rows;
+    MT.nnz = A.nnz();
+    CK(MT.rp.alloc(static_cast<size_t>(A.cols) + 1));
+    CK(MT.ci.alloc(static_cast<size_t>(A.nnz())));
+    CK(MT.v64.alloc(static_cast<size_t>(A.nnz())));
+    TransposeOut out{MT.rp.p, MT.ci.p, MT.v64.p};
+    if (build_transpose(A.rows, A.cols, A.nnz(), M.rp.p, M.ci.p, M.v64.p, out, s) != 0)
+        return fail(c, cudaGetLastError(), "build_transpose");
+    if (want_f32) {
+        CK(to_float(M.v32, M.v64, s));
+        CK(to_float(MT.v32, MT.v64, s));
+    }
+    // binning (host): A from its row pointer, A^T from column counts
+    std::vector<int32_t> lr;
+    bin_rows(A.rp, kLongRow, &lr, &M.n_short, &M.vw);
+    M.n_long = static_cast<int32_t>(lr.size());
+    CK(upload(M.long_rows, lr, s));
+    std::vector<int32_t> trp(static_cast<size_t>(A.cols) + 1, 0);
+    for (int32_t j : A.ci) ++trp[static_cast<size_t>(j) + 1];
+    for (int32_t j = 0; j < A.cols; ++j) trp[j + 1] += trp[j];
+    bin_rows(trp, kLongRow, &lr, &MT.n_short, &MT.vw);
+    MT.n_long = static_cast<int32_t>(lr.size());
+    CK(upload(MT.long_rows, lr, s));
+    CK(cudaStreamSynchronize(s));
+    return PDHG_OK;
+}
+
+int ensure_scaled(Ctx& c, const ScalingParams& sp) {
+    if (c.scaled && c.sp == sp) return PDHG_OK;
+    cudaStream_t s = c.stream;
+    c.sp = sp;
+    equilibrate(c.lp.A, sp, &c.rs, &c.cs);
+    HostLp sl;
+    build_scaled(c.lp, c.rs, c.cs, &sl);
+    const double sign = c.lp.maximize ? -1.0 : 1.0;
+    for (double& v : sl.c) v *= sign;  // pdhg.cpp:250-252
+    double cn = 0.0, bn = 0.0;
+    for (double v : sl.c) cn += v * v;
+    for (int32_t i = 0; i < sl.m; ++i) {
+        double b = 0.0;
+        if (std::isfinite(sl.row_lo[i])) b = std::fabs(sl.row_lo[i]);
+        if (std::isfinite(sl.row_hi[i])) b = std::max(b, std::fabs(sl.row_hi[i]));
+        bn += b * b;
+    }
+    c.cnorm2_s = std::sqrt(cn);
+    c.bnorm2_s = std::sqrt(bn);
+    int rc = upload_matrix(c, sl.A, c.As, c.ATs, true);
+    if (rc != PDHG_OK) return rc;
+    CK(upload(c.c_s, sl.c, s));
+    CK(upload(c.lo_s, sl.col_lo, s));
+    CK(upload(c.hi_s, sl.col_hi, s));
+    CK(upload(c.rlo_s, sl.row_lo, s));
+    CK(upload(c.rhi_s, sl.row_hi, s));
+    CK(upload(c.rs_d, c.rs, s));
+    CK(upload(c.cs_d, c.cs, s));
+    CK(to_float(c.c32, c.c_s, s));
+    CK(to_float(c.lo32, c.lo_s, s));
+    CK(to_float(c.hi32, c.hi_s, s));
+    CK(to_float(c.rlo32, c.rlo_s, s));
+    CK(to_float(c.rhi32, c.rhi_s, s));
+    CK(cudaStreamSynchronize(s));
+    c.scaled = true;
+    c.have_opnorm = false;
+    c.gen += 1;
+    return PDHG_OK;
+}
+
+// estimate_operator_norm (pdhg.cpp:48-79) with the exact kernels; the scalar
+// tail (sqrt, 1/x) runs on the host exactly as in the reference.
+int operator_norm(Ctx& c, int iterations, double* out) {
+    cudaStream_t s = c.stream;
+    const int32_t n = c.lp.n, m = c.lp.m;
+    CK(c.pw_u.alloc(static_cast<size_t>(n) + 1));
+    CK(c.pw_v.alloc(static_cast<size_t>(m) + 1));
+    CK(c.pw_w.alloc(static_cast<size_t>(m) + 1));
+    const int64_t ps = std::max(pairwise_partial_size(n), pairwise_partial_size(m));
+    CK(c.pw_part.alloc(static_cast<size_t>(ps)));
+    CK(c.pw_out.alloc(4));
+    launch_fill(c.pw_u.p, n, 1.0, s);
+    launch_fill(c.pw_v.p, m, 1.0, s);
+    launch_fill(c.pw_w.p, m, 0.0, s);
+    const DevCsr A = c.As.view(), AT = c.ATs.view();
+    double estimate = 0.0;
+    double h[2];
+    for (int it = 0; it < iterations; ++it) {
+        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s);
+        launch_pairwise_dot(c.pw_w.p, c.pw_w.p, m, c.pw_part.p, c.pw_out.p, s);
+        CK(cudaMemcpyAsync(h, c.pw_out.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const double wn = std::sqrt(h[0]);
+        if (wn < 1e-300) break;
+        launch_scale(c.pw_w.p, m, 1.0 / wn, s);
+        launch_pw_u(AT, c.pw_w.p, c.pw_u.p, s);
+        if (m > 0)
+            CK(cudaMemcpyAsync(c.pw_v.p, c.pw_w.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+        launch_pairwise_dot(c.pw_u.p, c.pw_u.p, n, c.pw_part.p, c.pw_out.p, s);
+        launch_pairwise_dot(c.pw_v.p, c.pw_v.p, m, c.pw_part.p, c.pw_out.p + 1, s);
+        CK(cudaMemcpyAsync(h, c.pw_out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const double un = std::sqrt(h[0]);
+        const double vn = std::sqrt(h[1]);
+        estimate = std::sqrt(un * un + vn * vn);
+        if (estimate < 1e-300) break;
+        launch_scale(c.pw_u.p, n, 1.0 / estimate, s);
+        launch_scale(c.pw_v.p, m, 1.0 / estimate, s);
+    }
+    CK(cudaGetLastError());
+    *out = estimate;
+    return PDHG_OK;
+}
+
+template <class T>
+Iterates<T> iterates(Ctx& c);
+template <>
+Iterates<double> iterates<double>(Ctx& c) {
+    Iterates<double> it;
+    it.x = c.x64.p;
+    it.xbar = c.xbar64.p;
+    it.s = c.s64.p;
+    it.y = c.y64.p;
+    it.xsum = c.xsum.p;
+    it.ysum = c.ysum.p;
+    return it;
+}
+template <>
+Iterates<float> iterates<float>(Ctx& c) {
+    Iterates<float> it;
+    it.x = c.x32.p;
+    it.xbar = c.xbar32.p;
+    it.s = c.s32.p;
+    it.y = c.y32.p;
+    it.psx = c.psx.p;
+    it.psy = c.psy.p;
+    it.xsum = c.xsum.p;
+    it.ysum = c.ysum.p;
+    return it;
+}
+
+int alloc_iterates(Ctx& c, bool f32) {
+    const size_t n = static_cast<size_t>(c.lp.n) + 1, m = static_cast<size_t>(c.lp.m) + 1;
+    CK(c.xsum.alloc(n));
+    CK(c.ysum.alloc(m));
+    if (f32) {
+        CK(c.x32.alloc(n));
+        CK(c.xbar32.alloc(n));
+        CK(c.s32.alloc(m));
+        CK(c.y32.alloc(m));
+        CK(c.psx.alloc(n));
+        CK(c.psy.alloc(m));
+    }
+    CK(c.x64.alloc(n));
+    CK(c.xbar64.alloc(n));
+    CK(c.s64.alloc(m));
+    CK(c.y64.alloc(m));
+    CK(c.act_avg.alloc(m));
+    CK(c.cand_xo.alloc(n));
+    CK(c.cand_yo.alloc(m));
+    const int g = std::max(fast_check_grid(c.As.view(), c.ATs.view()),
+                           static_cast<int>((c.lp.m + kBlock - 1) / kBlock + (c.lp.n + kBlock - 1) / kBlock) + 1);
+    CK(c.part.alloc(static_cast<size_t>(g) * 4 + 4));
+    CK(c.bx.alloc(n));
+    CK(c.by.alloc(m));
+    CK(c.xo.alloc(n));
+    CK(c.yo.alloc(m));
+    CK(c.rc.alloc(n));
+    CK(c.trow.alloc(m));
+    CK(c.tcol.alloc(n));
+    return PDHG_OK;
+}
+
+struct Launcher {
+    Ctx& c;
+    int prec;
+    ExactIter ei;
+    ExactCheck ec;
+    FastIter<float> fi32;
+    FastIter<double> fi64;
+    FastCheck<float> fc32;
+    FastCheck<double> fc64;
+
+    void iteration(int first, cudaStream_t s) {
+        if (prec == PDHG_PREC_FP64_EXACT) {
+            launch_exact_primal(ei, first, s);
+            launch_exact_dual(ei, first, s);
+        } else if (prec == PDHG_PREC_MIXED) {
+            launch_fast_primal(fi32, first, s);
+            launch_fast_dual(fi32, first, s);
+        } else {
+            launch_fast_primal(fi64, first, s);
+            launch_fast_dual(fi64, first, s);
+        }
+        c.launches += 2;
+    }
+    void check(long long period, cudaStream_t s) {
+        if (prec == PDHG_PREC_FP64_EXACT) {
+            ec.period_iters = period;
+            launch_exact_check(ec, s);
+            launch_exact_restart(ec, s);
+            c.launches += 3;
+        } else if (prec == PDHG_PREC_MIXED) {
+            fc32.period_iters = period;
+            launch_fast_check(fc32, s);
+            launch_fast_restart(fc32, s);
+            c.launches += 2 + (fc32.want_candidate ? 1 : 0);
+        } else {
+            fc64.period_iters = period;
+            launch_fast_check(fc64, s);
+            launch_fast_restart(fc64, s);
+            c.launches += 2 + (fc64.want_candidate ? 1 : 0);
+        }
+    }
+    long long launches_per_period(long long period) const {
+        const long long chk = prec == PDHG_PREC_FP64_EXACT ? 3 : 2 + (fc32.want_candidate ? 1 : 0);
+        return 2 * period + chk;
+    }
+};
+
+Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candidate) {
+    Launcher L{c, prec, {}, {}, {}, {}, {}, {}};
+    const DevProblem P = c.problem();
+    const double bt = o.tolerance > 1e-6 ? o.tolerance : 1e-6;
+    L.ei = ExactIter{c.As.view(), c.ATs.view(), P, iterates<double>(c), c.st.p};
+    CheckScratch cs{c.act_avg.p, c.cand_xo.p, c.cand_yo.p, c.part.p, 0};
+    L.ec = ExactCheck{c.As.view(), c.ATs.view(), c.Ao.view(), c.ATo.view(), P,
+                      iterates<double>(c), cs, o.tolerance, bt, o.restart_sufficient_decrease,
+                      o.restart_check_period, o.termination_rule, want_candidate ? 1 : 0,
+                      c.st.p, c.mail_dev};
+    L.fi32 = FastIter<float>{c.As.view(), c.ATs.view(), P, iterates<float>(c), c.st.p};
+    L.fi64 = FastIter<double>{c.As.view(), c.ATs.view(), P, iterates<double>(c), c.st.p};
+    L.fc32 = FastCheck<float>{c.As.view(), c.ATs.view(), P, iterates<float>(c), cs,
+                              o.tolerance, bt, o.restart_sufficient_decrease,
+                              o.restart_check_period, o.termination_rule,
+                              want_candidate ? 1 : 0, c.st.p, c.mail_dev, o.restart_rule,
+                              o.primal_weight_update, c.x_last.p, c.y_last.p};
+    L.fc64 = FastCheck<double>{c.As.view(), c.ATs.view(), P, iterates<double>(c), cs,
+                               o.tolerance, bt, o.restart_sufficient_decrease,
+                               o.restart_check_period, o.termination_rule,
+                               want_candidate ? 1 : 0, c.st.p, c.mail_dev, o.restart_rule,
+                               o.primal_weight_update, c.x_last.p, c.y_last.p};
+    return L;
+}
+
+// Fresh control state: tau = eta / omega, sigma = eta * omega.
+int reset_state(Ctx& c, double eta, double omega) {
+    DevState h;
+    std::memset(&h, 0, sizeof h);
+    h.status = PDHG_STATUS_NOT_SOLVED;
+    h.fresh = 1;
+    h.res_last = kInf;
+    h.res_prev_cand = kInf;
+    h.eta = eta;
+    h.omega = omega;
+    h.tau = omega == 1.0 ? eta : eta / omega;
+    h.sigma = omega == 1.0 ? eta : eta * omega;
+    CK(cudaMemcpyAsync(c.st.p, &h, sizeof h, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    std::memset(const_cast<Mailbox*>(c.mail), 0, sizeof(Mailbox));
+    return PDHG_OK;
+}
+
+int build_graph(Ctx& c, Launcher& L, long long period, const GraphSig& sig) {
+    if (c.graph != nullptr && c.graph_sig == sig) return PDHG_OK;
+    if (c.graph != nullptr) {
+        cudaGraphExecDestroy(c.graph);
+        c.graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    const long long before = c.launches;
+    CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    for (long long t = 0; t < period; ++t) L.iteration(t == 0 ? 1 : 0, c.stream);
+    L.check(period, c.stream);
+    cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+    c.launches = before;
+    if (e != cudaSuccess) return fail(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&c.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(c, e, "cudaGraphInstantiate");
+    c.graph_sig = sig;
+    return PDHG_OK;
+}
+
+double elapsed_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Host copies of the scaled iterates for the trace option.
+int trace_copy(Ctx& c, int prec, long long k, const pdhg_options& o) {
+    const int32_t n = c.lp.n, m = c.lp.m;
+    if (prec == PDHG_PREC_MIXED) {
+        std::vector<float> hx(static_cast<size_t>(n)), hy(static_cast<size_t>(m));
+        if (n) CK(cudaMemcpyAsync(hx.data(), c.x32.p, sizeof(float) * n, cudaMemcpyDeviceToHost, c.stream));
+        if (m) CK(cudaMemcpyAsync(hy.data(), c.y32.p, sizeof(float) * m, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        if (o.trace_x) for (int32_t j = 0; j < n; ++j) o.trace_x[k * n + j] = hx[j];
+        if (o.trace_y) for (int32_t i = 0; i < m; ++i) o.trace_y[k * m + i] = hy[i];
+    } else {
+        if (o.trace_x && n)
+            CK(cudaMemcpyAsync(o.trace_x + k * n, c.x64.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+        if (o.trace_y && m)
+            CK(cudaMemcpyAsync(o.trace_y + k * m, c.y64.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+    }
+    return PDHG_OK;
+}
+
+struct LoopOut {
+    long long iterations = 0;
+    int status = PDHG_STATUS_NOT_SOLVED;
+    bool device_done = false;
+    bool switch_precision = false;
+    long long budget_used = 0;
+};
+
+// Runs up to `budget` iterations with launcher L. Handles checkpoints, the
+// time limit, cancellation, verbose output and (mixed mode) stall detection.
+int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long long iter0,
+             std::chrono::steady_clock::time_point t0, bool allow_switch, LoopOut* out) {
+    const long long period = o.restart_check_period;
+    const long long n_periods = budget / period;
+    const long long tail = budget % period;
+    const bool want_cb = o.checkpoint != nullptr;
+    const int lookahead = (want_cb || o.verbose) ? 1 : kLookahead;
+    long long seen_checks = c.mail->checks;
+    bool stop_sent = false;
+    int stop_code = 0;
+    double best = kInf;
+    long long since_improve = 0;
+
+    auto on_check = [&](void) -> int {
+        // called after a period's event completed (lookahead 1 when callbacks are on)
+        const long long checks = c.mail->checks;
+        if (checks == seen_checks) return PDHG_OK;
+        seen_checks = checks;
+        const bool failed = c.mail->done && c.mail->status == PDHG_STATUS_NUMERICAL_FAILURE;
+        if (o.verbose && c.mail->restarted && !failed)
+            std::fprintf(stderr, "  [pdhg] restart at iter %lld, residual %.3g\n",
+                         static_cast<long long>(c.mail->iter), static_cast<double>(c.mail->avg_res));
+        if (want_cb && !failed) {
+            const int32_t n = c.lp.n, m = c.lp.m;
+            std::vector<double> hx(static_cast<size_t>(n)), hy(static_cast<size_t>(m));
+            if (n) CK(cudaMemcpyAsync(hx.data(), c.cand_xo.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+            if (m) CK(cudaMemcpyAsync(hy.data(), c.cand_yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+            CK(cudaStreamSynchronize(c.stream));
+            o.checkpoint(o.checkpoint_user, static_cast<long long>(c.mail->iter) - 1, hx.data(),
+                         hy.data(), c.mail->orig_res);
+        }
+        if (allow_switch && !c.mail->done) {
+            const double r = o.termination_rule == 1 ? c.mail->rel_kkt : c.mail->orig_res;
+            if (r < 0.98 * best) {
+                best = r;
+                since_improve = 0;
+            } else if (++since_improve >= 25 && !stop_sent) {
+                c.mail->stop_request = kStopSwitchPrecision;
+                stop_sent = true;
+                stop_code = kStopSwitchPrecision;
+            }
+        }
+        return PDHG_OK;
+    };
+    auto poll_stop = [&]() {
+        if (stop_sent) return;
+        if (o.cancel_flag != nullptr && *o.cancel_flag) {
+            stop_code = PDHG_STATUS_CANCELLED;
+        } else if (o.time_limit_seconds > 0.0 && elapsed_since(t0) > o.time_limit_seconds) {
+            stop_code = PDHG_STATUS_TIME_LIMIT;
+        }
+        if (stop_code != 0) {
+            c.mail->stop_request = stop_code;
+            stop_sent = true;
+        }
+    };
+
+    long long p = 0;
+    // Traced periods run kernel by kernel with a copy after each iteration.
+    const long long traced = o.trace_iters > 0 ? o.trace_iters - iter0 : 0;
+    while (p < n_periods && p * period < traced && !c.mail->done) {
+        poll_stop();
+        for (long long t = 0; t < period; ++t) {
+            L.iteration(t == 0 ? 1 : 0, c.stream);
+            const long long k = iter0 + p * period + t;
+            if (k < o.trace_iters) {
+                int rc = trace_copy(c, L.prec, k, o);
+                if (rc != PDHG_OK) return rc;
+            }
+        }
+        L.check(period, c.stream);
+        CK(cudaStreamSynchronize(c.stream));
+        ++p;
+        int rc = on_check();
+        if (rc != PDHG_OK) return rc;
+    }
+    if (p < n_periods && !c.mail->done) {
+        GraphSig sig;
+        sig.prec = L.prec;
+        sig.period = period;
+        sig.cand = want_cb ? 1 : 0;
+        sig.tol = o.tolerance;
+        sig.bt = L.ec.bound_tol;
+        sig.dec = o.restart_sufficient_decrease;
+        sig.rule = o.termination_rule;
+        sig.restart_rule = o.restart_rule;
+        sig.pw = o.primal_weight_update;
+        sig.gen = c.gen;
+        int rc = build_graph(c, L, period, sig);
+        if (rc != PDHG_OK) return rc;
+        std::deque<cudaEvent_t> inflight;
+        std::vector<cudaEvent_t> pool;
+        for (int i = 0; i < lookahead; ++i) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            pool.push_back(e);
+        }
+        int next_ev = 0;
+        const long long per = L.launches_per_period(period);
+        while (true) {
+            const bool can_launch = p < n_periods && !c.mail->done && !(stop_sent && stop_code != 0 && c.mail->done);
+            if (can_launch && static_cast<int>(inflight.size()) < lookahead) {
+                poll_stop();
+                CK(cudaGraphLaunch(c.graph, c.stream));
+                c.launches += per;
+                cudaEvent_t e = pool[next_ev];
+                next_ev = (next_ev + 1) % lookahead;
+                CK(cudaEventRecord(e, c.stream));
+                inflight.push_back(e);
+                ++p;
+                continue;
+            }
+            if (inflight.empty()) break;
+            CK(cudaEventSynchronize(inflight.front()));
+            inflight.pop_front();
+            int rc2 = on_check();
+            if (rc2 != PDHG_OK) return rc2;
+        }
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    const bool done = c.mail->done != 0;
+    if (!done && tail > 0 && !stop_sent) {
+        poll_stop();
+        if (!stop_sent) {
+            for (long long t = 0; t < tail; ++t) {
+                L.iteration(t == 0 ? 1 : 0, c.stream);
+                const long long k = iter0 + n_periods * period + t;
+                if (k < o.trace_iters) {
+                    int rc = trace_copy(c, L.prec, k, o);
+                    if (rc != PDHG_OK) return rc;
+                }
+            }
+            CK(cudaStreamSynchronize(c.stream));
+        }
+    }
+    DevState h;
+    CK(cudaMemcpy(&h, c.st.p, sizeof h, cudaMemcpyDeviceToHost));
+    out->device_done = h.done != 0;
+    if (h.done) {
+        out->iterations = h.stop_iter - iter0;
+        out->status = h.status;
+        if (h.status == kStopSwitchPrecision) out->switch_precision = true;
+    } else if (stop_sent && stop_code != 0 && stop_code != kStopSwitchPrecision) {
+        out->iterations = h.iter - iter0;
+        out->status = stop_code;
+    } else {
+        const bool ran_tail = !stop_sent && tail > 0;
+        out->iterations = n_periods * period + (ran_tail ? tail : 0);
+        out->status = PDHG_STATUS_ITERATION_LIMIT;
+    }
+    return PDHG_OK;
+}
+
+// Copies the scaled FP32 state into the FP64 iterates and restarts the
+// Cesaro average there (the FP64 polish phase of the mixed mode).
+__global__ void k_widen(Iterates<float> a, Iterates<double> b, int32_t n, int32_t m) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t < n) {
+        b.x[t] = a.x[t];
+        b.xbar[t] = a.xbar[t];
+        b.xsum[t] = 0.0;
+    }
+    if (t < m) {
+        b.y[t] = a.y[t];
+        b.s[t] = a.s[t];
+        b.ysum[t] = 0.0;
+    }
+}
+
+template <class T>
+__global__ void k_snapshot(Iterates<T> it, double* xl, double* yl, int32_t n, int32_t m) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t < n) xl[t] = static_cast<double>(it.x[t]);
+    if (t < m) yl[t] = static_cast<double>(it.y[t]);
+}
+
+__global__ void k_restart_state(DevState* st) {
+    st->done = 0;
+    st->status = PDHG_STATUS_NOT_SOLVED;
+    st->converged = 0;
+    st->fresh = 1;
+    st->restart = 0;
+    st->fold = 0;
+    st->since_restart = 0;
+    st->res_last = INFINITY;
+}
+
+int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, double* rcv) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::memset(info, 0, sizeof *info);
+    info->status = PDHG_STATUS_NOT_SOLVED;
+    c.launches = 0;
+    if (!c.loaded) {
+        c.err = "pdhg_solve: no problem loaded";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    if (!c.valid) {  // pdhg.cpp:223-228
+        info->status = PDHG_STATUS_NUMERICAL_FAILURE;
+        std::snprintf(info->message, sizeof info->message, "invalid problem: %s", c.why.c_str());
+        return PDHG_OK;
+    }
+    if (o.restart_check_period < 1 || o.power_iterations < 0 || o.precision < 0 ||
+        o.precision > 2 || o.termination_rule < 0 || o.termination_rule > 1 ||
+        o.restart_rule < 0 || o.restart_rule > 1 || o.primal_weight_update < 0 ||
+        o.primal_weight_update > 1) {
+        c.err = "pdhg_solve: invalid options";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    if (o.precision == PDHG_PREC_FP64_EXACT && (o.restart_rule != 0 || o.primal_weight_update)) {
+        c.err = "pdhg_solve: the adaptive restart rule and the primal weight need precision "
+                "mixed or fp64 (fp64_exact reproduces the reference, which has neither)";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    CK(cudaSetDevice(c.device));
+    ScalingParams sp;
+    sp.ruiz_iterations = o.ruiz_iterations;
+    sp.ruiz_tolerance = o.ruiz_tolerance;
+    sp.pock_chambolle_alpha = o.pock_chambolle_alpha;
+    sp.apply_ruiz = o.apply_ruiz != 0;
+    sp.apply_pock_chambolle = o.apply_pock_chambolle != 0;
+    int rc = ensure_scaled(c, sp);
+    if (rc != PDHG_OK) return rc;
+    if (!c.have_opnorm || c.opnorm_iters != o.power_iterations) {
+        rc = operator_norm(c, o.power_iterations, &c.opnorm);
+        if (rc != PDHG_OK) return rc;
+        c.have_opnorm = true;
+        c.opnorm_iters = o.power_iterations;
+    }
+    const double op = c.opnorm;
+    info->operator_norm_estimate = op;  // pdhg.cpp:261-265
+    const double step = (op > 1e-9) ? o.step_size_safety / op : o.step_size_safety;
+    // primal weight: 1 (tau = sigma = step) unless updated; then it starts at |c|/|b|
+    double omega = 1.0;
+    if (o.primal_weight_update && c.cnorm2_s > 1e-10 && c.bnorm2_s > 1e-10)
+        omega = c.cnorm2_s / c.bnorm2_s;
+
+    int prec = o.precision;
+    rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
+    if (rc != PDHG_OK) return rc;
+    CK(c.st.alloc(1));
+
+    // Initial point (pdhg.cpp:268-270) or the warm start, in scaled space.
+    const int32_t n = c.lp.n, m = c.lp.m;
+    const double sign = c.lp.maximize ? -1.0 : 1.0;
+    const double* x0d = nullptr;
+    const double* y0d = nullptr;
+    if (o.x0 != nullptr) {
+        std::vector<double> h(static_cast<size_t>(n));
+        for (int32_t j = 0; j < n; ++j) h[j] = o.x0[j] / c.cs[j];
+        CK(upload(c.x0s, h, c.stream));
+        x0d = c.x0s.p;
+    }
+    if (o.y0 != nullptr) {
+        std::vector<double> h(static_cast<size_t>(m));
+        for (int32_t i = 0; i < m; ++i) h[i] = o.y0[i] * sign / c.rs[i];
+        CK(upload(c.y0s, h, c.stream));
+        y0d = c.y0s.p;
+    }
+    const DevProblem P = c.problem();
+    if (prec == PDHG_PREC_MIXED)
+        launch_init_point<float>(P, c.As.view(), x0d, y0d, iterates<float>(c), c.stream);
+    else
+        launch_init_point<double>(P, c.As.view(), x0d, y0d, iterates<double>(c), c.stream);
+    c.launches += 1;
+    if (o.primal_weight_update) {
+        CK(c.x_last.alloc(static_cast<size_t>(n) + 1));
+        CK(c.y_last.alloc(static_cast<size_t>(m) + 1));
+        const int g = (std::max(n, m) + kBlock) / kBlock;
+        if (prec == PDHG_PREC_MIXED)
+            k_snapshot<float><<<g, kBlock, 0, c.stream>>>(iterates<float>(c), c.x_last.p, c.y_last.p, n, m);
+        else
+            k_snapshot<double><<<g, kBlock, 0, c.stream>>>(iterates<double>(c), c.x_last.p, c.y_last.p, n, m);
+        c.launches += 1;
+    }
+    rc = reset_state(c, step, omega);
+    if (rc != PDHG_OK) return rc;
+
+    long long iterations = 0;
+    int status = PDHG_STATUS_NOT_SOLVED;
+    const long long max_it = o.max_iterations > 0 ? o.max_iterations : 0;
+    // The reference checks cancellation, then the time limit, before every
+    // iteration (pdhg.cpp:288-293); these two catch the iteration-0 case.
+    bool early = false;
+    if (max_it > 0 && o.cancel_flag != nullptr && *o.cancel_flag) {
+        status = PDHG_STATUS_CANCELLED;
+        early = true;
+    } else if (max_it > 0 && o.time_limit_seconds > 0.0 && elapsed_since(t0) > o.time_limit_seconds) {
+        status = PDHG_STATUS_TIME_LIMIT;
+        early = true;
+    }
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, c.stream));
+    long long fp64_its = 0;
+    if (!early) {
+        const bool want_cb = o.checkpoint != nullptr;
+        Launcher L = make_launcher(c, prec, o, want_cb);
+        LoopOut lo;
+        const bool allow_switch = prec == PDHG_PREC_MIXED && o.polish_iterations != 0;
+        rc = run_loop(c, L, o, max_it, 0, t0, allow_switch, &lo);
+        if (rc != PDHG_OK) return rc;
+        iterations = lo.iterations;
+        status = lo.status;
+        if (lo.switch_precision) {
+            // FP64 phase from the FP32 point, for the remaining budget.
+            long long left = max_it - iterations;
+            if (o.polish_iterations > 0 && o.polish_iterations < left) left = o.polish_iterations;
+            k_widen<<<(std::max(n, m) + kBlock) / kBlock, kBlock, 0, c.stream>>>(
+                iterates<float>(c), iterates<double>(c), n, m);
+            k_restart_state<<<1, 1, 0, c.stream>>>(c.st.p);
+            c.launches += 2;
+            std::memset(const_cast<Mailbox*>(c.mail), 0, sizeof(Mailbox));
+            prec = PDHG_PREC_FP64;
+            Launcher L2 = make_launcher(c, prec, o, want_cb);
+            LoopOut lo2;
+            rc = run_loop(c, L2, o, left, iterations, t0, false, &lo2);
+            if (rc != PDHG_OK) return rc;
+            iterations += lo2.iterations;
+            fp64_its = lo2.iterations;
+            status = lo2.status;
+        }
+    }
+    CK(cudaEventRecord(ev1, c.stream));
+    CK(cudaEventSynchronize(ev1));
+    float loop_ms = 0.f;
+    cudaEventElapsedTime(&loop_ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+
+    DevState h;
+    CK(cudaMemcpy(&h, c.st.p, sizeof h, cudaMemcpyDeviceToHost));
+    info->iterations = iterations;
+    info->restarts = h.restarts;
+    info->relative_kkt = h.rel_kkt;
+    info->fp64_iterations = prec == PDHG_PREC_MIXED ? 0 : (fp64_its > 0 ? fp64_its : iterations);
+    info->device_seconds = loop_ms * 1e-3;
+    if (status == PDHG_STATUS_NUMERICAL_FAILURE) {  // pdhg.cpp:347-371 return early
+        info->status = status;
+        std::snprintf(info->message, sizeof info->message,
+                      h.fail_kind == 2 ? "non-finite KKT residual (original units) at iteration %lld"
+                                       : "non-finite KKT residual at iteration %lld",
+                      iterations);
+        info->has_point = 0;
+        info->kernel_launches = c.launches;
+        return PDHG_OK;
+    }
+    if (status == PDHG_STATUS_NOT_SOLVED) status = PDHG_STATUS_ITERATION_LIMIT;
+    info->status = status;
+
+    // Final result (pdhg.cpp:420-498) on the original problem.
+    if (prec == PDHG_PREC_MIXED)
+        launch_select_point<float>(iterates<float>(c), c.st.p, n, m, c.bx.p, c.by.p, c.stream);
+    else
+        launch_select_point<double>(iterates<double>(c), c.st.p, n, m, c.bx.p, c.by.p, c.stream);
+    FinalArgs fa;
+    fa.Ao = c.Ao.view();
+    fa.ATo = c.ATo.view();
+    fa.P = P;
+    fa.best_x64 = c.bx.p;
+    fa.best_y64 = c.by.p;
+    fa.f = FinalScratch{c.xo.p, c.yo.p, c.rc.p, c.trow.p, c.tcol.p};
+    fa.bound_tol = o.tolerance > 1e-6 ? o.tolerance : 1e-6;
+    fa.exact = o.precision == PDHG_PREC_FP64_EXACT ? 1 : 0;
+    fa.st = c.st.p;
+    launch_final(fa, c.stream);
+    c.launches += 5;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&h, c.st.p, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    if (x != nullptr && n) CK(cudaMemcpyAsync(x, c.xo.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    if (y != nullptr && m) CK(cudaMemcpyAsync(y, c.yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+    if (rcv != nullptr && n) CK(cudaMemcpyAsync(rcv, c.rc.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    info->objective = h.objective;
+    info->primal_infeasibility = h.pinf;
+    info->dual_infeasibility = h.dinf;
+    info->duality_gap = h.duality_gap;
+    info->has_point = 1;
+    info->kernel_launches = c.launches;
+    info->seconds = elapsed_since(t0);
+    return PDHG_OK;
+}
+
+int load(Ctx& c, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
+         const int32_t* col_idx, const double* values, const double* cv, double obj_const,
+         int maximize, const double* col_lo, const double* col_hi, const double* row_lo,
+         const double* row_hi) {
+    if (m < 0 || n < 0 || nnz < 0 || nnz > std::numeric_limits<int32_t>::max()) {
+        c.err = "pdhg_load_problem: sizes must be non-negative and fit int32 indices";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    if (row_ptr == nullptr || (nnz > 0 && (col_idx == nullptr || values == nullptr)) ||
+        (n > 0 && (cv == nullptr || col_lo == nullptr || col_hi == nullptr)) ||
+        (m > 0 && (row_lo == nullptr || row_hi == nullptr))) {
+        c.err = "pdhg_load_problem: null array";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    CK(cudaSetDevice(c.device));
+    c.loaded = false;
+    c.scaled = false;
+    c.have_opnorm = false;
+    c.gen += 1;
+    HostLp& lp = c.lp;
+    lp.m = m;
+    lp.n = n;
+    lp.obj_const = obj_const;
+    lp.maximize = maximize != 0;
+    lp.A.rows = m;
+    lp.A.cols = n;
+    lp.A.rp.assign(row_ptr, row_ptr + m + 1);
+    lp.A.ci.assign(col_idx, col_idx + nnz);
+    lp.A.v.assign(values, values + nnz);
+    lp.c.assign(cv, cv + n);
+    lp.col_lo.assign(col_lo, col_lo + n);
+    lp.col_hi.assign(col_hi, col_hi + n);
+    lp.row_lo.assign(row_lo, row_lo + m);
+    lp.row_hi.assign(row_hi, row_hi + m);
+    c.loaded = true;
+    c.valid = validate_lp(lp, &c.why);
+    if (!c.valid) return PDHG_OK;
+    int rc = upload_matrix(c, lp.A, c.Ao, c.ATo, false);
+    if (rc != PDHG_OK) return rc;
+    cudaStream_t s = c.stream;
+    CK(upload(c.c_o, lp.c, s));
+    CK(upload(c.lo_o, lp.col_lo, s));
+    CK(upload(c.hi_o, lp.col_hi, s));
+    CK(upload(c.rlo_o, lp.row_lo, s));
+    CK(upload(c.rhi_o, lp.row_hi, s));
+    c.bnorm = 0.0;
+    c.cnorm = 0.0;
+    for (int32_t i = 0; i < m; ++i) {
+        if (std::isfinite(lp.row_lo[i])) c.bnorm = std::max(c.bnorm, std::fabs(lp.row_lo[i]));
+        if (std::isfinite(lp.row_hi[i])) c.bnorm = std::max(c.bnorm, std::fabs(lp.row_hi[i]));
+    }
+    for (int32_t j = 0; j < n; ++j) c.cnorm = std::max(c.cnorm, std::fabs(lp.c[j]));
+    CK(cudaStreamSynchronize(s));
+    return ensure_scaled(c, ScalingParams{});
+}
+
+// ---- profiling ----------------------------------------------------------------
+
+double iter_bytes(const Ctx& c, int prec, bool primal) {
+    const double vb = prec == PDHG_PREC_MIXED ? 4.0 : 8.0;  // value / vector element bytes
+    const double nnz = static_cast<double>(c.As.nnz);
+    const double n = c.lp.n, m = c.lp.m;
+    // matrix stream (row pointer + index + value), one read of each gathered
+    // vector entry, the fused epilogue's vector reads and writes
+    if (primal) return 4.0 * (n + 1) + (4.0 + vb) * nnz + vb * m + vb * (5 * n) + vb * (3 * n);
+    return 4.0 * (m + 1) + (4.0 + vb) * nnz + vb * n + vb * (5 * m) + vb * (3 * m);
+}
+
+int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
+    std::memset(out, 0, sizeof *out);
+    if (!c.loaded || !c.valid || !c.have_opnorm) {
+        c.err = "pdhg_profile_kernels: solve a valid problem first";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    CK(cudaSetDevice(c.device));
+    int rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
+    if (rc != PDHG_OK) return rc;
+    CK(c.st.alloc(1));
+    pdhg_options o;
+    pdhg_default_options(&o);
+    o.precision = prec;
+    o.termination_rule = 1;
+    const double step = c.opnorm > 1e-9 ? 0.9 / c.opnorm : 0.9;
+    Launcher L = make_launcher(c, prec, o, false);
+    rc = reset_state(c, step, 1.0);
+    if (rc != PDHG_OK) return rc;
+    const DevProblem P = c.problem();
+    if (prec == PDHG_PREC_MIXED)
+        launch_init_point<float>(P, c.As.view(), nullptr, nullptr, iterates<float>(c), c.stream);
+    else
+        launch_init_point<double>(P, c.As.view(), nullptr, nullptr, iterates<double>(c), c.stream);
+    for (int i = 0; i < warmup; ++i) L.iteration(i == 0, c.stream);
+    std::vector<cudaEvent_t> ev(3 * static_cast<size_t>(iters) + 2);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int i = 0; i < iters; ++i) {
+        CK(cudaEventRecord(ev[3 * i], c.stream));
+        if (prec == PDHG_PREC_FP64_EXACT) launch_exact_primal(L.ei, 0, c.stream);
+        else if (prec == PDHG_PREC_MIXED) launch_fast_primal(L.fi32, 0, c.stream);
+        else launch_fast_primal(L.fi64, 0, c.stream);
+        CK(cudaEventRecord(ev[3 * i + 1], c.stream));
+        if (prec == PDHG_PREC_FP64_EXACT) launch_exact_dual(L.ei, 0, c.stream);
+        else if (prec == PDHG_PREC_MIXED) launch_fast_dual(L.fi32, 0, c.stream);
+        else launch_fast_dual(L.fi64, 0, c.stream);
+        CK(cudaEventRecord(ev[3 * i + 2], c.stream));
+    }
+    CK(cudaEventRecord(ev[3 * iters], c.stream));
+    L.check(1, c.stream);
+    CK(cudaEventRecord(ev[3 * iters + 1], c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    double tp = 0, td = 0;
+    for (int i = 0; i < iters; ++i) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+        tp += a;
+        td += b;
+    }
+    float tc = 0;
+    cudaEventElapsedTime(&tc, ev[3 * iters], ev[3 * iters + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    out->count = 3;
+    std::snprintf(out->name[0], 32, "primal");
+    std::snprintf(out->name[1], 32, "dual");
+    std::snprintf(out->name[2], 32, "check");
+    out->avg_ms[0] = iters ? tp / iters : 0;
+    out->avg_ms[1] = iters ? td / iters : 0;
+    out->avg_ms[2] = tc;
+    out->bytes[0] = iter_bytes(c, prec, true);
+    out->bytes[1] = iter_bytes(c, prec, false);
+    out->bytes[2] = 2.0 * (12.0 * c.As.nnz) + 8.0 * 10 * (c.lp.n + c.lp.m);
+    out->launches[0] = iters;
+    out->launches[1] = iters;
+    out->launches[2] = 1;
+    return PDHG_OK;
+}
+
+}  // namespace
+}  // namespace pdhg
+
+// ============================================================================
+// C-ABI
+// ============================================================================
+
+extern "C" {
+
+int pdhg_abi_version(void) { return PDHG_B200_ABI_VERSION; }
+
+void pdhg_default_options(pdhg_options* o) {
+    if (o == nullptr) return;
+    std::memset(o, 0, sizeof *o);
+    o->tolerance = 1e-4;  // pdhg.hpp:89-117
+    o->max_iterations = 1000000;
+    o->time_limit_seconds = 0.0;
+    o->restart_check_period = 40;
+    o->restart_sufficient_decrease = 0.5;
+    o->step_size_safety = 0.9;
+    o->power_iterations = 30;
+    o->verbose = 0;
+    o->ruiz_iterations = 8;  // scaling.hpp:299-309
+    o->ruiz_tolerance = 1e-2;
+    o->pock_chambolle_alpha = 1.0;
+    o->apply_ruiz = 1;
+    o->apply_pock_chambolle = 1;
+    o->precision = PDHG_PREC_FP64_EXACT;
+    o->termination_rule = 0;
+    o->polish_iterations = -1;
+}
+
+const char* pdhg_status_string(int s) {
+    switch (s) {  // pdhg.cpp:17-27
+        case PDHG_STATUS_OPTIMAL: return "optimal";
+        case PDHG_STATUS_ITERATION_LIMIT: return "iteration_limit";
+        case PDHG_STATUS_TIME_LIMIT: return "time_limit";
+        case PDHG_STATUS_NUMERICAL_FAILURE: return "numerical_failure";
+        case PDHG_STATUS_NOT_SOLVED: return "not_solved";
+        case PDHG_STATUS_CANCELLED: return "cancelled";
+    }
+    return "unknown";
+}
+
+const char* pdhg_error_string(int e) {
+    switch (e) {  // status.hpp:36-48
+        case PDHG_OK: return "ok";
+        case PDHG_ERR_UNSUPPORTED: return "unsupported by this backend";
+        case PDHG_ERR_NOT_IMPLEMENTED: return "not implemented yet";
+        case PDHG_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case PDHG_ERR_DIMENSION_MISMATCH: return "dimension mismatch";
+        case PDHG_ERR_OUT_OF_MEMORY: return "out of memory";
+        case PDHG_ERR_BACKEND: return "backend error";
+        case PDHG_ERR_NUMERICAL_FAILURE: return "numerical failure";
+    }
+    return "unknown status";
+}
+
+int pdhg_create(int device, pdhg_ctx** out) {
+    if (out == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+        return PDHG_ERR_UNSUPPORTED;
+    std::unique_ptr<pdhg_ctx> h;
+    try {
+        h.reset(new pdhg_ctx());
+    } catch (...) {
+        return PDHG_ERR_OUT_OF_MEMORY;
+    }
+    pdhg::Ctx& c = h->c;
+    c.device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return PDHG_ERR_BACKEND;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    void* mp = nullptr;
+    if (cudaHostAlloc(&mp, sizeof(pdhg::Mailbox), cudaHostAllocMapped) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    c.mail = static_cast<pdhg::Mailbox*>(mp);
+    std::memset(mp, 0, sizeof(pdhg::Mailbox));
+    void* dp = nullptr;
+    if (cudaHostGetDevicePointer(&dp, mp, 0) != cudaSuccess) return PDHG_ERR_BACKEND;
+    c.mail_dev = static_cast<pdhg::Mailbox*>(dp);
+    *out = h.release();
+    return PDHG_OK;
+}
+
+int pdhg_destroy(pdhg_ctx* ctx) {
+    if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->c.device);
+    if (ctx->c.stream != nullptr) cudaStreamSynchronize(ctx->c.stream);
+    delete ctx;
+    return PDHG_OK;
+}
+
+const char* pdhg_last_error(const pdhg_ctx* ctx) {
+    return ctx == nullptr ? "null context" : ctx->c.err.c_str();
+}
+
+void* pdhg_stream(const pdhg_ctx* ctx) {
+    return ctx == nullptr ? nullptr : static_cast<void*>(ctx->c.stream);
+}
+
+int pdhg_load_problem(pdhg_ctx* ctx, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_idx, const double* values, const double* c,
+                      double obj_const, int maximize, const double* col_lo,
+                      const double* col_hi, const double* row_lo, const double* row_hi) {
+    if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    try {
+        return pdhg::load(ctx->c, m, n, nnz, row_ptr, col_idx, values, c, obj_const, maximize,
+                          col_lo, col_hi, row_lo, row_hi);
+    } catch (const std::bad_alloc&) {
+        ctx->c.err = "host allocation failed";
+        return PDHG_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        ctx->c.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
+int pdhg_solve(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* info, double* x,
+               double* y, double* rc) {
+    if (ctx == nullptr || info == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg_options o;
+    if (options == nullptr) pdhg_default_options(&o);
+    else o = *options;
+    try {
+        return pdhg::solve(ctx->c, o, info, x, y, rc);
+    } catch (const std::bad_alloc&) {
+        ctx->c.err = "host allocation failed";
+        return PDHG_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        ctx->c.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
+int pdhg_profile_kernels(pdhg_ctx* ctx, int precision, int warmup, int iterations,
+                         pdhg_kernel_stats* out) {
+    if (ctx == nullptr || out == nullptr || iterations < 1 || warmup < 0 || precision < 0 ||
+        precision > 2)
+        return PDHG_ERR_INVALID_ARGUMENT;
+    try {
+        return pdhg::profile(ctx->c, precision, warmup, iterations, out);
+    } catch (const std::exception& e) {
+        ctx->c.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
+int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
+                  const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                  double alpha, const double* x, double beta, double* y) {
+    if (m < 0 || n < 0 || nnz < 0 || nnz > std::numeric_limits<int32_t>::max() ||
+        row_ptr == nullptr || y == nullptr || (nnz > 0 && (col_idx == nullptr || values == nullptr)))
+        return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg_ctx* h = nullptr;
+    int rc = pdhg_create(device, &h);
+    if (rc != PDHG_OK) return rc;
+    std::unique_ptr<pdhg_ctx> guard(h);
+    pdhg::Ctx& c = h->c;
+    pdhg::HostCsr A;
+    A.rows = m;
+    A.cols = n;
+    A.rp.assign(row_ptr, row_ptr + m + 1);
+    A.ci.assign(col_idx, col_idx + nnz);
+    A.v.assign(values, values + nnz);
+    rc = pdhg::upload_matrix(c, A, c.Ao, c.ATo, false);
+    if (rc != PDHG_OK) return rc;
+    const int32_t nx = transpose ? m : n, ny = transpose ? n : m;
+    pdhg::DBuf<double> dx, dy;
+    if (pdhg::upload(dx, x, static_cast<size_t>(nx), c.stream) != cudaSuccess ||
+        pdhg::upload(dy, y, static_cast<size_t>(ny), c.stream) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    if (transpose)
+        pdhg::launch_spmvT_exact(c.ATo.view(), alpha, dx.p, beta, dy.p, c.stream);
+    else
+        pdhg::launch_spmv_exact(c.Ao.view(), alpha, dx.p, beta, dy.p, c.stream);
+    if (ny > 0 && cudaMemcpyAsync(y, dy.p, sizeof(double) * ny, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return PDHG_ERR_BACKEND;
+    return PDHG_OK;
+}
+
+int pdhg_project_box(int device, int32_t n, const double* lo, const double* hi, double* x) {
+    if (n < 0 || (n > 0 && x == nullptr)) return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg_ctx* h = nullptr;
+    int rc = pdhg_create(device, &h);
+    if (rc != PDHG_OK) return rc;
+    std::unique_ptr<pdhg_ctx> guard(h);
+    pdhg::Ctx& c = h->c;
+    pdhg::DBuf<double> dx, dl, dh;
+    if (pdhg::upload(dx, x, static_cast<size_t>(n), c.stream) != cudaSuccess) return PDHG_ERR_BACKEND;
+    if (lo != nullptr && pdhg::upload(dl, lo, static_cast<size_t>(n), c.stream) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    if (hi != nullptr && pdhg::upload(dh, hi, static_cast<size_t>(n), c.stream) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    pdhg::launch_project_box(n, lo ? dl.p : nullptr, hi ? dh.p : nullptr, dx.p, c.stream);
+    if (n > 0 && cudaMemcpyAsync(x, dx.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return PDHG_ERR_BACKEND;
+    return PDHG_OK;
+}
+
+int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
+                 const int32_t* col_idx, const double* values, const pdhg_options* options,
+                 double* row_scale, double* col_scale) {
+    if (m < 0 || n < 0 || nnz < 0 || row_ptr == nullptr || row_scale == nullptr ||
+        col_scale == nullptr || (nnz > 0 && (col_idx == nullptr || values == nullptr)))
+        return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg_options o;
+    if (options == nullptr) pdhg_default_options(&o);
+    else o = *options;
+    pdhg::HostCsr A;
+    A.rows = m;
+    A.cols = n;
+    A.rp.assign(row_ptr, row_ptr + m + 1);
+    A.ci.assign(col_idx, col_idx + nnz);
+    A.v.assign(values, values + nnz);
+    pdhg::ScalingParams sp;
+    sp.ruiz_iterations = o.ruiz_iterations;
+    sp.ruiz_tolerance = o.ruiz_tolerance;
+    sp.pock_chambolle_alpha = o.pock_chambolle_alpha;
+    sp.apply_ruiz = o.apply_ruiz != 0;
+    sp.apply_pock_chambolle = o.apply_pock_chambolle != 0;
+    std::vector<double> rs, cs;
+    pdhg::equilibrate(A, sp, &rs, &cs);
+    std::memcpy(row_scale, rs.data(), sizeof(double) * m);
+    std::memcpy(col_scale, cs.data(), sizeof(double) * n);
+    return PDHG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,266 @@
+// engine.cuh -- device-side data layout of the PDHG engine.
+//
+// One LP lives in HBM for the whole solve (the reference keeps A resident the
+// same way, include/sovereign/backend.hpp:225-263, but stores only A and runs
+// A^T through a transpose flag; here A^T is a second CSR built on the device).
+//
+//   A_s, AT_s : the Ruiz+Pock-Chambolle scaled matrix and its transpose,
+//               FP64 values (+ FP32 copies for the mixed-precision kernels).
+//   A_o, AT_o : the original matrix and its transpose, FP64 (original-space
+//               residuals and the final result). Index arrays are shared with
+//               A_s/AT_s when scaling dropped no entry.
+//   vectors   : scaled c (objective sign applied), bounds, scale factors,
+//               iterates x, x_bar, s, y and the Cesaro sums, all dense.
+//   DevState  : the solver's control state (iteration counters, restart state,
+//               residuals, stop flag) -- decided on the device every check
+//               period, so the loop needs no host round trip.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace pdhg {
+
+constexpr int kBlock = 256;  // threads per CTA for every engine kernel
+
+struct DevCsr {
+    int32_t rows = 0, cols = 0;
+    int64_t nnz = 0;
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const double* v64 = nullptr;
+    const float* v32 = nullptr;
+    // Row binning for the warp-parallel kernels: rows longer than kLongRow are
+    // listed in long_rows and handled one CTA per row; the others by groups of
+    // `vw` lanes.
+    const int32_t* long_rows = nullptr;
+    int32_t n_long = 0;
+    int32_t n_short = 0;
+    int vw = 1;
+};
+
+constexpr int kLongRow = 512;
+
+// Accumulator slots (bit patterns of non-negative doubles, combined with
+// atomicMax -- order-independent, so exact).
+enum Acc {
+    ACC_CUR_P = 0, ACC_CUR_D, ACC_AVG_P, ACC_AVG_D,        // scaled-space residual parts
+    ACC_ORIG_P, ACC_ORIG_D,                               // exact mode: candidate, original space
+    ACC_OC_P, ACC_OC_D, ACC_OA_P, ACC_OA_D,               // fast mode: cur / avg, original space
+    ACC_FIN_PINF, ACC_FIN_DINF,                           // final result
+    ACC_COUNT = 16
+};
+
+enum Ticket { TK_CHECK1 = 0, TK_CHECK2, TK_FAST, TK_RESTART, TK_COUNT = 4 };
+
+struct DevState {
+    int done;         // 1 = every later kernel returns at once
+    int status;       // pdhg_status once done
+    int converged;
+    int fresh;        // the next period starts right after a restart
+    int restart;      // the last check restarted
+    int avg_better;   // the last check picked the average as candidate
+    int fail_kind;    // 1 = scaled residual non-finite, 2 = original residual non-finite
+    int fold;         // mixed mode: fold the FP32 period sums into the FP64 sums
+    long long iter;           // iterations completed before the current period
+    long long since_restart;  // iterations averaged at the last check
+    long long restarts;
+    long long stop_iter;      // iteration count reported on stop
+    long long checks;
+    double res_last;          // residual at the last restart (+inf before the first check)
+    double cur_res, avg_res, orig_res, rel_kkt;
+    double inv;               // 1 / iterations in the Cesaro average at the last check
+    double objective, dual_objective, duality_gap, pinf, dinf;
+    // step sizes: tau = eta / omega, sigma = eta * omega (omega = primal weight;
+    // the reference keeps omega = 1, tau = sigma, pdhg.cpp:263-265)
+    double tau, sigma, omega, eta;
+    double res_prev_cand;     // adaptive rule: candidate residual at the previous check
+    int restart_to_avg;       // adaptive rule: restart point is the average (else current)
+    int gap_finite;
+    unsigned long long acc[ACC_COUNT];
+    unsigned int ticket[TK_COUNT];
+};
+
+// Host-mapped pinned mailbox: the host writes stop requests (time limit,
+// cancellation), the last block of every check writes its decision here.
+struct Mailbox {
+    volatile int stop_request;  // 0, or the pdhg_status to stop with
+    volatile int done;
+    volatile int status;
+    volatile int restarted;
+    volatile long long iter;
+    volatile long long restarts;
+    volatile long long checks;
+    volatile double cur_res, avg_res, orig_res, rel_kkt;
+};
+
+// Problem vectors (device, FP64 unless noted).
+struct DevProblem {
+    int32_t m = 0, n = 0;
+    double obj_sign = 1.0;
+    double obj_const = 0.0;
+    const double *c = nullptr, *lo = nullptr, *hi = nullptr;    // scaled, c signed
+    const double *rlo = nullptr, *rhi = nullptr;                // scaled row bounds
+    const double *c_o = nullptr, *lo_o = nullptr, *hi_o = nullptr;
+    const double *rlo_o = nullptr, *rhi_o = nullptr;            // original
+    const double *rs = nullptr, *cs = nullptr;                  // row / column scale
+    const float *c32 = nullptr, *lo32 = nullptr, *hi32 = nullptr;
+    const float *rlo32 = nullptr, *rhi32 = nullptr;
+    double bnorm = 0.0, cnorm = 0.0;  // relative-KKT norms (original space)
+};
+
+// Iterates. T = double for the FP64 modes, float for the mixed mode; the
+// mixed mode keeps per-period FP32 partial sums (psx, psy) that the check
+// folds into the FP64 Cesaro sums (xsum, ysum).
+template <class T>
+struct Iterates {
+    T *x = nullptr, *xbar = nullptr, *s = nullptr, *y = nullptr;
+    T *psx = nullptr, *psy = nullptr;
+    double *xsum = nullptr, *ysum = nullptr;
+};
+
+struct CheckScratch {
+    double* act_avg = nullptr;   // m: A x_avg (unprojected), for the restart's slack
+    double* cand_xo = nullptr;   // n: the candidate in original units
+    double* cand_yo = nullptr;   // m
+    double* part = nullptr;      // block partial sums (deterministic reduction)
+    int part_blocks = 0;
+};
+
+struct FinalScratch {
+    double* xo = nullptr;   // n
+    double* yo = nullptr;   // m
+    double* rc = nullptr;   // n
+    double* trow = nullptr; // m: dual-objective row terms
+    double* tcol = nullptr; // n: dual-objective column terms
+};
+
+// ---- launchers (kernels_exact.cu) ------------------------------------------
+// tau and sigma live in DevState (they change with the primal weight).
+struct ExactIter {
+    DevCsr A, AT;
+    DevProblem P;
+    Iterates<double> it;
+    DevState* st;
+};
+void launch_exact_primal(const ExactIter& a, int first, cudaStream_t s);
+void launch_exact_dual(const ExactIter& a, int first, cudaStream_t s);
+
+struct ExactCheck {
+    DevCsr A, AT, Ao, ATo;
+    DevProblem P;
+    Iterates<double> it;
+    CheckScratch cs;
+    double tol, bound_tol, restart_decrease;
+    long long period_iters;
+    int termination_rule;
+    int want_candidate;
+    DevState* st;
+    Mailbox* mail;
+};
+void launch_exact_check(const ExactCheck& a, cudaStream_t s);
+void launch_exact_restart(const ExactCheck& a, cudaStream_t s);
+
+// ---- launchers (kernels_fast.cu) -------------------------------------------
+template <class T>
+struct FastIter {
+    DevCsr A, AT;
+    DevProblem P;
+    Iterates<T> it;
+    DevState* st;
+};
+template <class T>
+void launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s);
+template <class T>
+void launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s);
+template <class T>
+int fast_launches_per_iteration(const FastIter<T>& a);
+
+// Restart rules: 0 = the reference's (restart to the average when its residual
+// is <= restart_decrease x the residual at the last restart, pdhg.cpp:391-408);
+// 1 = adaptive: restart to the better of average / current on sufficient decay
+// (<= 0.2x), on necessary decay (<= 0.8x) without progress since the previous
+// check, or when the average spans >= 36% of all iterations.
+template <class T>
+struct FastCheck {
+    DevCsr A, AT;  // scaled, FP64 values used
+    DevProblem P;
+    Iterates<T> it;
+    CheckScratch cs;
+    double tol, bound_tol, restart_decrease;
+    long long period_iters;
+    int termination_rule;
+    int want_candidate;
+    DevState* st;
+    Mailbox* mail;
+    int restart_rule;
+    int primal_weight_update;  // omega <- sqrt(omega * |dy| / |dx|) at each restart
+    double* x_last;            // scaled point of the last restart (n)
+    double* y_last;            // (m)
+};
+template <class T>
+void launch_fast_check(const FastCheck<T>& a, cudaStream_t s);
+template <class T>
+void launch_fast_restart(const FastCheck<T>& a, cudaStream_t s);
+
+// ---- setup / final (kernels_exact.cu) ------------------------------------------
+// Exact pairwise sum of x[i]*y[i] (HostBackend::pairwise_dot order) into *out.
+void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* partial,
+                         double* out, cudaStream_t s);
+int64_t pairwise_partial_size(int64_t n);
+// Power-iteration pieces (estimate_operator_norm, pdhg.cpp:48-79).
+void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s);
+void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s);
+void launch_scale(double* x, int64_t n, double alpha, cudaStream_t s);
+void launch_fill(double* x, int64_t n, double v, cudaStream_t s);
+
+struct FinalArgs {
+    DevCsr Ao, ATo;
+    DevProblem P;
+    const double* best_x64 = nullptr;  // scaled best point, FP64 (or null)
+    const double* best_y64 = nullptr;
+    const float* best_x32 = nullptr;   // mixed mode current point
+    const float* best_y32 = nullptr;
+    FinalScratch f;
+    double bound_tol;
+    int exact;
+    DevState* st;
+};
+void launch_final(const FinalArgs& a, cudaStream_t s);
+
+// Best point selection for the final result: the check's candidate when
+// converged, else the current iterate (pdhg.cpp:420-423). Materialises the
+// scaled FP64 point into (bx, by).
+template <class T>
+void launch_select_point(const Iterates<T>& it, const DevState* st, int32_t n, int32_t m,
+                         double* bx, double* by, cudaStream_t s);
+
+// Initial point (pdhg.cpp:268-270) or warm start; FP64 scaled inputs.
+template <class T>
+void launch_init_point(const DevProblem& P, const DevCsr& A, const double* x0s,
+                       const double* y0s, Iterates<T> it, cudaStream_t s);
+
+// Backend primitives for the known-answer tests.
+void launch_spmv_exact(const DevCsr& A, double alpha, const double* x, double beta, double* y,
+                       cudaStream_t s);
+void launch_spmvT_exact(const DevCsr& AT, double alpha, const double* x, double beta, double* y,
+                        cudaStream_t s);
+int fast_check_grid(const DevCsr& A, const DevCsr& AT);
+void launch_project_box(int32_t n, const double* lo, const double* hi, double* x,
+                        cudaStream_t s);
+
+// Device CSR transpose: stable by column, so each A^T row lists its entries in
+// ascending original row order (the order the reference's scatter adds them,
+// src/l0/backend_host.cpp:439-444).
+struct TransposeOut {
+    int32_t* rp;
+    int32_t* ci;
+    double* v;
+};
+int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const double* v, TransposeOut out, cudaStream_t s);
+
+void launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
+
+}  // namespace pdhg

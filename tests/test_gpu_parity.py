@@ -1,0 +1,256 @@
+"""GPU parity: the CUDA engine, called through the C-ABI, against the
+reference's outputs (golden fixtures) and the oracle on the same inputs.
+
+* FP64-exact mode must reproduce the reference bit for bit: iterates of the
+  first 100 iterations, restart counts, iteration counts, statuses, results.
+* FP64 mode (warp-parallel sums): iterates within 1e-10 relative over the
+  first 100 iterations, final objective within 1e-8 relative wherever both
+  stop at the same iteration with the same status.
+* Mixed mode (FP32 iterates, FP64 checks): same status, objective within the
+  tolerance the relative-KKT rule promises.
+"""
+import numpy as np
+import pytest
+
+from conftest import PDHG_CASES, golden_problem, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine(pkg):
+    e = pkg.Engine(0)
+    yield e
+    e.close()
+
+
+def solve(pkg, engine, p, **kw):
+    trace = kw.pop("trace_iters", 0)
+    cancel = kw.pop("cancel", None)
+    x0 = kw.pop("x0", None)
+    y0 = kw.pop("y0", None)
+    opt = pkg.PdhgOptions(trace_iters=trace, **kw)
+    engine.load(p)
+    return engine.solve(opt, cancel=cancel, x0=x0, y0=y0)
+
+
+def same_as_golden(r, g):
+    assert r.status == g["ref_status"], (r.status, g["ref_status"], r.message)
+    assert r.message == g["ref_message"]
+    assert r.iterations == g["ref_iterations"]
+    assert r.restarts == g["ref_restarts"]
+    assert r.operator_norm_estimate == g["ref_operator_norm_estimate"]
+    for f in ("objective", "primal_infeasibility", "dual_infeasibility", "duality_gap"):
+        assert getattr(r, f) == g["ref_" + f], (f, getattr(r, f), g["ref_" + f])
+    if g["ref_has_point"]:
+        for f in ("primal", "dual", "reduced_costs"):
+            assert np.array_equal(getattr(r, f), g["ref_" + f]), f
+
+
+@pytest.mark.parametrize("name", PDHG_CASES)
+def test_exact_mode_is_bit_identical_to_the_reference(pkg, engine, name):
+    g = load_golden(name)
+    p = golden_problem(pkg, g)
+    tr = 100 if "trace_x" in g else 0
+    r = solve(pkg, engine, p, trace_iters=tr, **g["options"])
+    same_as_golden(r, g)
+    if tr:
+        keep = g.get("trace_iters_kept")
+        tx = r.trace_x if keep is None else r.trace_x[keep]
+        ty = r.trace_y if keep is None else r.trace_y[keep]
+        assert np.array_equal(tx, g["trace_x"]) and np.array_equal(ty, g["trace_y"])
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+
+@pytest.mark.parametrize("name", ["rand_eq_60x150", "rand_eq_max_40x100", "mixed_bounds_50x90",
+                                  "c0_2000x5000_tol1e-4"])
+def test_fp64_mode_tracks_the_reference(pkg, engine, name):
+    g = load_golden(name)
+    p = golden_problem(pkg, g)
+    r = solve(pkg, engine, p, precision="fp64", trace_iters=100, **g["options"])
+    keep = g.get("trace_iters_kept")
+    tx = r.trace_x if keep is None else r.trace_x[keep]
+    ty = r.trace_y if keep is None else r.trace_y[keep]
+    assert rel_err(tx, g["trace_x"]) <= 1e-10
+    assert rel_err(ty, g["trace_y"]) <= 1e-10
+    assert r.status == g["ref_status"]
+    if r.iterations == g["ref_iterations"]:
+        assert abs(r.objective - g["ref_objective"]) <= 1e-8 * max(1.0, abs(g["ref_objective"]))
+    else:  # a decision flipped at a threshold: both must still be converged answers
+        assert abs(r.iterations - g["ref_iterations"]) <= 2 * g["options"].get("restart_check_period", 40)
+
+
+@pytest.mark.parametrize("name", ["rand_eq_max_40x100", "c0_2000x5000_tol1e-4",
+                                  "pdhg_two_variable_optimum_matches_simplex", "smoke_tiny_lp"])
+def test_mixed_mode_converges_to_the_reference_optimum(pkg, engine, name):
+    g = load_golden(name)
+    p = golden_problem(pkg, g)
+    opts = dict(g["options"])
+    r = solve(pkg, engine, p, precision="mixed", termination_rule="relative_kkt", **opts)
+    assert r.status == "optimal", (r.status, r.message, r.relative_kkt)
+    tol = opts.get("tolerance", 1e-4)
+    assert r.relative_kkt < tol
+    # |objective error| of a point with relative KKT < tol is O(tol) relative
+    assert abs(r.objective - g["ref_objective"]) <= 20 * tol * (1 + abs(g["ref_objective"]))
+
+
+def test_checkpoints_match_the_oracle(pkg, orc, engine):
+    p = pkg.lpgen.random_equality_lp(30, 70, 3, seed=5)
+    seen = []
+    r = solve(pkg, engine, p, max_iterations=400, restart_check_period=50,
+              checkpoint=lambda it, x, y, res: seen.append((it, x, y, res)))
+    o = orc.oracle_solve(p, max_iterations=400, restart_check_period=50, checkpoints=True)
+    assert [s[0] for s in seen] == [c[0] for c in o.checkpoints] == list(range(49, 400, 50))
+    for a, b in zip(seen, o.checkpoints):
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[3] == b[3]
+    assert r.iterations == o.iterations
+
+
+def test_cancellation_and_time_limit(pkg, orc, engine):
+    p = pkg.lpgen.random_equality_lp(40, 90, 4, seed=8)
+    tok = pkg.CancellationToken()
+    tok.cancel()
+    r = solve(pkg, engine, p, cancel=tok)
+    o = orc.oracle_solve(p, cancel=True)
+    assert r.status == o.status == "cancelled"
+    assert r.iterations == o.iterations == 0
+    assert np.array_equal(r.primal, o.primal)
+    r = solve(pkg, engine, p, time_limit_seconds=1e-9)
+    assert r.status == "time_limit" and r.iterations == 0 and r.primal.shape == (90,)
+    # a limit that fires mid-solve stops at a check-period boundary
+    big = pkg.lpgen.random_equality_lp(2000, 5000, 5, seed=0)
+    r = solve(pkg, engine, big, tolerance=1e-9, time_limit_seconds=0.3)
+    assert r.status == "time_limit"
+    assert r.iterations > 0 and r.iterations % 40 == 0
+    assert r.seconds < 5.0
+
+
+@pytest.mark.parametrize("mutate,msg", [
+    (lambda p: p.col_lo.__setitem__(7, 11.0), "invalid problem: crossed bounds on column C7"),
+    (lambda p: p.c.__setitem__(3, np.inf), "invalid problem: non-finite objective coefficient in column C3"),
+    (lambda p: p.row_hi.__setitem__(2, np.nan), "invalid problem: NaN bound on row R2"),
+    (lambda p: p.val.__setitem__(0, np.nan), "invalid problem: non-finite coefficient"),
+    (lambda p: p.col_idx.__setitem__(1, 10_000), "invalid problem: column index out of range"),
+])
+def test_invalid_problems_report_like_the_reference(pkg, orc, engine, mutate, msg):
+    p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=6)
+    mutate(p)
+    r = solve(pkg, engine, p)
+    o = orc.oracle_solve(p)
+    assert r.status == o.status == "numerical_failure"
+    assert r.message == o.message == msg
+    assert r.primal.size == 0 and r.iterations == 0
+
+
+def test_edge_sizes(pkg, orc, engine):
+    # no iterations at all
+    p = pkg.lpgen.random_equality_lp(10, 25, 2, seed=4)
+    r = solve(pkg, engine, p, max_iterations=0)
+    o = orc.oracle_solve(p, max_iterations=0)
+    assert r.status == o.status == "iteration_limit" and r.iterations == 0
+    assert np.array_equal(r.primal, o.primal) and r.objective == o.objective
+    # fewer iterations than one check period (no check at all)
+    r = solve(pkg, engine, p, max_iterations=17)
+    o = orc.oracle_solve(p, max_iterations=17)
+    assert r.iterations == o.iterations == 17 and np.array_equal(r.primal, o.primal)
+    assert np.array_equal(r.dual, o.dual)
+    # a problem with empty rows and columns
+    q = pkg.Problem.from_coo(4, 5, [0, 0, 2], [1, 3, 3], [1.0, -2.0, 0.5], c=np.arange(5.0),
+                             col_lo=np.zeros(5), col_hi=np.full(5, 3.0),
+                             row_lo=np.array([-1.0, -np.inf, 0.0, 0.0]),
+                             row_hi=np.array([1.0, np.inf, 1.0, 0.0]))
+    r = solve(pkg, engine, q, max_iterations=500)
+    o = orc.oracle_solve(q, max_iterations=500)
+    assert (r.status, r.iterations, r.objective) == (o.status, o.iterations, o.objective)
+    assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
+
+
+def test_backend_known_answers(pkg):
+    g = load_golden("backend_known_answers")
+    A = golden_problem(pkg, g)
+    assert np.array_equal(pkg.csr_spmv(A, 1.0, g["x"], 0.0, np.zeros(4)), g["ax"])
+    assert np.array_equal(pkg.csr_spmv(A, 2.0, g["x"], 3.0, np.ones(4)), g["ax_alpha_beta"])
+    assert np.array_equal(pkg.csr_spmv(A, 1.0, g["y"], 0.0, np.zeros(3), transpose=True), g["aty"])
+    out = pkg.csr_spmv(A, 1.0, g["x"], 0.0, np.full(4, np.nan))
+    assert not np.isnan(out).any() and out[1] == 18.0
+    assert np.array_equal(pkg.csr_spmv(A, 1.0, g["x_host"], 0.0, np.zeros(4)), g["ax_host"])
+    # project_box (tests/test_l0_backend.cpp:333-360)
+    x = pkg.project_box([0.0, 0.0, -1.0, -5.0], [1.0, 10.0, 1.0, 5.0], [-3.0, 4.0, 7.0, 0.5])
+    assert np.array_equal(x, [0.0, 4.0, 1.0, 0.5])
+    x = pkg.project_box([0.0, 0.0], None, [-3.0, 1e9])
+    assert np.array_equal(x, [0.0, 1e9])
+
+
+def test_spmv_matches_the_oracle_on_a_large_badly_scaled_matrix(pkg, orc):
+    p = pkg.lpgen.badly_scaled_lp(3000, 8000, 6, seed=21)
+    x = np.random.default_rng(0).standard_normal(p.n)
+    y = np.random.default_rng(1).standard_normal(p.m)
+    assert np.array_equal(pkg.csr_spmv(p, -1.0, x, 0.0, np.zeros(p.m)),
+                          orc.oracle_spmv(p, -1.0, x, 0.0, np.zeros(p.m)))
+    assert np.array_equal(pkg.csr_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True),
+                          orc.oracle_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True))
+
+
+def test_exact_mode_on_a_power_law_lp_matches_the_oracle(pkg, orc, engine):
+    # long rows (> 512 nonzeros) exercise the one-CTA-per-row paths
+    p = pkg.lpgen.badly_scaled_lp(1500, 4000, 6, seed=22)
+    r = solve(pkg, engine, p, max_iterations=400, tolerance=1e-6)
+    o = orc.oracle_solve(p, max_iterations=400, tolerance=1e-6)
+    assert (r.status, r.iterations, r.restarts) == (o.status, o.iterations, o.restarts)
+    assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
+    assert r.objective == o.objective
+    # and the warp-parallel FP64 path stays within FP64 rounding of it
+    r2 = solve(pkg, engine, p, precision="fp64", max_iterations=400, tolerance=1e-6)
+    assert r2.iterations == o.iterations
+    assert rel_err(r2.primal, o.primal) < 1e-9 and rel_err(r2.dual, o.dual) < 1e-9
+
+
+def test_transportation_lp_adaptive_restarts(pkg, orc, engine):
+    # the reference rule never restarts here (its oracle run stalls); the
+    # adaptive rule solves it, and FP64 mode follows the oracle's restatement
+    p = pkg.lpgen.transportation_lp(40, 100, seed=1000)
+    kw = dict(termination_rule="relative_kkt", restart_rule="adaptive", max_iterations=200_000)
+    o = orc.oracle_solve(p, termination_rule=1, restart_rule=1, max_iterations=200_000)
+    assert o.status == "optimal"
+    r64 = solve(pkg, engine, p, precision="fp64", **kw)
+    assert r64.status == "optimal"
+    assert abs(r64.iterations - o.iterations) <= 200 and abs(r64.restarts - o.restarts) <= 2
+    assert abs(r64.objective - o.objective) <= 1e-4 * abs(o.objective)
+    r = solve(pkg, engine, p, precision="mixed", **kw)
+    assert r.status == "optimal", (r.status, r.relative_kkt, r.iterations)
+    assert r.relative_kkt < 1e-4
+    assert abs(r.objective - o.objective) <= 2e-3 * abs(o.objective)
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_fp64_adaptive_and_primal_weight_follow_the_oracle(pkg, orc, engine, seed):
+    p = pkg.lpgen.random_equality_lp(200, 500, 5, seed=seed)
+    for pw in (0, 1):
+        o = orc.oracle_solve(p, termination_rule=1, restart_rule=1, primal_weight_update=pw,
+                             max_iterations=100_000)
+        r = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt",
+                  restart_rule="adaptive", primal_weight_update=bool(pw), max_iterations=100_000)
+        assert r.status == o.status == "optimal"
+        assert r.restarts == o.restarts and r.iterations == o.iterations, (r.iterations, o.iterations)
+        assert abs(r.objective - o.objective) <= 1e-8 * abs(o.objective)
+
+
+def test_exact_mode_rejects_the_extensions(pkg, engine):
+    p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=1)
+    with pytest.raises(pkg.PdhgError):
+        solve(pkg, engine, p, restart_rule="adaptive")
+
+
+def test_warm_start_from_the_solution_converges_immediately(pkg, engine):
+    p = pkg.lpgen.random_equality_lp(60, 150, 4, seed=30)
+    cold = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt",
+                 max_iterations=200_000)
+    assert cold.status == "optimal"
+    warm = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt",
+                 max_iterations=200_000, x0=cold.primal, y0=cold.dual)
+    assert warm.status == "optimal"
+    assert warm.iterations < cold.iterations

@@ -1,0 +1,92 @@
+"""Pins the oracle (plain-C restatement) to the reference itself.
+
+oracle/_ref/libsovref.so is the reference's own PDHG path compiled from its
+sources (oracle/Makefile). On identical inputs the restatement must reproduce
+it bit for bit: iterates, restarts, statuses, every result field.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_problem, load_golden
+
+pytestmark = pytest.mark.filterwarnings("ignore")
+
+
+def _ref_or_skip(orc):
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+
+
+def _same(a, b):
+    assert a.status == b.status, (a.status, b.status, a.message, b.message)
+    assert a.message == b.message
+    assert a.iterations == b.iterations
+    assert a.restarts == b.restarts
+    for f in ("objective", "primal_infeasibility", "dual_infeasibility", "duality_gap",
+              "operator_norm_estimate"):
+        va, vb = getattr(a, f), getattr(b, f)
+        assert va == vb or (np.isnan(va) and np.isnan(vb)), (f, va, vb)
+    for f in ("primal", "dual", "reduced_costs"):
+        va, vb = getattr(a, f), getattr(b, f)
+        assert (va is None) == (vb is None)
+        if va is not None:
+            assert np.array_equal(va, vb), f
+
+
+@pytest.mark.parametrize("seed,maximize", [(1, False), (2, True), (3, False)])
+def test_oracle_is_the_reference_on_random_lps(pkg, orc, seed, maximize):
+    _ref_or_skip(orc)
+    p = pkg.lpgen.random_equality_lp(40, 90, 4, seed=seed, maximize=maximize)
+    kw = dict(max_iterations=4000, trace_iters=30)
+    a, b = orc.oracle_solve(p, **kw), orc.reference_solve(p, **kw)
+    _same(a, b)
+    assert np.array_equal(a.trace_x, b.trace_x) and np.array_equal(a.trace_y, b.trace_y)
+
+
+def test_oracle_is_the_reference_with_restarts_and_every_bound_type(pkg, orc):
+    _ref_or_skip(orc)
+    g = load_golden("mixed_bounds_50x90")
+    p = golden_problem(pkg, g)
+    for kw in (dict(max_iterations=3000), dict(max_iterations=2000, restart_check_period=3,
+                                                restart_sufficient_decrease=0.9)):
+        _same(orc.oracle_solve(p, **kw), orc.reference_solve(p, **kw))
+
+
+def test_checkpoints_match(pkg, orc):
+    _ref_or_skip(orc)
+    p = pkg.lpgen.random_equality_lp(30, 70, 3, seed=5)
+    a = orc.oracle_solve(p, max_iterations=400, restart_check_period=50, checkpoints=True)
+    b = orc.reference_solve(p, max_iterations=400, restart_check_period=50, checkpoints=True)
+    assert [c[0] for c in a.checkpoints] == [c[0] for c in b.checkpoints] == list(range(49, 400, 50))
+    for ca, cb in zip(a.checkpoints, b.checkpoints):
+        assert np.array_equal(ca[1], cb[1]) and np.array_equal(ca[2], cb[2]) and ca[3] == cb[3]
+
+
+def test_time_limit_and_invalid_input_match(pkg, orc):
+    _ref_or_skip(orc)
+    p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=6)
+    _same(orc.oracle_solve(p, time_limit_seconds=1e-9), orc.reference_solve(p, time_limit_seconds=1e-9))
+    bad = pkg.lpgen.random_equality_lp(20, 50, 3, seed=6)
+    bad.col_lo[7] = 11.0  # crossed: lo > hi = 10
+    _same(orc.oracle_solve(bad), orc.reference_solve(bad))
+    bad2 = pkg.lpgen.random_equality_lp(20, 50, 3, seed=6)
+    bad2.c[3] = np.inf
+    _same(orc.oracle_solve(bad2), orc.reference_solve(bad2))
+    bad3 = pkg.lpgen.random_equality_lp(20, 50, 3, seed=6)
+    bad3.row_hi[2] = np.nan
+    _same(orc.oracle_solve(bad3), orc.reference_solve(bad3))
+
+
+def test_scaling_and_spmv_match(pkg, orc):
+    _ref_or_skip(orc)
+    p = pkg.lpgen.badly_scaled_lp(300, 700, 5, seed=9)
+    for kw in ({}, {"apply_ruiz": 0}, {"apply_pock_chambolle": 0}, {"ruiz_iterations": 3}):
+        ra, ca = orc.oracle_scaling(p, **kw)
+        rb, cb = orc.reference_scaling(p, **kw)
+        assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
+    x = np.random.default_rng(0).standard_normal(p.n)
+    y = np.random.default_rng(1).standard_normal(p.m)
+    assert np.array_equal(orc.oracle_spmv(p, -1.0, x, 0.0, np.zeros(p.m)),
+                          orc.reference_spmv(p, -1.0, x, 0.0, np.zeros(p.m)))
+    assert np.array_equal(orc.oracle_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True),
+                          orc.reference_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True))
