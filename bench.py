@@ -217,6 +217,21 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def profile_case(args) -> None:
+    """One solve on a transportation LP of the given size: the ncu target."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg = importlib.import_module("sovereign-solver_b200")
+    prob = pkg.lpgen.transportation_lp(args.supplies, args.demands, seed=1000)
+    with pkg.Engine(0) as eng:
+        eng.load(prob)
+        r = eng.solve(pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
+                                      restart_rule="adaptive", tolerance=1e-12,
+                                      max_iterations=args.iters_per_step), want_point=False)
+    print(json.dumps({"profile_case": f"transportation {args.supplies}x{args.demands}",
+                      "iterations": r.iterations, "status": r.status}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,7 +243,15 @@ def main() -> None:
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--full-solve-cap", type=int, default=60_000)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="profiler target: load the LP and run one solve of --iters-per-step "
+                         "iterations, nothing else")
+    ap.add_argument("--supplies", type=int, default=SUPPLIES)
+    ap.add_argument("--demands", type=int, default=DEMANDS)
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

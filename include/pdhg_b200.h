@@ -185,11 +185,16 @@ int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
                   double alpha, const double* x, double beta, double* y);
 int pdhg_project_box(int device, int32_t n, const double* lo, const double* hi, double* x);
 
-/* Scaling::equilibrate(CsrMatrix) (src/l1/scaling.cpp:19-104) as the engine
- * computes it (host FP64, reference order). */
+/* Scaling::equilibrate(CsrMatrix) (src/l1/scaling.cpp:19-104) on the host
+ * (FP64, the reference's order), for callers without a device. */
 int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
                  const int32_t* col_idx, const double* values, const pdhg_options* options,
                  double* row_scale, double* col_scale);
+
+/* The row / column factors the engine computed on the device for the loaded
+ * problem (Scaling::row_scale / col_scale, scaling.hpp:332-333), bit-identical
+ * to pdhg_scaling's. Host buffers of m and n doubles. */
+int pdhg_get_scaling(pdhg_ctx* ctx, double* row_scale, double* col_scale);
 
 #ifdef __cplusplus
 }

@@ -101,6 +101,7 @@ struct GraphSig {
 
 struct Ctx {
     int device = 0;
+    int sm_count = 148;
     cudaStream_t stream = nullptr;
     std::string err;
     long long gen = 0;  // bumps on every load / rescale
@@ -110,8 +111,7 @@ struct Ctx {
     HostLp lp;
     ScalingParams sp;
     bool scaled = false;
-    std::vector<double> rs, cs;
-    double bnorm = 0, cnorm = 0;        // relative-KKT norms, original space (inf-norms)
+    double bnorm = 0, cnorm = 0;       // relative-KKT norms, original space (inf-norms)
     double cnorm2_s = 0, bnorm2_s = 0;  // initial primal weight |c|_2 / |b|_2, scaled space
 
     MatDev Ao, ATo, As, ATs;
@@ -209,77 +209,156 @@ cudaError_t to_float(DBuf<float>& d, const DBuf<double>& src, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// CSR + transpose on the device, with row binning of both.
-int upload_matrix(Ctx& c, const HostCsr& A, MatDev& M, MatDev& MT, bool want_f32) {
+// Row binning on the device: long-row list, short-row count, lanes per short
+// row (about half the mean short-row length, a power of two in [1, 32]).
+int bin_matrix(Ctx& c, MatDev& M) {
     cudaStream_t s = c.stream;
-    M.rows = A.rows;
-    M.cols = A.cols;
-    M.nnz = A.nnz();
-    CK(upload(M.rp, A.rp, s));
-    CK(upload(M.ci, A.ci, s));
-    CK(upload(M.v64, A.v, s));
-    MT.rows = A.cols;
-    MT.cols = A.rows;
-    MT.nnz = A.nnz();
-    CK(MT.rp.alloc(static_cast<size_t>(A.cols) + 1));
-    CK(MT.ci.alloc(static_cast<size_t>(A.nnz())));
-    CK(MT.v64.alloc(static_cast<size_t>(A.nnz())));
-    TransposeOut out{MT.rp.p, MT.ci.p, MT.v64.p};
-    if (build_transpose(A.rows, A.cols, A.nnz(), M.rp.p, M.ci.p, M.v64.p, out, s) != 0)
-        return fail(c, cudaGetLastError(), "build_transpose");
-    if (want_f32) {
-        CK(to_float(M.v32, M.v64, s));
-        CK(to_float(MT.v32, MT.v64, s));
-    }
-    // binning (host): A from its row pointer, A^T from column counts
-    std::vector<int32_t> lr;
-    bin_rows(A.rp, kLongRow, &lr, &M.n_short, &M.vw);
-    M.n_long = static_cast<int32_t>(lr.size());
-    CK(upload(M.long_rows, lr, s));
-    std::vector<int32_t> trp(static_cast<size_t>(A.cols) + 1, 0);
-    for (int32_t j : A.ci) ++trp[static_cast<size_t>(j) + 1];
-    for (int32_t j = 0; j < A.cols; ++j) trp[j + 1] += trp[j];
-    bin_rows(trp, kLongRow, &lr, &MT.n_short, &MT.vw);
-    MT.n_long = static_cast<int32_t>(lr.size());
-    CK(upload(MT.long_rows, lr, s));
+    CK(M.long_rows.alloc(static_cast<size_t>(M.rows) + 1));
+    DBuf<unsigned long long> cnt;
+    CK(cnt.alloc(3));
+    CK(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), s));
+    launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
+    unsigned long long h[3];
+    CK(cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    M.n_long = static_cast<int32_t>(h[0]);
+    M.n_short = static_cast<int32_t>(h[1]);
+    const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
+    int w = 1;
+    while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;
+    M.vw = w;
     return PDHG_OK;
 }
 
+// A from host arrays (the caller's, read in place) and A^T built on the device.
+int upload_matrix(Ctx& c, int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,
+                  const int32_t* ci, const double* v, MatDev& M, MatDev& MT) {
+    cudaStream_t s = c.stream;
+    M.rows = rows;
+    M.cols = cols;
+    M.nnz = nnz;
+    CK(upload(M.rp, rp, static_cast<size_t>(rows) + 1, s));
+    CK(upload(M.ci, ci, static_cast<size_t>(nnz), s));
+    CK(upload(M.v64, v, static_cast<size_t>(nnz), s));
+    MT.rows = cols;
+    MT.cols = rows;
+    MT.nnz = nnz;
+    CK(MT.rp.alloc(static_cast<size_t>(cols) + 1));
+    CK(MT.ci.alloc(static_cast<size_t>(nnz)));
+    CK(MT.v64.alloc(static_cast<size_t>(nnz)));
+    TransposeOut out{MT.rp.p, MT.ci.p, MT.v64.p};
+    if (build_transpose(rows, cols, nnz, M.rp.p, M.ci.p, M.v64.p, out, s) != 0)
+        return fail(c, cudaGetLastError(), "build_transpose");
+    int rc = bin_matrix(c, M);
+    if (rc != PDHG_OK) return rc;
+    return bin_matrix(c, MT);
+}
+
+template <class T>
+cudaError_t copy_dev(DBuf<T>& d, const T* src, size_t n, cudaStream_t s) {
+    cudaError_t e = d.alloc(n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(d.p, src, sizeof(T) * n, cudaMemcpyDeviceToDevice, s);
+}
+
+// Scaling::equilibrate(Problem) (scaling.cpp:155-205) on the device, from the
+// original A / A^T already resident: factors, scaled matrices, scaled vectors.
 int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     if (c.scaled && c.sp == sp) return PDHG_OK;
     cudaStream_t s = c.stream;
+    const int32_t m = c.lp.m, n = c.lp.n;
+    const int64_t nnz = c.Ao.nnz;
     c.sp = sp;
-    equilibrate(c.lp.A, sp, &c.rs, &c.cs);
-    HostLp sl;
-    build_scaled(c.lp, c.rs, c.cs, &sl);
-    const double sign = c.lp.maximize ? -1.0 : 1.0;
-    for (double& v : sl.c) v *= sign;  // pdhg.cpp:250-252
-    double cn = 0.0, bn = 0.0;
-    for (double v : sl.c) cn += v * v;
-    for (int32_t i = 0; i < sl.m; ++i) {
-        double b = 0.0;
-        if (std::isfinite(sl.row_lo[i])) b = std::fabs(sl.row_lo[i]);
-        if (std::isfinite(sl.row_hi[i])) b = std::max(b, std::fabs(sl.row_hi[i]));
-        bn += b * b;
+    CK(c.rs_d.alloc(static_cast<size_t>(m) + 1));
+    CK(c.cs_d.alloc(static_cast<size_t>(n) + 1));
+    launch_fill(c.rs_d.p, m, 1.0, s);
+    launch_fill(c.cs_d.p, n, 1.0, s);
+    DBuf<double> rbuf, cbuf;
+    CK(rbuf.alloc(static_cast<size_t>(m) + 1));
+    CK(cbuf.alloc(static_cast<size_t>(n) + 1));
+    DBuf<IntakeState> is;
+    CK(is.alloc(1));
+    CK(cudaMemsetAsync(is.p, 0, sizeof(IntakeState), s));
+    const DevCsr A = c.Ao.view(), AT = c.ATo.view();
+    if (sp.apply_ruiz)  // scaling.cpp:36-74
+        for (int sweep = 0; sweep < sp.ruiz_iterations; ++sweep)
+            launch_ruiz_sweep(A, AT, c.rs_d.p, c.cs_d.p, rbuf.p, cbuf.p, sp.ruiz_tolerance, is.p, s);
+    if (sp.apply_pock_chambolle)  // scaling.cpp:80-101
+        launch_pock_chambolle(A, AT, c.rs_d.p, c.cs_d.p, rbuf.p, cbuf.p, sp.pock_chambolle_alpha, s);
+    // scaled values of A and A^T; entries the reference's rebuild drops are counted
+    DBuf<unsigned long long> dropped;
+    CK(dropped.alloc(1));
+    CK(cudaMemsetAsync(dropped.p, 0, sizeof(unsigned long long), s));
+    CK(c.As.v64.alloc(static_cast<size_t>(nnz)));
+    launch_scale_values(A, 0, c.rs_d.p, c.cs_d.p, c.As.v64.p, dropped.p, s);
+    unsigned long long ndrop = 0;
+    CK(cudaMemcpyAsync(&ndrop, dropped.p, sizeof ndrop, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c.As.rows = m;
+    c.As.cols = n;
+    c.ATs.rows = n;
+    c.ATs.cols = m;
+    if (ndrop == 0) {
+        c.As.nnz = nnz;
+        c.ATs.nnz = nnz;
+        CK(copy_dev(c.As.rp, c.Ao.rp.p, static_cast<size_t>(m) + 1, s));
+        CK(copy_dev(c.As.ci, c.Ao.ci.p, static_cast<size_t>(nnz), s));
+        CK(copy_dev(c.ATs.rp, c.ATo.rp.p, static_cast<size_t>(n) + 1, s));
+        CK(copy_dev(c.ATs.ci, c.ATo.ci.p, static_cast<size_t>(nnz), s));
+        CK(c.ATs.v64.alloc(static_cast<size_t>(nnz)));
+        CK(cudaMemsetAsync(dropped.p, 0, sizeof(unsigned long long), s));
+        launch_scale_values(AT, 1, c.rs_d.p, c.cs_d.p, c.ATs.v64.p, dropped.p, s);
+    } else {
+        // compaction (sparse.cpp:55 drops |v| <= 1e-14), then a fresh transpose
+        DBuf<int32_t> kept;
+        CK(kept.alloc(static_cast<size_t>(m) + 1));
+        launch_kept_counts(A, c.As.v64.p, kept.p, s);
+        CK(c.As.rp.alloc(static_cast<size_t>(m) + 1));
+        if (prefix_rows(kept.p, m, c.As.rp.p, s) != 0) return fail(c, cudaGetLastError(), "prefix_rows");
+        const int64_t nk = static_cast<int64_t>(nnz - static_cast<int64_t>(ndrop));
+        DBuf<double> vk;
+        CK(c.As.ci.alloc(static_cast<size_t>(nk)));
+        CK(vk.alloc(static_cast<size_t>(nk)));
+        launch_compact(A, c.As.v64.p, c.As.rp.p, c.As.ci.p, vk.p, s);
+        CK(copy_dev(c.As.v64, vk.p, static_cast<size_t>(nk), s));
+        c.As.nnz = nk;
+        c.ATs.nnz = nk;
+        CK(c.ATs.rp.alloc(static_cast<size_t>(n) + 1));
+        CK(c.ATs.ci.alloc(static_cast<size_t>(nk)));
+        CK(c.ATs.v64.alloc(static_cast<size_t>(nk)));
+        TransposeOut out{c.ATs.rp.p, c.ATs.ci.p, c.ATs.v64.p};
+        if (build_transpose(m, n, nk, c.As.rp.p, c.As.ci.p, c.As.v64.p, out, s) != 0)
+            return fail(c, cudaGetLastError(), "build_transpose");
     }
-    c.cnorm2_s = std::sqrt(cn);
-    c.bnorm2_s = std::sqrt(bn);
-    int rc = upload_matrix(c, sl.A, c.As, c.ATs, true);
+    CK(to_float(c.As.v32, c.As.v64, s));
+    CK(to_float(c.ATs.v32, c.ATs.v64, s));
+    int rc = bin_matrix(c, c.As);
     if (rc != PDHG_OK) return rc;
-    CK(upload(c.c_s, sl.c, s));
-    CK(upload(c.lo_s, sl.col_lo, s));
-    CK(upload(c.hi_s, sl.col_hi, s));
-    CK(upload(c.rlo_s, sl.row_lo, s));
-    CK(upload(c.rhi_s, sl.row_hi, s));
-    CK(upload(c.rs_d, c.rs, s));
-    CK(upload(c.cs_d, c.cs, s));
+    rc = bin_matrix(c, c.ATs);
+    if (rc != PDHG_OK) return rc;
+    const double sign = c.lp.maximize ? -1.0 : 1.0;
+    CK(c.c_s.alloc(static_cast<size_t>(n) + 1));
+    CK(c.lo_s.alloc(static_cast<size_t>(n) + 1));
+    CK(c.hi_s.alloc(static_cast<size_t>(n) + 1));
+    CK(c.rlo_s.alloc(static_cast<size_t>(m) + 1));
+    CK(c.rhi_s.alloc(static_cast<size_t>(m) + 1));
+    launch_scale_vectors(m, n, c.rs_d.p, c.cs_d.p, c.c_o.p, c.lo_o.p, c.hi_o.p, c.rlo_o.p,
+                         c.rhi_o.p, sign, c.c_s.p, c.lo_s.p, c.hi_s.p, c.rlo_s.p, c.rhi_s.p, s);
     CK(to_float(c.c32, c.c_s, s));
     CK(to_float(c.lo32, c.lo_s, s));
     CK(to_float(c.hi32, c.hi_s, s));
     CK(to_float(c.rlo32, c.rlo_s, s));
     CK(to_float(c.rhi32, c.rhi_s, s));
+    DBuf<double> part;
+    CK(part.alloc(static_cast<size_t>(norms_part_size(m, n))));
+    launch_norms(m, n, c.c_s.p, c.rlo_s.p, c.rhi_s.p, c.c_o.p, c.rlo_o.p, c.rhi_o.p, part.p, is.p, s);
+    IntakeState h;
+    CK(cudaMemcpyAsync(&h, is.p, sizeof h, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    c.cnorm2_s = std::sqrt(h.norms[0]);
+    c.bnorm2_s = std::sqrt(h.norms[1]);
+    c.cnorm = h.norms[2];
+    c.bnorm = h.norms[3];
     c.scaled = true;
     c.have_opnorm = false;
     c.gen += 1;
@@ -452,12 +531,12 @@ Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candid
                               o.tolerance, bt, o.restart_sufficient_decrease,
                               o.restart_check_period, o.termination_rule,
                               want_candidate ? 1 : 0, c.st.p, c.mail_dev, o.restart_rule,
-                              o.primal_weight_update, c.x_last.p, c.y_last.p};
+                              o.primal_weight_update, c.x_last.p, c.y_last.p, 8 * c.sm_count};
     L.fc64 = FastCheck<double>{c.As.view(), c.ATs.view(), P, iterates<double>(c), cs,
                                o.tolerance, bt, o.restart_sufficient_decrease,
                                o.restart_check_period, o.termination_rule,
                                want_candidate ? 1 : 0, c.st.p, c.mail_dev, o.restart_rule,
-                               o.primal_weight_update, c.x_last.p, c.y_last.p};
+                               o.primal_weight_update, c.x_last.p, c.y_last.p, 8 * c.sm_count};
     return L;
 }
 
@@ -704,6 +783,13 @@ __global__ void k_widen(Iterates<float> a, Iterates<double> b, int32_t n, int32_
     }
 }
 
+// v <- v / scale (primal) or (v * sign) / scale (dual), in place.
+__global__ void k_to_scaled(double* v, const double* scale, double sign, int dual, int32_t n) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= n) return;
+    v[t] = dual ? (v[t] * sign) / scale[t] : v[t] / scale[t];
+}
+
 template <class T>
 __global__ void k_snapshot(Iterates<T> it, double* xl, double* yl, int32_t n, int32_t m) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
@@ -781,16 +867,18 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     const double sign = c.lp.maximize ? -1.0 : 1.0;
     const double* x0d = nullptr;
     const double* y0d = nullptr;
+    // x_s = x / col_scale, y_s = (y * obj_sign) / row_scale (inverse of
+    // unscale_to_original, pdhg.cpp:205-214)
     if (o.x0 != nullptr) {
-        std::vector<double> h(static_cast<size_t>(n));
-        for (int32_t j = 0; j < n; ++j) h[j] = o.x0[j] / c.cs[j];
-        CK(upload(c.x0s, h, c.stream));
+        CK(upload(c.x0s, o.x0, static_cast<size_t>(n), c.stream));
+        if (n > 0)
+            k_to_scaled<<<(n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.x0s.p, c.cs_d.p, 1.0, 0, n);
         x0d = c.x0s.p;
     }
     if (o.y0 != nullptr) {
-        std::vector<double> h(static_cast<size_t>(m));
-        for (int32_t i = 0; i < m; ++i) h[i] = o.y0[i] * sign / c.rs[i];
-        CK(upload(c.y0s, h, c.stream));
+        CK(upload(c.y0s, o.y0, static_cast<size_t>(m), c.stream));
+        if (m > 0)
+            k_to_scaled<<<(m + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.y0s.p, c.rs_d.p, sign, 1, m);
         y0d = c.y0s.p;
     }
     const DevProblem P = c.problem();
@@ -937,40 +1025,37 @@ int load(Ctx& c, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
     c.scaled = false;
     c.have_opnorm = false;
     c.gen += 1;
-    HostLp& lp = c.lp;
+    HostLp& lp = c.lp;  // scalars only: the arrays stay with the caller / on the device
     lp.m = m;
     lp.n = n;
     lp.obj_const = obj_const;
     lp.maximize = maximize != 0;
     lp.A.rows = m;
     lp.A.cols = n;
-    lp.A.rp.assign(row_ptr, row_ptr + m + 1);
-    lp.A.ci.assign(col_idx, col_idx + nnz);
-    lp.A.v.assign(values, values + nnz);
-    lp.c.assign(cv, cv + n);
-    lp.col_lo.assign(col_lo, col_lo + n);
-    lp.col_hi.assign(col_hi, col_hi + n);
-    lp.row_lo.assign(row_lo, row_lo + m);
-    lp.row_hi.assign(row_hi, row_hi + m);
+    LpView view;
+    view.m = m;
+    view.n = n;
+    view.nnz = nnz;
+    view.rp = row_ptr;
+    view.ci = col_idx;
+    view.v = values;
+    view.c = cv;
+    view.obj_const = obj_const;
+    view.col_lo = col_lo;
+    view.col_hi = col_hi;
+    view.row_lo = row_lo;
+    view.row_hi = row_hi;
     c.loaded = true;
-    c.valid = validate_lp(lp, &c.why);
+    c.valid = validate_lp(view, &c.why);
     if (!c.valid) return PDHG_OK;
-    int rc = upload_matrix(c, lp.A, c.Ao, c.ATo, false);
+    int rc = upload_matrix(c, m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo);
     if (rc != PDHG_OK) return rc;
     cudaStream_t s = c.stream;
-    CK(upload(c.c_o, lp.c, s));
-    CK(upload(c.lo_o, lp.col_lo, s));
-    CK(upload(c.hi_o, lp.col_hi, s));
-    CK(upload(c.rlo_o, lp.row_lo, s));
-    CK(upload(c.rhi_o, lp.row_hi, s));
-    c.bnorm = 0.0;
-    c.cnorm = 0.0;
-    for (int32_t i = 0; i < m; ++i) {
-        if (std::isfinite(lp.row_lo[i])) c.bnorm = std::max(c.bnorm, std::fabs(lp.row_lo[i]));
-        if (std::isfinite(lp.row_hi[i])) c.bnorm = std::max(c.bnorm, std::fabs(lp.row_hi[i]));
-    }
-    for (int32_t j = 0; j < n; ++j) c.cnorm = std::max(c.cnorm, std::fabs(lp.c[j]));
-    CK(cudaStreamSynchronize(s));
+    CK(upload(c.c_o, cv, static_cast<size_t>(n), s));
+    CK(upload(c.lo_o, col_lo, static_cast<size_t>(n), s));
+    CK(upload(c.hi_o, col_hi, static_cast<size_t>(n), s));
+    CK(upload(c.rlo_o, row_lo, static_cast<size_t>(m), s));
+    CK(upload(c.rhi_o, row_hi, static_cast<size_t>(m), s));
     return ensure_scaled(c, ScalingParams{});
 }
 
@@ -1127,6 +1212,8 @@ int pdhg_create(int device, pdhg_ctx** out) {
     pdhg::Ctx& c = h->c;
     c.device = device;
     if (cudaSetDevice(device) != cudaSuccess) return PDHG_ERR_BACKEND;
+    cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (c.sm_count <= 0) c.sm_count = 148;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
         return PDHG_ERR_BACKEND;
     void* mp = nullptr;
@@ -1155,6 +1242,24 @@ const char* pdhg_last_error(const pdhg_ctx* ctx) {
 
 void* pdhg_stream(const pdhg_ctx* ctx) {
     return ctx == nullptr ? nullptr : static_cast<void*>(ctx->c.stream);
+}
+
+int pdhg_get_scaling(pdhg_ctx* ctx, double* row_scale, double* col_scale) {
+    if (ctx == nullptr || row_scale == nullptr || col_scale == nullptr)
+        return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg::Ctx& c = ctx->c;
+    if (!c.loaded || !c.valid || !c.scaled) {
+        c.err = "pdhg_get_scaling: no valid problem loaded";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    if (cudaSetDevice(c.device) != cudaSuccess) return PDHG_ERR_BACKEND;
+    if (c.lp.m > 0 && cudaMemcpy(row_scale, c.rs_d.p, sizeof(double) * c.lp.m,
+                                 cudaMemcpyDeviceToHost) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    if (c.lp.n > 0 && cudaMemcpy(col_scale, c.cs_d.p, sizeof(double) * c.lp.n,
+                                 cudaMemcpyDeviceToHost) != cudaSuccess)
+        return PDHG_ERR_BACKEND;
+    return PDHG_OK;
 }
 
 int pdhg_load_problem(pdhg_ctx* ctx, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
@@ -1215,13 +1320,7 @@ int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
     if (rc != PDHG_OK) return rc;
     std::unique_ptr<pdhg_ctx> guard(h);
     pdhg::Ctx& c = h->c;
-    pdhg::HostCsr A;
-    A.rows = m;
-    A.cols = n;
-    A.rp.assign(row_ptr, row_ptr + m + 1);
-    A.ci.assign(col_idx, col_idx + nnz);
-    A.v.assign(values, values + nnz);
-    rc = pdhg::upload_matrix(c, A, c.Ao, c.ATo, false);
+    rc = pdhg::upload_matrix(c, m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo);
     if (rc != PDHG_OK) return rc;
     const int32_t nx = transpose ? m : n, ny = transpose ? n : m;
     pdhg::DBuf<double> dx, dy;

@@ -198,6 +198,7 @@ struct FastCheck {
     int primal_weight_update;  // omega <- sqrt(omega * |dy| / |dx|) at each restart
     double* x_last;            // scaled point of the last restart (n)
     double* y_last;            // (m)
+    int grid_cap;              // CTAs of the (grid-stride) check kernel: SMs x 8
 };
 template <class T>
 void launch_fast_check(const FastCheck<T>& a, cudaStream_t s);
@@ -262,5 +263,35 @@ int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const 
                     const double* v, TransposeOut out, cudaStream_t s);
 
 void launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
+
+// ---- intake (intake.cu) --------------------------------------------------------
+struct IntakeState {
+    unsigned long long worst;  // Ruiz: max |row/col max - 1| of the sweep (bit pattern)
+    unsigned int ticket;
+    int ruiz_done;             // set when a sweep's worst < tolerance (scaling.cpp:72)
+    double norms[4];           // |c_s|^2, |b_s|^2, max|c_o|, max finite |row bound|
+};
+void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
+                unsigned long long* counters, cudaStream_t s);
+void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
+                       double* row_max, double* col_max, double tol, IntakeState* is,
+                       cudaStream_t s);
+void launch_pock_chambolle(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
+                           double* row_sum, double* col_sum, double alpha, cudaStream_t s);
+void launch_scale_values(const DevCsr& M, int transposed, const double* rs, const double* cs,
+                         double* out, unsigned long long* dropped, cudaStream_t s);
+void launch_kept_counts(const DevCsr& M, const double* vs, int32_t* cnt, cudaStream_t s);
+void launch_compact(const DevCsr& M, const double* vs, const int32_t* new_rp, int32_t* ci_out,
+                    double* v_out, cudaStream_t s);
+void launch_scale_vectors(int32_t m, int32_t n, const double* rs, const double* cs,
+                          const double* c, const double* lo, const double* hi, const double* rlo,
+                          const double* rhi, double sign, double* c_s, double* lo_s,
+                          double* hi_s, double* rlo_s, double* rhi_s, cudaStream_t s);
+int norms_part_size(int32_t m, int32_t n);
+void launch_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
+                  const double* rhi_s, const double* c_o, const double* rlo_o,
+                  const double* rhi_o, double* part, IntakeState* is, cudaStream_t s);
+// Inclusive prefix sum of n int32 counts into out[1..n], out[0] = 0 (CUB).
+int prefix_rows(const int32_t* cnt, int32_t n, int32_t* out, cudaStream_t s);
 
 }  // namespace pdhg

@@ -21,7 +21,7 @@ std::string row_name(int32_t i) { return "R" + std::to_string(i); }
 
 }  // namespace
 
-bool validate_lp(const HostLp& lp, std::string* why) {
+bool validate_lp(const LpView& lp, std::string* why) {
     // Problem::validate (src/io/problem.cpp:50-), in its order.
     if (!std::isfinite(lp.obj_const)) {
         *why = "objective constant is not finite";
@@ -52,32 +52,35 @@ bool validate_lp(const HostLp& lp, std::string* why) {
         }
     }
     // CsrMatrix::validate (src/l0/sparse.cpp:94-128).
-    const HostCsr& A = lp.A;
-    if (A.rp[0] != 0) {
+    if (lp.rp[0] != 0) {
         *why = "row_ptr does not start at 0";
         return false;
     }
-    if (A.rp[A.rows] != A.nnz()) {
+    if (lp.rp[lp.m] != lp.nnz) {
         *why = "row_ptr does not end at nnz";
         return false;
     }
-    for (int32_t r = 0; r < A.rows; ++r) {
-        const int32_t b = A.rp[r], e = A.rp[r + 1];
+    for (int32_t r = 0; r < lp.m; ++r) {
+        const int32_t b = lp.rp[r], e = lp.rp[r + 1];
         if (b > e) {
             *why = "row_ptr is not monotone";
             return false;
         }
+        if (b < 0 || e > lp.nnz) {  // guards the reads below for any row_ptr
+            *why = "row_ptr is not monotone";
+            return false;
+        }
         for (int32_t k = b; k < e; ++k) {
-            const int32_t c = A.ci[k];
-            if (c < 0 || c >= A.cols) {
+            const int32_t c = lp.ci[k];
+            if (c < 0 || c >= lp.n) {
                 *why = "column index out of range";
                 return false;
             }
-            if (k > b && A.ci[k - 1] >= c) {
+            if (k > b && lp.ci[k - 1] >= c) {
                 *why = "column indices not strictly ascending";
                 return false;
             }
-            if (!std::isfinite(A.v[k])) {
+            if (!std::isfinite(lp.v[k])) {
                 *why = "non-finite coefficient";
                 return false;
             }

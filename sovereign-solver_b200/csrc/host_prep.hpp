@@ -41,9 +41,21 @@ struct ScalingParams {
     }
 };
 
+// The caller's arrays, read in place (no copy).
+struct LpView {
+    int32_t m = 0, n = 0;
+    int64_t nnz = 0;
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const double* v = nullptr;
+    const double* c = nullptr;
+    double obj_const = 0.0;
+    const double *col_lo = nullptr, *col_hi = nullptr, *row_lo = nullptr, *row_hi = nullptr;
+};
+
 // True when the LP passes the reference's checks; otherwise `why` gets the
 // reference's message (rows/columns named R<i>/C<j>).
-bool validate_lp(const HostLp& lp, std::string* why);
+bool validate_lp(const LpView& lp, std::string* why);
 
 // Scaling::equilibrate(CsrMatrix): row_scale (rows), col_scale (cols).
 void equilibrate(const HostCsr& A, const ScalingParams& p, std::vector<double>* rs,

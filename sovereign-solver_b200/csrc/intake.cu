@@ -1,0 +1,296 @@
+// intake.cu -- problem intake on the device: row binning and Ruiz +
+// Pock-Chambolle scaling (Scaling::equilibrate, src/l1/scaling.cpp:19-104 and
+// :155-205) without a host pass over the matrix.
+//
+// The factors are bit-identical to the reference's host computation:
+//   * Ruiz row/column maxima of |a| * r_i * c_j are order-free (max), each
+//     product formed as (|a| * r_i) * c_j like scaling.cpp:48-50;
+//   * the update r_i /= sqrt(max) uses IEEE sqrt and division;
+//   * Pock-Chambolle sums are added by one thread per row (per A^T row for the
+//     columns) in the reference's order (CSR order for rows, ascending row for
+//     columns, scaling.cpp:85-96); with alpha = 1 the exponents are 1 and the
+//     term is the magnitude itself (pow(m, 1) == m exactly), other alphas call
+//     the device pow;
+//   * the early exit of the Ruiz sweeps (worst < tolerance) is decided by the
+//     last CTA of each update and read by the next sweep's kernels.
+#include <cmath>
+
+#include "engine.cuh"
+
+namespace pdhg {
+
+namespace {
+
+__host__ __device__ inline int nblocks(int64_t n) {
+    return static_cast<int>((n + kBlock - 1) / kBlock);
+}
+
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ bool fb(double v) { return v > -INFINITY && v < INFINITY; }
+__device__ __forceinline__ double safe_sqrt(double v) { return v > 0.0 ? sqrt(v) : 1.0; }
+
+__device__ __forceinline__ bool last_cta(unsigned int* ticket) {
+    __shared__ bool am_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    return am_last;
+}
+
+// Row lengths -> long-row list, number and total length of short rows.
+__global__ void k_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
+                      unsigned long long* counters) {
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= rows) return;
+    const int len = rp[r + 1] - rp[r];
+    if (len > long_threshold) {
+        const unsigned long long slot = atomicAdd(&counters[0], 1ull);
+        long_rows[slot] = r;
+    } else {
+        atomicAdd(&counters[1], 1ull);
+        atomicAdd(&counters[2], static_cast<unsigned long long>(len));
+    }
+}
+
+// Ruiz maxima of one orientation: out[row] = max_k |v| * rs[i] * cs[j] where
+// (i, j) is the entry's (row, column) of the ORIGINAL matrix (transposed: the
+// CSR row is j and its column index is i). One warp per row.
+__global__ void k_ruiz_max(DevCsr M, int transposed, const double* rs, const double* cs,
+                           const IntakeState* is, double* out) {
+    if (is->ruiz_done) return;
+    const int64_t warp = (blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= M.rows) return;
+    const int r = static_cast<int>(warp);
+    double mx = 0.0;
+    for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
+        const int c = M.ci[k];
+        const double s = transposed ? fabs(M.v64[k]) * rs[c] * cs[r]
+                                    : fabs(M.v64[k]) * rs[r] * cs[c];
+        mx = smax(mx, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) out[r] = mx;
+}
+
+__global__ void k_ruiz_update(int32_t m, int32_t n, double* rs, double* cs,
+                              const double* row_max, const double* col_max, double tol,
+                              IntakeState* is) {
+    if (is->ruiz_done) return;
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    double worst = 0.0;
+    if (t < m && row_max[t] > 0.0) {
+        rs[t] /= safe_sqrt(row_max[t]);
+        worst = fabs(row_max[t] - 1.0);
+    }
+    if (t < n && col_max[t] > 0.0) {
+        cs[t] /= safe_sqrt(col_max[t]);
+        worst = smax(worst, fabs(col_max[t] - 1.0));
+    }
+    for (int o = 16; o > 0; o >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    if ((threadIdx.x & 31) == 0 && worst > 0.0)
+        atomicMax(&is->worst, static_cast<unsigned long long>(__double_as_longlong(worst)));
+    if (!last_cta(&is->ticket) || threadIdx.x != 0) return;
+    const double w = __longlong_as_double(static_cast<long long>(
+        *reinterpret_cast<volatile unsigned long long*>(&is->worst)));
+    if (w < tol) is->ruiz_done = 1;  // scaling.cpp:72
+    is->worst = 0ull;
+    is->ticket = 0u;
+}
+
+__device__ __forceinline__ double pc_term(double mag, double e) {
+    return e == 1.0 ? mag : pow(mag, e);
+}
+
+// Pock-Chambolle sums, one thread per row, in the reference's order.
+__global__ void k_pc_sum(DevCsr M, int transposed, const double* rs, const double* cs,
+                         double expo, double* out) {
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= M.rows) return;
+    double sum = 0.0;
+    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) {
+        const int c = M.ci[k];
+        const double mag = transposed ? fabs(M.v64[k]) * rs[c] * cs[r]
+                                      : fabs(M.v64[k]) * rs[r] * cs[c];
+        if (mag <= 0.0) continue;
+        sum = __dadd_rn(sum, pc_term(mag, expo));
+    }
+    out[r] = sum;
+}
+
+__global__ void k_pc_update(int32_t m, int32_t n, double* rs, double* cs, const double* row_sum,
+                            const double* col_sum) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t < m && row_sum[t] > 0.0) rs[t] /= safe_sqrt(row_sum[t]);
+    if (t < n && col_sum[t] > 0.0) cs[t] /= safe_sqrt(col_sum[t]);
+}
+
+// Scaled values (v * rs_i) * cs_j (Scaling::apply, scaling.cpp:127-128);
+// counts entries the rebuild would drop (|v| <= 1e-14, sparse.cpp:55).
+__global__ void k_scale_values(DevCsr M, int transposed, const double* rs, const double* cs,
+                               double* out, unsigned long long* dropped) {
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= M.rows) return;
+    unsigned long long d = 0;
+    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) {
+        const int c = M.ci[k];
+        const double v = transposed ? M.v64[k] * rs[c] * cs[r] : M.v64[k] * rs[r] * cs[c];
+        out[k] = v;
+        d += fabs(v) <= 1e-14 ? 1ull : 0ull;
+    }
+    if (d) atomicAdd(dropped, d);
+}
+
+// Kept-entry counts per row (the compaction path when entries are dropped).
+__global__ void k_kept_counts(DevCsr M, const double* vs, int32_t* cnt) {
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= M.rows) return;
+    int c = 0;
+    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) c += fabs(vs[k]) <= 1e-14 ? 0 : 1;
+    cnt[r] = c;
+}
+
+__global__ void k_compact(DevCsr M, const double* vs, const int32_t* new_rp, int32_t* ci_out,
+                          double* v_out) {
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= M.rows) return;
+    int o = new_rp[r];
+    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) {
+        if (fabs(vs[k]) <= 1e-14) continue;
+        ci_out[o] = M.ci[k];
+        v_out[o] = vs[k];
+        ++o;
+    }
+}
+
+// Scaled problem vectors (scaling.cpp:172-192, then c *= obj_sign, pdhg.cpp:250-252).
+__global__ void k_scale_vectors(int32_t m, int32_t n, const double* rs, const double* cs,
+                                const double* c, const double* lo, const double* hi,
+                                const double* rlo, const double* rhi, double sign, double* c_s,
+                                double* lo_s, double* hi_s, double* rlo_s, double* rhi_s) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t < n) {
+        const double s = cs[t];
+        c_s[t] = (c[t] * s) * sign;
+        lo_s[t] = fb(lo[t]) ? lo[t] / s : lo[t];
+        hi_s[t] = fb(hi[t]) ? hi[t] / s : hi[t];
+    }
+    if (t < m) {
+        const double s = rs[t];
+        rlo_s[t] = fb(rlo[t]) ? rlo[t] * s : rlo[t];
+        rhi_s[t] = fb(rhi[t]) ? rhi[t] * s : rhi[t];
+    }
+}
+
+// Norms: [0] |c_s|_2^2, [1] |b_s|_2^2 (b_i = largest finite |scaled row bound|),
+// [2] max |c_o|, [3] max finite |row bound|, original. Block partials + last CTA.
+__global__ void k_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
+                        const double* rhi_s, const double* c_o, const double* rlo_o,
+                        const double* rhi_o, double* part, IntakeState* is) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    if (t < n) {
+        q[0] = c_s[t] * c_s[t];
+        q[2] = fabs(c_o[t]);
+    }
+    if (t < m) {
+        double b = 0.0;
+        if (fb(rlo_s[t])) b = fabs(rlo_s[t]);
+        if (fb(rhi_s[t])) b = smax(b, fabs(rhi_s[t]));
+        q[1] = b * b;
+        double bo = 0.0;
+        if (fb(rlo_o[t])) bo = fabs(rlo_o[t]);
+        if (fb(rhi_o[t])) bo = smax(bo, fabs(rhi_o[t]));
+        q[3] = bo;
+    }
+    __shared__ double sh[4][kBlock];
+    for (int i = 0; i < 4; ++i) sh[i][threadIdx.x] = q[i];
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
+            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 4; ++i) part[4 * blockIdx.x + i] = sh[i][0];
+    if (!last_cta(&is->ticket) || threadIdx.x != 0) return;
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    const volatile double* p = part;
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+        r[0] += p[4 * b];
+        r[1] += p[4 * b + 1];
+        r[2] = fmax(r[2], p[4 * b + 2]);
+        r[3] = fmax(r[3], p[4 * b + 3]);
+    }
+    for (int i = 0; i < 4; ++i) is->norms[i] = r[i];
+    is->ticket = 0u;
+}
+
+}  // namespace
+
+void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
+                unsigned long long* counters, cudaStream_t s) {
+    if (rows > 0) k_bin<<<nblocks(rows), kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+}
+
+void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
+                       double* row_max, double* col_max, double tol, IntakeState* is,
+                       cudaStream_t s) {
+    if (A.rows > 0)
+        k_ruiz_max<<<nblocks(static_cast<int64_t>(A.rows) * 32), kBlock, 0, s>>>(A, 0, rs, cs, is, row_max);
+    if (AT.rows > 0)
+        k_ruiz_max<<<nblocks(static_cast<int64_t>(AT.rows) * 32), kBlock, 0, s>>>(AT, 1, rs, cs, is, col_max);
+    const int32_t nmax = A.rows > AT.rows ? A.rows : AT.rows;
+    k_ruiz_update<<<nmax > 0 ? nblocks(nmax) : 1, kBlock, 0, s>>>(A.rows, AT.rows, rs, cs,
+                                                                 row_max, col_max, tol, is);
+}
+
+void launch_pock_chambolle(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
+                           double* row_sum, double* col_sum, double alpha, cudaStream_t s) {
+    // both sums from the factors before this step (scaling.cpp:85-96), then the update
+    if (A.rows > 0) k_pc_sum<<<nblocks(A.rows), kBlock, 0, s>>>(A, 0, rs, cs, 2.0 - alpha, row_sum);
+    if (AT.rows > 0) k_pc_sum<<<nblocks(AT.rows), kBlock, 0, s>>>(AT, 1, rs, cs, alpha, col_sum);
+    const int32_t nmax = A.rows > AT.rows ? A.rows : AT.rows;
+    if (nmax > 0) k_pc_update<<<nblocks(nmax), kBlock, 0, s>>>(A.rows, AT.rows, rs, cs, row_sum, col_sum);
+}
+
+void launch_scale_values(const DevCsr& M, int transposed, const double* rs, const double* cs,
+                         double* out, unsigned long long* dropped, cudaStream_t s) {
+    if (M.rows > 0) k_scale_values<<<nblocks(M.rows), kBlock, 0, s>>>(M, transposed, rs, cs, out, dropped);
+}
+
+void launch_kept_counts(const DevCsr& M, const double* vs, int32_t* cnt, cudaStream_t s) {
+    if (M.rows > 0) k_kept_counts<<<nblocks(M.rows), kBlock, 0, s>>>(M, vs, cnt);
+}
+
+void launch_compact(const DevCsr& M, const double* vs, const int32_t* new_rp, int32_t* ci_out,
+                    double* v_out, cudaStream_t s) {
+    if (M.rows > 0) k_compact<<<nblocks(M.rows), kBlock, 0, s>>>(M, vs, new_rp, ci_out, v_out);
+}
+
+void launch_scale_vectors(int32_t m, int32_t n, const double* rs, const double* cs,
+                          const double* c, const double* lo, const double* hi, const double* rlo,
+                          const double* rhi, double sign, double* c_s, double* lo_s,
+                          double* hi_s, double* rlo_s, double* rhi_s, cudaStream_t s) {
+    const int32_t nmax = m > n ? m : n;
+    if (nmax > 0)
+        k_scale_vectors<<<nblocks(nmax), kBlock, 0, s>>>(m, n, rs, cs, c, lo, hi, rlo, rhi, sign,
+                                                         c_s, lo_s, hi_s, rlo_s, rhi_s);
+}
+
+int norms_part_size(int32_t m, int32_t n) { return 4 * (nblocks(m > n ? m : n) + 1); }
+
+void launch_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
+                  const double* rhi_s, const double* c_o, const double* rlo_o,
+                  const double* rhi_o, double* part, IntakeState* is, cudaStream_t s) {
+    const int32_t nmax = m > n ? m : n;
+    k_norms<<<nmax > 0 ? nblocks(nmax) : 1, kBlock, 0, s>>>(m, n, c_s, rlo_s, rhi_s, c_o, rlo_o,
+                                                           rhi_o, part, is);
+}
+
+}  // namespace pdhg

@@ -833,6 +833,18 @@ void launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s) {
     if (n > 0) k_to_float<<<grid64(n), kBlock, 0, s>>>(src, dst, n);
 }
 
+int prefix_rows(const int32_t* cnt, int32_t n, int32_t* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(int32_t), s);
+    if (n <= 0) return static_cast<int>(cudaGetLastError() != cudaSuccess);
+    size_t bytes = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, bytes, cnt, out + 1, n, s);
+    void* tmp = nullptr;
+    if (cudaMallocAsync(&tmp, bytes + 16, s) != cudaSuccess) return 1;
+    cub::DeviceScan::InclusiveSum(tmp, bytes, cnt, out + 1, n, s);
+    cudaFreeAsync(tmp, s);
+    return static_cast<int>(cudaGetLastError() != cudaSuccess);
+}
+
 int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci,
                     const double* v, TransposeOut out, cudaStream_t s) {
     cudaError_t err = cudaSuccess;

@@ -113,12 +113,6 @@ __device__ double block_sum_det(double v) {
     return r;
 }
 
-__device__ __forceinline__ void block_acc_max(unsigned long long* slot, double v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0 && v > 0.0)
-        atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(v)));
-}
-
 __device__ __forceinline__ double acc_read(unsigned long long* slot) {
     return __longlong_as_double(
         static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(slot)));
@@ -134,7 +128,9 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
 }
 
 // Long-row dot product: 128-bit loads of values and column indices on the
-// aligned body, scalar head and tail. Gathers go through the read-only path.
+// aligned body, scalar head and tail. The matrix is streamed (evict-first,
+// ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go
+// through the read-only path.
 template <class T>
 __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
                                           const T* __restrict__ v, const T* __restrict__ xg,
@@ -143,14 +139,14 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
     int bA = ((b + W - 1) / W) * W;
     if (bA > e) bA = e;
     T acc = T(0);
-    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldg(v + k) * __ldg(xg + __ldg(ci + k));
+    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
     const int nvec = (e - bA) / W;
     if constexpr (W == 4) {
         const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
         const float4* v4 = reinterpret_cast<const float4*>(v + bA);
         for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const int4 c = __ldg(ci4 + q);
-            const float4 w = __ldg(v4 + q);
+            const int4 c = __ldcs(ci4 + q);
+            const float4 w = __ldcs(v4 + q);
             acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
                    w.w * __ldg(xg + c.w);
         }
@@ -158,13 +154,13 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
         const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
         const double2* v2 = reinterpret_cast<const double2*>(v + bA);
         for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const int2 c = __ldg(ci2 + q);
-            const double2 w = __ldg(v2 + q);
+            const int2 c = __ldcs(ci2 + q);
+            const double2 w = __ldcs(v2 + q);
             acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
         }
     }
     for (int k = bA + nvec * W + threadIdx.x; k < e; k += kBlock)
-        acc += __ldg(v + k) * __ldg(xg + __ldg(ci + k));
+        acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
     return block_total(acc);
 }
 
@@ -172,18 +168,21 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
 // Iteration kernels
 // ---------------------------------------------------------------------------
 
+// Epilogue traffic: every per-column array is streamed (evict-first loads and
+// stores) except x_bar, whose lines the dual kernel gathers next and should
+// find in L2; y likewise stays at normal priority for the next primal gather.
 template <class T>
 __device__ __forceinline__ void primal_epilogue(const FastIter<T>& a, const PV<T>& pv, int j,
                                                 T aty, int first, bool fresh, T tau) {
-    const T g = pv.c[j] - aty;
-    const T xo = a.it.x[j];
-    const T xn = clampT<T>(xo - tau * g, pv.lo[j], pv.hi[j]);
+    const T g = __ldcs(pv.c + j) - aty;
+    const T xo = __ldcs(a.it.x + j);
+    const T xn = clampT<T>(xo - tau * g, __ldcs(pv.lo + j), __ldcs(pv.hi + j));
     a.it.xbar[j] = T(2) * xn - xo;
-    a.it.x[j] = xn;
+    __stcs(a.it.x + j, xn);
     if constexpr (std::is_same<T, float>::value) {
-        a.it.psx[j] = first ? xn : a.it.psx[j] + xn;
+        __stcs(a.it.psx + j, first ? xn : __ldcs(a.it.psx + j) + xn);
     } else {
-        a.it.xsum[j] = fresh ? xn : a.it.xsum[j] + xn;
+        __stcs(a.it.xsum + j, fresh ? xn : __ldcs(a.it.xsum + j) + xn);
     }
 }
 
@@ -191,16 +190,16 @@ template <class T>
 __device__ __forceinline__ void dual_epilogue(const FastIter<T>& a, const PV<T>& pv, int i,
                                               T ax, int first, bool fresh, T tau, T sigma) {
     const T yo = a.it.y[i];
-    const T so = a.it.s[i];
-    const T sn = clampT<T>(so - tau * yo, pv.rlo[i], pv.rhi[i]);
+    const T so = __ldcs(a.it.s + i);
+    const T sn = clampT<T>(so - tau * yo, __ldcs(pv.rlo + i), __ldcs(pv.rhi + i));
     const T sbar = T(2) * sn - so;
     const T yn = yo + sigma * (sbar - ax);
     a.it.y[i] = yn;
-    a.it.s[i] = sn;
+    __stcs(a.it.s + i, sn);
     if constexpr (std::is_same<T, float>::value) {
-        a.it.psy[i] = first ? yn : a.it.psy[i] + yn;
+        __stcs(a.it.psy + i, first ? yn : __ldcs(a.it.psy + i) + yn);
     } else {
-        a.it.ysum[i] = fresh ? yn : a.it.ysum[i] + yn;
+        __stcs(a.it.ysum + i, fresh ? yn : __ldcs(a.it.ysum + i) + yn);
     }
 }
 
@@ -223,10 +222,10 @@ __global__ void __launch_bounds__(kBlock) fast_iter(FastIter<T> a, int first, in
         const int lane = threadIdx.x & (VW - 1);
         const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
         if (r >= M.rows) return;
-        const int b = __ldg(M.rp + r), e = __ldg(M.rp + r + 1);
+        const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
         if (e - b > kLongRow) return;  // the row's CTA handles it
         T acc = T(0);
-        for (int k = b + lane; k < e; k += VW) acc += __ldg(vals + k) * __ldg(xg + __ldg(M.ci + k));
+        for (int k = b + lane; k < e; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
         if (VW > 1) acc = group_sum(acc, VW);
         if (lane == 0) {
             if (PRIMAL) primal_epilogue(a, pv, r, acc, first, fresh, tau);
@@ -312,6 +311,7 @@ __device__ __forceinline__ double avg_y(const Iterates<T>& it, int i, double inv
     return s * inv;
 }
 
+// Per-row terms, merged into the thread's running maxima / sums.
 template <class T>
 __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double act_c,
                                           double act_a, double inv, Terms& t) {
@@ -320,20 +320,20 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
     const double lo = P.rlo[i], hi = P.rhi[i];
     const double yc = static_cast<double>(a.it.y[i]);
     const double ya = avg_y(a.it, i, inv);
-    t.cp = primal_term(act_c, lo, hi);
-    t.ap = primal_term(act_a, lo, hi);
-    t.cd = cs_term(yc, act_c, lo, hi, a.tol);
-    t.ad = cs_term(ya, act_a, lo, hi, a.tol);
+    t.cp = smax(t.cp, primal_term(act_c, lo, hi));
+    t.ap = smax(t.ap, primal_term(act_a, lo, hi));
+    t.cd = smax(t.cd, cs_term(yc, act_c, lo, hi, a.tol));
+    t.ad = smax(t.ad, cs_term(ya, act_a, lo, hi, a.tol));
     const double rs = P.rs[i];
     const double lo_o = P.rlo_o[i], hi_o = P.rhi_o[i];
     const double aoc = act_c / rs, aoa = act_a / rs;
-    t.ocp = primal_term(aoc, lo_o, hi_o);
-    t.oap = primal_term(aoa, lo_o, hi_o);
-    t.ocd = cs_term(yc * rs, aoc, lo_o, hi_o, a.bound_tol);
-    t.oad = cs_term(ya * rs, aoa, lo_o, hi_o, a.bound_tol);
+    t.ocp = smax(t.ocp, primal_term(aoc, lo_o, hi_o));
+    t.oap = smax(t.oap, primal_term(aoa, lo_o, hi_o));
+    t.ocd = smax(t.ocd, cs_term(yc * rs, aoc, lo_o, hi_o, a.bound_tol));
+    t.oad = smax(t.oad, cs_term(ya * rs, aoa, lo_o, hi_o, a.bound_tol));
     if (a.termination_rule == 1) {  // internal (minimize) sense: y_int = y_s * rs
-        t.dobj_c = clipped_inf(yc * rs, lo_o, hi_o);
-        t.dobj_a = clipped_inf(ya * rs, lo_o, hi_o);
+        t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
+        t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
     }
 }
 
@@ -346,21 +346,47 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
     const double xc = static_cast<double>(a.it.x[j]);
     const double xa = avg_x(a.it, j, inv);
     const double rc = cj - aty_c, ra = cj - aty_a;
-    t.cd = cs_term(rc, xc, lo, hi, a.tol);
-    t.ad = cs_term(ra, xa, lo, hi, a.tol);
+    t.cd = smax(t.cd, cs_term(rc, xc, lo, hi, a.tol));
+    t.ad = smax(t.ad, cs_term(ra, xa, lo, hi, a.tol));
     const double cs = P.cs[j];
     const double lo_o = P.lo_o[j], hi_o = P.hi_o[j];
-    t.ocd = cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol);
-    t.oad = cs_term(ra / cs, xa * cs, lo_o, hi_o, a.bound_tol);
+    t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol));
+    t.oad = smax(t.oad, cs_term(ra / cs, xa * cs, lo_o, hi_o, a.bound_tol));
     if (a.termination_rule == 1) {  // internal sense: c_int x = sign c_o x, r_int = r_s / cs
-        t.pobj_c = P.obj_sign * P.c_o[j] * (xc * cs);
-        t.pobj_a = P.obj_sign * P.c_o[j] * (xa * cs);
-        t.dobj_c = clipped_inf(rc / cs, lo_o, hi_o);
-        t.dobj_a = clipped_inf(ra / cs, lo_o, hi_o);
+        t.pobj_c += P.obj_sign * P.c_o[j] * (xc * cs);
+        t.pobj_a += P.obj_sign * P.c_o[j] * (xa * cs);
+        t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
+        t.dobj_a += clipped_inf(ra / cs, lo_o, hi_o);
     }
 }
 
-// Grid: [row short | row long | col short | col long]
+// Block maxima of the 8 residual terms, one atomicMax per CTA and slot.
+__device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
+    __shared__ double sh[8][kBlock / 32];
+    double v[8] = {t.cp, t.cd, t.ap, t.ad, t.ocp, t.ocd, t.oap, t.oad};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sh[q][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double x = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) x = fmax(x, sh[threadIdx.x][w]);
+        // v[0..3] -> ACC_CUR_P..ACC_AVG_D, v[4..7] -> ACC_OC_P..ACC_OA_D
+        const int slot = threadIdx.x < 4 ? ACC_CUR_P + static_cast<int>(threadIdx.x)
+                                         : ACC_OC_P + static_cast<int>(threadIdx.x) - 4;
+        if (x > 0.0)
+            atomicMax(&acc[slot], static_cast<unsigned long long>(__double_as_longlong(x)));
+    }
+    __syncthreads();
+}
+
+// Grid-stride over virtual blocks [row short | row long | col short | col long];
+// the grid itself is capped (a few CTAs per SM), so each CTA sums its rows into
+// per-thread running terms and takes part in one reduction.
 template <class T>
 __global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_blocks, int cs_blocks) {
     DevState* st = a.st;
@@ -368,89 +394,83 @@ __global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_bloc
     const long long k_avg = st->since_restart + a.period_iters;
     const double inv = 1.0 / static_cast<double>(k_avg);
     Terms t;
-    const int b0 = rs_blocks, b1 = b0 + a.A.n_long, b2 = b1 + cs_blocks;
-    const int bid = blockIdx.x;
-    if (bid < b1) {
-        // rows of A: act = A x (current and average)
-        const DevCsr& M = a.A;
-        if (bid < b0) {
-            const int vw = M.vw;
-            const int lane = threadIdx.x & (vw - 1);
-            const int r = (bid * kBlock + threadIdx.x) / vw;
-            if (r < M.rows) {
-                const int b = M.rp[r], e = M.rp[r + 1];
-                if (e - b <= kLongRow) {
-                    double ac = 0.0, aa = 0.0;
-                    for (int k = b + lane; k < e; k += vw) {
-                        const int j = M.ci[k];
-                        const double v = M.v64[k];
-                        ac += v * static_cast<double>(a.it.x[j]);
-                        aa += v * avg_x(a.it, j, inv);
+    const int b0 = rs_blocks, b1 = b0 + a.A.n_long, b2 = b1 + cs_blocks, b3 = b2 + a.AT.n_long;
+    for (int bid = blockIdx.x; bid < b3; bid += gridDim.x) {
+        if (bid < b1) {
+            // rows of A: act = A x (current and average)
+            const DevCsr& M = a.A;
+            if (bid < b0) {
+                const int vw = M.vw;
+                const int lane = threadIdx.x & (vw - 1);
+                const int r = (bid * kBlock + threadIdx.x) / vw;
+                if (r < M.rows) {
+                    const int b = M.rp[r], e = M.rp[r + 1];
+                    if (e - b <= kLongRow) {
+                        double ac = 0.0, aa = 0.0;
+                        for (int k = b + lane; k < e; k += vw) {
+                            const int j = M.ci[k];
+                            const double v = M.v64[k];
+                            ac += v * static_cast<double>(a.it.x[j]);
+                            aa += v * avg_x(a.it, j, inv);
+                        }
+                        ac = group_sum(ac, vw);
+                        aa = group_sum(aa, vw);
+                        if (lane == 0) row_terms(a, r, ac, aa, inv, t);
                     }
-                    ac = group_sum(ac, vw);
-                    aa = group_sum(aa, vw);
-                    if (lane == 0) row_terms(a, r, ac, aa, inv, t);
                 }
+            } else {
+                const int r = M.long_rows[bid - b0];
+                const int b = M.rp[r], e = M.rp[r + 1];
+                double ac = 0.0, aa = 0.0;
+                for (int k = b + threadIdx.x; k < e; k += kBlock) {
+                    const int j = M.ci[k];
+                    const double v = M.v64[k];
+                    ac += v * static_cast<double>(a.it.x[j]);
+                    aa += v * avg_x(a.it, j, inv);
+                }
+                ac = block_total(ac);
+                aa = block_total(aa);
+                if (threadIdx.x == 0) row_terms(a, r, ac, aa, inv, t);
             }
         } else {
-            const int r = M.long_rows[bid - b0];
-            const int b = M.rp[r], e = M.rp[r + 1];
-            double ac = 0.0, aa = 0.0;
-            for (int k = b + threadIdx.x; k < e; k += kBlock) {
-                const int j = M.ci[k];
-                const double v = M.v64[k];
-                ac += v * static_cast<double>(a.it.x[j]);
-                aa += v * avg_x(a.it, j, inv);
-            }
-            ac = block_total(ac);
-            aa = block_total(aa);
-            if (threadIdx.x == 0) row_terms(a, r, ac, aa, inv, t);
-        }
-    } else {
-        // rows of A^T: aty = A^T y (current and average)
-        const DevCsr& M = a.AT;
-        if (bid < b2) {
-            const int vw = M.vw;
-            const int lane = threadIdx.x & (vw - 1);
-            const int r = ((bid - b1) * kBlock + threadIdx.x) / vw;
-            if (r < M.rows) {
-                const int b = M.rp[r], e = M.rp[r + 1];
-                if (e - b <= kLongRow) {
-                    double ac = 0.0, aa = 0.0;
-                    for (int k = b + lane; k < e; k += vw) {
-                        const int i = M.ci[k];
-                        const double v = M.v64[k];
-                        ac += v * static_cast<double>(a.it.y[i]);
-                        aa += v * avg_y(a.it, i, inv);
+            // rows of A^T: aty = A^T y (current and average)
+            const DevCsr& M = a.AT;
+            if (bid < b2) {
+                const int vw = M.vw;
+                const int lane = threadIdx.x & (vw - 1);
+                const int r = ((bid - b1) * kBlock + threadIdx.x) / vw;
+                if (r < M.rows) {
+                    const int b = M.rp[r], e = M.rp[r + 1];
+                    if (e - b <= kLongRow) {
+                        double ac = 0.0, aa = 0.0;
+                        for (int k = b + lane; k < e; k += vw) {
+                            const int i = M.ci[k];
+                            const double v = M.v64[k];
+                            ac += v * static_cast<double>(a.it.y[i]);
+                            aa += v * avg_y(a.it, i, inv);
+                        }
+                        ac = group_sum(ac, vw);
+                        aa = group_sum(aa, vw);
+                        if (lane == 0) col_terms(a, r, ac, aa, inv, t);
                     }
-                    ac = group_sum(ac, vw);
-                    aa = group_sum(aa, vw);
-                    if (lane == 0) col_terms(a, r, ac, aa, inv, t);
                 }
+            } else {
+                const int r = M.long_rows[bid - b2];
+                const int b = M.rp[r], e = M.rp[r + 1];
+                double ac = 0.0, aa = 0.0;
+                for (int k = b + threadIdx.x; k < e; k += kBlock) {
+                    const int i = M.ci[k];
+                    const double v = M.v64[k];
+                    ac += v * static_cast<double>(a.it.y[i]);
+                    aa += v * avg_y(a.it, i, inv);
+                }
+                ac = block_total(ac);
+                aa = block_total(aa);
+                if (threadIdx.x == 0) col_terms(a, r, ac, aa, inv, t);
             }
-        } else {
-            const int r = M.long_rows[bid - b2];
-            const int b = M.rp[r], e = M.rp[r + 1];
-            double ac = 0.0, aa = 0.0;
-            for (int k = b + threadIdx.x; k < e; k += kBlock) {
-                const int i = M.ci[k];
-                const double v = M.v64[k];
-                ac += v * static_cast<double>(a.it.y[i]);
-                aa += v * avg_y(a.it, i, inv);
-            }
-            ac = block_total(ac);
-            aa = block_total(aa);
-            if (threadIdx.x == 0) col_terms(a, r, ac, aa, inv, t);
         }
     }
-    block_acc_max(&st->acc[ACC_CUR_P], t.cp);
-    block_acc_max(&st->acc[ACC_CUR_D], t.cd);
-    block_acc_max(&st->acc[ACC_AVG_P], t.ap);
-    block_acc_max(&st->acc[ACC_AVG_D], t.ad);
-    block_acc_max(&st->acc[ACC_OC_P], t.ocp);
-    block_acc_max(&st->acc[ACC_OC_D], t.ocd);
-    block_acc_max(&st->acc[ACC_OA_P], t.oap);
-    block_acc_max(&st->acc[ACC_OA_D], t.oad);
+    block_max_terms(t, st->acc);
     if (a.termination_rule == 1) {
         const double s0 = block_sum_det(t.pobj_c);
         const double s1 = block_sum_det(t.dobj_c);
@@ -677,6 +697,7 @@ void launch_fast_check(const FastCheck<T>& a, cudaStream_t s) {
     const int rsb = short_blocks_for(a.A);
     const int csb = short_blocks_for(a.AT);
     int grid = rsb + a.A.n_long + csb + a.AT.n_long;
+    if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid == 0) grid = 1;
     fast_check<T><<<grid, kBlock, 0, s>>>(a, rsb, csb);
     if (a.want_candidate) {

@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
         L.pdhg_project_box.argtypes = [C.c_int, C.c_int32, _dp, _dp, _dp]
         L.pdhg_scaling.argtypes = [C.c_int32, C.c_int32, C.c_int64, _ip, _ip, _dp,
                                    C.POINTER(_Options), _dp, _dp]
+        L.pdhg_get_scaling.argtypes = [C.c_void_p, _dp, _dp]
         _lib = L
     return _lib
 
@@ -313,6 +314,14 @@ class Engine:
             r.trace_x = tx[:, : p.n]
             r.trace_y = ty[:, : p.m]
         return r
+
+    def scaling(self) -> tuple[np.ndarray, np.ndarray]:
+        """Row / column factors the engine computed on the device for the loaded LP."""
+        p = self.problem
+        rs = np.zeros(max(p.m, 1))
+        cs = np.zeros(max(p.n, 1))
+        _check(lib().pdhg_get_scaling(self._h, _d(rs), _d(cs)), "pdhg_get_scaling", self._h)
+        return rs[: p.m], cs[: p.n]
 
     def profile_kernels(self, precision: str = "mixed", warmup: int = 3,
                         iterations: int = 20) -> list[dict]:

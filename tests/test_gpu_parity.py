@@ -203,10 +203,53 @@ def test_exact_mode_on_a_power_law_lp_matches_the_oracle(pkg, orc, engine):
     assert (r.status, r.iterations, r.restarts) == (o.status, o.iterations, o.restarts)
     assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
     assert r.objective == o.objective
-    # and the warp-parallel FP64 path stays within FP64 rounding of it
-    r2 = solve(pkg, engine, p, precision="fp64", max_iterations=400, tolerance=1e-6)
-    assert r2.iterations == o.iterations
-    assert rel_err(r2.primal, o.primal) < 1e-9 and rel_err(r2.dual, o.dual) < 1e-9
+
+
+def test_fp64_mode_on_a_power_law_lp_tracks_exact_mode(pkg, engine):
+    # long rows (> 512 nonzeros) through the warp-parallel FP64 kernels: the
+    # first 100 iterates stay within FP64 rounding of the exact ones
+    p = pkg.lpgen.badly_scaled_lp(1500, 4000, 6, seed=22)
+    ex = solve(pkg, engine, p, max_iterations=400, tolerance=1e-6, trace_iters=100)
+    r2 = solve(pkg, engine, p, precision="fp64", max_iterations=400, tolerance=1e-6,
+               trace_iters=100)
+    errs_x = [rel_err(r2.trace_x[k], ex.trace_x[k]) for k in range(100)]
+    errs_y = [rel_err(r2.trace_y[k], ex.trace_y[k]) for k in range(100)]
+    first_bad = next((k for k in range(100) if max(errs_x[k], errs_y[k]) > 1e-10), None)
+    assert first_bad is None, (first_bad, errs_x[first_bad], errs_y[first_bad], ex.restarts,
+                               r2.restarts)
+    assert r2.iterations == ex.iterations
+
+
+def test_device_scaling_is_the_reference_scaling(pkg, orc, engine):
+    for p in (pkg.lpgen.badly_scaled_lp(1500, 4000, 6, seed=22),
+              pkg.lpgen.random_equality_lp(300, 700, 5, seed=2),
+              golden_problem(pkg, load_golden("scaling_ill_scaled"))):
+        engine.load(p)
+        rs, cs = engine.scaling()
+        ors, ocs = orc.oracle_scaling(p)
+        assert np.array_equal(rs, ors) and np.array_equal(cs, ocs)
+    # non-default scaling options rescale on the device at solve time
+    p = pkg.lpgen.badly_scaled_lp(800, 2000, 5, seed=23)
+    engine.load(p)
+    for kw in ({"apply_pock_chambolle": False}, {"apply_ruiz": False}, {"ruiz_iterations": 2}):
+        engine.solve(pkg.PdhgOptions(max_iterations=0, **kw))
+        rs, cs = engine.scaling()
+        ors, ocs = orc.oracle_scaling(p, **{k: int(v) for k, v in kw.items()})
+        assert np.array_equal(rs, ors) and np.array_equal(cs, ocs), kw
+
+
+def test_entries_dropped_by_scaling_match_the_reference(pkg, orc, engine):
+    # a coefficient that scaling drives to |v| <= 1e-14 leaves the scaled matrix
+    # (the reference's from_triplets rebuild drops it, src/l0/sparse.cpp:55)
+    p = pkg.Problem.from_coo(3, 3, [0, 0, 1, 1, 2, 2], [0, 1, 1, 2, 0, 2],
+                             [1e6, 1e-14, 2.0, 1.0, 3.0, 1e-9], c=np.array([1.0, -1.0, 0.5]),
+                             col_lo=np.zeros(3), col_hi=np.full(3, 5.0),
+                             row_lo=np.array([-1.0, 0.0, 1.0]), row_hi=np.array([2.0, 3.0, 4.0]))
+    r = solve(pkg, engine, p, max_iterations=2000)
+    o = orc.oracle_solve(p, max_iterations=2000)
+    assert (r.status, r.iterations, r.restarts) == (o.status, o.iterations, o.restarts)
+    assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
+    assert r.objective == o.objective
 
 
 def test_transportation_lp_adaptive_restarts(pkg, orc, engine):
