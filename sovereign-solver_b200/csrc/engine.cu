@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/pdhg_b200.h"
+#include "dev_buffer.cuh"
 #include "engine.cuh"
 #include "host_prep.hpp"
 
@@ -34,53 +35,6 @@ namespace {
 constexpr double kInf = std::numeric_limits<double>::infinity();
 constexpr int kLookahead = 4;
 constexpr int kStopSwitchPrecision = 100;  // internal stop code: FP32 phase stalled
-
-template <class T>
-struct DBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf&) = delete;
-    DBuf& operator=(const DBuf&) = delete;
-    ~DBuf() { release(); }
-    void release() {
-        if (p != nullptr) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t alloc(size_t count) {
-        if (count == n && p != nullptr) return cudaSuccess;
-        release();
-        n = count;
-        if (count == 0) return cudaSuccess;
-        return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count);
-    }
-};
-
-struct MatDev {
-    int32_t rows = 0, cols = 0;
-    int64_t nnz = 0;
-    DBuf<int32_t> rp, ci, long_rows;
-    DBuf<double> v64;
-    DBuf<float> v32;
-    int32_t n_long = 0, n_short = 0;
-    int vw = 1;
-    DevCsr view() const {
-        DevCsr d;
-        d.rows = rows;
-        d.cols = cols;
-        d.nnz = nnz;
-        d.rp = rp.p;
-        d.ci = ci.p;
-        d.v64 = v64.p;
-        d.v32 = v32.p;
-        d.long_rows = long_rows.p;
-        d.n_long = n_long;
-        d.n_short = n_short;
-        d.vw = vw;
-        return d;
-    }
-};
 
 // Everything a captured check-period graph bakes into its kernel parameters.
 struct GraphSig {
@@ -190,77 +144,6 @@ int fail(Ctx& c, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return fail(c, e_, #expr);      \
     } while (0)
 
-template <class T>
-cudaError_t upload(DBuf<T>& d, const T* h, size_t n, cudaStream_t s) {
-    cudaError_t e = d.alloc(n);
-    if (e != cudaSuccess || n == 0) return e;
-    return cudaMemcpyAsync(d.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s);
-}
-
-template <class T>
-cudaError_t upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
-    return upload(d, h.data(), h.size(), s);
-}
-
-cudaError_t to_float(DBuf<float>& d, const DBuf<double>& src, cudaStream_t s) {
-    cudaError_t e = d.alloc(src.n);
-    if (e != cudaSuccess) return e;
-    launch_to_float(src.p, d.p, static_cast<int64_t>(src.n), s);
-    return cudaGetLastError();
-}
-
-// Row binning on the device: long-row list, short-row count, lanes per short
-// row (about half the mean short-row length, a power of two in [1, 32]).
-int bin_matrix(Ctx& c, MatDev& M) {
-    cudaStream_t s = c.stream;
-    CK(M.long_rows.alloc(static_cast<size_t>(M.rows) + 1));
-    DBuf<unsigned long long> cnt;
-    CK(cnt.alloc(3));
-    CK(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), s));
-    launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
-    unsigned long long h[3];
-    CK(cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    M.n_long = static_cast<int32_t>(h[0]);
-    M.n_short = static_cast<int32_t>(h[1]);
-    const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
-    int w = 1;
-    while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;
-    M.vw = w;
-    return PDHG_OK;
-}
-
-// A from host arrays (the caller's, read in place) and A^T built on the device.
-int upload_matrix(Ctx& c, int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,
-                  const int32_t* ci, const double* v, MatDev& M, MatDev& MT) {
-    cudaStream_t s = c.stream;
-    M.rows = rows;
-    M.cols = cols;
-    M.nnz = nnz;
-    CK(upload(M.rp, rp, static_cast<size_t>(rows) + 1, s));
-    CK(upload(M.ci, ci, static_cast<size_t>(nnz), s));
-    CK(upload(M.v64, v, static_cast<size_t>(nnz), s));
-    MT.rows = cols;
-    MT.cols = rows;
-    MT.nnz = nnz;
-    CK(MT.rp.alloc(static_cast<size_t>(cols) + 1));
-    CK(MT.ci.alloc(static_cast<size_t>(nnz)));
-    CK(MT.v64.alloc(static_cast<size_t>(nnz)));
-    TransposeOut out{MT.rp.p, MT.ci.p, MT.v64.p};
-    if (build_transpose(rows, cols, nnz, M.rp.p, M.ci.p, M.v64.p, out, s) != 0)
-        return fail(c, cudaGetLastError(), "build_transpose");
-    int rc = bin_matrix(c, M);
-    if (rc != PDHG_OK) return rc;
-    return bin_matrix(c, MT);
-}
-
-template <class T>
-cudaError_t copy_dev(DBuf<T>& d, const T* src, size_t n, cudaStream_t s) {
-    cudaError_t e = d.alloc(n);
-    if (e != cudaSuccess || n == 0) return e;
-    return cudaMemcpyAsync(d.p, src, sizeof(T) * n, cudaMemcpyDeviceToDevice, s);
-}
-
 // Scaling::equilibrate(Problem) (scaling.cpp:155-205) on the device, from the
 // original A / A^T already resident: factors, scaled matrices, scaled vectors.
 int ensure_scaled(Ctx& c, const ScalingParams& sp) {
@@ -332,9 +215,9 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     }
     CK(to_float(c.As.v32, c.As.v64, s));
     CK(to_float(c.ATs.v32, c.ATs.v64, s));
-    int rc = bin_matrix(c, c.As);
+    int rc = bin_matrix(c.As, s, &c.err);
     if (rc != PDHG_OK) return rc;
-    rc = bin_matrix(c, c.ATs);
+    rc = bin_matrix(c.ATs, s, &c.err);
     if (rc != PDHG_OK) return rc;
     const double sign = c.lp.maximize ? -1.0 : 1.0;
     CK(c.c_s.alloc(static_cast<size_t>(n) + 1));
@@ -988,6 +871,8 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     fa.bound_tol = o.tolerance > 1e-6 ? o.tolerance : 1e-6;
     fa.exact = o.precision == PDHG_PREC_FP64_EXACT ? 1 : 0;
     fa.st = c.st.p;
+    fa.part = c.part.p;
+    fa.part_blocks = static_cast<int>(std::min<size_t>(c.part.n / 3, 8 * static_cast<size_t>(c.sm_count)));
     launch_final(fa, c.stream);
     c.launches += 5;
     CK(cudaGetLastError());
@@ -1048,7 +933,7 @@ int load(Ctx& c, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
     c.loaded = true;
     c.valid = validate_lp(view, &c.why);
     if (!c.valid) return PDHG_OK;
-    int rc = upload_matrix(c, m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo);
+    int rc = upload_matrix(m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo, c.stream, &c.err);
     if (rc != PDHG_OK) return rc;
     cudaStream_t s = c.stream;
     CK(upload(c.c_o, cv, static_cast<size_t>(n), s));
@@ -1320,7 +1205,7 @@ int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
     if (rc != PDHG_OK) return rc;
     std::unique_ptr<pdhg_ctx> guard(h);
     pdhg::Ctx& c = h->c;
-    rc = pdhg::upload_matrix(c, m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo);
+    rc = pdhg::upload_matrix(m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo, c.stream, &c.err);
     if (rc != PDHG_OK) return rc;
     const int32_t nx = transpose ? m : n, ny = transpose ? n : m;
     pdhg::DBuf<double> dx, dy;

@@ -227,6 +227,8 @@ struct FinalArgs {
     double bound_tol;
     int exact;
     DevState* st;
+    double* part = nullptr;   // 3 doubles per CTA of the fast-mode sums
+    int part_blocks = 0;      // CTAs that fit in part (and at most a few per SM)
 };
 void launch_final(const FinalArgs& a, cudaStream_t s);
 

@@ -1,0 +1,260 @@
+// fast_common.cuh -- device helpers shared by the single-LP throughput kernels
+// (kernels_fast.cu) and the batched kernels (batch.cu): precision-generic
+// vector access, group/block reductions, the long-row dot product, the fused
+// iteration epilogue and the residual terms of the check.
+#pragma once
+
+#include <type_traits>
+
+#include "engine.cuh"
+
+namespace pdhg {
+namespace {
+
+constexpr int kStatusOptimal = 0;
+constexpr int kStatusNumericalFailure = 3;
+
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ bool fb(double v) { return v > -INFINITY && v < INFINITY; }
+
+template <class T>
+__device__ __forceinline__ T clampT(T v, T lo, T hi) {
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+
+template <class T>
+__device__ __forceinline__ const T* mvals(const DevCsr& A);
+template <>
+__device__ __forceinline__ const float* mvals<float>(const DevCsr& A) { return A.v32; }
+template <>
+__device__ __forceinline__ const double* mvals<double>(const DevCsr& A) { return A.v64; }
+
+template <class T>
+struct PV {
+    const T *c, *lo, *hi, *rlo, *rhi;
+};
+template <class T>
+__device__ __forceinline__ PV<T> pvec(const DevProblem& P);
+template <>
+__device__ __forceinline__ PV<float> pvec<float>(const DevProblem& P) {
+    return {P.c32, P.lo32, P.hi32, P.rlo32, P.rhi32};
+}
+template <>
+__device__ __forceinline__ PV<double> pvec<double>(const DevProblem& P) {
+    return {P.c, P.lo, P.hi, P.rlo, P.rhi};
+}
+
+__device__ __forceinline__ unsigned group_mask(int vw) {
+    if (vw >= 32) return 0xffffffffu;
+    const unsigned base = (threadIdx.x & 31u) & ~static_cast<unsigned>(vw - 1);
+    return ((1u << vw) - 1u) << base;
+}
+
+template <class T>
+__device__ __forceinline__ T group_sum(T v, int vw) {
+    const unsigned mask = group_mask(vw);
+    for (int o = vw / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+// Block-wide sum; every thread calls it and gets the total.
+template <class T>
+__device__ T block_total(T v) {
+    __shared__ T sh[kBlock / 32];
+    __shared__ T tot;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        T w = threadIdx.x < kBlock / 32 ? sh[threadIdx.x] : T(0);
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) tot = w;
+    }
+    __syncthreads();
+    const T r = tot;
+    __syncthreads();
+    return r;
+}
+
+// Deterministic block sum for the check's partial sums.
+__device__ double block_sum_det(double v) {
+    __shared__ double sh[kBlock];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ double acc_read(unsigned long long* slot) {
+    return __longlong_as_double(
+        static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(slot)));
+}
+
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ bool am_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    return am_last;
+}
+
+// Long-row dot product: 128-bit loads of values and column indices on the
+// aligned body, scalar head and tail. The matrix is streamed (evict-first,
+// ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go
+// through the read-only path.
+template <class T>
+__device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
+                                          const T* __restrict__ v, const T* __restrict__ xg,
+                                          int b, int e) {
+    constexpr int W = 16 / sizeof(T);
+    int bA = ((b + W - 1) / W) * W;
+    if (bA > e) bA = e;
+    T acc = T(0);
+    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
+    const int nvec = (e - bA) / W;
+    if constexpr (W == 4) {
+        const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
+        const float4* v4 = reinterpret_cast<const float4*>(v + bA);
+        int q = threadIdx.x;
+        // four independent 128-bit loads of each stream in flight per thread
+        for (; q + 3 * kBlock < nvec; q += 4 * kBlock) {
+            int4 c[4];
+            float4 w[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                c[u] = __ldcs(ci4 + q + u * kBlock);
+                w[u] = __ldcs(v4 + q + u * kBlock);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                acc += w[u].x * __ldg(xg + c[u].x) + w[u].y * __ldg(xg + c[u].y) +
+                       w[u].z * __ldg(xg + c[u].z) + w[u].w * __ldg(xg + c[u].w);
+        }
+        for (; q < nvec; q += kBlock) {
+            const int4 c = __ldcs(ci4 + q);
+            const float4 w = __ldcs(v4 + q);
+            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
+                   w.w * __ldg(xg + c.w);
+        }
+    } else {
+        const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
+        const double2* v2 = reinterpret_cast<const double2*>(v + bA);
+        for (int q = threadIdx.x; q < nvec; q += kBlock) {
+            const int2 c = __ldcs(ci2 + q);
+            const double2 w = __ldcs(v2 + q);
+            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
+        }
+    }
+    for (int k = bA + nvec * W + threadIdx.x; k < e; k += kBlock)
+        acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
+    return block_total(acc);
+}
+
+
+// Epilogue traffic: every per-column array is streamed (evict-first loads and
+// stores) except x_bar, whose lines the dual kernel gathers next and should
+// find in L2; y likewise stays at normal priority for the next primal gather.
+// The epilogue's operands are loaded before the row's SpMV loads are issued
+// (they do not depend on them), so both streams are in flight together.
+template <class T>
+struct EpiIn {
+    T a, b, lo, hi, ps;  // primal: c, x, lo, hi, sum; dual: y, s, row lo, row hi, sum
+};
+
+template <class T, bool PRIMAL>
+__device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>& pv, int r,
+                                             int first, bool fresh) {
+    EpiIn<T> in;
+    if (PRIMAL) {
+        in.a = __ldcs(pv.c + r);
+        in.b = __ldcs(it.x + r);
+        in.lo = __ldcs(pv.lo + r);
+        in.hi = __ldcs(pv.hi + r);
+        if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psx + r);
+        else in.ps = fresh ? T(0) : __ldcs(it.xsum + r);
+    } else {
+        in.a = it.y[r];
+        in.b = __ldcs(it.s + r);
+        in.lo = __ldcs(pv.rlo + r);
+        in.hi = __ldcs(pv.rhi + r);
+        if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psy + r);
+        else in.ps = fresh ? T(0) : __ldcs(it.ysum + r);
+    }
+    return in;
+}
+
+// primal: x+ = proj(x - tau (c - aty)), x_bar = 2x+ - x, sum += x+
+// dual:   s+ = proj(s - tau y), y+ = y + sigma (2s+ - s - ax), sum += y+
+template <class T, bool PRIMAL>
+__device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, const EpiIn<T>& in,
+                                          T tau, T sigma) {
+    if (PRIMAL) {
+        const T xo = in.b;
+        const T xn = clampT<T>(xo - tau * (in.a - dot), in.lo, in.hi);
+        it.xbar[r] = T(2) * xn - xo;
+        __stcs(it.x + r, xn);
+        if constexpr (std::is_same<T, float>::value) __stcs(it.psx + r, in.ps + xn);
+        else __stcs(it.xsum + r, in.ps + xn);
+    } else {
+        const T yo = in.a, so = in.b;
+        const T sn = clampT<T>(so - tau * yo, in.lo, in.hi);
+        const T yn = yo + sigma * ((T(2) * sn - so) - dot);
+        it.y[r] = yn;
+        __stcs(it.s + r, sn);
+        if constexpr (std::is_same<T, float>::value) __stcs(it.psy + r, in.ps + yn);
+        else __stcs(it.ysum + r, in.ps + yn);
+    }
+}
+
+__device__ __forceinline__ double cs_term(double v, double act, double lo, double hi,
+                                          double bt) {
+    const bool at_lo = fb(lo) && fabs(act - lo) < bt;
+    const bool at_hi = fb(hi) && fabs(act - hi) < bt;
+    if (!at_lo && !at_hi) return fabs(v);
+    if (at_lo && !at_hi) return smax(0.0, -v);
+    if (at_hi && !at_lo) return smax(0.0, v);
+    return 0.0;
+}
+
+__device__ __forceinline__ double primal_term(double act, double lo, double hi) {
+    double p = 0.0;
+    if (fb(lo)) p = smax(p, lo - act);
+    if (fb(hi)) p = smax(p, act - hi);
+    return p;
+}
+
+__device__ __forceinline__ double clipped_inf(double coeff, double lo, double hi) {
+    if (coeff > 0.0) return fb(lo) ? coeff * lo : 0.0;
+    if (coeff < 0.0) return fb(hi) ? coeff * hi : 0.0;
+    return 0.0;
+}
+
+struct Terms {
+    double cp = 0, cd = 0, ap = 0, ad = 0;         // scaled: cur / avg, primal / dual
+    double ocp = 0, ocd = 0, oap = 0, oad = 0;     // original space
+    double pobj_c = 0, dobj_c = 0, pobj_a = 0, dobj_a = 0;
+};
+
+template <class T>
+__device__ __forceinline__ double avg_x(const Iterates<T>& it, int j, double inv) {
+    double s = it.xsum[j];
+    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psx[j]);
+    return s * inv;
+}
+template <class T>
+__device__ __forceinline__ double avg_y(const Iterates<T>& it, int i, double inv) {
+    double s = it.ysum[i];
+    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psy[i]);
+    return s * inv;
+}
+
+}  // namespace
+}  // namespace pdhg

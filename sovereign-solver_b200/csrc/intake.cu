@@ -38,40 +38,85 @@ __device__ __forceinline__ bool last_cta(unsigned int* ticket) {
     return am_last;
 }
 
-// Row lengths -> long-row list, number and total length of short rows.
+__device__ __forceinline__ unsigned group_mask(int vw) {
+    if (vw >= 32) return 0xffffffffu;
+    const unsigned base = (threadIdx.x & 31u) & ~static_cast<unsigned>(vw - 1);
+    return ((1u << vw) - 1u) << base;
+}
+
+// Row lengths -> long-row list, number and total length of short rows
+// (grid-stride, one atomic per CTA and counter).
 __global__ void k_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                       unsigned long long* counters) {
-    const int r = blockIdx.x * kBlock + threadIdx.x;
-    if (r >= rows) return;
-    const int len = rp[r + 1] - rp[r];
-    if (len > long_threshold) {
-        const unsigned long long slot = atomicAdd(&counters[0], 1ull);
-        long_rows[slot] = r;
-    } else {
-        atomicAdd(&counters[1], 1ull);
-        atomicAdd(&counters[2], static_cast<unsigned long long>(len));
+    unsigned long long ns = 0, nz = 0;
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; r < rows;
+         r += static_cast<int64_t>(gridDim.x) * kBlock) {
+        const int len = rp[r + 1] - rp[r];
+        if (len > long_threshold) {
+            const unsigned long long slot = atomicAdd(&counters[0], 1ull);
+            long_rows[slot] = static_cast<int32_t>(r);
+        } else {
+            ns += 1;
+            nz += static_cast<unsigned long long>(len);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ns += __shfl_xor_sync(0xffffffffu, ns, o);
+        nz += __shfl_xor_sync(0xffffffffu, nz, o);
+    }
+    __shared__ unsigned long long sh[2][kBlock / 32];
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][threadIdx.x >> 5] = ns;
+        sh[1][threadIdx.x >> 5] = nz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kBlock / 32; ++w) t += sh[threadIdx.x][w];
+        if (t) atomicAdd(&counters[1 + threadIdx.x], t);
     }
 }
 
-// Ruiz maxima of one orientation: out[row] = max_k |v| * rs[i] * cs[j] where
-// (i, j) is the entry's (row, column) of the ORIGINAL matrix (transposed: the
-// CSR row is j and its column index is i). One warp per row.
-__global__ void k_ruiz_max(DevCsr M, int transposed, const double* rs, const double* cs,
-                           const IntakeState* is, double* out) {
+// (|v| * rs_i) * cs_j for entry k of row r (transposed: the row is column j).
+__device__ __forceinline__ double scaled_mag(const DevCsr& M, int transposed, const double* rs,
+                                             const double* cs, int r, int k) {
+    const int c = M.ci[k];
+    return transposed ? fabs(M.v64[k]) * rs[c] * cs[r] : fabs(M.v64[k]) * rs[r] * cs[c];
+}
+
+// Ruiz maxima of one orientation (order-free): short rows by groups of M.vw
+// lanes, long rows by one CTA each, as in the iteration kernels.
+__global__ void __launch_bounds__(kBlock) k_ruiz_max(DevCsr M, int transposed, const double* rs,
+                                                     const double* cs, const IntakeState* is,
+                                                     double* out, int short_blocks) {
     if (is->ruiz_done) return;
-    const int64_t warp = (blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= M.rows) return;
-    const int r = static_cast<int>(warp);
-    double mx = 0.0;
-    for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
-        const int c = M.ci[k];
-        const double s = transposed ? fabs(M.v64[k]) * rs[c] * cs[r]
-                                    : fabs(M.v64[k]) * rs[r] * cs[c];
-        mx = smax(mx, s);
+    if (static_cast<int>(blockIdx.x) < short_blocks) {
+        const int vw = M.vw;
+        const int lane = threadIdx.x & (vw - 1);
+        const int r = (blockIdx.x * kBlock + threadIdx.x) / vw;
+        if (r >= M.rows) return;
+        const int b = M.rp[r], e = M.rp[r + 1];
+        if (e - b > kLongRow) return;
+        double mx = 0.0;
+        for (int k = b + lane; k < e; k += vw) mx = smax(mx, scaled_mag(M, transposed, rs, cs, r, k));
+        const unsigned mask = group_mask(vw);
+        for (int o = vw / 2; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(mask, mx, o));
+        if (lane == 0) out[r] = mx;
+    } else {
+        const int r = M.long_rows[blockIdx.x - short_blocks];
+        double mx = 0.0;
+        for (int k = M.rp[r] + threadIdx.x; k < M.rp[r + 1]; k += kBlock)
+            mx = smax(mx, scaled_mag(M, transposed, rs, cs, r, k));
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        __shared__ double sh[kBlock / 32];
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < kBlock / 32; ++w) t = fmax(t, sh[w]);
+            out[r] = t;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) out[r] = mx;
 }
 
 __global__ void k_ruiz_update(int32_t m, int32_t n, double* rs, double* cs,
@@ -89,8 +134,14 @@ __global__ void k_ruiz_update(int32_t m, int32_t n, double* rs, double* cs,
         worst = smax(worst, fabs(col_max[t] - 1.0));
     }
     for (int o = 16; o > 0; o >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
-    if ((threadIdx.x & 31) == 0 && worst > 0.0)
-        atomicMax(&is->worst, static_cast<unsigned long long>(__double_as_longlong(worst)));
+    __shared__ double shw[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) shw[threadIdx.x >> 5] = worst;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double w = 0.0;
+        for (int i = 0; i < kBlock / 32; ++i) w = fmax(w, shw[i]);
+        if (w > 0.0) atomicMax(&is->worst, static_cast<unsigned long long>(__double_as_longlong(w)));
+    }
     if (!last_cta(&is->ticket) || threadIdx.x != 0) return;
     const double w = __longlong_as_double(static_cast<long long>(
         *reinterpret_cast<volatile unsigned long long*>(&is->worst)));
@@ -103,16 +154,25 @@ __device__ __forceinline__ double pc_term(double mag, double e) {
     return e == 1.0 ? mag : pow(mag, e);
 }
 
-// Pock-Chambolle sums, one thread per row, in the reference's order.
+// Pock-Chambolle sums, one thread per row, in the reference's order; the
+// loads of four entries are issued before their terms are added.
 __global__ void k_pc_sum(DevCsr M, int transposed, const double* rs, const double* cs,
                          double expo, double* out) {
     const int r = blockIdx.x * kBlock + threadIdx.x;
     if (r >= M.rows) return;
     double sum = 0.0;
-    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) {
-        const int c = M.ci[k];
-        const double mag = transposed ? fabs(M.v64[k]) * rs[c] * cs[r]
-                                      : fabs(M.v64[k]) * rs[r] * cs[c];
+    const int b = M.rp[r], e = M.rp[r + 1];
+    int k = b;
+    for (; k + 4 <= e; k += 4) {
+        double mg[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) mg[u] = scaled_mag(M, transposed, rs, cs, r, k + u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (mg[u] > 0.0) sum = __dadd_rn(sum, pc_term(mg[u], expo));
+    }
+    for (; k < e; ++k) {
+        const double mag = scaled_mag(M, transposed, rs, cs, r, k);
         if (mag <= 0.0) continue;
         sum = __dadd_rn(sum, pc_term(mag, expo));
     }
@@ -128,18 +188,23 @@ __global__ void k_pc_update(int32_t m, int32_t n, double* rs, double* cs, const 
 
 // Scaled values (v * rs_i) * cs_j (Scaling::apply, scaling.cpp:127-128);
 // counts entries the rebuild would drop (|v| <= 1e-14, sparse.cpp:55).
+// Elementwise: a warp walks each row, so long rows spread over 32 lanes.
 __global__ void k_scale_values(DevCsr M, int transposed, const double* rs, const double* cs,
                                double* out, unsigned long long* dropped) {
-    const int r = blockIdx.x * kBlock + threadIdx.x;
-    if (r >= M.rows) return;
+    const int64_t warp = (blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     unsigned long long d = 0;
-    for (int k = M.rp[r]; k < M.rp[r + 1]; ++k) {
-        const int c = M.ci[k];
-        const double v = transposed ? M.v64[k] * rs[c] * cs[r] : M.v64[k] * rs[r] * cs[c];
-        out[k] = v;
-        d += fabs(v) <= 1e-14 ? 1ull : 0ull;
+    if (warp < M.rows) {
+        const int r = static_cast<int>(warp);
+        for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
+            const int c = M.ci[k];
+            const double v = transposed ? M.v64[k] * rs[c] * cs[r] : M.v64[k] * rs[r] * cs[c];
+            out[k] = v;
+            d += fabs(v) <= 1e-14 ? 1ull : 0ull;
+        }
     }
-    if (d) atomicAdd(dropped, d);
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if (lane == 0 && d) atomicAdd(dropped, d);
 }
 
 // Kept-entry counts per row (the compaction path when entries are dropped).
@@ -184,25 +249,31 @@ __global__ void k_scale_vectors(int32_t m, int32_t n, const double* rs, const do
 }
 
 // Norms: [0] |c_s|_2^2, [1] |b_s|_2^2 (b_i = largest finite |scaled row bound|),
-// [2] max |c_o|, [3] max finite |row bound|, original. Block partials + last CTA.
-__global__ void k_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
-                        const double* rhi_s, const double* c_o, const double* rlo_o,
-                        const double* rhi_o, double* part, IntakeState* is) {
-    const int t = blockIdx.x * kBlock + threadIdx.x;
+// [2] max |c_o|, [3] max finite |row bound|, original. Grid-stride over a capped
+// grid, block partials, and a parallel reduction of the partials in the last CTA.
+__global__ void __launch_bounds__(kBlock) k_norms(int32_t m, int32_t n, const double* c_s,
+                                                  const double* rlo_s, const double* rhi_s,
+                                                  const double* c_o, const double* rlo_o,
+                                                  const double* rhi_o, double* part,
+                                                  IntakeState* is) {
     double q[4] = {0.0, 0.0, 0.0, 0.0};
-    if (t < n) {
-        q[0] = c_s[t] * c_s[t];
-        q[2] = fabs(c_o[t]);
-    }
-    if (t < m) {
-        double b = 0.0;
-        if (fb(rlo_s[t])) b = fabs(rlo_s[t]);
-        if (fb(rhi_s[t])) b = smax(b, fabs(rhi_s[t]));
-        q[1] = b * b;
-        double bo = 0.0;
-        if (fb(rlo_o[t])) bo = fabs(rlo_o[t]);
-        if (fb(rhi_o[t])) bo = smax(bo, fabs(rhi_o[t]));
-        q[3] = bo;
+    const int32_t nmax = m > n ? m : n;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; t < nmax;
+         t += static_cast<int64_t>(gridDim.x) * kBlock) {
+        if (t < n) {
+            q[0] += c_s[t] * c_s[t];
+            q[2] = fmax(q[2], fabs(c_o[t]));
+        }
+        if (t < m) {
+            double b = 0.0;
+            if (fb(rlo_s[t])) b = fabs(rlo_s[t]);
+            if (fb(rhi_s[t])) b = smax(b, fabs(rhi_s[t]));
+            q[1] += b * b;
+            double bo = 0.0;
+            if (fb(rlo_o[t])) bo = fabs(rlo_o[t]);
+            if (fb(rhi_o[t])) bo = smax(bo, fabs(rhi_o[t]));
+            q[3] = fmax(q[3], bo);
+        }
     }
     __shared__ double sh[4][kBlock];
     for (int i = 0; i < 4; ++i) sh[i][threadIdx.x] = q[i];
@@ -218,33 +289,56 @@ __global__ void k_norms(int32_t m, int32_t n, const double* c_s, const double* r
     }
     if (threadIdx.x == 0)
         for (int i = 0; i < 4; ++i) part[4 * blockIdx.x + i] = sh[i][0];
-    if (!last_cta(&is->ticket) || threadIdx.x != 0) return;
+    if (!last_cta(&is->ticket)) return;
+    // last CTA: each thread folds a strided subset of the partials in block order
     double r[4] = {0.0, 0.0, 0.0, 0.0};
     const volatile double* p = part;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock) {
         r[0] += p[4 * b];
         r[1] += p[4 * b + 1];
         r[2] = fmax(r[2], p[4 * b + 2]);
         r[3] = fmax(r[3], p[4 * b + 3]);
     }
-    for (int i = 0; i < 4; ++i) is->norms[i] = r[i];
-    is->ticket = 0u;
+    for (int i = 0; i < 4; ++i) sh[i][threadIdx.x] = r[i];
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
+            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 4; ++i) is->norms[i] = sh[i][0];
+        is->ticket = 0u;
+    }
 }
 
 }  // namespace
 
+constexpr int kGridCap = 2048;  // grid-stride kernels: enough CTAs to fill every SM
+
 void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                 unsigned long long* counters, cudaStream_t s) {
-    if (rows > 0) k_bin<<<nblocks(rows), kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+    const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
+    if (rows > 0) k_bin<<<g, kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+}
+
+inline int short_blocks(const DevCsr& M) {
+    if (M.n_short == 0) return 0;
+    return static_cast<int>((static_cast<int64_t>(M.rows) * M.vw + kBlock - 1) / kBlock);
 }
 
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
                        double* row_max, double* col_max, double tol, IntakeState* is,
                        cudaStream_t s) {
-    if (A.rows > 0)
-        k_ruiz_max<<<nblocks(static_cast<int64_t>(A.rows) * 32), kBlock, 0, s>>>(A, 0, rs, cs, is, row_max);
-    if (AT.rows > 0)
-        k_ruiz_max<<<nblocks(static_cast<int64_t>(AT.rows) * 32), kBlock, 0, s>>>(AT, 1, rs, cs, is, col_max);
+    const int sa = short_blocks(A), st = short_blocks(AT);
+    if (sa + A.n_long > 0)
+        k_ruiz_max<<<sa + A.n_long, kBlock, 0, s>>>(A, 0, rs, cs, is, row_max, sa);
+    if (st + AT.n_long > 0)
+        k_ruiz_max<<<st + AT.n_long, kBlock, 0, s>>>(AT, 1, rs, cs, is, col_max, st);
     const int32_t nmax = A.rows > AT.rows ? A.rows : AT.rows;
     k_ruiz_update<<<nmax > 0 ? nblocks(nmax) : 1, kBlock, 0, s>>>(A.rows, AT.rows, rs, cs,
                                                                  row_max, col_max, tol, is);
@@ -261,7 +355,8 @@ void launch_pock_chambolle(const DevCsr& A, const DevCsr& AT, double* rs, double
 
 void launch_scale_values(const DevCsr& M, int transposed, const double* rs, const double* cs,
                          double* out, unsigned long long* dropped, cudaStream_t s) {
-    if (M.rows > 0) k_scale_values<<<nblocks(M.rows), kBlock, 0, s>>>(M, transposed, rs, cs, out, dropped);
+    if (M.rows > 0)
+        k_scale_values<<<nblocks(static_cast<int64_t>(M.rows) * 32), kBlock, 0, s>>>(M, transposed, rs, cs, out, dropped);
 }
 
 void launch_kept_counts(const DevCsr& M, const double* vs, int32_t* cnt, cudaStream_t s) {
@@ -283,14 +378,15 @@ void launch_scale_vectors(int32_t m, int32_t n, const double* rs, const double* 
                                                          c_s, lo_s, hi_s, rlo_s, rhi_s);
 }
 
-int norms_part_size(int32_t m, int32_t n) { return 4 * (nblocks(m > n ? m : n) + 1); }
+int norms_part_size(int32_t m, int32_t n) { return 4 * (kGridCap + 1); }
 
 void launch_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
                   const double* rhi_s, const double* c_o, const double* rlo_o,
                   const double* rhi_o, double* part, IntakeState* is, cudaStream_t s) {
     const int32_t nmax = m > n ? m : n;
-    k_norms<<<nmax > 0 ? nblocks(nmax) : 1, kBlock, 0, s>>>(m, n, c_s, rlo_s, rhi_s, c_o, rlo_o,
-                                                           rhi_o, part, is);
+    int g = nmax > 0 ? nblocks(nmax) : 1;
+    if (g > kGridCap) g = kGridCap;
+    k_norms<<<g, kBlock, 0, s>>>(m, n, c_s, rlo_s, rhi_s, c_o, rlo_o, rhi_o, part, is);
 }
 
 }  // namespace pdhg

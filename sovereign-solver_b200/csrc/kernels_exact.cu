@@ -90,6 +90,28 @@ __host__ __device__ inline int blocks_for(int64_t n) {
     return static_cast<int>((n + kBlock - 1) / kBlock);
 }
 
+// acc = init; for k in [b, e): acc = acc + v[k] * g(ci[k]), rounded after each
+// product and each sum, in k order. The loads of four terms are issued before
+// their products are added, so the memory latency of a long row overlaps while
+// the sum keeps the reference's order exactly.
+template <class G>
+__device__ __forceinline__ double ordered_dot(int b, int e, const int32_t* __restrict__ ci,
+                                              const double* __restrict__ v, G g, double init) {
+    double acc = init;
+    int k = b;
+    for (; k + 4 <= e; k += 4) {
+        const int c0 = ci[k], c1 = ci[k + 1], c2 = ci[k + 2], c3 = ci[k + 3];
+        const double v0 = v[k], v1 = v[k + 1], v2 = v[k + 2], v3 = v[k + 3];
+        const double g0 = g(c0), g1 = g(c1), g2 = g(c2), g3 = g(c3);
+        acc = __dadd_rn(acc, __dmul_rn(v0, g0));
+        acc = __dadd_rn(acc, __dmul_rn(v1, g1));
+        acc = __dadd_rn(acc, __dmul_rn(v2, g2));
+        acc = __dadd_rn(acc, __dmul_rn(v3, g3));
+    }
+    for (; k < e; ++k) acc = __dadd_rn(acc, __dmul_rn(v[k], g(ci[k])));
+    return acc;
+}
+
 // ---------------------------------------------------------------------------
 // One PDHG iteration (src/l1/pdhg.cpp:295-331)
 // ---------------------------------------------------------------------------
@@ -103,10 +125,9 @@ __global__ void __launch_bounds__(kBlock) ex_primal(ExactIter a, int first) {
     if (st->done) return;
     const int j = blockIdx.x * kBlock + threadIdx.x;
     if (j >= a.AT.rows) return;
-    double g = a.P.c[j];
-    const int e = a.AT.rp[j + 1];
-    for (int k = a.AT.rp[j]; k < e; ++k)
-        g = __dadd_rn(g, __dmul_rn(a.AT.v64[k], -a.it.y[a.AT.ci[k]]));
+    const double* y = a.it.y;
+    const double g = ordered_dot(a.AT.rp[j], a.AT.rp[j + 1], a.AT.ci, a.AT.v64,
+                                 [y](int i) { return -y[i]; }, a.P.c[j]);
     const double xo = a.it.x[j];
     const double xn = clampd(__dadd_rn(xo, __dmul_rn(-st->tau, g)), a.P.lo[j], a.P.hi[j]);
     a.it.xbar[j] = __dadd_rn(2.0 * xn, -xo);  // scale(2.0) then axpy(-1.0, x)
@@ -126,10 +147,9 @@ __global__ void __launch_bounds__(kBlock) ex_dual(ExactIter a, int first) {
     const double so = a.it.s[i];
     const double sn = clampd(__dadd_rn(so, __dmul_rn(-st->tau, yo)), a.P.rlo[i], a.P.rhi[i]);
     const double sbar = __dadd_rn(2.0 * sn, -so);
-    double sum = 0.0;
-    const int e = a.A.rp[i + 1];
-    for (int k = a.A.rp[i]; k < e; ++k)
-        sum = __dadd_rn(sum, __dmul_rn(a.A.v64[k], a.it.xbar[a.A.ci[k]]));
+    const double* xbar = a.it.xbar;
+    const double sum = ordered_dot(a.A.rp[i], a.A.rp[i + 1], a.A.ci, a.A.v64,
+                                   [xbar](int j) { return xbar[j]; }, 0.0);
     const double kb = __dadd_rn(-sum, sbar);
     const double yn = __dadd_rn(yo, __dmul_rn(st->sigma, kb));
     a.it.y[i] = yn;
@@ -176,14 +196,12 @@ __global__ void __launch_bounds__(kBlock) ex_check1(ExactCheck a) {
     if (static_cast<int>(blockIdx.x) < row_blocks) {
         const int i = blockIdx.x * kBlock + threadIdx.x;
         if (i < a.A.rows) {
-            double act_c = 0.0, act_a = 0.0;
-            const int e = a.A.rp[i + 1];
-            for (int k = a.A.rp[i]; k < e; ++k) {
-                const int j = a.A.ci[k];
-                const double v = a.A.v64[k];
-                act_c = __dadd_rn(act_c, __dmul_rn(v, a.it.x[j]));
-                act_a = __dadd_rn(act_a, __dmul_rn(v, __dmul_rn(a.it.xsum[j], inv)));
-            }
+            const double* x = a.it.x;
+            const double* xs = a.it.xsum;
+            const int b = a.A.rp[i], e = a.A.rp[i + 1];
+            const double act_c = ordered_dot(b, e, a.A.ci, a.A.v64, [x](int j) { return x[j]; }, 0.0);
+            const double act_a = ordered_dot(b, e, a.A.ci, a.A.v64,
+                                             [xs, inv](int j) { return __dmul_rn(xs[j], inv); }, 0.0);
             a.cs.act_avg[i] = act_a;
             const double lo = a.P.rlo[i], hi = a.P.rhi[i];
             cp = primal_term(act_c, lo, hi);
@@ -194,14 +212,12 @@ __global__ void __launch_bounds__(kBlock) ex_check1(ExactCheck a) {
     } else {
         const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
         if (j < a.AT.rows) {
-            double aty_c = 0.0, aty_a = 0.0;
-            const int e = a.AT.rp[j + 1];
-            for (int k = a.AT.rp[j]; k < e; ++k) {
-                const int i = a.AT.ci[k];
-                const double v = a.AT.v64[k];
-                aty_c = __dadd_rn(aty_c, __dmul_rn(v, a.it.y[i]));
-                aty_a = __dadd_rn(aty_a, __dmul_rn(v, __dmul_rn(a.it.ysum[i], inv)));
-            }
+            const double* y = a.it.y;
+            const double* ys = a.it.ysum;
+            const int b = a.AT.rp[j], e = a.AT.rp[j + 1];
+            const double aty_c = ordered_dot(b, e, a.AT.ci, a.AT.v64, [y](int i) { return y[i]; }, 0.0);
+            const double aty_a = ordered_dot(b, e, a.AT.ci, a.AT.v64,
+                                             [ys, inv](int i) { return __dmul_rn(ys[i], inv); }, 0.0);
             const double cj = a.P.c[j];
             const double lo = a.P.lo[j], hi = a.P.hi[j];
             cd = cs_term(__dadd_rn(cj, -aty_c), a.it.x[j], lo, hi, bt);
@@ -248,13 +264,12 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
     if (static_cast<int>(blockIdx.x) < row_blocks) {
         const int i = blockIdx.x * kBlock + threadIdx.x;
         if (i < a.Ao.rows) {
-            double act = 0.0;
-            const int e = a.Ao.rp[i + 1];
-            for (int k = a.Ao.rp[i]; k < e; ++k) {
-                const int j = a.Ao.ci[k];
-                const double xs = ab ? __dmul_rn(a.it.xsum[j], inv) : a.it.x[j];
-                act = __dadd_rn(act, __dmul_rn(a.Ao.v64[k], __dmul_rn(xs, a.P.cs[j])));
-            }
+            const double* xv = a.it.x;
+            const double* xsum = a.it.xsum;
+            const double* cs = a.P.cs;
+            const double act = ordered_dot(
+                a.Ao.rp[i], a.Ao.rp[i + 1], a.Ao.ci, a.Ao.v64,
+                [=](int j) { return __dmul_rn(ab ? __dmul_rn(xsum[j], inv) : xv[j], cs[j]); }, 0.0);
             const double ys = ab ? __dmul_rn(a.it.ysum[i], inv) : a.it.y[i];
             const double yo = __dmul_rn(__dmul_rn(ys, sign), a.P.rs[i]);
             if (a.want_candidate) a.cs.cand_yo[i] = yo;
@@ -270,14 +285,16 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
     } else {
         const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
         if (j < a.ATo.rows) {
-            double aty = 0.0;
-            const int e = a.ATo.rp[j + 1];
-            for (int k = a.ATo.rp[j]; k < e; ++k) {
-                const int i = a.ATo.ci[k];
-                const double ys = ab ? __dmul_rn(a.it.ysum[i], inv) : a.it.y[i];
-                const double yo = __dmul_rn(__dmul_rn(ys, sign), a.P.rs[i]);
-                aty = __dadd_rn(aty, __dmul_rn(a.ATo.v64[k], yo));
-            }
+            const double* yv = a.it.y;
+            const double* ysum = a.it.ysum;
+            const double* rsv = a.P.rs;
+            const double aty = ordered_dot(
+                a.ATo.rp[j], a.ATo.rp[j + 1], a.ATo.ci, a.ATo.v64,
+                [=](int i) {
+                    const double ys = ab ? __dmul_rn(ysum[i], inv) : yv[i];
+                    return __dmul_rn(__dmul_rn(ys, sign), rsv[i]);
+                },
+                0.0);
             const double xs = ab ? __dmul_rn(a.it.xsum[j], inv) : a.it.x[j];
             const double xo = __dmul_rn(xs, a.P.cs[j]);
             if (a.want_candidate) a.cs.cand_xo[j] = xo;
@@ -387,9 +404,7 @@ __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, cons
                                                  double* w) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= A.rows) return;
-    double sum = 0.0;
-    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-        sum = __dadd_rn(sum, __dmul_rn(A.v64[k], u[A.ci[k]]));
+    const double sum = ordered_dot(A.rp[i], A.rp[i + 1], A.ci, A.v64, [u](int j) { return u[j]; }, 0.0);
     w[i] = __dadd_rn(-sum, v[i]);
 }
 
@@ -398,10 +413,7 @@ __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, cons
 __global__ void __launch_bounds__(kBlock) k_pw_u(DevCsr AT, const double* w, double* u) {
     const int j = blockIdx.x * kBlock + threadIdx.x;
     if (j >= AT.rows) return;
-    double sum = 0.0;
-    for (int k = AT.rp[j]; k < AT.rp[j + 1]; ++k)
-        sum = __dadd_rn(sum, __dmul_rn(AT.v64[k], -w[AT.ci[k]]));
-    u[j] = sum;
+    u[j] = ordered_dot(AT.rp[j], AT.rp[j + 1], AT.ci, AT.v64, [w](int i) { return -w[i]; }, 0.0);
 }
 
 __global__ void k_scale(double* x, int64_t n, double alpha) {
@@ -477,6 +489,22 @@ __global__ void k_pw_fold_level(const double* in, double* out, int64_t half) {
     if (t < half) out[t] = __dadd_rn(in[2 * t], in[2 * t + 1]);
 }
 
+// Folds the remaining 2^levels (<= 1024) values in one CTA, level by level,
+// pairs (2t, 2t+1) -> t exactly as k_pw_fold_level; every thread runs the same
+// number of levels, so the barriers are uniform.
+__global__ void __launch_bounds__(512) k_pw_fold_tail(double* a, double* b, int levels,
+                                                      double* out) {
+    for (int lvl = levels; lvl > 0; --lvl) {
+        const int half = 1 << (lvl - 1);
+        for (int t = threadIdx.x; t < half; t += blockDim.x) b[t] = __dadd_rn(a[2 * t], a[2 * t + 1]);
+        __syncthreads();
+        double* tmp = a;
+        a = b;
+        b = tmp;
+    }
+    if (threadIdx.x == 0) *out = a[0];
+}
+
 // ---------------------------------------------------------------------------
 // Final result (pdhg.cpp:428-498)
 // ---------------------------------------------------------------------------
@@ -506,9 +534,9 @@ __global__ void __launch_bounds__(kBlock) k_fin_rowscols(FinalArgs a) {
     if (static_cast<int>(blockIdx.x) < row_blocks) {
         const int i = blockIdx.x * kBlock + threadIdx.x;
         if (i < a.Ao.rows) {
-            double act = 0.0;
-            for (int k = a.Ao.rp[i]; k < a.Ao.rp[i + 1]; ++k)
-                act = __dadd_rn(act, __dmul_rn(a.Ao.v64[k], a.f.xo[a.Ao.ci[k]]));
+            const double* xo = a.f.xo;
+            const double act = ordered_dot(a.Ao.rp[i], a.Ao.rp[i + 1], a.Ao.ci, a.Ao.v64,
+                                           [xo](int j) { return xo[j]; }, 0.0);
             const double lo = a.P.rlo_o[i], hi = a.P.rhi_o[i];
             pinf = primal_term(act, lo, hi);
             const bool at_lo = fb(lo) && fabs(act - lo) <= bt;
@@ -519,9 +547,9 @@ __global__ void __launch_bounds__(kBlock) k_fin_rowscols(FinalArgs a) {
     } else {
         const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
         if (j < a.ATo.rows) {
-            double aty = 0.0;
-            for (int k = a.ATo.rp[j]; k < a.ATo.rp[j + 1]; ++k)
-                aty = __dadd_rn(aty, __dmul_rn(a.ATo.v64[k], a.f.yo[a.ATo.ci[k]]));
+            const double* yo = a.f.yo;
+            const double aty = ordered_dot(a.ATo.rp[j], a.ATo.rp[j + 1], a.ATo.ci, a.ATo.v64,
+                                           [yo](int i) { return yo[i]; }, 0.0);
             const double rc = __dadd_rn(a.P.c_o[j], -aty);
             a.f.rc[j] = rc;
             const double lo = a.P.lo_o[j], hi = a.P.hi_o[j];
@@ -564,28 +592,45 @@ __global__ void k_fin_sums_exact(FinalArgs a) {
     st->acc[ACC_FIN_PINF] = st->acc[ACC_FIN_DINF] = 0ull;
 }
 
-// Deterministic tree sums (fast modes): one CTA, fixed association.
-__global__ void __launch_bounds__(kBlock) k_fin_sums_tree(FinalArgs a) {
+// Deterministic tree sums (fast modes): grid-stride over a capped grid, block
+// partials in a.f.trow's tail-free scratch (st->acc is not used for sums), and
+// the partials folded in block order by the last CTA.
+__global__ void __launch_bounds__(kBlock) k_fin_sums_tree(FinalArgs a, double* part) {
     DevState* st = a.st;
-    __shared__ int any_inf;
-    if (threadIdx.x == 0) any_inf = 0;
-    __syncthreads();
-    double po = 0.0, du = 0.0;
-    for (int j = threadIdx.x; j < a.P.n; j += kBlock) {
+    double po = 0.0, du = 0.0, inf = 0.0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kBlock;
+    for (int64_t j = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; j < a.P.n; j += stride) {
         po += a.P.c_o[j] * a.f.xo[j];
         const double t = a.f.tcol[j];
-        if (!isfinite(t)) any_inf = 1; else du += t;
+        if (!isfinite(t)) inf = 1.0; else du += t;
     }
-    for (int i = threadIdx.x; i < a.P.m; i += kBlock) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; i < a.P.m; i += stride) {
         const double t = a.f.trow[i];
-        if (!isfinite(t)) any_inf = 1; else du += t;
+        if (!isfinite(t)) inf = 1.0; else du += t;
     }
     po = block_sum(po);
     du = block_sum(du);
-    __syncthreads();
+    inf = block_sum(inf);
     if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = po;
+        part[3 * blockIdx.x + 1] = du;
+        part[3 * blockIdx.x + 2] = inf;
+    }
+    if (!last_block(&st->ticket[TK_RESTART])) return;
+    double rp = 0.0, rd = 0.0, ri = 0.0;
+    const volatile double* p = part;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock) {
+        rp += p[3 * b];
+        rd += p[3 * b + 1];
+        ri += p[3 * b + 2];
+    }
+    po = block_sum(rp);
+    du = block_sum(rd);
+    inf = block_sum(ri);
+    if (threadIdx.x == 0) {
+        st->ticket[TK_RESTART] = 0u;
         const double acc = a.P.obj_const + po;
-        const bool fin = any_inf == 0;
+        const bool fin = inf == 0.0;
         st->objective = acc;
         st->dual_objective = du;
         st->gap_finite = fin ? 1 : 0;
@@ -658,9 +703,7 @@ __global__ void k_spmv_exact(DevCsr A, double alpha, const double* x, double bet
     // HostBackend::spmv, backend_host.cpp:415-423 (beta == 0 overwrites)
     const int r = blockIdx.x * kBlock + threadIdx.x;
     if (r >= A.rows) return;
-    double sum = 0.0;
-    for (int k = A.rp[r]; k < A.rp[r + 1]; ++k)
-        sum = __dadd_rn(sum, __dmul_rn(A.v64[k], x[A.ci[k]]));
+    const double sum = ordered_dot(A.rp[r], A.rp[r + 1], A.ci, A.v64, [x](int j) { return x[j]; }, 0.0);
     y[r] = (beta == 0.0) ? __dmul_rn(alpha, sum)
                          : __dadd_rn(__dmul_rn(alpha, sum), __dmul_rn(beta, y[r]));
 }
@@ -671,10 +714,9 @@ __global__ void k_spmv_exact(DevCsr A, double alpha, const double* x, double bet
 __global__ void k_spmvT_exact(DevCsr AT, double alpha, const double* x, double beta, double* y) {
     const int c = blockIdx.x * kBlock + threadIdx.x;
     if (c >= AT.rows) return;
-    double acc = (beta == 0.0) ? 0.0 : __dmul_rn(y[c], beta);
-    for (int k = AT.rp[c]; k < AT.rp[c + 1]; ++k)
-        acc = __dadd_rn(acc, __dmul_rn(AT.v64[k], __dmul_rn(alpha, x[AT.ci[k]])));
-    y[c] = acc;
+    const double init = (beta == 0.0) ? 0.0 : __dmul_rn(y[c], beta);
+    y[c] = ordered_dot(AT.rp[c], AT.rp[c + 1], AT.ci, AT.v64,
+                       [x, alpha](int r) { return __dmul_rn(alpha, x[r]); }, init);
 }
 
 __global__ void k_project_box(int32_t n, const double* lo, const double* hi, double* x) {
@@ -761,14 +803,15 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
     double* a = partial;
     double* b = partial + count;
     k_pw_level<<<grid64(count), kBlock, 0, s>>>(x, y, n, d, a);
-    for (int lvl = d; lvl > 0; --lvl) {
+    int lvl = d;
+    for (; lvl > 10; --lvl) {  // wide levels: one launch each
         const int64_t half = int64_t{1} << (lvl - 1);
         k_pw_fold_level<<<grid64(half), kBlock, 0, s>>>(a, b, half);
         double* t = a;
         a = b;
         b = t;
     }
-    cudaMemcpyAsync(out, a, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    k_pw_fold_tail<<<1, 512, 0, s>>>(a, b, lvl, out);  // the last <= 1024 values in one CTA
 }
 
 void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s) {
@@ -789,10 +832,13 @@ void launch_final(const FinalArgs& a, cudaStream_t s) {
     if (nmax > 0) k_fin_unscale<<<blocks_for(nmax), kBlock, 0, s>>>(a);
     const int g = blocks_for(a.Ao.rows) + blocks_for(a.ATo.rows);
     if (g > 0) k_fin_rowscols<<<g, kBlock, 0, s>>>(a);
-    if (a.exact)
+    if (a.exact) {
         k_fin_sums_exact<<<1, 32, 0, s>>>(a);
-    else
-        k_fin_sums_tree<<<1, kBlock, 0, s>>>(a);
+    } else {
+        int gs = blocks_for(nmax > 0 ? nmax : 1);
+        if (gs > a.part_blocks) gs = a.part_blocks;
+        k_fin_sums_tree<<<gs > 0 ? gs : 1, kBlock, 0, s>>>(a, a.part);
+    }
 }
 
 template <class T>

@@ -27,181 +27,15 @@
 #include <type_traits>
 
 #include "engine.cuh"
+#include "fast_common.cuh"
 
 namespace pdhg {
 
 namespace {
 
-constexpr int kStatusOptimal = 0;
-constexpr int kStatusNumericalFailure = 3;
-
-__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ bool fb(double v) { return v > -INFINITY && v < INFINITY; }
-
-template <class T>
-__device__ __forceinline__ T clampT(T v, T lo, T hi) {
-    if (v < lo) v = lo;
-    if (v > hi) v = hi;
-    return v;
-}
-
-template <class T>
-__device__ __forceinline__ const T* mvals(const DevCsr& A);
-template <>
-__device__ __forceinline__ const float* mvals<float>(const DevCsr& A) { return A.v32; }
-template <>
-__device__ __forceinline__ const double* mvals<double>(const DevCsr& A) { return A.v64; }
-
-template <class T>
-struct PV {
-    const T *c, *lo, *hi, *rlo, *rhi;
-};
-template <class T>
-__device__ __forceinline__ PV<T> pvec(const DevProblem& P);
-template <>
-__device__ __forceinline__ PV<float> pvec<float>(const DevProblem& P) {
-    return {P.c32, P.lo32, P.hi32, P.rlo32, P.rhi32};
-}
-template <>
-__device__ __forceinline__ PV<double> pvec<double>(const DevProblem& P) {
-    return {P.c, P.lo, P.hi, P.rlo, P.rhi};
-}
-
-__device__ __forceinline__ unsigned group_mask(int vw) {
-    if (vw >= 32) return 0xffffffffu;
-    const unsigned base = (threadIdx.x & 31u) & ~static_cast<unsigned>(vw - 1);
-    return ((1u << vw) - 1u) << base;
-}
-
-template <class T>
-__device__ __forceinline__ T group_sum(T v, int vw) {
-    const unsigned mask = group_mask(vw);
-    for (int o = vw / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
-    return v;
-}
-
-// Block-wide sum; every thread calls it and gets the total.
-template <class T>
-__device__ T block_total(T v) {
-    __shared__ T sh[kBlock / 32];
-    __shared__ T tot;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        T w = threadIdx.x < kBlock / 32 ? sh[threadIdx.x] : T(0);
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        if (threadIdx.x == 0) tot = w;
-    }
-    __syncthreads();
-    const T r = tot;
-    __syncthreads();
-    return r;
-}
-
-// Deterministic block sum for the check's partial sums.
-__device__ double block_sum_det(double v) {
-    __shared__ double sh[kBlock];
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int s = kBlock / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    const double r = sh[0];
-    __syncthreads();
-    return r;
-}
-
-__device__ __forceinline__ double acc_read(unsigned long long* slot) {
-    return __longlong_as_double(
-        static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(slot)));
-}
-
-__device__ __forceinline__ bool last_block(unsigned int* ticket) {
-    __shared__ bool am_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-    __syncthreads();
-    return am_last;
-}
-
-// Long-row dot product: 128-bit loads of values and column indices on the
-// aligned body, scalar head and tail. The matrix is streamed (evict-first,
-// ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go
-// through the read-only path.
-template <class T>
-__device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
-                                          const T* __restrict__ v, const T* __restrict__ xg,
-                                          int b, int e) {
-    constexpr int W = 16 / sizeof(T);
-    int bA = ((b + W - 1) / W) * W;
-    if (bA > e) bA = e;
-    T acc = T(0);
-    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
-    const int nvec = (e - bA) / W;
-    if constexpr (W == 4) {
-        const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
-        const float4* v4 = reinterpret_cast<const float4*>(v + bA);
-        for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const int4 c = __ldcs(ci4 + q);
-            const float4 w = __ldcs(v4 + q);
-            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
-                   w.w * __ldg(xg + c.w);
-        }
-    } else {
-        const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
-        const double2* v2 = reinterpret_cast<const double2*>(v + bA);
-        for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const int2 c = __ldcs(ci2 + q);
-            const double2 w = __ldcs(v2 + q);
-            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
-        }
-    }
-    for (int k = bA + nvec * W + threadIdx.x; k < e; k += kBlock)
-        acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
-    return block_total(acc);
-}
-
 // ---------------------------------------------------------------------------
 // Iteration kernels
 // ---------------------------------------------------------------------------
-
-// Epilogue traffic: every per-column array is streamed (evict-first loads and
-// stores) except x_bar, whose lines the dual kernel gathers next and should
-// find in L2; y likewise stays at normal priority for the next primal gather.
-template <class T>
-__device__ __forceinline__ void primal_epilogue(const FastIter<T>& a, const PV<T>& pv, int j,
-                                                T aty, int first, bool fresh, T tau) {
-    const T g = __ldcs(pv.c + j) - aty;
-    const T xo = __ldcs(a.it.x + j);
-    const T xn = clampT<T>(xo - tau * g, __ldcs(pv.lo + j), __ldcs(pv.hi + j));
-    a.it.xbar[j] = T(2) * xn - xo;
-    __stcs(a.it.x + j, xn);
-    if constexpr (std::is_same<T, float>::value) {
-        __stcs(a.it.psx + j, first ? xn : __ldcs(a.it.psx + j) + xn);
-    } else {
-        __stcs(a.it.xsum + j, fresh ? xn : __ldcs(a.it.xsum + j) + xn);
-    }
-}
-
-template <class T>
-__device__ __forceinline__ void dual_epilogue(const FastIter<T>& a, const PV<T>& pv, int i,
-                                              T ax, int first, bool fresh, T tau, T sigma) {
-    const T yo = a.it.y[i];
-    const T so = __ldcs(a.it.s + i);
-    const T sn = clampT<T>(so - tau * yo, __ldcs(pv.rlo + i), __ldcs(pv.rhi + i));
-    const T sbar = T(2) * sn - so;
-    const T yn = yo + sigma * (sbar - ax);
-    a.it.y[i] = yn;
-    __stcs(a.it.s + i, sn);
-    if constexpr (std::is_same<T, float>::value) {
-        __stcs(a.it.psy + i, first ? yn : __ldcs(a.it.psy + i) + yn);
-    } else {
-        __stcs(a.it.ysum + i, fresh ? yn : __ldcs(a.it.ysum + i) + yn);
-    }
-}
 
 // PRIMAL = true: rows of A^T gather y; false: rows of A gather x_bar.
 template <class T, int VW, bool PRIMAL>
@@ -222,23 +56,21 @@ __global__ void __launch_bounds__(kBlock) fast_iter(FastIter<T> a, int first, in
         const int lane = threadIdx.x & (VW - 1);
         const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
         if (r >= M.rows) return;
+        EpiIn<T> in{};
+        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
         const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
         if (e - b > kLongRow) return;  // the row's CTA handles it
         T acc = T(0);
         for (int k = b + lane; k < e; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
         if (VW > 1) acc = group_sum(acc, VW);
-        if (lane == 0) {
-            if (PRIMAL) primal_epilogue(a, pv, r, acc, first, fresh, tau);
-            else dual_epilogue(a, pv, r, acc, first, fresh, tau, sigma);
-        }
+        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     } else {
         const int r = __ldg(M.long_rows + (blockIdx.x - short_blocks));
+        EpiIn<T> in{};
+        if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
         const int b = __ldg(M.rp + r), e = __ldg(M.rp + r + 1);
         const T acc = long_row_dot<T>(M.ci, vals, xg, b, e);
-        if (threadIdx.x == 0) {
-            if (PRIMAL) primal_epilogue(a, pv, r, acc, first, fresh, tau);
-            else dual_epilogue(a, pv, r, acc, first, fresh, tau, sigma);
-        }
+        if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     }
 }
 
@@ -268,48 +100,6 @@ void launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Check kernel
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ double cs_term(double v, double act, double lo, double hi,
-                                          double bt) {
-    const bool at_lo = fb(lo) && fabs(act - lo) < bt;
-    const bool at_hi = fb(hi) && fabs(act - hi) < bt;
-    if (!at_lo && !at_hi) return fabs(v);
-    if (at_lo && !at_hi) return smax(0.0, -v);
-    if (at_hi && !at_lo) return smax(0.0, v);
-    return 0.0;
-}
-
-__device__ __forceinline__ double primal_term(double act, double lo, double hi) {
-    double p = 0.0;
-    if (fb(lo)) p = smax(p, lo - act);
-    if (fb(hi)) p = smax(p, act - hi);
-    return p;
-}
-
-__device__ __forceinline__ double clipped_inf(double coeff, double lo, double hi) {
-    if (coeff > 0.0) return fb(lo) ? coeff * lo : 0.0;
-    if (coeff < 0.0) return fb(hi) ? coeff * hi : 0.0;
-    return 0.0;
-}
-
-struct Terms {
-    double cp = 0, cd = 0, ap = 0, ad = 0;         // scaled: cur / avg, primal / dual
-    double ocp = 0, ocd = 0, oap = 0, oad = 0;     // original space
-    double pobj_c = 0, dobj_c = 0, pobj_a = 0, dobj_a = 0;
-};
-
-template <class T>
-__device__ __forceinline__ double avg_x(const Iterates<T>& it, int j, double inv) {
-    double s = it.xsum[j];
-    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psx[j]);
-    return s * inv;
-}
-template <class T>
-__device__ __forceinline__ double avg_y(const Iterates<T>& it, int i, double inv) {
-    double s = it.ysum[i];
-    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psy[i]);
-    return s * inv;
-}
 
 // Per-row terms, merged into the thread's running maxima / sums.
 template <class T>
