@@ -185,6 +185,29 @@ int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
                   double alpha, const double* x, double beta, double* y);
 int pdhg_project_box(int device, int32_t n, const double* lo, const double* hi, double* x);
 
+/* pdhg_csr_spmv for callers that cannot allocate device memory. This entry has
+ * no counterpart in the reference; it exists for code that must not call
+ * cudaMalloc or any allocating routine where it needs the product: frameworks
+ * that own every device byte through their own pool (an allocation behind the
+ * pool's back can fail or fragment it), latency-critical loops that must stay
+ * away from the driver's allocator (an allocation can synchronise the device).
+ * Every pointer is a DEVICE pointer the caller owns; the
+ * work is queued on `stream` (a cudaStream_t, NULL = default stream) on the
+ * current device and the call returns without waiting. Results are
+ * bit-identical to pdhg_csr_spmv's.
+ * The transposed product needs A^T: it is built in a fixed scratch array that
+ * every GPU loading this library reserves until exit (about 5 MB). Limits for
+ * transpose != 0: n <= 262,144 columns and nnz <= 262,144 nonzeros; larger
+ * sizes return PDHG_ERR_INVALID_ARGUMENT before any work is queued
+ * (transpose == 0 uses no scratch and has no limit). The first transposed call
+ * on a device looks up the scratch address for that device: make it before any
+ * stream capture. All calls share the one array, so calls that overlap on the
+ * GPU (different streams, no ordering between them) race; serialise them. */
+int pdhg_csr_spmv_noalloc(int transpose, int32_t m, int32_t n, int64_t nnz,
+                          const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                          const double* d_values, double alpha, const double* d_x, double beta,
+                          double* d_y, void* stream);
+
 /* Scaling::equilibrate(CsrMatrix) (src/l1/scaling.cpp:19-104) on the host
  * (FP64, the reference's order), for callers without a device. */
 int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,

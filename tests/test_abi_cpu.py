@@ -92,4 +92,5 @@ def test_header_documents_each_entry_with_a_reference_citation():
         block = src[src.rfind("/*", 0, end): i] + src[i: src.index("\n", semi)]
         assert re.search(r"\w+\.(?:cpp|hpp):\d+", block) or n in (
             "pdhg_abi_version", "pdhg_default_options", "pdhg_last_error",
-            "pdhg_profile_kernels", "pdhg_destroy", "pdhg_stream"), n
+            "pdhg_profile_kernels", "pdhg_destroy", "pdhg_stream",
+            "pdhg_csr_spmv_noalloc"), n
