@@ -163,6 +163,29 @@ int pdhg_load_problem(pdhg_ctx* ctx, int32_t m, int32_t n, int64_t nnz, const in
 int pdhg_solve(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* info, double* x,
                double* y, double* rc);
 
+/* Batched extension: `count` independent LPs solved together, each exactly as
+ * its own Pdhg::solve would (pdhg.cpp:218-502; the reference runs one per
+ * thread, race.cpp:126) -- own scaling, step sizes, restarts, termination and
+ * result -- in one device loop. The instances are stacked block-diagonally:
+ * instance k owns rows [row_off[k], row_off[k+1]) and columns
+ * [col_off[k], col_off[k+1]) of one CSR (row_ptr over all rows, col_idx global,
+ * each row's columns inside its instance's range); c, col_lo, col_hi (n) and
+ * row_lo, row_hi (m) are stacked the same way; obj_const and maximize have one
+ * entry per instance. Validation is per instance (problem.cpp:50-,
+ * sparse.cpp:94-128): an invalid instance gets PDHG_STATUS_NUMERICAL_FAILURE
+ * "invalid problem: ..." in its info and the others solve. Structure the
+ * stacking cannot hold (offsets, a column outside the instance) returns
+ * PDHG_ERR_INVALID_ARGUMENT. Precision MIXED or FP64 only; no checkpoint and
+ * no trace. x, y, rc are stacked like the inputs (any may be NULL); infos has
+ * `count` entries. A loaded batch stays on the context beside the single LP. */
+int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off,
+                    const int32_t* col_off, int64_t nnz, const int32_t* row_ptr,
+                    const int32_t* col_idx, const double* values, const double* c,
+                    const double* obj_const, const int* maximize, const double* col_lo,
+                    const double* col_hi, const double* row_lo, const double* row_hi);
+int pdhg_solve_batch(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* infos, double* x,
+                     double* y, double* rc);
+
 /* Per-kernel timing of the iteration kernels on the loaded problem (CUDA events
  * on the engine's stream around each launch, after `warmup` untimed iterations).
  * Runs `iterations` iterations from the state the last pdhg_solve left. */

@@ -461,8 +461,9 @@ static double original_residual(const orc_problem* p, double obj_sign, const dou
     if (rel != NULL) {
         /* Gap in the internal always-minimize sense (objective and duals times
          * obj_sign), where inf over the box is the weak-duality bound for
-         * either original sense. */
-        double bnorm = 0.0, cnorm = 0.0, pobj = obj_sign * p->obj_const, dobj = 0.0;
+         * either original sense. The objective constant shifts both sides. */
+        double bnorm = 0.0, cnorm = 0.0, pobj = obj_sign * p->obj_const;
+        double dobj = obj_sign * p->obj_const;
         for (int32_t i = 0; i < p->m; ++i) {
             if (finite_bound(p->row_lo[i])) bnorm = smax(bnorm, fabs(p->row_lo[i]));
             if (finite_bound(p->row_hi[i])) bnorm = smax(bnorm, fabs(p->row_hi[i]));

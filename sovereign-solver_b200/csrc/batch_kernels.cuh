@@ -1,0 +1,117 @@
+// batch_kernels.cuh -- device side of the batched engine (batch.cu).
+//
+// A batch is a block-diagonal LP: instance k owns rows [row_off[k],
+// row_off[k+1]) and columns [col_off[k], col_off[k+1]) of one CSR (and of its
+// device-built transpose). Each instance keeps its own PDHG state on the
+// device (InstState: step sizes, primal weight, Cesaro window, restart and
+// termination state), exactly the per-LP state of the single engine.
+//
+// Two kinds of kernels:
+//   * row kernels (iterations, power-iteration products, Ruiz maxima): the
+//     single engine's kernels with an instance lookup per row (row_inst /
+//     col_inst) for the instance's step sizes and done flag;
+//   * instance kernels: one CTA per instance (check + decision, restart,
+//     norms, Ruiz update, final result), so every per-instance reduction and
+//     decision is made inside one CTA without atomics or tickets.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "engine.cuh"
+
+namespace pdhg {
+
+struct InstState {
+    int done, status, converged, fresh;
+    int restart, restart_to_avg, avg_better, fold;
+    int fail_kind, ruiz_done, pw_done, valid;
+    int stalled, polished;  // mixed mode: FP32 phase stopped improving / finished in FP64
+    long long since_restart, restarts, stop_iter;
+    long long since_improve, switch_iter;
+    long long idle;  // global iterations a stalled instance waited for the FP64 phase
+    double best_res;
+    double res_last, res_prev_cand, cur_res, avg_res, orig_res, rel_kkt, inv;
+    double tau, sigma, omega, eta;
+    double obj_sign, obj_const, bnorm, cnorm, cnorm2_s, bnorm2_s;
+    double opnorm;
+    double objective, dual_objective, gap, pinf, dinf;
+};
+
+struct BatchGlobal {
+    int done;          // every instance finished (or the budget ended)
+    int active;        // instances still iterating
+    long long iter;    // iterations completed before the current period
+    long long checks;
+};
+
+struct BatchView {
+    int32_t count = 0, m = 0, n = 0;
+    const int32_t *row_off = nullptr, *col_off = nullptr;
+    const int32_t *row_inst = nullptr, *col_inst = nullptr;
+    DevCsr A, AT;    // scaled
+    DevCsr Ao, ATo;  // original
+    DevProblem P;    // vectors; obj_sign / obj_const are per instance
+    InstState* is = nullptr;
+    BatchGlobal* g = nullptr;
+    Mailbox* mail = nullptr;
+};
+
+struct BatchParams {
+    double tol, bound_tol, restart_decrease;
+    long long period;
+    int termination_rule, restart_rule, primal_weight_update;
+    int allow_switch;  // FP32 phase: hand a stalled instance over to FP64
+    double* x_last;
+    double* y_last;
+    double* act_avg;
+};
+
+// launchers (batch_kernels.cu)
+template <class T>
+void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, int first,
+                       cudaStream_t s);
+template <class T>
+void launch_batch_check(const BatchView& b, const Iterates<T>& it, const BatchParams& p,
+                        cudaStream_t s);
+template <class T>
+void launch_batch_restart(const BatchView& b, const Iterates<T>& it, const BatchParams& p,
+                          cudaStream_t s);
+void launch_batch_tick(const BatchView& b, long long period, long long budget_iters,
+                       cudaGraphConditionalHandle handle, int use_handle, cudaStream_t s);
+void launch_batch_fill_inst(const int32_t* off, int32_t count, int32_t* out, cudaStream_t s);
+void launch_batch_warm(const BatchView& b, double* x0, double* y0, cudaStream_t s);
+
+// power iteration per instance (estimate_operator_norm, pdhg.cpp:48-79)
+void launch_batch_pw_w(const BatchView& b, const double* u, const double* v, double* w,
+                       cudaStream_t s);
+void launch_batch_pw_norm_w(const BatchView& b, double* w, cudaStream_t s);
+void launch_batch_pw_u(const BatchView& b, const double* w, double* u, cudaStream_t s);
+void launch_batch_pw_norm_uv(const BatchView& b, const double* w, double* u, double* v,
+                             cudaStream_t s);
+void launch_batch_steps(const BatchView& b, double safety, int primal_weight, cudaStream_t s);
+
+// intake per instance (Scaling::equilibrate, scaling.cpp:19-104)
+void launch_batch_ruiz_max(const BatchView& b, const DevCsr& M, int transposed, const double* rs,
+                           const double* cs, double* out, cudaStream_t s);
+void launch_batch_ruiz_update(const BatchView& b, double* rs, double* cs, const double* row_max,
+                              const double* col_max, double tol, cudaStream_t s);
+void launch_batch_scale_vectors(const BatchView& b, double* c_s, double* lo_s, double* hi_s,
+                                double* rlo_s, double* rhi_s, cudaStream_t s);
+void launch_batch_norms(const BatchView& b, cudaStream_t s);
+
+// Internal status of an instance whose FP32 phase stalled (mixed mode).
+constexpr int kBatchStalled = 100;
+
+// FP32 iterates widened into the FP64 ones (the polish phase starts there).
+void launch_batch_widen(const BatchView& b, const Iterates<float>& f, const Iterates<double>& d,
+                        cudaStream_t s);
+
+// final result per instance (pdhg.cpp:420-498); `which`: -1 every instance,
+// 0 those not polished, 1 the polished ones.
+template <class T>
+void launch_batch_final(const BatchView& b, const Iterates<T>& it, double bound_tol,
+                        double* xo, double* yo, double* rc, int which, cudaStream_t s);
+
+}  // namespace pdhg

@@ -4,7 +4,10 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -38,10 +41,11 @@ struct DBuf {
 struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
-    DBuf<int32_t> rp, ci, long_rows;
+    DBuf<int32_t> rp, ci, long_rows, wrows;
     DBuf<double> v64;
     DBuf<float> v32;
-    int32_t n_long = 0, n_short = 0;
+    DBuf<char> tscratch;  // build_transpose scratch when this matrix is a transpose
+    int32_t n_long = 0, n_short = 0, n_wrows = 0;
     int vw = 1;
     DevCsr view() const {
         DevCsr d;
@@ -56,6 +60,8 @@ struct MatDev {
         d.n_long = n_long;
         d.n_short = n_short;
         d.vw = vw;
+        d.wrows = wrows.p;
+        d.n_wrows = n_wrows;
         return d;
     }
 };
@@ -86,25 +92,57 @@ inline cudaError_t to_float(DBuf<float>& d, const DBuf<double>& src, cudaStream_
     return cudaGetLastError();
 }
 
+// Opt-in phase timing for load and solve: with PDHG_B200_PHASE_TIMES=1 in the
+// environment every mark waits for the stream and prints, to stderr, the host
+// wall time since the previous mark. Off (no waits, no output) otherwise.
+inline bool phase_times_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("PDHG_B200_PHASE_TIMES");
+        return e != nullptr && e[0] == '1';
+    }();
+    return on;
+}
+
+struct PhaseClock {
+    bool on;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t;
+    explicit PhaseClock(cudaStream_t st)
+        : on(phase_times_enabled()), s(st), t(std::chrono::steady_clock::now()) {}
+    void mark(const char* what) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[pdhg phase] %-22s %10.3f ms\n", what,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+
 inline int cuda_fail(std::string* err, cudaError_t e, const char* what) {
     *err = std::string(what) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? PDHG_ERR_OUT_OF_MEMORY : PDHG_ERR_BACKEND;
 }
 
 // Row binning on the device: long-row list, short-row count, lanes per short
-// row (about half the mean short-row length, a power of two in [1, 32]).
+// row (about half the mean short-row length, a power of two in [1, 32]), and
+// the warp-row list of the ordered kernels.
 inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     cudaError_t e = M.long_rows.alloc(static_cast<size_t>(M.rows) + 1);
     if (e != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+    if ((e = M.wrows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
+        return cuda_fail(err, e, "bin_matrix");
     DBuf<unsigned long long> cnt;
-    if ((e = cnt.alloc(3)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
-    cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), s);
+    if ((e = cnt.alloc(6)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+    cudaMemsetAsync(cnt.p, 0, 6 * sizeof(unsigned long long), s);
     launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
-    unsigned long long h[3];
+    launch_bin(M.rp.p, M.rows, kWarpRow, M.wrows.p, cnt.p + 3, s);
+    unsigned long long h[6];
     cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     M.n_long = static_cast<int32_t>(h[0]);
     M.n_short = static_cast<int32_t>(h[1]);
+    M.n_wrows = static_cast<int32_t>(h[3]);
     const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
     int w = 1;
     while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;
@@ -112,10 +150,19 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     return PDHG_OK;
 }
 
-// A from host arrays (read in place) and A^T built on the device, both binned.
-inline int upload_matrix(int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,
-                         const int32_t* ci, const double* v, MatDev& M, MatDev& MT,
-                         cudaStream_t s, std::string* err) {
+// row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,
+// non-decreasing. Every device kernel that walks rows relies on it.
+inline bool row_ptr_ok(int32_t rows, int64_t nnz, const int32_t* rp) {
+    if (rp[0] != 0 || rp[rows] != nnz) return false;
+    for (int32_t r = 0; r < rows; ++r)
+        if (rp[r] > rp[r + 1]) return false;
+    return true;
+}
+
+// A's arrays to the device, read in place from the caller's host buffers.
+inline int upload_csr(int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,
+                      const int32_t* ci, const double* v, MatDev& M, cudaStream_t s,
+                      std::string* err) {
     cudaError_t e;
     M.rows = rows;
     M.cols = cols;
@@ -123,20 +170,71 @@ inline int upload_matrix(int32_t rows, int32_t cols, int64_t nnz, const int32_t*
     if ((e = upload(M.rp, rp, static_cast<size_t>(rows) + 1, s)) != cudaSuccess ||
         (e = upload(M.ci, ci, static_cast<size_t>(nnz), s)) != cudaSuccess ||
         (e = upload(M.v64, v, static_cast<size_t>(nnz), s)) != cudaSuccess)
-        return cuda_fail(err, e, "upload_matrix");
-    MT.rows = cols;
-    MT.cols = rows;
-    MT.nnz = nnz;
-    if ((e = MT.rp.alloc(static_cast<size_t>(cols) + 1)) != cudaSuccess ||
-        (e = MT.ci.alloc(static_cast<size_t>(nnz))) != cudaSuccess ||
-        (e = MT.v64.alloc(static_cast<size_t>(nnz))) != cudaSuccess)
-        return cuda_fail(err, e, "upload_matrix");
+        return cuda_fail(err, e, "upload_csr");
+    return PDHG_OK;
+}
+
+// The device problem checks (launch_validate) on data already resident;
+// *flags gets the OR of the failing kinds (0: nothing failed).
+inline int device_checks(const MatDev& M, const double* c, const double* clo, const double* chi,
+                         const double* rlo, const double* rhi, unsigned* flags, cudaStream_t s,
+                         std::string* err) {
+    DBuf<unsigned> f;
+    cudaError_t e = f.alloc(1);
+    if (e != cudaSuccess) return cuda_fail(err, e, "device_checks");
+    cudaMemsetAsync(f.p, 0, sizeof(unsigned), s);
+    launch_validate(M.rows, M.cols, M.rp.p, M.ci.p, M.v64.p, c, clo, chi, rlo, rhi, M.nnz, f.p, s);
+    cudaMemcpyAsync(flags, f.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "device_checks");
+    return PDHG_OK;
+}
+
+// A^T built on the device from the resident A, then both binned.
+inline int finish_matrix(MatDev& M, MatDev& MT, cudaStream_t s, std::string* err) {
+    cudaError_t e;
+    PhaseClock pc(s);
+    MT.rows = M.cols;
+    MT.cols = M.rows;
+    MT.nnz = M.nnz;
+    if ((e = MT.rp.alloc(static_cast<size_t>(M.cols) + 1)) != cudaSuccess ||
+        (e = MT.ci.alloc(static_cast<size_t>(M.nnz))) != cudaSuccess ||
+        (e = MT.v64.alloc(static_cast<size_t>(M.nnz))) != cudaSuccess)
+        return cuda_fail(err, e, "finish_matrix");
+    if ((e = MT.tscratch.alloc(transpose_scratch_bytes(M.rows, M.cols, M.nnz))) != cudaSuccess)
+        return cuda_fail(err, e, "finish_matrix");
     TransposeOut out{MT.rp.p, MT.ci.p, MT.v64.p};
-    if (build_transpose(rows, cols, nnz, M.rp.p, M.ci.p, M.v64.p, out, s) != 0)
+    if (build_transpose(M.rows, M.cols, M.nnz, M.rp.p, M.ci.p, M.v64.p, out, MT.tscratch.p, s) != 0)
         return cuda_fail(err, cudaGetLastError(), "build_transpose");
+    pc.mark("matrix: transpose");
     int rc = bin_matrix(M, s, err);
     if (rc != PDHG_OK) return rc;
-    return bin_matrix(MT, s, err);
+    rc = bin_matrix(MT, s, err);
+    pc.mark("matrix: bins");
+    return rc;
+}
+
+// A matrix on its own (no problem around it): row_ptr checked on the host and
+// the column indices on the device, then A^T and the bins. A matrix whose
+// structure would send a kernel out of bounds returns PDHG_ERR_INVALID_ARGUMENT
+// before any kernel indexes by it; unsorted columns and non-finite values are
+// the caller's (the product is formed as given).
+inline int upload_matrix(int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,
+                         const int32_t* ci, const double* v, MatDev& M, MatDev& MT,
+                         cudaStream_t s, std::string* err) {
+    if (!row_ptr_ok(rows, nnz, rp)) {
+        *err = "invalid CSR matrix: row_ptr must start at 0, end at nnz and not decrease";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    int rc = upload_csr(rows, cols, nnz, rp, ci, v, M, s, err);
+    if (rc != PDHG_OK) return rc;
+    unsigned flags = 0;
+    rc = device_checks(M, nullptr, nullptr, nullptr, nullptr, nullptr, &flags, s, err);
+    if (rc != PDHG_OK) return rc;
+    if (flags & 4u) {
+        *err = "invalid CSR matrix: column index out of range";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    return finish_matrix(M, MT, s, err);
 }
 
 }  // namespace pdhg

@@ -13,6 +13,7 @@
 // cancellation reach the device through a host-mapped mailbox that the check
 // reads (granularity: one check period, where the reference polls every
 // iteration, pdhg.cpp:288-293).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -89,7 +90,10 @@ struct Ctx {
     GraphSig graph_sig;
     long long launches = 0;
 
+    BatchCtx* batch = nullptr;  // pdhg_load_batch / pdhg_solve_batch
+
     ~Ctx() {
+        if (batch != nullptr) batch_delete(batch);
         if (graph != nullptr) cudaGraphExecDestroy(graph);
         if (mail != nullptr) cudaFreeHost(mail);
         if (stream != nullptr) cudaStreamDestroy(stream);
@@ -152,6 +156,7 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     const int32_t m = c.lp.m, n = c.lp.n;
     const int64_t nnz = c.Ao.nnz;
     c.sp = sp;
+    PhaseClock pc(s);
     CK(c.rs_d.alloc(static_cast<size_t>(m) + 1));
     CK(c.cs_d.alloc(static_cast<size_t>(n) + 1));
     launch_fill(c.rs_d.p, m, 1.0, s);
@@ -166,8 +171,10 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     if (sp.apply_ruiz)  // scaling.cpp:36-74
         for (int sweep = 0; sweep < sp.ruiz_iterations; ++sweep)
             launch_ruiz_sweep(A, AT, c.rs_d.p, c.cs_d.p, rbuf.p, cbuf.p, sp.ruiz_tolerance, is.p, s);
+    pc.mark("scale: ruiz");
     if (sp.apply_pock_chambolle)  // scaling.cpp:80-101
         launch_pock_chambolle(A, AT, c.rs_d.p, c.cs_d.p, rbuf.p, cbuf.p, sp.pock_chambolle_alpha, s);
+    pc.mark("scale: pock-chambolle");
     // scaled values of A and A^T; entries the reference's rebuild drops are counted
     DBuf<unsigned long long> dropped;
     CK(dropped.alloc(1));
@@ -209,10 +216,12 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
         CK(c.ATs.rp.alloc(static_cast<size_t>(n) + 1));
         CK(c.ATs.ci.alloc(static_cast<size_t>(nk)));
         CK(c.ATs.v64.alloc(static_cast<size_t>(nk)));
+        CK(c.ATs.tscratch.alloc(transpose_scratch_bytes(m, n, nk)));
         TransposeOut out{c.ATs.rp.p, c.ATs.ci.p, c.ATs.v64.p};
-        if (build_transpose(m, n, nk, c.As.rp.p, c.As.ci.p, c.As.v64.p, out, s) != 0)
+        if (build_transpose(m, n, nk, c.As.rp.p, c.As.ci.p, c.As.v64.p, out, c.ATs.tscratch.p, s) != 0)
             return fail(c, cudaGetLastError(), "build_transpose");
     }
+    pc.mark("scale: values");
     CK(to_float(c.As.v32, c.As.v64, s));
     CK(to_float(c.ATs.v32, c.ATs.v64, s));
     int rc = bin_matrix(c.As, s, &c.err);
@@ -238,6 +247,7 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     IntakeState h;
     CK(cudaMemcpyAsync(&h, is.p, sizeof h, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    pc.mark("scale: bins, vectors");
     c.cnorm2_s = std::sqrt(h.norms[0]);
     c.bnorm2_s = std::sqrt(h.norms[1]);
     c.cnorm = h.norms[2];
@@ -338,8 +348,9 @@ int alloc_iterates(Ctx& c, bool f32) {
     CK(c.act_avg.alloc(m));
     CK(c.cand_xo.alloc(n));
     CK(c.cand_yo.alloc(m));
-    const int g = std::max(fast_check_grid(c.As.view(), c.ATs.view()),
-                           static_cast<int>((c.lp.m + kBlock - 1) / kBlock + (c.lp.n + kBlock - 1) / kBlock) + 1);
+    const int g = std::max({fast_check_grid(c.As.view(), c.ATs.view()),
+                            exact_check_grid(c.As.view(), c.ATs.view()),
+                            exact_check_grid(c.Ao.view(), c.ATo.view())}) + 1;
     CK(c.part.alloc(static_cast<size_t>(g) * 4 + 4));
     CK(c.bx.alloc(n));
     CK(c.by.alloc(m));
@@ -724,14 +735,17 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     sp.pock_chambolle_alpha = o.pock_chambolle_alpha;
     sp.apply_ruiz = o.apply_ruiz != 0;
     sp.apply_pock_chambolle = o.apply_pock_chambolle != 0;
+    PhaseClock pc(c.stream);
     int rc = ensure_scaled(c, sp);
     if (rc != PDHG_OK) return rc;
+    pc.mark("solve: scaling");
     if (!c.have_opnorm || c.opnorm_iters != o.power_iterations) {
         rc = operator_norm(c, o.power_iterations, &c.opnorm);
         if (rc != PDHG_OK) return rc;
         c.have_opnorm = true;
         c.opnorm_iters = o.power_iterations;
     }
+    pc.mark("solve: operator norm");
     const double op = c.opnorm;
     info->operator_norm_estimate = op;  // pdhg.cpp:261-265
     const double step = (op > 1e-9) ? o.step_size_safety / op : o.step_size_safety;
@@ -799,6 +813,7 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
+    pc.mark("solve: initial point");
     CK(cudaEventRecord(ev0, c.stream));
     long long fp64_its = 0;
     if (!early) {
@@ -835,6 +850,7 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     cudaEventElapsedTime(&loop_ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    pc.mark("solve: iterations");
 
     DevState h;
     CK(cudaMemcpy(&h, c.st.p, sizeof h, cudaMemcpyDeviceToHost));
@@ -881,6 +897,7 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     if (y != nullptr && m) CK(cudaMemcpyAsync(y, c.yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
     if (rcv != nullptr && n) CK(cudaMemcpyAsync(rcv, c.rc.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    pc.mark("solve: result, download");
     info->objective = h.objective;
     info->primal_infeasibility = h.pinf;
     info->dual_infeasibility = h.dinf;
@@ -931,16 +948,37 @@ int load(Ctx& c, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
     view.row_lo = row_lo;
     view.row_hi = row_hi;
     c.loaded = true;
-    c.valid = validate_lp(view, &c.why);
-    if (!c.valid) return PDHG_OK;
-    int rc = upload_matrix(m, n, nnz, row_ptr, col_idx, values, c.Ao, c.ATo, c.stream, &c.err);
-    if (rc != PDHG_OK) return rc;
+    PhaseClock pc(c.stream);
+    // Validation (problem.cpp:50-, sparse.cpp:94-128). row_ptr and the
+    // objective constant are checked here; everything else on the device
+    // after the upload. Whenever anything fails, the host check runs over the
+    // whole problem for the reference's first failure and message.
+    if (!std::isfinite(obj_const) || !row_ptr_ok(m, nnz, row_ptr)) {
+        c.valid = validate_lp(view, &c.why);
+        if (!c.valid) return PDHG_OK;
+    }
     cudaStream_t s = c.stream;
+    int rc = upload_csr(m, n, nnz, row_ptr, col_idx, values, c.Ao, s, &c.err);
+    if (rc != PDHG_OK) return rc;
     CK(upload(c.c_o, cv, static_cast<size_t>(n), s));
     CK(upload(c.lo_o, col_lo, static_cast<size_t>(n), s));
     CK(upload(c.hi_o, col_hi, static_cast<size_t>(n), s));
     CK(upload(c.rlo_o, row_lo, static_cast<size_t>(m), s));
     CK(upload(c.rhi_o, row_hi, static_cast<size_t>(m), s));
+    pc.mark("load: upload");
+    unsigned flags = 0;
+    rc = device_checks(c.Ao, c.c_o.p, c.lo_o.p, c.hi_o.p, c.rlo_o.p, c.rhi_o.p, &flags, s, &c.err);
+    if (rc != PDHG_OK) return rc;
+    pc.mark("load: device checks");
+    c.valid = true;
+    c.why.clear();
+    if (flags != 0) {
+        c.valid = validate_lp(view, &c.why);
+        if (!c.valid) return PDHG_OK;
+    }
+    rc = finish_matrix(c.Ao, c.ATo, s, &c.err);
+    if (rc != PDHG_OK) return rc;
+    pc.mark("load: transpose, bins");
     return ensure_scaled(c, ScalingParams{});
 }
 
@@ -1153,8 +1191,11 @@ int pdhg_load_problem(pdhg_ctx* ctx, int32_t m, int32_t n, int64_t nnz, const in
                       const double* col_hi, const double* row_lo, const double* row_hi) {
     if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
     try {
-        return pdhg::load(ctx->c, m, n, nnz, row_ptr, col_idx, values, c, obj_const, maximize,
-                          col_lo, col_hi, row_lo, row_hi);
+        pdhg::PhaseClock pc(ctx->c.stream);
+        const int rc = pdhg::load(ctx->c, m, n, nnz, row_ptr, col_idx, values, c, obj_const,
+                                  maximize, col_lo, col_hi, row_lo, row_hi);
+        pc.mark("pdhg_load_problem");
+        return rc;
     } catch (const std::bad_alloc&) {
         ctx->c.err = "host allocation failed";
         return PDHG_ERR_OUT_OF_MEMORY;
@@ -1171,7 +1212,10 @@ int pdhg_solve(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* info, doub
     if (options == nullptr) pdhg_default_options(&o);
     else o = *options;
     try {
-        return pdhg::solve(ctx->c, o, info, x, y, rc);
+        pdhg::PhaseClock pc(ctx->c.stream);
+        const int r = pdhg::solve(ctx->c, o, info, x, y, rc);
+        pc.mark("pdhg_solve");
+        return r;
     } catch (const std::bad_alloc&) {
         ctx->c.err = "host allocation failed";
         return PDHG_ERR_OUT_OF_MEMORY;
@@ -1190,6 +1234,46 @@ int pdhg_profile_kernels(pdhg_ctx* ctx, int precision, int warmup, int iteration
         return pdhg::profile(ctx->c, precision, warmup, iterations, out);
     } catch (const std::exception& e) {
         ctx->c.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
+int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off, const int32_t* col_off,
+                    int64_t nnz, const int32_t* row_ptr, const int32_t* col_idx,
+                    const double* values, const double* c, const double* obj_const,
+                    const int* maximize, const double* col_lo, const double* col_hi,
+                    const double* row_lo, const double* row_hi) {
+    if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg::Ctx& cx = ctx->c;
+    try {
+        if (cudaSetDevice(cx.device) != cudaSuccess) return PDHG_ERR_BACKEND;
+        if (cx.batch == nullptr) {
+            cx.batch = pdhg::batch_new(cx.device, cx.stream, cx.err);
+            if (cx.batch == nullptr) {
+                cx.err = "pdhg_load_batch: cannot allocate the batch state";
+                return PDHG_ERR_OUT_OF_MEMORY;
+            }
+        }
+        return pdhg::batch_load_abi(*cx.batch, count, row_off, col_off, nnz, row_ptr, col_idx,
+                                    values, c, obj_const, maximize, col_lo, col_hi, row_lo, row_hi);
+    } catch (const std::exception& e) {
+        cx.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
+int pdhg_solve_batch(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* infos, double* x,
+                     double* y, double* rc) {
+    if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg::Ctx& cx = ctx->c;
+    if (cx.batch == nullptr || pdhg::batch_count(*cx.batch) == 0) {
+        cx.err = "pdhg_solve_batch: no batch loaded";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        return pdhg::batch_solve_abi(*cx.batch, options, infos, x, y, rc);
+    } catch (const std::exception& e) {
+        cx.err = e.what();
         return PDHG_ERR_BACKEND;
     }
 }

@@ -19,6 +19,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
+
+#include "../../include/pdhg_b200.h"
 
 namespace pdhg {
 
@@ -38,9 +41,15 @@ struct DevCsr {
     int32_t n_long = 0;
     int32_t n_short = 0;
     int vw = 1;
+    // Row binning for the ordered (FP64-exact) kernels: rows longer than
+    // kWarpRow are listed in wrows and handled one warp per row; without the
+    // list every row runs on one thread.
+    const int32_t* wrows = nullptr;
+    int32_t n_wrows = 0;
 };
 
 constexpr int kLongRow = 512;
+constexpr int kWarpRow = 32;
 
 // Accumulator slots (bit patterns of non-negative doubles, combined with
 // atomicMax -- order-independent, so exact).
@@ -250,6 +259,7 @@ void launch_spmv_exact(const DevCsr& A, double alpha, const double* x, double be
 void launch_spmvT_exact(const DevCsr& AT, double alpha, const double* x, double beta, double* y,
                         cudaStream_t s);
 int fast_check_grid(const DevCsr& A, const DevCsr& AT);
+int exact_check_grid(const DevCsr& A, const DevCsr& AT);  // blocks of an exact check / final launch
 void launch_project_box(int32_t n, const double* lo, const double* hi, double* x,
                         cudaStream_t s);
 
@@ -261,8 +271,11 @@ struct TransposeOut {
     int32_t* ci;
     double* v;
 };
+// The transpose works in caller-owned scratch of transpose_scratch_bytes()
+// bytes (256-byte aligned), so repeated loads of one size reuse it.
+size_t transpose_scratch_bytes(int32_t m, int32_t n, int64_t nnz);
 int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci,
-                    const double* v, TransposeOut out, cudaStream_t s);
+                    const double* v, TransposeOut out, void* scratch, cudaStream_t s);
 
 void launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
 
@@ -273,6 +286,12 @@ struct IntakeState {
     int ruiz_done;             // set when a sweep's worst < tolerance (scaling.cpp:72)
     double norms[4];           // |c_s|^2, |b_s|^2, max|c_o|, max finite |row bound|
 };
+// Device problem checks, OR-ed into *flags: 1 a column, 2 a row, 4 an entry's
+// column out of range, 8 an entry out of order or non-finite. c == NULL skips
+// the column checks and rlo == NULL the row checks.
+void launch_validate(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                     const double* c, const double* clo, const double* chi, const double* rlo,
+                     const double* rhi, int64_t nnz, unsigned* flags, cudaStream_t s);
 void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                 unsigned long long* counters, cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
@@ -295,5 +314,19 @@ void launch_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
                   const double* rhi_o, double* part, IntakeState* is, cudaStream_t s);
 // Inclusive prefix sum of n int32 counts into out[1..n], out[0] = 0 (CUB).
 int prefix_rows(const int32_t* cnt, int32_t n, int32_t* out, cudaStream_t s);
+
+// The batched engine (batch.cu), owned by a context: it uses the context's
+// stream and writes its errors into the context's error text.
+struct BatchCtx;
+BatchCtx* batch_new(int device, cudaStream_t stream, std::string& err);
+void batch_delete(BatchCtx* b);
+int batch_load_abi(BatchCtx& c, int32_t count, const int32_t* row_off, const int32_t* col_off,
+                   int64_t nnz, const int32_t* rp, const int32_t* ci, const double* v,
+                   const double* cv, const double* obj_const, const int* maximize,
+                   const double* col_lo, const double* col_hi, const double* row_lo,
+                   const double* row_hi);
+int batch_solve_abi(BatchCtx& c, const pdhg_options* options, pdhg_info* infos, double* x,
+                    double* y, double* rc);
+int32_t batch_count(const BatchCtx& c);
 
 }  // namespace pdhg

@@ -6,16 +6,19 @@
 //   * Ruiz row/column maxima of |a| * r_i * c_j are order-free (max), each
 //     product formed as (|a| * r_i) * c_j like scaling.cpp:48-50;
 //   * the update r_i /= sqrt(max) uses IEEE sqrt and division;
-//   * Pock-Chambolle sums are added by one thread per row (per A^T row for the
-//     columns) in the reference's order (CSR order for rows, ascending row for
-//     columns, scaling.cpp:85-96); with alpha = 1 the exponents are 1 and the
+//   * Pock-Chambolle sums are added per row (per A^T row for the columns) in
+//     the reference's order (CSR order for rows, ascending row for columns,
+//     scaling.cpp:85-96), by one thread or, for long rows, one warp that adds
+//     in the same order (ordered.cuh); with alpha = 1 the exponents are 1 and the
 //     term is the magnitude itself (pow(m, 1) == m exactly), other alphas call
 //     the device pow;
 //   * the early exit of the Ruiz sweeps (worst < tolerance) is decided by the
 //     last CTA of each update and read by the next sweep's kernels.
+#include <algorithm>
 #include <cmath>
 
 #include "engine.cuh"
+#include "ordered.cuh"
 
 namespace pdhg {
 
@@ -42,6 +45,46 @@ __device__ __forceinline__ unsigned group_mask(int vw) {
     if (vw >= 32) return 0xffffffffu;
     const unsigned base = (threadIdx.x & 31u) & ~static_cast<unsigned>(vw - 1);
     return ((1u << vw) - 1u) << base;
+}
+
+// Problem checks of Problem::validate (src/io/problem.cpp:50-) and
+// CsrMatrix::validate (src/l0/sparse.cpp:94-128) as flags: bit 0 a column
+// (non-finite cost, NaN or crossed bounds), bit 1 a row (NaN or crossed
+// bounds), bit 2 an entry's column out of range, bit 3 an entry not strictly
+// ascending in its row or with a non-finite value. row_ptr itself must already be known monotone and
+// within [0, nnz]. Which item fails first, and the message, is left to the
+// host check, which only runs when a flag is set. Entries are checked by
+// groups of `lanes` threads per row. c == NULL skips the column checks,
+// rlo == NULL the row checks (a matrix on its own).
+__global__ void __launch_bounds__(kBlock) k_validate(int32_t m, int32_t n, const int32_t* rp,
+                                                     const int32_t* ci, const double* v,
+                                                     const double* c, const double* clo,
+                                                     const double* chi, const double* rlo,
+                                                     const double* rhi, int lanes,
+                                                     unsigned* flags) {
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kBlock;
+    const int64_t t0 = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    unsigned bad = 0;
+    for (int64_t j = t0; c != nullptr && j < n; j += stride) {
+        const double lo = clo[j], hi = chi[j];
+        if (!isfinite(c[j]) || isnan(lo) || isnan(hi) || lo > hi) bad |= 1u;
+    }
+    for (int64_t i = t0; rlo != nullptr && i < m; i += stride) {
+        const double lo = rlo[i], hi = rhi[i];
+        if (isnan(lo) || isnan(hi) || lo > hi) bad |= 2u;
+    }
+    const int64_t groups = static_cast<int64_t>(m) * lanes;
+    for (int64_t g = t0; g < groups; g += stride) {
+        const int64_t r = g / lanes;
+        const int b = rp[r], e = rp[r + 1];
+        for (int k = b + static_cast<int>(g % lanes); k < e; k += lanes) {
+            const int col = ci[k];
+            if (col < 0 || col >= n) bad |= 4u;
+            if ((k > b && ci[k - 1] >= col) || !isfinite(v[k])) bad |= 8u;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicOr(flags, bad);
 }
 
 // Row lengths -> long-row list, number and total length of short rows
@@ -156,27 +199,40 @@ __device__ __forceinline__ double pc_term(double mag, double e) {
 
 // Pock-Chambolle sums, one thread per row, in the reference's order; the
 // loads of four entries are issued before their terms are added.
-__global__ void k_pc_sum(DevCsr M, int transposed, const double* rs, const double* cs,
-                         double expo, double* out) {
-    const int r = blockIdx.x * kBlock + threadIdx.x;
-    if (r >= M.rows) return;
-    double sum = 0.0;
+// Skipped entries (magnitude 0) are added as +0.0 in the warp path: the sum
+// starts at +0.0 and every term is >= +0.0, so adding +0.0 changes no bit.
+__global__ void __launch_bounds__(kBlock) k_pc_sum(DevCsr M, int transposed, const double* rs,
+                                                   const double* cs, double expo, double* out) {
+    const RowTask t = row_task(M, blockIdx.x);
+    if (t.row < 0) return;
+    const int r = t.row;
     const int b = M.rp[r], e = M.rp[r + 1];
-    int k = b;
-    for (; k + 4 <= e; k += 4) {
-        double mg[4];
+    double sum = 0.0;
+    if (t.warp) {
+        sum = ordered_sum_warp(
+            b, e,
+            [&](int k) {
+                const double mag = scaled_mag(M, transposed, rs, cs, r, k);
+                return mag > 0.0 ? pc_term(mag, expo) : 0.0;
+            },
+            0.0, warp_stage());
+    } else {
+        int k = b;
+        for (; k + 4 <= e; k += 4) {
+            double mg[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) mg[u] = scaled_mag(M, transposed, rs, cs, r, k + u);
+            for (int u = 0; u < 4; ++u) mg[u] = scaled_mag(M, transposed, rs, cs, r, k + u);
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (mg[u] > 0.0) sum = __dadd_rn(sum, pc_term(mg[u], expo));
+            for (int u = 0; u < 4; ++u)
+                if (mg[u] > 0.0) sum = __dadd_rn(sum, pc_term(mg[u], expo));
+        }
+        for (; k < e; ++k) {
+            const double mag = scaled_mag(M, transposed, rs, cs, r, k);
+            if (mag <= 0.0) continue;
+            sum = __dadd_rn(sum, pc_term(mag, expo));
+        }
     }
-    for (; k < e; ++k) {
-        const double mag = scaled_mag(M, transposed, rs, cs, r, k);
-        if (mag <= 0.0) continue;
-        sum = __dadd_rn(sum, pc_term(mag, expo));
-    }
-    out[r] = sum;
+    if (t.lead) out[r] = sum;
 }
 
 __global__ void k_pc_update(int32_t m, int32_t n, double* rs, double* cs, const double* row_sum,
@@ -186,25 +242,40 @@ __global__ void k_pc_update(int32_t m, int32_t n, double* rs, double* cs, const 
     if (t < n && col_sum[t] > 0.0) cs[t] /= safe_sqrt(col_sum[t]);
 }
 
+// Lanes per row for the elementwise row kernels: the mean row length rounded
+// up to a power of two in [1, 32].
+inline int row_lanes(int32_t rows, int64_t nnz) {
+    const int64_t mean = rows > 0 ? (nnz + rows - 1) / rows : 1;
+    int w = 1;
+    while (w < 32 && w < mean) w *= 2;
+    return w;
+}
+
 // Scaled values (v * rs_i) * cs_j (Scaling::apply, scaling.cpp:127-128);
 // counts entries the rebuild would drop (|v| <= 1e-14, sparse.cpp:55).
-// Elementwise: a warp walks each row, so long rows spread over 32 lanes.
-__global__ void k_scale_values(DevCsr M, int transposed, const double* rs, const double* cs,
-                               double* out, unsigned long long* dropped) {
-    const int64_t warp = (blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+// Elementwise: groups of `lanes` threads walk a row each (four entries per
+// lane in flight), so short and long rows both keep the lanes busy.
+__global__ void __launch_bounds__(kBlock) k_scale_values(DevCsr M, int transposed, const double* rs,
+                                                         const double* cs, double* out,
+                                                         unsigned long long* dropped, int lanes) {
+    const int64_t tid = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    const int64_t r64 = tid / lanes;
+    const int sub = static_cast<int>(tid % lanes);
     unsigned long long d = 0;
-    if (warp < M.rows) {
-        const int r = static_cast<int>(warp);
-        for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
-            const int c = M.ci[k];
-            const double v = transposed ? M.v64[k] * rs[c] * cs[r] : M.v64[k] * rs[r] * cs[c];
+    if (r64 < M.rows) {
+        const int r = static_cast<int>(r64);
+        const int e = M.rp[r + 1];
+        const double rr = transposed ? cs[r] : rs[r];
+        const double* other = transposed ? rs : cs;
+#pragma unroll 4
+        for (int k = M.rp[r] + sub; k < e; k += lanes) {
+            const double v = transposed ? M.v64[k] * other[M.ci[k]] * rr : M.v64[k] * rr * other[M.ci[k]];
             out[k] = v;
             d += fabs(v) <= 1e-14 ? 1ull : 0ull;
         }
     }
     for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-    if (lane == 0 && d) atomicAdd(dropped, d);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(dropped, d);
 }
 
 // Kept-entry counts per row (the compaction path when entries are dropped).
@@ -347,16 +418,19 @@ void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs
 void launch_pock_chambolle(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
                            double* row_sum, double* col_sum, double alpha, cudaStream_t s) {
     // both sums from the factors before this step (scaling.cpp:85-96), then the update
-    if (A.rows > 0) k_pc_sum<<<nblocks(A.rows), kBlock, 0, s>>>(A, 0, rs, cs, 2.0 - alpha, row_sum);
-    if (AT.rows > 0) k_pc_sum<<<nblocks(AT.rows), kBlock, 0, s>>>(AT, 1, rs, cs, alpha, col_sum);
+    if (A.rows > 0) k_pc_sum<<<mat_blocks(A), kBlock, 0, s>>>(A, 0, rs, cs, 2.0 - alpha, row_sum);
+    if (AT.rows > 0) k_pc_sum<<<mat_blocks(AT), kBlock, 0, s>>>(AT, 1, rs, cs, alpha, col_sum);
     const int32_t nmax = A.rows > AT.rows ? A.rows : AT.rows;
     if (nmax > 0) k_pc_update<<<nblocks(nmax), kBlock, 0, s>>>(A.rows, AT.rows, rs, cs, row_sum, col_sum);
 }
 
 void launch_scale_values(const DevCsr& M, int transposed, const double* rs, const double* cs,
                          double* out, unsigned long long* dropped, cudaStream_t s) {
-    if (M.rows > 0)
-        k_scale_values<<<nblocks(static_cast<int64_t>(M.rows) * 32), kBlock, 0, s>>>(M, transposed, rs, cs, out, dropped);
+    if (M.rows > 0) {
+        const int lanes = row_lanes(M.rows, M.nnz);
+        k_scale_values<<<nblocks(static_cast<int64_t>(M.rows) * lanes), kBlock, 0, s>>>(
+            M, transposed, rs, cs, out, dropped, lanes);
+    }
 }
 
 void launch_kept_counts(const DevCsr& M, const double* vs, int32_t* cnt, cudaStream_t s) {
@@ -376,6 +450,16 @@ void launch_scale_vectors(int32_t m, int32_t n, const double* rs, const double* 
     if (nmax > 0)
         k_scale_vectors<<<nblocks(nmax), kBlock, 0, s>>>(m, n, rs, cs, c, lo, hi, rlo, rhi, sign,
                                                          c_s, lo_s, hi_s, rlo_s, rhi_s);
+}
+
+void launch_validate(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                     const double* c, const double* clo, const double* chi, const double* rlo,
+                     const double* rhi, int64_t nnz, unsigned* flags, cudaStream_t s) {
+    const int lanes = row_lanes(m, nnz);
+    const int64_t work = std::max<int64_t>(std::max<int64_t>(m, n), static_cast<int64_t>(m) * lanes);
+    int g = work > 0 ? nblocks(work) : 1;
+    if (g > kGridCap) g = kGridCap;
+    k_validate<<<g, kBlock, 0, s>>>(m, n, rp, ci, v, c, clo, chi, rlo, rhi, lanes, flags);
 }
 
 int norms_part_size(int32_t m, int32_t n) { return 4 * (kGridCap + 1); }

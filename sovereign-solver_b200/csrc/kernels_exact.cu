@@ -4,8 +4,10 @@
 // (src/l0/sparse.cpp:130-154) add every sum sequentially, in row (or column)
 // order, with a separate rounding for each product and each addition (its
 // Release build targets generic x86-64: no FMA). These kernels give each row
-// of A (or of A^T) to one thread, which adds the products in the same order
-// with __dmul_rn / __dadd_rn, so nothing is contracted and nothing reordered.
+// of A (or of A^T) to one thread -- or, for rows longer than kWarpRow, to one
+// warp whose lanes evaluate the products together and then add them in row
+// order -- with __dmul_rn / __dadd_rn, so nothing is contracted and nothing
+// reordered.
 // Max-reductions are exact in any order and use atomicMax on the bit patterns
 // of non-negative doubles. Decisions (restart, termination) are taken by the
 // last CTA of each check kernel, on the device.
@@ -19,6 +21,7 @@
 #include <cstdio>
 
 #include "engine.cuh"
+#include "ordered.cuh"
 
 namespace pdhg {
 
@@ -90,27 +93,6 @@ __host__ __device__ inline int blocks_for(int64_t n) {
     return static_cast<int>((n + kBlock - 1) / kBlock);
 }
 
-// acc = init; for k in [b, e): acc = acc + v[k] * g(ci[k]), rounded after each
-// product and each sum, in k order. The loads of four terms are issued before
-// their products are added, so the memory latency of a long row overlaps while
-// the sum keeps the reference's order exactly.
-template <class G>
-__device__ __forceinline__ double ordered_dot(int b, int e, const int32_t* __restrict__ ci,
-                                              const double* __restrict__ v, G g, double init) {
-    double acc = init;
-    int k = b;
-    for (; k + 4 <= e; k += 4) {
-        const int c0 = ci[k], c1 = ci[k + 1], c2 = ci[k + 2], c3 = ci[k + 3];
-        const double v0 = v[k], v1 = v[k + 1], v2 = v[k + 2], v3 = v[k + 3];
-        const double g0 = g(c0), g1 = g(c1), g2 = g(c2), g3 = g(c3);
-        acc = __dadd_rn(acc, __dmul_rn(v0, g0));
-        acc = __dadd_rn(acc, __dmul_rn(v1, g1));
-        acc = __dadd_rn(acc, __dmul_rn(v2, g2));
-        acc = __dadd_rn(acc, __dmul_rn(v3, g3));
-    }
-    for (; k < e; ++k) acc = __dadd_rn(acc, __dmul_rn(v[k], g(ci[k])));
-    return acc;
-}
 
 // ---------------------------------------------------------------------------
 // One PDHG iteration (src/l1/pdhg.cpp:295-331)
@@ -123,11 +105,12 @@ __global__ void __launch_bounds__(kBlock) ex_primal(ExactIter a, int first) {
     DevState* st = a.st;
     if (first && blockIdx.x == 0 && threadIdx.x == 0) st->restart = 0;  // consumed by ex_restart
     if (st->done) return;
-    const int j = blockIdx.x * kBlock + threadIdx.x;
-    if (j >= a.AT.rows) return;
+    const RowTask t = row_task(a.AT, blockIdx.x);
+    if (t.row < 0) return;
+    const int j = t.row;
     const double* y = a.it.y;
-    const double g = ordered_dot(a.AT.rp[j], a.AT.rp[j + 1], a.AT.ci, a.AT.v64,
-                                 [y](int i) { return -y[i]; }, a.P.c[j]);
+    const double g = row_dot(t, a.AT, [y](int i) { return -y[i]; }, a.P.c[j]);
+    if (!t.lead) return;
     const double xo = a.it.x[j];
     const double xn = clampd(__dadd_rn(xo, __dmul_rn(-st->tau, g)), a.P.lo[j], a.P.hi[j]);
     a.it.xbar[j] = __dadd_rn(2.0 * xn, -xo);  // scale(2.0) then axpy(-1.0, x)
@@ -141,15 +124,16 @@ __global__ void __launch_bounds__(kBlock) ex_primal(ExactIter a, int first) {
 __global__ void __launch_bounds__(kBlock) ex_dual(ExactIter a, int first) {
     DevState* st = a.st;
     if (st->done) return;
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= a.A.rows) return;
+    const RowTask t = row_task(a.A, blockIdx.x);
+    if (t.row < 0) return;
+    const int i = t.row;
+    const double* xbar = a.it.xbar;
+    const double sum = row_dot(t, a.A, [xbar](int j) { return xbar[j]; }, 0.0);
+    if (!t.lead) return;
     const double yo = a.it.y[i];
     const double so = a.it.s[i];
     const double sn = clampd(__dadd_rn(so, __dmul_rn(-st->tau, yo)), a.P.rlo[i], a.P.rhi[i]);
     const double sbar = __dadd_rn(2.0 * sn, -so);
-    const double* xbar = a.it.xbar;
-    const double sum = ordered_dot(a.A.rp[i], a.A.rp[i + 1], a.A.ci, a.A.v64,
-                                   [xbar](int j) { return xbar[j]; }, 0.0);
     const double kb = __dadd_rn(-sum, sbar);
     const double yn = __dadd_rn(yo, __dmul_rn(st->sigma, kb));
     a.it.y[i] = yn;
@@ -190,38 +174,40 @@ __global__ void __launch_bounds__(kBlock) ex_check1(ExactCheck a) {
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
     const double inv = 1.0 / static_cast<double>(k_avg);
-    const int row_blocks = blocks_for(a.A.rows);
+    const int row_blocks = mat_blocks(a.A);
     const double bt = a.tol;
     double cp = 0.0, cd = 0.0, ap = 0.0, ad = 0.0;
     if (static_cast<int>(blockIdx.x) < row_blocks) {
-        const int i = blockIdx.x * kBlock + threadIdx.x;
-        if (i < a.A.rows) {
+        const RowTask t = row_task(a.A, blockIdx.x);
+        if (t.row >= 0) {
+            const int i = t.row;
             const double* x = a.it.x;
             const double* xs = a.it.xsum;
-            const int b = a.A.rp[i], e = a.A.rp[i + 1];
-            const double act_c = ordered_dot(b, e, a.A.ci, a.A.v64, [x](int j) { return x[j]; }, 0.0);
-            const double act_a = ordered_dot(b, e, a.A.ci, a.A.v64,
-                                             [xs, inv](int j) { return __dmul_rn(xs[j], inv); }, 0.0);
-            a.cs.act_avg[i] = act_a;
-            const double lo = a.P.rlo[i], hi = a.P.rhi[i];
-            cp = primal_term(act_c, lo, hi);
-            ap = primal_term(act_a, lo, hi);
-            cd = cs_term(a.it.y[i], act_c, lo, hi, bt);
-            ad = cs_term(__dmul_rn(a.it.ysum[i], inv), act_a, lo, hi, bt);
+            const double act_c = row_dot(t, a.A, [x](int j) { return x[j]; }, 0.0);
+            const double act_a = row_dot(t, a.A, [xs, inv](int j) { return __dmul_rn(xs[j], inv); }, 0.0);
+            if (t.lead) {
+                a.cs.act_avg[i] = act_a;
+                const double lo = a.P.rlo[i], hi = a.P.rhi[i];
+                cp = primal_term(act_c, lo, hi);
+                ap = primal_term(act_a, lo, hi);
+                cd = cs_term(a.it.y[i], act_c, lo, hi, bt);
+                ad = cs_term(__dmul_rn(a.it.ysum[i], inv), act_a, lo, hi, bt);
+            }
         }
     } else {
-        const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
-        if (j < a.AT.rows) {
+        const RowTask t = row_task(a.AT, blockIdx.x - row_blocks);
+        if (t.row >= 0) {
+            const int j = t.row;
             const double* y = a.it.y;
             const double* ys = a.it.ysum;
-            const int b = a.AT.rp[j], e = a.AT.rp[j + 1];
-            const double aty_c = ordered_dot(b, e, a.AT.ci, a.AT.v64, [y](int i) { return y[i]; }, 0.0);
-            const double aty_a = ordered_dot(b, e, a.AT.ci, a.AT.v64,
-                                             [ys, inv](int i) { return __dmul_rn(ys[i], inv); }, 0.0);
-            const double cj = a.P.c[j];
-            const double lo = a.P.lo[j], hi = a.P.hi[j];
-            cd = cs_term(__dadd_rn(cj, -aty_c), a.it.x[j], lo, hi, bt);
-            ad = cs_term(__dadd_rn(cj, -aty_a), __dmul_rn(a.it.xsum[j], inv), lo, hi, bt);
+            const double aty_c = row_dot(t, a.AT, [y](int i) { return y[i]; }, 0.0);
+            const double aty_a = row_dot(t, a.AT, [ys, inv](int i) { return __dmul_rn(ys[i], inv); }, 0.0);
+            if (t.lead) {
+                const double cj = a.P.c[j];
+                const double lo = a.P.lo[j], hi = a.P.hi[j];
+                cd = cs_term(__dadd_rn(cj, -aty_c), a.it.x[j], lo, hi, bt);
+                ad = cs_term(__dadd_rn(cj, -aty_a), __dmul_rn(a.it.xsum[j], inv), lo, hi, bt);
+            }
         }
     }
     block_acc_max(&st->acc[ACC_CUR_P], cp);
@@ -258,18 +244,20 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
     const double inv = st->inv;
     const bool ab = st->avg_better != 0;
     const double sign = a.P.obj_sign;
-    const int row_blocks = blocks_for(a.Ao.rows);
+    const int row_blocks = mat_blocks(a.Ao);
     const double bt = a.bound_tol;
     double op = 0.0, od = 0.0, pobj = 0.0, dobj = 0.0;
     if (static_cast<int>(blockIdx.x) < row_blocks) {
-        const int i = blockIdx.x * kBlock + threadIdx.x;
-        if (i < a.Ao.rows) {
+        const RowTask t = row_task(a.Ao, blockIdx.x);
+        if (t.row >= 0) {
+            const int i = t.row;
             const double* xv = a.it.x;
             const double* xsum = a.it.xsum;
             const double* cs = a.P.cs;
-            const double act = ordered_dot(
-                a.Ao.rp[i], a.Ao.rp[i + 1], a.Ao.ci, a.Ao.v64,
+            const double act = row_dot(
+                t, a.Ao,
                 [=](int j) { return __dmul_rn(ab ? __dmul_rn(xsum[j], inv) : xv[j], cs[j]); }, 0.0);
+          if (t.lead) {
             const double ys = ab ? __dmul_rn(a.it.ysum[i], inv) : a.it.y[i];
             const double yo = __dmul_rn(__dmul_rn(ys, sign), a.P.rs[i]);
             if (a.want_candidate) a.cs.cand_yo[i] = yo;
@@ -281,20 +269,23 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
                 if (yi > 0.0) dobj = fb(lo) ? yi * lo : 0.0;
                 else if (yi < 0.0) dobj = fb(hi) ? yi * hi : 0.0;
             }
+          }
         }
     } else {
-        const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
-        if (j < a.ATo.rows) {
+        const RowTask t = row_task(a.ATo, blockIdx.x - row_blocks);
+        if (t.row >= 0) {
+            const int j = t.row;
             const double* yv = a.it.y;
             const double* ysum = a.it.ysum;
             const double* rsv = a.P.rs;
-            const double aty = ordered_dot(
-                a.ATo.rp[j], a.ATo.rp[j + 1], a.ATo.ci, a.ATo.v64,
+            const double aty = row_dot(
+                t, a.ATo,
                 [=](int i) {
                     const double ys = ab ? __dmul_rn(ysum[i], inv) : yv[i];
                     return __dmul_rn(__dmul_rn(ys, sign), rsv[i]);
                 },
                 0.0);
+          if (t.lead) {
             const double xs = ab ? __dmul_rn(a.it.xsum[j], inv) : a.it.x[j];
             const double xo = __dmul_rn(xs, a.P.cs[j]);
             if (a.want_candidate) a.cs.cand_xo[j] = xo;
@@ -307,6 +298,7 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
                 if (ri > 0.0) dobj = fb(lo) ? ri * lo : 0.0;
                 else if (ri < 0.0) dobj = fb(hi) ? ri * hi : 0.0;
             }
+          }
         }
     }
     block_acc_max(&st->acc[ACC_ORIG_P], op);
@@ -343,7 +335,8 @@ __global__ void __launch_bounds__(kBlock) ex_check2(ExactCheck a) {
                     ps += part[2 * b];
                     ds += part[2 * b + 1];
                 }
-                ps += sign * a.P.obj_const;
+                ps += sign * a.P.obj_const;  // the constant shifts both objectives
+                ds += sign * a.P.obj_const;
                 const double gap = fabs(ps - ds) / (1.0 + fabs(ps) + fabs(ds));
                 rel = smax(smax(opv / (1.0 + a.P.bnorm), odv / (1.0 + a.P.cnorm)), gap);
             }
@@ -402,18 +395,19 @@ __global__ void __launch_bounds__(kBlock) ex_restart(ExactCheck a) {
 // w = -(A u) + v  (spmv(A, -1, u, 0, w) then axpy(1, v, w), pdhg.cpp:59-60)
 __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, const double* v,
                                                  double* w) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= A.rows) return;
-    const double sum = ordered_dot(A.rp[i], A.rp[i + 1], A.ci, A.v64, [u](int j) { return u[j]; }, 0.0);
-    w[i] = __dadd_rn(-sum, v[i]);
+    const RowTask t = row_task(A, blockIdx.x);
+    if (t.row < 0) return;
+    const double sum = row_dot(t, A, [u](int j) { return u[j]; }, 0.0);
+    if (t.lead) w[t.row] = __dadd_rn(-sum, v[t.row]);
 }
 
 // u = A^T (-w) via spmv_transpose(A, -1, w, 0, u) (pdhg.cpp:67): u starts at
 // 0 and adds val * (-w_r) in row order.
 __global__ void __launch_bounds__(kBlock) k_pw_u(DevCsr AT, const double* w, double* u) {
-    const int j = blockIdx.x * kBlock + threadIdx.x;
-    if (j >= AT.rows) return;
-    u[j] = ordered_dot(AT.rp[j], AT.rp[j + 1], AT.ci, AT.v64, [w](int i) { return -w[i]; }, 0.0);
+    const RowTask t = row_task(AT, blockIdx.x);
+    if (t.row < 0) return;
+    const double sum = row_dot(t, AT, [w](int i) { return -w[i]; }, 0.0);
+    if (t.lead) u[t.row] = sum;
 }
 
 __global__ void k_scale(double* x, int64_t n, double alpha) {
@@ -528,28 +522,31 @@ __device__ __forceinline__ double inf_over_box(double coeff, double lo, double h
 // terms (pdhg.cpp:476-491). Exact order in both orientations.
 __global__ void __launch_bounds__(kBlock) k_fin_rowscols(FinalArgs a) {
     DevState* st = a.st;
-    const int row_blocks = blocks_for(a.Ao.rows);
+    const int row_blocks = mat_blocks(a.Ao);
     const double bt = a.bound_tol;
     double pinf = 0.0, dinf = 0.0;
     if (static_cast<int>(blockIdx.x) < row_blocks) {
-        const int i = blockIdx.x * kBlock + threadIdx.x;
-        if (i < a.Ao.rows) {
+        const RowTask t = row_task(a.Ao, blockIdx.x);
+        if (t.row >= 0) {
+            const int i = t.row;
             const double* xo = a.f.xo;
-            const double act = ordered_dot(a.Ao.rp[i], a.Ao.rp[i + 1], a.Ao.ci, a.Ao.v64,
-                                           [xo](int j) { return xo[j]; }, 0.0);
+            const double act = row_dot(t, a.Ao, [xo](int j) { return xo[j]; }, 0.0);
+          if (t.lead) {
             const double lo = a.P.rlo_o[i], hi = a.P.rhi_o[i];
             pinf = primal_term(act, lo, hi);
             const bool at_lo = fb(lo) && fabs(act - lo) <= bt;
             const bool at_hi = fb(hi) && fabs(act - hi) <= bt;
             if (!at_lo && !at_hi) dinf = fabs(a.f.yo[i]);
             a.f.trow[i] = inf_over_box(a.f.yo[i], lo, hi);
+          }
         }
     } else {
-        const int j = (blockIdx.x - row_blocks) * kBlock + threadIdx.x;
-        if (j < a.ATo.rows) {
+        const RowTask t = row_task(a.ATo, blockIdx.x - row_blocks);
+        if (t.row >= 0) {
+            const int j = t.row;
             const double* yo = a.f.yo;
-            const double aty = ordered_dot(a.ATo.rp[j], a.ATo.rp[j + 1], a.ATo.ci, a.ATo.v64,
-                                           [yo](int i) { return yo[i]; }, 0.0);
+            const double aty = row_dot(t, a.ATo, [yo](int i) { return yo[i]; }, 0.0);
+          if (t.lead) {
             const double rc = __dadd_rn(a.P.c_o[j], -aty);
             a.f.rc[j] = rc;
             const double lo = a.P.lo_o[j], hi = a.P.hi_o[j];
@@ -558,6 +555,7 @@ __global__ void __launch_bounds__(kBlock) k_fin_rowscols(FinalArgs a) {
             const bool at_hi = fb(hi) && fabs(xo - hi) <= bt;
             if (!at_lo && !at_hi) dinf = fabs(rc);
             a.f.tcol[j] = inf_over_box(rc, lo, hi);
+          }
         }
     }
     block_acc_max(&st->acc[ACC_FIN_PINF], pinf);
@@ -701,9 +699,11 @@ __global__ void k_init_point(DevProblem P, DevCsr A, const double* x0s, const do
 
 __global__ void k_spmv_exact(DevCsr A, double alpha, const double* x, double beta, double* y) {
     // HostBackend::spmv, backend_host.cpp:415-423 (beta == 0 overwrites)
-    const int r = blockIdx.x * kBlock + threadIdx.x;
-    if (r >= A.rows) return;
-    const double sum = ordered_dot(A.rp[r], A.rp[r + 1], A.ci, A.v64, [x](int j) { return x[j]; }, 0.0);
+    const RowTask t = row_task(A, blockIdx.x);
+    if (t.row < 0) return;
+    const double sum = row_dot(t, A, [x](int j) { return x[j]; }, 0.0);
+    if (!t.lead) return;
+    const int r = t.row;
     y[r] = (beta == 0.0) ? __dmul_rn(alpha, sum)
                          : __dadd_rn(__dmul_rn(alpha, sum), __dmul_rn(beta, y[r]));
 }
@@ -712,11 +712,12 @@ __global__ void k_spmv_exact(DevCsr A, double alpha, const double* x, double bet
 // CSR: y_c starts at 0 (beta == 0) or y_c * beta, then adds val * (alpha x_r)
 // in ascending row order.
 __global__ void k_spmvT_exact(DevCsr AT, double alpha, const double* x, double beta, double* y) {
-    const int c = blockIdx.x * kBlock + threadIdx.x;
-    if (c >= AT.rows) return;
+    const RowTask t = row_task(AT, blockIdx.x);
+    if (t.row < 0) return;
+    const int c = t.row;
     const double init = (beta == 0.0) ? 0.0 : __dmul_rn(y[c], beta);
-    y[c] = ordered_dot(AT.rp[c], AT.rp[c + 1], AT.ci, AT.v64,
-                       [x, alpha](int r) { return __dmul_rn(alpha, x[r]); }, init);
+    const double sum = row_dot(t, AT, [x, alpha](int r) { return __dmul_rn(alpha, x[r]); }, init);
+    if (t.lead) y[c] = sum;
 }
 
 __global__ void k_project_box(int32_t n, const double* lo, const double* hi, double* x) {
@@ -732,10 +733,13 @@ __global__ void k_project_box(int32_t n, const double* lo, const double* hi, dou
 // Transpose
 // ---------------------------------------------------------------------------
 
-__global__ void k_row_of_entry(int32_t m, const int32_t* rp, int32_t* row) {
-    const int r = blockIdx.x * kBlock + threadIdx.x;
+// Groups of `lanes` threads (about the mean row length) fill a row each.
+__global__ void k_row_of_entry(int32_t m, const int32_t* rp, int32_t* row, int lanes) {
+    const int64_t tid = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    const int64_t r = tid / lanes;
     if (r >= m) return;
-    for (int k = rp[r]; k < rp[r + 1]; ++k) row[k] = r;
+    const int e = rp[r + 1];
+    for (int k = rp[r] + static_cast<int>(tid % lanes); k < e; k += lanes) row[k] = static_cast<int32_t>(r);
 }
 
 __global__ void k_iota(int32_t* v, int64_t n) {
@@ -770,15 +774,17 @@ inline int grid64(int64_t n) { return static_cast<int>((n + kBlock - 1) / kBlock
 // Launchers
 // ---------------------------------------------------------------------------
 
+int exact_check_grid(const DevCsr& A, const DevCsr& AT) { return mat_blocks(A) + mat_blocks(AT); }
+
 void launch_exact_primal(const ExactIter& a, int first, cudaStream_t s) {
-    if (a.AT.rows > 0) ex_primal<<<blocks_for(a.AT.rows), kBlock, 0, s>>>(a, first);
+    if (a.AT.rows > 0) ex_primal<<<mat_blocks(a.AT), kBlock, 0, s>>>(a, first);
 }
 void launch_exact_dual(const ExactIter& a, int first, cudaStream_t s) {
-    if (a.A.rows > 0) ex_dual<<<blocks_for(a.A.rows), kBlock, 0, s>>>(a, first);
+    if (a.A.rows > 0) ex_dual<<<mat_blocks(a.A), kBlock, 0, s>>>(a, first);
 }
 void launch_exact_check(const ExactCheck& a, cudaStream_t s) {
-    const int g1 = blocks_for(a.A.rows) + blocks_for(a.AT.rows);
-    const int g2 = blocks_for(a.Ao.rows) + blocks_for(a.ATo.rows);
+    const int g1 = mat_blocks(a.A) + mat_blocks(a.AT);
+    const int g2 = mat_blocks(a.Ao) + mat_blocks(a.ATo);
     ex_check1<<<g1 > 0 ? g1 : 1, kBlock, 0, s>>>(a);
     ex_check2<<<g2 > 0 ? g2 : 1, kBlock, 0, s>>>(a);
 }
@@ -815,10 +821,10 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
 }
 
 void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s) {
-    if (A.rows > 0) k_pw_w<<<blocks_for(A.rows), kBlock, 0, s>>>(A, u, v, w);
+    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w);
 }
 void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s) {
-    if (AT.rows > 0) k_pw_u<<<blocks_for(AT.rows), kBlock, 0, s>>>(AT, w, u);
+    if (AT.rows > 0) k_pw_u<<<mat_blocks(AT), kBlock, 0, s>>>(AT, w, u);
 }
 void launch_scale(double* x, int64_t n, double alpha, cudaStream_t s) {
     if (n > 0) k_scale<<<grid64(n), kBlock, 0, s>>>(x, n, alpha);
@@ -830,7 +836,7 @@ void launch_fill(double* x, int64_t n, double v, cudaStream_t s) {
 void launch_final(const FinalArgs& a, cudaStream_t s) {
     const int32_t nmax = a.P.n > a.P.m ? a.P.n : a.P.m;
     if (nmax > 0) k_fin_unscale<<<blocks_for(nmax), kBlock, 0, s>>>(a);
-    const int g = blocks_for(a.Ao.rows) + blocks_for(a.ATo.rows);
+    const int g = mat_blocks(a.Ao) + mat_blocks(a.ATo);
     if (g > 0) k_fin_rowscols<<<g, kBlock, 0, s>>>(a);
     if (a.exact) {
         k_fin_sums_exact<<<1, 32, 0, s>>>(a);
@@ -865,11 +871,11 @@ template void launch_init_point<float>(const DevProblem&, const DevCsr&, const d
 
 void launch_spmv_exact(const DevCsr& A, double alpha, const double* x, double beta, double* y,
                        cudaStream_t s) {
-    if (A.rows > 0) k_spmv_exact<<<blocks_for(A.rows), kBlock, 0, s>>>(A, alpha, x, beta, y);
+    if (A.rows > 0) k_spmv_exact<<<mat_blocks(A), kBlock, 0, s>>>(A, alpha, x, beta, y);
 }
 void launch_spmvT_exact(const DevCsr& AT, double alpha, const double* x, double beta, double* y,
                         cudaStream_t s) {
-    if (AT.rows > 0) k_spmvT_exact<<<blocks_for(AT.rows), kBlock, 0, s>>>(AT, alpha, x, beta, y);
+    if (AT.rows > 0) k_spmvT_exact<<<mat_blocks(AT), kBlock, 0, s>>>(AT, alpha, x, beta, y);
 }
 void launch_project_box(int32_t n, const double* lo, const double* hi, double* x,
                         cudaStream_t s) {
@@ -891,50 +897,80 @@ int prefix_rows(const int32_t* cnt, int32_t n, int32_t* out, cudaStream_t s) {
     return static_cast<int>(cudaGetLastError() != cudaSuccess);
 }
 
+namespace {
+
+// Scratch layout of build_transpose: column counts, scan temp, row of each
+// entry, sorted keys, entry ids in and out, sort temp; 256-byte aligned parts.
+struct TransposeLayout {
+    size_t cnt = 0, scan_tmp = 0, row = 0, keys = 0, ids_in = 0, ids_out = 0, sort_tmp = 0;
+    size_t scan_bytes = 0, sort_bytes = 0, total = 0;
+    int bits = 1;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+TransposeLayout transpose_layout(int32_t m, int32_t n, int64_t nnz) {
+    TransposeLayout L;
+    while ((int64_t{1} << L.bits) < static_cast<int64_t>(n)) ++L.bits;
+    cub::DeviceScan::InclusiveSum(nullptr, L.scan_bytes, static_cast<const int32_t*>(nullptr),
+                                  static_cast<int32_t*>(nullptr), n > 0 ? n : 1);
+    cub::DeviceRadixSort::SortPairs(nullptr, L.sort_bytes, static_cast<const int32_t*>(nullptr),
+                                    static_cast<int32_t*>(nullptr),
+                                    static_cast<const int32_t*>(nullptr),
+                                    static_cast<int32_t*>(nullptr),
+                                    static_cast<int>(nnz > 0 ? nnz : 1), 0, L.bits);
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        const size_t at = off;
+        off += align256(bytes);
+        return at;
+    };
+    const size_t e = sizeof(int32_t) * static_cast<size_t>(nnz > 0 ? nnz : 1);
+    L.cnt = take(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
+    L.scan_tmp = take(L.scan_bytes + 16);
+    L.row = take(e);
+    L.keys = take(e);
+    L.ids_in = take(e);
+    L.ids_out = take(e);
+    L.sort_tmp = take(L.sort_bytes + 16);
+    L.total = off;
+    (void)m;
+    return L;
+}
+
+}  // namespace
+
+size_t transpose_scratch_bytes(int32_t m, int32_t n, int64_t nnz) {
+    return transpose_layout(m, n, nnz).total;
+}
+
 int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci,
-                    const double* v, TransposeOut out, cudaStream_t s) {
-    cudaError_t err = cudaSuccess;
+                    const double* v, TransposeOut out, void* scratch, cudaStream_t s) {
+    const TransposeLayout L = transpose_layout(m, n, nnz);
+    char* base = static_cast<char*>(scratch);
     // counts -> row pointer of A^T
-    int32_t* cnt = nullptr;
-    err = cudaMallocAsync(&cnt, sizeof(int32_t) * (static_cast<size_t>(n) + 1), s);
-    if (err != cudaSuccess) return 1;
+    int32_t* cnt = reinterpret_cast<int32_t*>(base + L.cnt);
     cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (static_cast<size_t>(n) + 1), s);
     if (nnz > 0) k_col_count<<<grid64(nnz), kBlock, 0, s>>>(ci, nnz, cnt + 1);
-    size_t scan_bytes = 0;
-    cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, cnt + 1, out.rp + 1, n, s);
-    void* scan_tmp = nullptr;
-    err = cudaMallocAsync(&scan_tmp, scan_bytes + 16, s);
-    if (err != cudaSuccess) return 1;
     cudaMemsetAsync(out.rp, 0, sizeof(int32_t), s);
-    if (n > 0) cub::DeviceScan::InclusiveSum(scan_tmp, scan_bytes, cnt + 1, out.rp + 1, n, s);
-    cudaFreeAsync(scan_tmp, s);
-    cudaFreeAsync(cnt, s);
+    size_t scan_bytes = L.scan_bytes;
+    if (n > 0) cub::DeviceScan::InclusiveSum(base + L.scan_tmp, scan_bytes, cnt + 1, out.rp + 1, n, s);
     if (nnz == 0) return static_cast<int>(cudaGetLastError() != cudaSuccess);
     // stable sort of entry ids by column
-    int32_t *row = nullptr, *keys_out = nullptr, *ids_in = nullptr, *ids_out = nullptr;
-    err = cudaMallocAsync(&row, sizeof(int32_t) * nnz, s);
-    if (err == cudaSuccess) err = cudaMallocAsync(&keys_out, sizeof(int32_t) * nnz, s);
-    if (err == cudaSuccess) err = cudaMallocAsync(&ids_in, sizeof(int32_t) * nnz, s);
-    if (err == cudaSuccess) err = cudaMallocAsync(&ids_out, sizeof(int32_t) * nnz, s);
-    if (err != cudaSuccess) return 1;
-    if (m > 0) k_row_of_entry<<<blocks_for(m), kBlock, 0, s>>>(m, rp, row);
+    int32_t* row = reinterpret_cast<int32_t*>(base + L.row);
+    int32_t* keys_out = reinterpret_cast<int32_t*>(base + L.keys);
+    int32_t* ids_in = reinterpret_cast<int32_t*>(base + L.ids_in);
+    int32_t* ids_out = reinterpret_cast<int32_t*>(base + L.ids_out);
+    if (m > 0) {
+        int lanes = 1;
+        while (lanes < 32 && static_cast<int64_t>(lanes) * m < nnz) lanes *= 2;
+        k_row_of_entry<<<grid64(static_cast<int64_t>(m) * lanes), kBlock, 0, s>>>(m, rp, row, lanes);
+    }
     k_iota<<<grid64(nnz), kBlock, 0, s>>>(ids_in, nnz);
-    int bits = 1;
-    while ((int64_t{1} << bits) < static_cast<int64_t>(n)) ++bits;
-    size_t sort_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, ci, keys_out, ids_in, ids_out,
-                                    static_cast<int>(nnz), 0, bits, s);
-    void* sort_tmp = nullptr;
-    err = cudaMallocAsync(&sort_tmp, sort_bytes + 16, s);
-    if (err != cudaSuccess) return 1;
-    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, ci, keys_out, ids_in, ids_out,
-                                    static_cast<int>(nnz), 0, bits, s);
+    size_t sort_bytes = L.sort_bytes;
+    cub::DeviceRadixSort::SortPairs(base + L.sort_tmp, sort_bytes, ci, keys_out, ids_in, ids_out,
+                                    static_cast<int>(nnz), 0, L.bits, s);
     k_gather_t<<<grid64(nnz), kBlock, 0, s>>>(ids_out, row, v, nnz, out.ci, out.v);
-    cudaFreeAsync(sort_tmp, s);
-    cudaFreeAsync(row, s);
-    cudaFreeAsync(keys_out, s);
-    cudaFreeAsync(ids_in, s);
-    cudaFreeAsync(ids_out, s);
     return static_cast<int>(cudaGetLastError() != cudaSuccess);
 }
 

@@ -314,7 +314,8 @@ __global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_bloc
                     ps += part[4 * b + off];
                     ds += part[4 * b + off + 1];
                 }
-                ps += a.P.obj_sign * a.P.obj_const;
+                ps += a.P.obj_sign * a.P.obj_const;  // the constant shifts both objectives
+                ds += a.P.obj_sign * a.P.obj_const;
                 const double gap = fabs(ps - ds) / (1.0 + fabs(ps) + fabs(ds));
                 rel = smax(smax(op / (1.0 + a.P.bnorm), od / (1.0 + a.P.cnorm)), gap);
             }

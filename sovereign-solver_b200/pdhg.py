@@ -103,6 +103,10 @@ def lib() -> C.CDLL:
         L.pdhg_scaling.argtypes = [C.c_int32, C.c_int32, C.c_int64, _ip, _ip, _dp,
                                    C.POINTER(_Options), _dp, _dp]
         L.pdhg_get_scaling.argtypes = [C.c_void_p, _dp, _dp]
+        L.pdhg_load_batch.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, C.c_int64, _ip, _ip, _dp,
+                                      _dp, _dp, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
+        L.pdhg_solve_batch.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Info), _dp,
+                                       _dp, _dp]
         _lib = L
     return _lib
 
@@ -193,6 +197,77 @@ def _i(a: np.ndarray):
     return a.ctypes.data_as(_ip)
 
 
+def _c_options(opt: PdhgOptions) -> _Options:
+    o = _Options()
+    lib().pdhg_default_options(C.byref(o))
+    for f in fields(PdhgOptions):
+        name = f.name
+        val = getattr(opt, name)
+        if name == "precision":
+            o.precision = PREC[val]
+        elif name == "termination_rule":
+            o.termination_rule = 1 if val in ("relative_kkt", 1) else 0
+        elif name == "restart_rule":
+            o.restart_rule = 1 if val in ("adaptive", 1) else 0
+        elif name in ("checkpoint", "trace_iters"):
+            continue
+        else:
+            setattr(o, name, type(getattr(o, name))(val))
+    return o
+
+
+def _c_start(o: _Options, keep: list, cancel, x0, y0) -> None:
+    """Cancellation flag and warm start into the C options (arrays kept alive in keep)."""
+    if cancel is not None:
+        o.cancel_flag = C.pointer(cancel._flag)
+    if x0 is not None:
+        x0a = np.ascontiguousarray(x0, dtype=np.float64)
+        keep.append(x0a)
+        o.x0 = _d(x0a)
+    if y0 is not None:
+        y0a = np.ascontiguousarray(y0, dtype=np.float64)
+        keep.append(y0a)
+        o.y0 = _d(y0a)
+
+
+def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray) -> PdhgResult:
+    hp = bool(info.has_point)
+    return PdhgResult(
+        status=STATUS[info.status], objective=info.objective,
+        primal=x.copy() if hp else np.zeros(0), dual=y.copy() if hp else np.zeros(0),
+        reduced_costs=rc.copy() if hp else np.zeros(0),
+        primal_infeasibility=info.primal_infeasibility,
+        dual_infeasibility=info.dual_infeasibility, duality_gap=info.duality_gap,
+        iterations=info.iterations, restarts=info.restarts, seconds=info.seconds,
+        operator_norm_estimate=info.operator_norm_estimate,
+        message=info.message.decode(), relative_kkt=info.relative_kkt,
+        fp64_iterations=info.fp64_iterations, kernel_launches=info.kernel_launches,
+        device_seconds=info.device_seconds)
+
+
+def stack_batch(problems: list[Problem]) -> dict:
+    """The block-diagonal stacking pdhg_load_batch takes: instance k's rows and
+    columns follow instance k-1's; column indices become global."""
+    ms = np.array([p.m for p in problems], dtype=np.int64)
+    ns = np.array([p.n for p in problems], dtype=np.int64)
+    nnzs = np.array([p.nnz for p in problems], dtype=np.int64)
+    row_off = np.concatenate([[0], np.cumsum(ms)]).astype(np.int32)
+    col_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int32)
+    nz_off = np.concatenate([[0], np.cumsum(nnzs)])
+    rp = [np.asarray(p.row_ptr[:-1], dtype=np.int64) + nz_off[k] for k, p in enumerate(problems)]
+    row_ptr = np.concatenate(rp + [[nz_off[-1]]]).astype(np.int32)
+    col_idx = np.concatenate([np.asarray(p.col_idx, dtype=np.int64) + col_off[k]
+                              for k, p in enumerate(problems)] + [np.zeros(0, np.int64)])
+    cat = lambda name: np.ascontiguousarray(np.concatenate(  # noqa: E731
+        [np.asarray(getattr(p, name), dtype=np.float64) for p in problems] + [np.zeros(0)]))
+    return {"row_off": row_off, "col_off": col_off, "nnz": int(nz_off[-1]),
+            "row_ptr": row_ptr, "col_idx": col_idx.astype(np.int32),
+            "val": cat("val"), "c": cat("c"), "col_lo": cat("col_lo"), "col_hi": cat("col_hi"),
+            "row_lo": cat("row_lo"), "row_hi": cat("row_hi"),
+            "obj_const": np.array([float(p.obj_const) for p in problems], dtype=np.float64),
+            "maximize": np.array([int(bool(p.maximize)) for p in problems], dtype=np.intc)}
+
+
 class Engine:
     """One engine context on one device (the analogue of one ``sov::Backend``)."""
 
@@ -244,23 +319,7 @@ class Engine:
             raise PdhgError(3, "Engine.solve: no problem loaded")
         p = self.problem
         opt = opt or PdhgOptions()
-        o = _Options()
-        lib().pdhg_default_options(C.byref(o))
-        for f in fields(PdhgOptions):
-            name = f.name
-            val = getattr(opt, name)
-            if name == "precision":
-                o.precision = PREC[val]
-            elif name == "termination_rule":
-                o.termination_rule = 1 if val in ("relative_kkt", 1) else 0
-            elif name == "restart_rule":
-                o.restart_rule = 1 if val in ("adaptive", 1) else 0
-            elif name == "checkpoint":
-                continue
-            elif name == "trace_iters":
-                continue
-            else:
-                setattr(o, name, type(getattr(o, name))(val))
+        o = _c_options(opt)
         keep: list = []
         if opt.checkpoint is not None:
             user_cb = opt.checkpoint
@@ -272,16 +331,7 @@ class Engine:
             cfn = CHECKPOINT_FN(cb)
             keep.append(cfn)
             o.checkpoint = cfn
-        if cancel is not None:
-            o.cancel_flag = C.pointer(cancel._flag)
-        if x0 is not None:
-            x0a = np.ascontiguousarray(x0, dtype=np.float64)
-            keep.append(x0a)
-            o.x0 = _d(x0a)
-        if y0 is not None:
-            y0a = np.ascontiguousarray(y0, dtype=np.float64)
-            keep.append(y0a)
-            o.y0 = _d(y0a)
+        _c_start(o, keep, cancel, x0, y0)
         tx = ty = None
         if opt.trace_iters > 0:
             tx = np.zeros((opt.trace_iters, max(p.n, 1)))
@@ -297,23 +347,57 @@ class Engine:
         _check(lib().pdhg_solve(self._h, C.byref(o), C.byref(info),
                                 _d(x) if want_point else null, _d(y) if want_point else null,
                                 _d(rc) if want_point else null), "pdhg_solve", self._h)
-        hp = bool(info.has_point)
-        r = PdhgResult(
-            status=STATUS[info.status], objective=info.objective,
-            primal=x[: p.n].copy() if hp else np.zeros(0),
-            dual=y[: p.m].copy() if hp else np.zeros(0),
-            reduced_costs=rc[: p.n].copy() if hp else np.zeros(0),
-            primal_infeasibility=info.primal_infeasibility,
-            dual_infeasibility=info.dual_infeasibility, duality_gap=info.duality_gap,
-            iterations=info.iterations, restarts=info.restarts, seconds=info.seconds,
-            operator_norm_estimate=info.operator_norm_estimate,
-            message=info.message.decode(), relative_kkt=info.relative_kkt,
-            fp64_iterations=info.fp64_iterations, kernel_launches=info.kernel_launches,
-            device_seconds=info.device_seconds)
+        r = _result(info, x[: p.n], y[: p.m], rc[: p.n])
         if tx is not None:
             r.trace_x = tx[:, : p.n]
             r.trace_y = ty[:, : p.m]
         return r
+
+    def load_batch(self, problems: list[Problem]) -> None:
+        """Loads LPs to be solved together by ``solve_batch`` (pdhg_load_batch)."""
+        b = stack_batch(problems)
+        self._batch = (b, [(p.m, p.n) for p in problems])
+        ci = b["col_idx"] if b["col_idx"].size else np.zeros(1, np.int32)
+        va = b["val"] if b["val"].size else np.zeros(1)
+        nz = lambda a: a if a.size else np.zeros(1)  # noqa: E731
+        _check(lib().pdhg_load_batch(
+            self._h, len(problems), _i(b["row_off"]), _i(b["col_off"]), b["nnz"],
+            _i(b["row_ptr"]), _i(ci), _d(va), _d(nz(b["c"])), _d(b["obj_const"]),
+            b["maximize"].ctypes.data_as(C.POINTER(C.c_int)), _d(nz(b["col_lo"])),
+            _d(nz(b["col_hi"])), _d(nz(b["row_lo"])), _d(nz(b["row_hi"]))),
+            "pdhg_load_batch", self._h)
+
+    def solve_batch(self, opt: PdhgOptions | None = None,
+                    cancel: CancellationToken | None = None,
+                    x0: list[np.ndarray] | None = None, y0: list[np.ndarray] | None = None,
+                    want_point: bool = True) -> list[PdhgResult]:
+        """One ``PdhgResult`` per loaded instance (pdhg_solve_batch). Precision
+        ``mixed`` (the default here) or ``fp64``; x0 / y0 are per-instance lists."""
+        if getattr(self, "_batch", None) is None:
+            raise PdhgError(3, "Engine.solve_batch: no batch loaded")
+        b, shapes = self._batch
+        opt = opt or PdhgOptions(precision="mixed")
+        o = _c_options(opt)
+        o.trace_iters = opt.trace_iters  # the engine rejects traces in a batch
+        keep: list = []
+        _c_start(o, keep, cancel, None if x0 is None else np.concatenate(x0),
+                 None if y0 is None else np.concatenate(y0))
+        count = len(shapes)
+        infos = (_Info * count)()
+        m, n = int(b["row_off"][-1]), int(b["col_off"][-1])
+        x, y, rc = np.zeros(max(n, 1)), np.zeros(max(m, 1)), np.zeros(max(n, 1))
+        null = C.cast(None, _dp)
+        _check(lib().pdhg_solve_batch(self._h, C.byref(o), infos,
+                                      _d(x) if want_point else null,
+                                      _d(y) if want_point else null,
+                                      _d(rc) if want_point else null),
+               "pdhg_solve_batch", self._h)
+        out = []
+        for k in range(count):
+            r0, r1 = int(b["row_off"][k]), int(b["row_off"][k + 1])
+            c0, c1 = int(b["col_off"][k]), int(b["col_off"][k + 1])
+            out.append(_result(infos[k], x[c0:c1], y[r0:r1], rc[c0:c1]))
+        return out
 
     def scaling(self) -> tuple[np.ndarray, np.ndarray]:
         """Row / column factors the engine computed on the device for the loaded LP."""
