@@ -312,7 +312,7 @@ def main() -> None:
                 "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                 "peak_source": peaks["source"], "traffic": traffic_from_profile(),
                 "algorithmic_bytes_per_launch": dom["bytes"], "avg_launch_ms": dom["avg_ms"],
-                "kernels": ks}
+                "kernels": ks, "tuning": eng.tuning("mixed")}
 
     # ---- end to end through the C-ABI from pinned host memory (e2e) ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define PDHG_B200_ABI_VERSION 1
+#define PDHG_B200_ABI_VERSION 2
 
 /* Return codes: the order and meaning of sov::Status (status.hpp:25-34). */
 typedef enum {
@@ -107,6 +107,9 @@ typedef struct pdhg_options {
     int trace_iters;         /* record scaled-space x, y after each of the first trace_iters */
     double* trace_x;         /* iterations: trace_iters * n, host (test support) */
     double* trace_y;         /* trace_iters * m, host */
+    int autotune;            /* 1 (default): MIXED / FP64 time the iteration kernels' shapes
+                                on the first solve of a loaded LP with >= 2^20 nonzeros and
+                                keep the fastest (see pdhg_get_tuning); 0 = fixed defaults */
 } pdhg_options;
 
 /* sov::PdhgResult (pdhg.hpp:136-153) minus the vectors, which pdhg_solve
@@ -185,6 +188,17 @@ int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off,
                     const double* col_hi, const double* row_lo, const double* row_hi);
 int pdhg_solve_batch(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* infos, double* x,
                      double* y, double* rc);
+
+/* Iteration-kernel shapes in use for the loaded problem in `precision`
+ * (PDHG_PREC_MIXED or PDHG_PREC_FP64): out[0] lanes per short row and out[1]
+ * long-row strategy (0: one CTA per row; 1: one warp per row up to 16,384
+ * entries) of the primal pass (rows of A^T), out[2], out[3] the same for the
+ * dual pass (rows of A), out[4] = 1 when chosen by timing, 0 for the defaults
+ * (no solve yet, autotune off, or a small LP). Engine extension: the autotuner
+ * times the candidates once per matrix shape and precision, and keeps the
+ * choice in memory, and also in the JSON file named by the environment
+ * variable PDHG_B200_TUNE_CACHE when it is set. */
+int pdhg_get_tuning(const pdhg_ctx* ctx, int precision, int* out);
 
 /* Per-kernel timing of the iteration kernels on the loaded problem (CUDA events
  * on the engine's stream around each launch, after `warmup` untimed iterations).

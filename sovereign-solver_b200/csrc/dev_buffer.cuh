@@ -41,11 +41,11 @@ struct DBuf {
 struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
-    DBuf<int32_t> rp, ci, long_rows, wrows;
+    DBuf<int32_t> rp, ci, long_rows, wrows, mid_rows, huge_rows;
     DBuf<double> v64;
     DBuf<float> v32;
     DBuf<char> tscratch;  // build_transpose scratch when this matrix is a transpose
-    int32_t n_long = 0, n_short = 0, n_wrows = 0;
+    int32_t n_long = 0, n_short = 0, n_wrows = 0, n_mid = 0, n_huge = 0;
     int vw = 1;
     DevCsr view() const {
         DevCsr d;
@@ -62,6 +62,10 @@ struct MatDev {
         d.vw = vw;
         d.wrows = wrows.p;
         d.n_wrows = n_wrows;
+        d.mid_rows = mid_rows.p;
+        d.huge_rows = huge_rows.p;
+        d.n_mid = n_mid;
+        d.n_huge = n_huge;
         return d;
     }
 };
@@ -130,19 +134,25 @@ inline int cuda_fail(std::string* err, cudaError_t e, const char* what) {
 inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     cudaError_t e = M.long_rows.alloc(static_cast<size_t>(M.rows) + 1);
     if (e != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
-    if ((e = M.wrows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
+    if ((e = M.wrows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess ||
+        (e = M.mid_rows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess ||
+        (e = M.huge_rows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
         return cuda_fail(err, e, "bin_matrix");
     DBuf<unsigned long long> cnt;
-    if ((e = cnt.alloc(6)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
-    cudaMemsetAsync(cnt.p, 0, 6 * sizeof(unsigned long long), s);
+    if ((e = cnt.alloc(8)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+    cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s);
     launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
     launch_bin(M.rp.p, M.rows, kWarpRow, M.wrows.p, cnt.p + 3, s);
-    unsigned long long h[6];
+    launch_bin_range(M.rp.p, M.rows, kLongRow, kHugeRow, M.mid_rows.p, cnt.p + 6, s);
+    launch_bin_range(M.rp.p, M.rows, kHugeRow, 0x7fffffff, M.huge_rows.p, cnt.p + 7, s);
+    unsigned long long h[8];
     cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     M.n_long = static_cast<int32_t>(h[0]);
     M.n_short = static_cast<int32_t>(h[1]);
     M.n_wrows = static_cast<int32_t>(h[3]);
+    M.n_mid = static_cast<int32_t>(h[6]);
+    M.n_huge = static_cast<int32_t>(h[7]);
     const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
     int w = 1;
     while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;

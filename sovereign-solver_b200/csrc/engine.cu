@@ -17,10 +17,13 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -91,6 +94,14 @@ struct Ctx {
     long long launches = 0;
 
     BatchCtx* batch = nullptr;  // pdhg_load_batch / pdhg_solve_batch
+
+    // Iteration-kernel shapes per fast precision ([0] MIXED, [1] FP64):
+    // {primal lanes, primal long mode, dual lanes, dual long mode}; reset on load.
+    struct Tuning {
+        bool have = false;
+        bool timed = false;
+        int shape[4] = {0, 0, 0, 0};
+    } tuning[2];
 
     ~Ctx() {
         if (batch != nullptr) batch_delete(batch);
@@ -255,6 +266,8 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     c.scaled = true;
     c.have_opnorm = false;
     c.gen += 1;
+    c.tuning[0] = Ctx::Tuning{};  // new matrices: shapes are chosen again
+    c.tuning[1] = Ctx::Tuning{};
     return PDHG_OK;
 }
 
@@ -376,14 +389,14 @@ struct Launcher {
         if (prec == PDHG_PREC_FP64_EXACT) {
             launch_exact_primal(ei, first, s);
             launch_exact_dual(ei, first, s);
+            c.launches += 2;
         } else if (prec == PDHG_PREC_MIXED) {
-            launch_fast_primal(fi32, first, s);
-            launch_fast_dual(fi32, first, s);
+            c.launches += launch_fast_primal(fi32, first, s);
+            c.launches += launch_fast_dual(fi32, first, s);
         } else {
-            launch_fast_primal(fi64, first, s);
-            launch_fast_dual(fi64, first, s);
+            c.launches += launch_fast_primal(fi64, first, s);
+            c.launches += launch_fast_dual(fi64, first, s);
         }
-        c.launches += 2;
     }
     void check(long long period, cudaStream_t s) {
         if (prec == PDHG_PREC_FP64_EXACT) {
@@ -405,9 +418,25 @@ struct Launcher {
     }
     long long launches_per_period(long long period) const {
         const long long chk = prec == PDHG_PREC_FP64_EXACT ? 3 : 2 + (fc32.want_candidate ? 1 : 0);
-        return 2 * period + chk;
+        long long per_iter = 2;
+        long long clear = 0;  // the flag reset when the primal pass has no rows
+        if (prec != PDHG_PREC_FP64_EXACT) {
+            per_iter = prec == PDHG_PREC_MIXED ? fast_launches_per_iteration(fi32)
+                                               : fast_launches_per_iteration(fi64);
+            clear = c.lp.n == 0 ? 1 : 0;
+        }
+        return per_iter * period + clear + chk;
     }
 };
+
+template <class T>
+void apply_tuning(const Ctx::Tuning& t, FastIter<T>& fi) {
+    if (!t.have) return;
+    fi.AT.iter_vw = t.shape[0];
+    fi.AT.long_mode = t.shape[1];
+    fi.A.iter_vw = t.shape[2];
+    fi.A.long_mode = t.shape[3];
+}
 
 Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candidate) {
     Launcher L{c, prec, {}, {}, {}, {}, {}, {}};
@@ -421,6 +450,10 @@ Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candid
                       c.st.p, c.mail_dev};
     L.fi32 = FastIter<float>{c.As.view(), c.ATs.view(), P, iterates<float>(c), c.st.p};
     L.fi64 = FastIter<double>{c.As.view(), c.ATs.view(), P, iterates<double>(c), c.st.p};
+    if (o.autotune) {
+        apply_tuning(c.tuning[0], L.fi32);
+        apply_tuning(c.tuning[1], L.fi64);
+    }
     L.fc32 = FastCheck<float>{c.As.view(), c.ATs.view(), P, iterates<float>(c), cs,
                               o.tolerance, bt, o.restart_sufficient_decrease,
                               o.restart_check_period, o.termination_rule,
@@ -702,6 +735,161 @@ __global__ void k_restart_state(DevState* st) {
     st->res_last = INFINITY;
 }
 
+// ---- autotuner of the iteration kernels ----------------------------------------
+//
+// For each pass (primal over A^T, dual over A) the candidates are the lanes
+// per short row around the binning's choice (vw/2, vw, 2vw) and, when the
+// matrix has rows longer than kLongRow, both long-row strategies. Each is
+// timed with CUDA events on the engine's stream (2 launches to warm, 5
+// timed) and replaces the current best only when faster by more than 5%, so
+// noise does not flip the choice. LPs below kTuneMinNnz nonzeros are
+// launch-latency bound and keep the defaults (and their summation order).
+// Choices are cached per shape signature for the process, and in the JSON
+// file named by PDHG_B200_TUNE_CACHE ({"signature": [lanes, mode], ...}).
+
+constexpr int64_t kTuneMinNnz = int64_t{1} << 20;
+
+std::mutex g_tune_mutex;
+std::map<std::string, std::pair<int, int>> g_tune_cache;
+bool g_tune_file_read = false;
+
+const char* tune_file() {
+    const char* f = std::getenv("PDHG_B200_TUNE_CACHE");
+    return (f != nullptr && f[0] != '\0') ? f : nullptr;
+}
+
+// Reads `"key": [a, b]` entries of the cache file (called with the mutex held).
+void tune_read_file() {
+    if (g_tune_file_read) return;
+    g_tune_file_read = true;
+    const char* path = tune_file();
+    if (path == nullptr) return;
+    std::FILE* f = std::fopen(path, "r");
+    if (f == nullptr) return;
+    std::string txt;
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) txt.append(buf, k);
+    std::fclose(f);
+    size_t pos = 0;
+    while ((pos = txt.find('"', pos)) != std::string::npos) {
+        const size_t end = txt.find('"', pos + 1);
+        if (end == std::string::npos) break;
+        const std::string key = txt.substr(pos + 1, end - pos - 1);
+        int a = 0, b = 0;
+        const size_t lb = txt.find('[', end);
+        if (lb != std::string::npos && std::sscanf(txt.c_str() + lb, "[%d , %d]", &a, &b) == 2 &&
+            a >= 1 && a <= 32 && (a & (a - 1)) == 0 && (b == 0 || b == 1))
+            g_tune_cache[key] = {a, b};
+        pos = end + 1;
+    }
+}
+
+void tune_write_file() {
+    const char* path = tune_file();
+    if (path == nullptr) return;
+    std::FILE* f = std::fopen(path, "w");
+    if (f == nullptr) return;
+    std::fprintf(f, "{\n");
+    size_t i = 0;
+    for (const auto& kv : g_tune_cache)
+        std::fprintf(f, "  \"%s\": [%d, %d]%s\n", kv.first.c_str(), kv.second.first,
+                     kv.second.second, ++i < g_tune_cache.size() ? "," : "");
+    std::fprintf(f, "}\n");
+    std::fclose(f);
+}
+
+std::string tune_sig(const char* prec, const char* pass, const DevCsr& M) {
+    char b[256];
+    std::snprintf(b, sizeof b, "%s/%s/rows%d/cols%d/nnz%lld/short%d/long%d/mid%d/huge%d/vw%d",
+                  prec, pass, M.rows, M.cols, static_cast<long long>(M.nnz), M.n_short, M.n_long,
+                  M.n_mid, M.n_huge, M.vw);
+    return b;
+}
+
+template <class T>
+float time_pass(Ctx& c, FastIter<T>& fi, bool primal, cudaEvent_t e0, cudaEvent_t e1) {
+    auto run = [&]() {
+        if (primal) launch_fast_primal(fi, 0, c.stream);
+        else launch_fast_dual(fi, 0, c.stream);
+    };
+    run();
+    run();
+    cudaEventRecord(e0, c.stream);
+    for (int r = 0; r < 5; ++r) run();
+    cudaEventRecord(e1, c.stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+}
+
+// Chooses {lanes, mode} for one pass; fi's matrix fields are set to the choice.
+template <class T>
+void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* lanes,
+               int* mode, cudaEvent_t e0, cudaEvent_t e1) {
+    DevCsr& M = primal ? fi.AT : fi.A;
+    M.iter_vw = M.vw;
+    M.long_mode = 0;
+    *lanes = M.vw;
+    *mode = 0;
+    if (M.rows == 0 || M.nnz < kTuneMinNnz) return;
+    const std::string key = tune_sig(prec_tag, primal ? "primal" : "dual", M);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        tune_read_file();
+        const auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            M.iter_vw = *lanes = it->second.first;
+            M.long_mode = *mode = it->second.second;
+            return;
+        }
+    }
+    std::vector<int> vws{M.vw};
+    if (M.n_short > 0) {
+        if (M.vw > 1) vws.push_back(M.vw / 2);
+        if (M.vw < 32) vws.push_back(M.vw * 2);
+    }
+    std::vector<int> modes{0};
+    if (M.n_mid > 0) modes.push_back(1);
+    float best = time_pass(c, fi, primal, e0, e1);
+    for (int vw : vws)
+        for (int md : modes) {
+            if (vw == *lanes && md == *mode) continue;
+            M.iter_vw = vw;
+            M.long_mode = md;
+            const float t = time_pass(c, fi, primal, e0, e1);
+            if (t < 0.95f * best) {
+                best = t;
+                *lanes = vw;
+                *mode = md;
+            }
+        }
+    M.iter_vw = *lanes;
+    M.long_mode = *mode;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = {*lanes, *mode};
+    tune_write_file();
+}
+
+// Runs on the solve's own buffers before the initial point is written (the
+// timed passes only overwrite iterates that the initial point resets).
+template <class T>
+int tune_iteration(Ctx& c, Launcher& L, FastIter<T>& fi, Ctx::Tuning& t, const char* tag) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    tune_pass(c, fi, true, tag, &t.shape[0], &t.shape[1], e0, e1);
+    tune_pass(c, fi, false, tag, &t.shape[2], &t.shape[3], e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    t.have = true;
+    t.timed = c.ATs.nnz >= kTuneMinNnz;
+    (void)L;
+    return PDHG_OK;
+}
+
 int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, double* rcv) {
     const auto t0 = std::chrono::steady_clock::now();
     std::memset(info, 0, sizeof *info);
@@ -758,6 +946,18 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
     if (rc != PDHG_OK) return rc;
     CK(c.st.alloc(1));
+    if (prec != PDHG_PREC_FP64_EXACT && o.autotune) {
+        Ctx::Tuning& t = c.tuning[prec == PDHG_PREC_MIXED ? 0 : 1];
+        if (!t.have) {
+            rc = reset_state(c, step, omega);  // live state for the timed passes
+            if (rc != PDHG_OK) return rc;
+            Launcher L = make_launcher(c, prec, o, false);
+            rc = prec == PDHG_PREC_MIXED ? tune_iteration(c, L, L.fi32, t, "f32")
+                                         : tune_iteration(c, L, L.fi64, t, "f64");
+            if (rc != PDHG_OK) return rc;
+        }
+        pc.mark("solve: autotune");
+    }
 
     // Initial point (pdhg.cpp:268-270) or the warm start, in scaled space.
     const int32_t n = c.lp.n, m = c.lp.m;
@@ -1092,6 +1292,7 @@ void pdhg_default_options(pdhg_options* o) {
     o->precision = PDHG_PREC_FP64_EXACT;
     o->termination_rule = 0;
     o->polish_iterations = -1;
+    o->autotune = 1;
 }
 
 const char* pdhg_status_string(int s) {
@@ -1236,6 +1437,24 @@ int pdhg_profile_kernels(pdhg_ctx* ctx, int precision, int warmup, int iteration
         ctx->c.err = e.what();
         return PDHG_ERR_BACKEND;
     }
+}
+
+int pdhg_get_tuning(const pdhg_ctx* ctx, int precision, int* out) {
+    if (ctx == nullptr || out == nullptr ||
+        (precision != PDHG_PREC_MIXED && precision != PDHG_PREC_FP64))
+        return PDHG_ERR_INVALID_ARGUMENT;
+    const pdhg::Ctx& c = ctx->c;
+    const pdhg::Ctx::Tuning& t = c.tuning[precision == PDHG_PREC_MIXED ? 0 : 1];
+    if (t.have) {
+        for (int i = 0; i < 4; ++i) out[i] = t.shape[i];
+    } else {
+        out[0] = c.ATs.vw;
+        out[1] = 0;
+        out[2] = c.As.vw;
+        out[3] = 0;
+    }
+    out[4] = t.timed ? 1 : 0;
+    return PDHG_OK;
 }
 
 int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off, const int32_t* col_off,

@@ -46,10 +46,21 @@ struct DevCsr {
     // list every row runs on one thread.
     const int32_t* wrows = nullptr;
     int32_t n_wrows = 0;
+    // The iteration kernels split the long rows once more: up to kHugeRow
+    // entries one warp per row (mid_rows), longer ones one CTA per row.
+    const int32_t* mid_rows = nullptr;
+    const int32_t* huge_rows = nullptr;
+    int32_t n_mid = 0, n_huge = 0;
+    // Iteration-kernel shape (the autotuner's choice): lanes per short row
+    // (0 = vw) and the long-row strategy (0: one CTA per row over long_rows;
+    // 1: one warp per mid row, one CTA per huge row).
+    int iter_vw = 0;
+    int long_mode = 0;
 };
 
 constexpr int kLongRow = 512;
 constexpr int kWarpRow = 32;
+constexpr int kHugeRow = 16384;
 
 // Accumulator slots (bit patterns of non-negative doubles, combined with
 // atomicMax -- order-independent, so exact).
@@ -180,9 +191,9 @@ struct FastIter {
     DevState* st;
 };
 template <class T>
-void launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s);
+int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s);  // kernels launched
 template <class T>
-void launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s);
+int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s);
 template <class T>
 int fast_launches_per_iteration(const FastIter<T>& a);
 
@@ -292,6 +303,9 @@ struct IntakeState {
 void launch_validate(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
                      const double* c, const double* clo, const double* chi, const double* rlo,
                      const double* rhi, int64_t nnz, unsigned* flags, cudaStream_t s);
+// Rows with lo < length <= hi appended to `list`, their number added to *count.
+void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
+                      unsigned long long* count, cudaStream_t s);
 void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                 unsigned long long* counters, cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,

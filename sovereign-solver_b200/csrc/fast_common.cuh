@@ -158,6 +158,77 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
     return block_total(acc);
 }
 
+// 128-bit vectors of each stream a lane keeps in flight in warp_row_dot (a
+// build knob: registers against memory-level parallelism).
+#ifndef PDHG_WARP_UNROLL
+#define PDHG_WARP_UNROLL 4
+#endif
+constexpr int kWarpUnroll = PDHG_WARP_UNROLL;
+
+// Load used for the x / y gathers of warp_row_dot (a build knob).
+#ifndef PDHG_GATHER
+#define PDHG_GATHER __ldg
+#endif
+
+// The same dot by one warp (rows of kLongRow..kHugeRow entries): 128-bit loads
+// of values and indices, kWarpUnroll of each in flight per lane, then a
+// shuffle reduction -- no block barrier, so a CTA's eight warps finish
+// independently. Every lane returns the total.
+template <class T>
+__device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ ci,
+                                          const T* __restrict__ v, const T* __restrict__ xg,
+                                          int b, int e) {
+    constexpr int W = 16 / sizeof(T);
+    const int lane = threadIdx.x & 31;
+    int bA = ((b + W - 1) / W) * W;
+    if (bA > e) bA = e;
+    T acc = T(0);
+    for (int k = b + lane; k < bA; k += 32) acc += __ldcs(v + k) * PDHG_GATHER(xg + __ldcs(ci + k));
+    const int nvec = (e - bA) / W;
+    // rounds of up to kWarpUnroll vectors per lane in flight; the last round
+    // is predicated instead of falling back to one vector at a time
+    if constexpr (W == 4) {
+        const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
+        const float4* v4 = reinterpret_cast<const float4*>(v + bA);
+        for (int q = lane; q < nvec; q += 32 * kWarpUnroll) {
+            int4 c[kWarpUnroll];
+            float4 w[kWarpUnroll];
+#pragma unroll
+            for (int u = 0; u < kWarpUnroll; ++u) {
+                const bool ok = q + 32 * u < nvec;
+                c[u] = ok ? __ldcs(ci4 + q + 32 * u) : make_int4(0, 0, 0, 0);
+                w[u] = ok ? __ldcs(v4 + q + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < kWarpUnroll; ++u)
+                if (q + 32 * u < nvec)
+                    acc += w[u].x * PDHG_GATHER(xg + c[u].x) + w[u].y * PDHG_GATHER(xg + c[u].y) +
+                           w[u].z * PDHG_GATHER(xg + c[u].z) + w[u].w * PDHG_GATHER(xg + c[u].w);
+        }
+    } else {
+        const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
+        const double2* v2 = reinterpret_cast<const double2*>(v + bA);
+        for (int q = lane; q < nvec; q += 32 * kWarpUnroll) {
+            int2 c[kWarpUnroll];
+            double2 w[kWarpUnroll];
+#pragma unroll
+            for (int u = 0; u < kWarpUnroll; ++u) {
+                const bool ok = q + 32 * u < nvec;
+                c[u] = ok ? __ldcs(ci2 + q + 32 * u) : make_int2(0, 0);
+                w[u] = ok ? __ldcs(v2 + q + 32 * u) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kWarpUnroll; ++u)
+                if (q + 32 * u < nvec)
+                    acc += w[u].x * PDHG_GATHER(xg + c[u].x) + w[u].y * PDHG_GATHER(xg + c[u].y);
+        }
+    }
+    for (int k = bA + nvec * W + lane; k < e; k += 32)
+        acc += __ldcs(v + k) * PDHG_GATHER(xg + __ldcs(ci + k));
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
 
 // Epilogue traffic: every per-column array is streamed (evict-first loads and
 // stores) except x_bar, whose lines the dual kernel gathers next and should

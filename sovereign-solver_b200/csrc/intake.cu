@@ -120,6 +120,28 @@ __global__ void k_bin(const int32_t* rp, int32_t rows, int long_threshold, int32
     }
 }
 
+// Rows with lo < length <= hi appended to `list` (grid-stride; one atomic per
+// warp that has any).
+__global__ void k_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
+                            unsigned long long* count) {
+    for (int64_t r0 = blockIdx.x * static_cast<int64_t>(kBlock); r0 < rows;
+         r0 += static_cast<int64_t>(gridDim.x) * kBlock) {
+        const int64_t r = r0 + threadIdx.x;
+        bool in = false;
+        if (r < rows) {
+            const int len = rp[r + 1] - rp[r];
+            in = len > lo && len <= hi;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, in);
+        if (mask == 0u) continue;
+        const int lane = threadIdx.x & 31;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(count, static_cast<unsigned long long>(__popc(mask)));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (in) list[base + __popc(mask & ((1u << lane) - 1u))] = static_cast<int32_t>(r);
+    }
+}
+
 // (|v| * rs_i) * cs_j for entry k of row r (transposed: the row is column j).
 __device__ __forceinline__ double scaled_mag(const DevCsr& M, int transposed, const double* rs,
                                              const double* cs, int r, int k) {
@@ -395,6 +417,12 @@ void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* lo
                 unsigned long long* counters, cudaStream_t s) {
     const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
     if (rows > 0) k_bin<<<g, kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+}
+
+void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
+                      unsigned long long* count, cudaStream_t s) {
+    const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
+    if (rows > 0) k_bin_range<<<g, kBlock, 0, s>>>(rp, rows, lo, hi, list, count);
 }
 
 inline int short_blocks(const DevCsr& M) {

@@ -8,13 +8,13 @@
 //   dual:   over the rows of A: s+ = proj_S(s - tau y), s_bar = 2s+ - s,
 //           y += sigma (s_bar - A x_bar), Cesaro sum.
 //
-// Work split inside one grid (uniform per CTA, no divergence):
-//   CTAs [0, short_blocks)           rows with <= kLongRow nonzeros, VW lanes
-//                                    per row (VW = power of two ~ mean length),
-//                                    lanes stride the row, shuffle reduction;
-//   CTAs [short_blocks, +n_long)     one CTA per long row (listed), 128-bit
-//                                    vector loads of values and indices, block
-//                                    reduction.
+// Work split by row length (one or two launches per pass, see below):
+//   rows with <= kLongRow nonzeros    VW lanes per row (VW = power of two ~
+//                                     mean length), lanes stride the row,
+//                                     shuffle reduction;
+//   rows of kLongRow..kHugeRow        one warp per row, 128-bit vector loads
+//                                     of values and indices, shuffle reduction;
+//   longer rows                       one CTA per row, block reduction.
 // The epilogue of a short row runs on the group's lane 0, so consecutive
 // groups touch consecutive vector entries (coalesced).
 //
@@ -29,6 +29,19 @@
 #include "engine.cuh"
 #include "fast_common.cuh"
 
+// CTAs per SM the iteration kernels are compiled to fit (register budget);
+// build knobs, 1 = no constraint. The short-row kernel is lean: eight CTAs
+// (32 registers) fit in FP32, six in FP64 without spills.
+#ifndef PDHG_SHORT_MIN_CTAS
+#define PDHG_SHORT_MIN_CTAS 8
+#endif
+#ifndef PDHG_SHORT_MIN_CTAS_F64
+#define PDHG_SHORT_MIN_CTAS_F64 6
+#endif
+#ifndef PDHG_LONG_MIN_CTAS
+#define PDHG_LONG_MIN_CTAS 4
+#endif
+
 namespace pdhg {
 
 namespace {
@@ -36,15 +49,29 @@ namespace {
 // ---------------------------------------------------------------------------
 // Iteration kernels
 // ---------------------------------------------------------------------------
+//
+// One SpMV-plus-update pass is split by row length into two kernels, so the
+// short-row kernel keeps its registers (and occupancy) low:
+//   fast_iter       rows of at most kLongRow entries, groups of VW lanes;
+//   fast_iter_long  rows longer than kLongRow: one CTA each (long_mode 0), or
+//                   one warp each up to kHugeRow entries and one CTA each
+//                   above (long_mode 1).
+// `reset` is set on the first kernel of a period's first pass: it clears the
+// flags the previous period's restart kernel consumed.
+
+__device__ __forceinline__ void iter_reset(DevState* st, int reset) {
+    if (reset && blockIdx.x == 0 && threadIdx.x == 0) {
+        st->restart = 0;
+        st->fold = 0;
+    }
+}
 
 // PRIMAL = true: rows of A^T gather y; false: rows of A gather x_bar.
 template <class T, int VW, bool PRIMAL>
-__global__ void __launch_bounds__(kBlock) fast_iter(FastIter<T> a, int first, int short_blocks) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS : PDHG_SHORT_MIN_CTAS_F64)
+    fast_iter(FastIter<T> a, int first, int reset) {
     DevState* st = a.st;
-    if (PRIMAL && first && blockIdx.x == 0 && threadIdx.x == 0) {
-        st->restart = 0;  // consumed by the previous period's restart kernel
-        st->fold = 0;
-    }
+    iter_reset(st, reset);
     if (st->done) return;
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     const T* __restrict__ vals = mvals<T>(M);
@@ -52,20 +79,45 @@ __global__ void __launch_bounds__(kBlock) fast_iter(FastIter<T> a, int first, in
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    if (static_cast<int>(blockIdx.x) < short_blocks) {
-        const int lane = threadIdx.x & (VW - 1);
-        const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
-        if (r >= M.rows) return;
+    const int lane = threadIdx.x & (VW - 1);
+    const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
+    if (r >= M.rows) return;
+    EpiIn<T> in{};
+    if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
+    const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
+    if (e - b > kLongRow) return;  // fast_iter_long handles it
+    T acc = T(0);
+    for (int k = b + lane; k < e; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
+    if (VW > 1) acc = group_sum(acc, VW);
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
+}
+
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, PDHG_LONG_MIN_CTAS)
+    fast_iter_long(FastIter<T> a, int first, int reset, int mid_blocks, int mode) {
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const T* __restrict__ vals = mvals<T>(M);
+    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
+    const PV<T> pv = pvec<T>(a.P);
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    if (mode == 1 && static_cast<int>(blockIdx.x) < mid_blocks) {
+        // one warp per row
+        const int w = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (w >= M.n_mid) return;
+        const int r = __ldg(M.mid_rows + w);
+        const int lane = threadIdx.x & 31;
         EpiIn<T> in{};
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
-        const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
-        if (e - b > kLongRow) return;  // the row's CTA handles it
-        T acc = T(0);
-        for (int k = b + lane; k < e; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
-        if (VW > 1) acc = group_sum(acc, VW);
+        const T acc = warp_row_dot<T>(M.ci, vals, xg, __ldg(M.rp + r), __ldg(M.rp + r + 1));
         if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     } else {
-        const int r = __ldg(M.long_rows + (blockIdx.x - short_blocks));
+        // one CTA per row: every long row (mode 0) or those above kHugeRow
+        const int r = mode == 0 ? __ldg(M.long_rows + blockIdx.x)
+                                : __ldg(M.huge_rows + (blockIdx.x - mid_blocks));
         EpiIn<T> in{};
         if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
         const int b = __ldg(M.rp + r), e = __ldg(M.rp + r + 1);
@@ -74,27 +126,55 @@ __global__ void __launch_bounds__(kBlock) fast_iter(FastIter<T> a, int first, in
     }
 }
 
-inline int short_blocks_for(const DevCsr& M) {
-    if (M.n_short == 0) return 0;
-    return static_cast<int>((static_cast<int64_t>(M.rows) * M.vw + kBlock - 1) / kBlock);
+__global__ void k_clear_flags(DevState* st) {
+    if (threadIdx.x == 0) {
+        st->restart = 0;
+        st->fold = 0;
+    }
 }
 
+inline int iter_lanes(const DevCsr& M) { return M.iter_vw > 0 ? M.iter_vw : M.vw; }
+
+inline int short_blocks_for(const DevCsr& M) {
+    if (M.n_short == 0) return 0;
+    return static_cast<int>((static_cast<int64_t>(M.rows) * iter_lanes(M) + kBlock - 1) / kBlock);
+}
+
+// Kernels one pass over M launches besides the flag reset.
+inline int pass_launches(const DevCsr& M) {
+    if (M.rows == 0) return 0;
+    return (short_blocks_for(M) > 0 ? 1 : 0) + (M.n_long > 0 ? 1 : 0);
+}
+
+// Returns the number of kernels launched.
 template <class T, bool PRIMAL>
-void launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
+int launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     if (M.rows == 0) {
-        return;
+        if (PRIMAL && first) {
+            k_clear_flags<<<1, 32, 0, s>>>(a.st);
+            return 1;
+        }
+        return 0;
     }
     const int sb = short_blocks_for(M);
-    const int grid = sb + M.n_long;
-    switch (M.vw) {
-        case 1: fast_iter<T, 1, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
-        case 2: fast_iter<T, 2, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
-        case 4: fast_iter<T, 4, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
-        case 8: fast_iter<T, 8, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
-        case 16: fast_iter<T, 16, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
-        default: fast_iter<T, 32, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, sb); break;
+    const int mode = M.long_mode;
+    const int mb = mode == 1 ? (M.n_mid + kBlock / 32 - 1) / (kBlock / 32) : 0;
+    const int lb = mode == 1 ? mb + M.n_huge : M.n_long;
+    const int reset_short = (PRIMAL && first) ? 1 : 0;
+    const int reset_long = (PRIMAL && first && sb == 0) ? 1 : 0;
+    if (sb > 0) {
+        switch (iter_lanes(M)) {
+            case 1: fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            case 2: fast_iter<T, 2, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            case 4: fast_iter<T, 4, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            case 8: fast_iter<T, 8, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            case 16: fast_iter<T, 16, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            default: fast_iter<T, 32, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+        }
     }
+    if (lb > 0) fast_iter_long<T, PRIMAL><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb, mode);
+    return (sb > 0 ? 1 : 0) + (lb > 0 ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -471,16 +551,16 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
 }  // namespace
 
 template <class T>
-void launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s) {
-    launch_iter<T, true>(a, first, s);
+int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s) {
+    return launch_iter<T, true>(a, first, s);
 }
 template <class T>
-void launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s) {
-    launch_iter<T, false>(a, first, s);
+int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s) {
+    return launch_iter<T, false>(a, first, s);
 }
 template <class T>
 int fast_launches_per_iteration(const FastIter<T>& a) {
-    return (a.AT.rows > 0 ? 1 : 0) + (a.A.rows > 0 ? 1 : 0);
+    return pass_launches(a.AT) + pass_launches(a.A);
 }
 
 template <class T>
@@ -507,10 +587,10 @@ int fast_check_grid(const DevCsr& A, const DevCsr& AT) {
     return short_blocks_for(A) + A.n_long + short_blocks_for(AT) + AT.n_long + 1;
 }
 
-template void launch_fast_primal<float>(const FastIter<float>&, int, cudaStream_t);
-template void launch_fast_primal<double>(const FastIter<double>&, int, cudaStream_t);
-template void launch_fast_dual<float>(const FastIter<float>&, int, cudaStream_t);
-template void launch_fast_dual<double>(const FastIter<double>&, int, cudaStream_t);
+template int launch_fast_primal<float>(const FastIter<float>&, int, cudaStream_t);
+template int launch_fast_primal<double>(const FastIter<double>&, int, cudaStream_t);
+template int launch_fast_dual<float>(const FastIter<float>&, int, cudaStream_t);
+template int launch_fast_dual<double>(const FastIter<double>&, int, cudaStream_t);
 template int fast_launches_per_iteration<float>(const FastIter<float>&);
 template int fast_launches_per_iteration<double>(const FastIter<double>&);
 template void launch_fast_check<float>(const FastCheck<float>&, cudaStream_t);

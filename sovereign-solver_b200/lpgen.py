@@ -151,6 +151,29 @@ def badly_scaled_lp(m: int = 200_000, n: int = 500_000, k: int = 8, seed: int = 
     return A
 
 
+def row_lengths_lp(lengths: list[int], n: int, seed: int = 0) -> Problem:
+    """Equality LP of config-0 structure whose row i has exactly lengths[i]
+    nonzeros (distinct random columns), to exercise every row-length tier of
+    the kernels (short rows, warp rows, CTA rows)."""
+    rng = np.random.default_rng(seed)
+    m = len(lengths)
+    cols = [np.sort(rng.choice(n, size=k, replace=False)) for k in lengths]
+    row_ptr = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum([len(c) for c in cols], out=row_ptr[1:])
+    col_idx = np.concatenate(cols).astype(np.int64)
+    val = rng.standard_normal(col_idx.size)
+    A = Problem(m=m, n=n, row_ptr=row_ptr, col_idx=col_idx, val=val, c=np.zeros(n),
+                col_lo=np.zeros(n), col_hi=np.full(n, 10.0), row_lo=np.zeros(m),
+                row_hi=np.zeros(m), name=f"row_lengths_{m}x{n}_s{seed}")
+    x0 = rng.uniform(0.0, 10.0, n)
+    y0 = rng.standard_normal(m)
+    b = csr_matvec(A, x0)
+    A.row_lo = b.copy()
+    A.row_hi = b.copy()
+    A.c = csr_rmatvec(A, y0) + rng.uniform(0.0, 1.0, n)
+    return A
+
+
 def batch_family(count: int = 4096, seed_base: int = 3000, m_lo: int = 50,
                  m_hi: int = 5000) -> list[Problem]:
     out = []

@@ -44,7 +44,8 @@ class _Options(C.Structure):
                 ("restart_rule", C.c_int), ("primal_weight_update", C.c_int),
                 ("x0", _dp), ("y0", _dp), ("checkpoint", CHECKPOINT_FN),
                 ("checkpoint_user", C.c_void_p), ("cancel_flag", C.POINTER(C.c_int)),
-                ("trace_iters", C.c_int), ("trace_x", _dp), ("trace_y", _dp)]
+                ("trace_iters", C.c_int), ("trace_x", _dp), ("trace_y", _dp),
+                ("autotune", C.c_int)]
 
 
 class _Info(C.Structure):
@@ -103,6 +104,7 @@ def lib() -> C.CDLL:
         L.pdhg_scaling.argtypes = [C.c_int32, C.c_int32, C.c_int64, _ip, _ip, _dp,
                                    C.POINTER(_Options), _dp, _dp]
         L.pdhg_get_scaling.argtypes = [C.c_void_p, _dp, _dp]
+        L.pdhg_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.pdhg_load_batch.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, C.c_int64, _ip, _ip, _dp,
                                       _dp, _dp, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.pdhg_solve_batch.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Info), _dp,
@@ -150,6 +152,7 @@ class PdhgOptions:
     primal_weight_update: bool = False
     checkpoint: Optional[Callable[[int, np.ndarray, np.ndarray, float], None]] = None
     trace_iters: int = 0
+    autotune: bool = True
 
 
 @dataclass
@@ -406,6 +409,13 @@ class Engine:
         cs = np.zeros(max(p.n, 1))
         _check(lib().pdhg_get_scaling(self._h, _d(rs), _d(cs)), "pdhg_get_scaling", self._h)
         return rs[: p.m], cs[: p.n]
+
+    def tuning(self, precision: str = "mixed") -> dict:
+        """The iteration-kernel shapes in use for the loaded LP (pdhg_get_tuning)."""
+        out = (C.c_int * 5)()
+        _check(lib().pdhg_get_tuning(self._h, PREC[precision], out), "pdhg_get_tuning", self._h)
+        return {"primal_lanes": out[0], "primal_long_mode": out[1], "dual_lanes": out[2],
+                "dual_long_mode": out[3], "timed": bool(out[4])}
 
     def profile_kernels(self, precision: str = "mixed", warmup: int = 3,
                         iterations: int = 20) -> list[dict]:

@@ -46,7 +46,8 @@ def test_defaults_are_the_reference_defaults(pkg):
     assert o.ruiz_iterations == 8 and o.ruiz_tolerance == 1e-2
     assert o.pock_chambolle_alpha == 1.0 and o.apply_ruiz == 1 and o.apply_pock_chambolle == 1
     assert o.precision == 0 and o.termination_rule == 0
-    assert lib.pdhg_abi_version() == 1
+    assert o.autotune == 1  # an engine extension; it never applies to fp64_exact
+    assert lib.pdhg_abi_version() == 2
     d = pkg.PdhgOptions()
     assert d.tolerance == o.tolerance and d.max_iterations == o.max_iterations
 
@@ -93,4 +94,4 @@ def test_header_documents_each_entry_with_a_reference_citation():
         assert re.search(r"\w+\.(?:cpp|hpp):\d+", block) or n in (
             "pdhg_abi_version", "pdhg_default_options", "pdhg_last_error",
             "pdhg_profile_kernels", "pdhg_destroy", "pdhg_stream",
-            "pdhg_csr_spmv_noalloc"), n
+            "pdhg_csr_spmv_noalloc", "pdhg_get_tuning"), n

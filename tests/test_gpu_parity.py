@@ -220,6 +220,25 @@ def test_fp64_mode_on_a_power_law_lp_tracks_exact_mode(pkg, engine):
     assert r2.iterations == ex.iterations
 
 
+def test_fp64_mode_tracks_exact_mode_across_row_tiers(pkg, engine):
+    # rows of 8 (lane groups), 600 and 3,000 (one warp) and 20,000 nonzeros
+    # (one CTA): the FP64 iterates stay within 1e-10 of the exact ones over
+    # the first 100 iterations (no check among them, so no restart decision
+    # can flip), and mixed mode converges to the same optimum
+    p = pkg.lpgen.row_lengths_lp([20_000] + [3_000] * 4 + [600] * 20 + [8] * 200, 25_000, seed=5)
+    kw = dict(max_iterations=300, tolerance=1e-12, restart_check_period=150)
+    ex = solve(pkg, engine, p, trace_iters=100, **kw)
+    r2 = solve(pkg, engine, p, precision="fp64", trace_iters=100, **kw)
+    for k in range(100):
+        assert rel_err(r2.trace_x[k], ex.trace_x[k]) <= 1e-10, k
+        assert rel_err(r2.trace_y[k], ex.trace_y[k]) <= 1e-10, k
+    full = dict(termination_rule="relative_kkt", restart_rule="adaptive", max_iterations=200_000)
+    r64 = solve(pkg, engine, p, precision="fp64", **full)
+    r32 = solve(pkg, engine, p, precision="mixed", **full)
+    assert r64.status == r32.status == "optimal"
+    assert abs(r32.objective - r64.objective) <= 2e-3 * max(1.0, abs(r64.objective))
+
+
 def test_device_scaling_is_the_reference_scaling(pkg, orc, engine):
     for p in (pkg.lpgen.badly_scaled_lp(1500, 4000, 6, seed=22),
               pkg.lpgen.random_equality_lp(300, 700, 5, seed=2),
