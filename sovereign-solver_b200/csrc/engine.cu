@@ -845,26 +845,31 @@ void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* 
             return;
         }
     }
+    // candidates, the binning's choice first
+    std::vector<std::pair<int, int>> cand{{M.vw, 0}};
     std::vector<int> vws{M.vw};
     if (M.n_short > 0) {
         if (M.vw > 1) vws.push_back(M.vw / 2);
         if (M.vw < 32) vws.push_back(M.vw * 2);
     }
-    std::vector<int> modes{0};
-    if (M.n_mid > 0) modes.push_back(1);
-    float best = time_pass(c, fi, primal, e0, e1);
-    for (int vw : vws)
-        for (int md : modes) {
-            if (vw == *lanes && md == *mode) continue;
-            M.iter_vw = vw;
-            M.long_mode = md;
-            const float t = time_pass(c, fi, primal, e0, e1);
-            if (t < 0.95f * best) {
-                best = t;
-                *lanes = vw;
-                *mode = md;
-            }
+    for (int vw : vws) {
+        if (vw != M.vw) cand.push_back({vw, 0});
+        if (M.n_mid > 0) cand.push_back({vw, 1});
+    }
+    // two rounds over all candidates, each keeping its faster time, so no
+    // candidate is judged on a cold GPU (clocks ramping, first launches)
+    std::vector<float> t(cand.size(), 3.0e38f);
+    for (int round = 0; round < 2; ++round)
+        for (size_t i = 0; i < cand.size(); ++i) {
+            M.iter_vw = cand[i].first;
+            M.long_mode = cand[i].second;
+            t[i] = std::min(t[i], time_pass(c, fi, primal, e0, e1));
         }
+    size_t pick = 0;
+    for (size_t i = 1; i < cand.size(); ++i)
+        if (t[i] < 0.95f * t[pick]) pick = i;
+    *lanes = cand[pick].first;
+    *mode = cand[pick].second;
     M.iter_vw = *lanes;
     M.long_mode = *mode;
     std::lock_guard<std::mutex> lock(g_tune_mutex);

@@ -39,7 +39,10 @@
 #define PDHG_SHORT_MIN_CTAS_F64 6
 #endif
 #ifndef PDHG_LONG_MIN_CTAS
-#define PDHG_LONG_MIN_CTAS 4
+#define PDHG_LONG_MIN_CTAS 6
+#endif
+#ifndef PDHG_WARPROW_MIN_CTAS
+#define PDHG_WARPROW_MIN_CTAS 4
 #endif
 
 namespace pdhg {
@@ -92,9 +95,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
 }
 
-template <class T, bool PRIMAL>
-__global__ void __launch_bounds__(kBlock, PDHG_LONG_MIN_CTAS)
-    fast_iter_long(FastIter<T> a, int first, int reset, int mid_blocks, int mode) {
+template <class T, bool PRIMAL, int MODE>
+__global__ void __launch_bounds__(kBlock, MODE == 0 ? PDHG_LONG_MIN_CTAS : PDHG_WARPROW_MIN_CTAS)
+    fast_iter_long(FastIter<T> a, int first, int reset, int mid_blocks) {
     DevState* st = a.st;
     iter_reset(st, reset);
     if (st->done) return;
@@ -104,7 +107,7 @@ __global__ void __launch_bounds__(kBlock, PDHG_LONG_MIN_CTAS)
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    if (mode == 1 && static_cast<int>(blockIdx.x) < mid_blocks) {
+    if (MODE == 1 && static_cast<int>(blockIdx.x) < mid_blocks) {
         // one warp per row
         const int w = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
         if (w >= M.n_mid) return;
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(kBlock, PDHG_LONG_MIN_CTAS)
         if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     } else {
         // one CTA per row: every long row (mode 0) or those above kHugeRow
-        const int r = mode == 0 ? __ldg(M.long_rows + blockIdx.x)
+        const int r = MODE == 0 ? __ldg(M.long_rows + blockIdx.x)
                                 : __ldg(M.huge_rows + (blockIdx.x - mid_blocks));
         EpiIn<T> in{};
         if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
@@ -173,7 +176,10 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
             default: fast_iter<T, 32, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
         }
     }
-    if (lb > 0) fast_iter_long<T, PRIMAL><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb, mode);
+    if (lb > 0) {
+        if (mode == 1) fast_iter_long<T, PRIMAL, 1><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb);
+        else fast_iter_long<T, PRIMAL, 0><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb);
+    }
     return (sb > 0 ? 1 : 0) + (lb > 0 ? 1 : 0);
 }
 
