@@ -217,6 +217,42 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def batch_line(pkg, eng, args, rank: int) -> dict:
+    """Config 3: a seeded family of config-0-structure LPs (m log-uniform in
+    [50, 5000], n = 2-3 m, 4-10 nonzeros per column), solved to 1e-4 relative
+    KKT in one batched solve (pdhg_solve_batch: one CUDA-graph launch), beside
+    the plain single-LP engine on the first instances of the same family."""
+    ps = pkg.lpgen.batch_family(args.batch_instances, seed_base=3000 + 100_000 * rank)
+    opt = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
+                          restart_rule="adaptive", tolerance=1e-4, max_iterations=200_000)
+    with pkg.Engine(eng.device) as e:
+        e.load_batch(ps)
+        e.solve_batch(opt, want_point=False)  # warm-up
+        t0 = time.perf_counter()
+        e.load_batch(ps)
+        rs = e.solve_batch(opt, want_point=False)
+        t_batch = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        plain = []
+        for p in ps[: args.plain_instances]:
+            e.load(p)
+            plain.append(e.solve(opt, want_point=False))
+        t_plain = time.perf_counter() - t0
+    solved = sum(r.status == "optimal" for r in rs)
+    plain_solved = sum(r.status == "optimal" for r in plain)
+    its = sorted(r.iterations for r in rs)
+    return {"workload": f"{len(ps)} seeded LPs, m log-uniform [50, 5000], n = 2-3 m, "
+                        f"4-10 nnz/column ({sum(p.nnz for p in ps):,} nnz), rel KKT 1e-4, mixed",
+            "solved": solved, "seconds": t_batch, "solves_per_s": solved / t_batch,
+            "iterations_median": its[len(its) // 2], "iterations_max": its[-1],
+            "polished": sum(r.fp64_iterations > 0 for r in rs),
+            "gpu_launches": rs[0].kernel_launches if rs else 0,
+            "plain_gpu": {"instances": len(plain), "solved": plain_solved, "seconds": t_plain,
+                          "solves_per_s": plain_solved / t_plain},
+            "timing": "host wall clock around load + solve on both sides (pdhg_load_batch + "
+                      "pdhg_solve_batch; per instance pdhg_load_problem + pdhg_solve)"}
+
+
 def profile_case(args) -> None:
     """One solve on a transportation LP of the given size: the ncu target."""
     import torch
@@ -243,6 +279,10 @@ def main() -> None:
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--full-solve-cap", type=int, default=60_000)
+    ap.add_argument("--batch-instances", type=int, default=256,
+                    help="config-3 family size for the batched line (0 = skip)")
+    ap.add_argument("--plain-instances", type=int, default=16,
+                    help="instances of that family solved one at a time for comparison")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiler target: load the LP and run one solve of --iters-per-step "
                          "iterations, nothing else")
@@ -363,6 +403,8 @@ def main() -> None:
     full = eng.solve(solve_opts, want_point=False)
     full_s = time.perf_counter() - t0
 
+    batch = batch_line(pkg, eng, args, rank) if args.batch_instances > 0 else None
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -384,6 +426,8 @@ def main() -> None:
                        "lps_solved_per_s": (1.0 / full_s) if full.status == "optimal" else 0.0,
                        "restarts": full.restarts, "objective": full.objective},
     }
+    if batch is not None:
+        line["batch"] = batch
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prob)
     eng.close()

@@ -245,6 +245,40 @@ int pdhg_csr_spmv_noalloc(int transpose, int32_t m, int32_t n, int64_t nnz,
                           const double* d_values, double alpha, const double* d_x, double beta,
                           double* d_y, void* stream);
 
+/* Learned warm start: the network that maps an LP family's parameters to
+ * solution-basis coefficients. No counterpart in the reference (its PDHG has
+ * no warm start, pdhg.cpp:268-270 starts from proj(0), 0); the engine uses
+ * the prediction through pdhg_options.x0 / y0. A 2-hidden-layer ReLU MLP
+ * (n_in -> hidden -> hidden -> n_out, all multiples of 8) whose products run
+ * on the tensor cores (tcgen05, BF16 operands, FP32 accumulation) and whose
+ * training is Adam on FP32 master weights. Parameter order everywhere:
+ * W1 (hidden x n_in, row-major), b1, W2 (hidden x hidden), b2,
+ * W3 (n_out x hidden), b3. Batches are multiples of 8 up to max_batch; all
+ * buffers are host FP32. */
+typedef struct pdhg_mlp pdhg_mlp;
+int pdhg_mlp_create(int device, int n_in, int hidden, int n_out, int max_batch, pdhg_mlp** out);
+int pdhg_mlp_destroy(pdhg_mlp* mlp);
+const char* pdhg_mlp_last_error(const pdhg_mlp* mlp);
+int64_t pdhg_mlp_param_count(const pdhg_mlp* mlp);
+int pdhg_mlp_set_params(pdhg_mlp* mlp, const float* params); /* also resets Adam */
+int pdhg_mlp_get_params(pdhg_mlp* mlp, float* params);
+/* y (batch x n_out) = network(x (batch x n_in)) */
+int pdhg_mlp_forward(pdhg_mlp* mlp, int batch, const float* x, float* y);
+/* One forward + backward: gradients of L = sum (y - t)^2 / (batch n_out)
+ * in parameter order, and L itself. */
+int pdhg_mlp_gradients(pdhg_mlp* mlp, int batch, const float* x, const float* t,
+                       float* grads, float* loss);
+/* Adam over `epochs` shuffled passes of `samples` rows of x / t (seeded),
+ * mini-batches of `batch`; epoch_loss (epochs entries, may be NULL) gets each
+ * epoch's mean loss. */
+int pdhg_mlp_train(pdhg_mlp* mlp, int64_t samples, const float* x, const float* t, int epochs,
+                   int batch, float lr, uint64_t seed, float* epoch_loss);
+/* The network's tensor-core GEMM alone (engine extension, for tests):
+ * c (m x n) = a (m x k) b (n x k)^T (+ bias (n), ReLU), operands rounded to
+ * BF16, FP32 accumulation; k a multiple of 8; host FP32 buffers. */
+int pdhg_gemm_bf16(int device, int m, int n, int k, const float* a, const float* b,
+                   const float* bias, int relu, float* c);
+
 /* Scaling::equilibrate(CsrMatrix) (src/l1/scaling.cpp:19-104) on the host
  * (FP64, the reference's order), for callers without a device. */
 int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,

@@ -1,11 +1,13 @@
 """B200-native PDHG LP engine (drop-in for sovereign-solver's ``Pdhg::solve``).
 
 The engine is ``libpdhg_b200.so`` (CUDA kernels + C-ABI, include/pdhg_b200.h).
-This package holds its Python face (``pdhg``), the LP container (``problem``)
-and the seeded workload generators (``lpgen``).
+This package holds its Python face (``pdhg``), the LP container (``problem``),
+the seeded workload generators (``lpgen``) and the learned warm start's
+network (``mlp``).
 """
 from .problem import INF, Problem  # noqa: F401
 from . import lpgen  # noqa: F401
+from . import mlp  # noqa: F401
 from .pdhg import (  # noqa: F401
     CancellationToken, Engine, Pdhg, PdhgError, PdhgOptions, PdhgResult, csr_spmv, project_box,
     scaling,

@@ -278,6 +278,7 @@ class Engine:
         h = C.c_void_p()
         _check(lib().pdhg_create(device, C.byref(h)), "pdhg_create")
         self._h = h
+        self.device = device
         self.problem: Optional[Problem] = None
 
     def stream_handle(self) -> int:
