@@ -253,6 +253,71 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
                       "pdhg_solve_batch; per instance pdhg_load_problem + pdhg_solve)"}
 
 
+def warmstart_line(pkg, eng, args, rank: int) -> dict:
+    """Config 4 at reduced size: a parametric family over a config-2-structure
+    base (500 rows, 1,200 columns, 6,000 nonzeros; 64 parameters moving b and
+    c by ~10%). Training solves from the batched engine, basis + network
+    (tensor-core training), then on held-out parameters: plain single-LP GPU
+    PDHG from the cold start, batched cold, and batched with the gated learned
+    warm start. Solves/s include, for the warm line, prediction and gating."""
+    W = pkg.warmstart
+    fam = pkg.lpgen.parametric_family(500, 1200, 5, seed=4001)
+    opt = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
+                          restart_rule="adaptive", primal_weight_update=True, tolerance=1e-4,
+                          max_iterations=300_000)
+    tr_th = fam.thetas(args.ws_train, seed=1 + 1000 * rank)
+    te_th = fam.thetas(args.ws_test, seed=2 + 1000 * rank)
+    tr = [fam.instance(t) for t in tr_th]
+    te = [fam.instance(t) for t in te_th]
+    with pkg.Engine(eng.device) as e:
+        t0 = time.perf_counter()
+        res = W.solve_family(e, tr, opt)
+        t_train_solves = time.perf_counter() - t0
+        ws = W.LearnedWarmStart(fam, rank=64, hidden=512, device=eng.device)
+        t0 = time.perf_counter()
+        rep = ws.fit(tr_th, res, epochs=600, batch=64, lr=1e-3)
+        t_fit = time.perf_counter() - t0
+        W.solve_family(e, te[:8], opt)  # warm-up
+        t0 = time.perf_counter()
+        cold = W.solve_family(e, te, opt)
+        t_cold = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        x0s, y0s, used, kw, kc = ws.starts(e, te, te_th, opt)
+        warm = W.solve_family(e, te, opt, x0s, y0s)
+        t_warm = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        plain = []
+        for p in te[: args.plain_instances]:
+            e.load(p)
+            plain.append(e.solve(opt, want_point=False))
+        t_plain = time.perf_counter() - t0
+    ok = lambda rs: sum(r.status == "optimal" for r in rs)  # noqa: E731
+    plain_rate = ok(plain) / t_plain
+    warm_rate = ok(warm) / t_warm
+    return {"workload": f"parametric family over a config-2-structure base (500 x 1,200, 6,000 "
+                        f"nnz, 64 parameters, b and c moved ~10%); {len(tr)} training solves, "
+                        f"{len(te)} held-out; mixed, rel KKT 1e-4, adaptive restarts, primal "
+                        f"weight",
+            "training": {"solves_s": t_train_solves, "solved": ok(res), "fit_s": t_fit,
+                         "basis_rank": rep.rank, "explained_primal": rep.explained_primal,
+                         "explained_dual": rep.explained_dual, "val_loss": ws.val_loss},
+            "gate": {"warm_used": int(used.sum()), "start_kkt_warm_median": float(np.median(kw)),
+                     "start_kkt_cold_median": float(np.median(kc))},
+            "plain_gpu": {"instances": len(plain), "solved": ok(plain), "seconds": t_plain,
+                          "solves_per_s": plain_rate,
+                          "iterations_mean": float(np.mean([r.iterations for r in plain]))},
+            "batched_cold": {"solved": ok(cold), "seconds": t_cold, "solves_per_s": ok(cold) / t_cold,
+                             "iterations_mean": float(np.mean([r.iterations for r in cold]))},
+            "batched_learned_warm": {"solved": ok(warm), "seconds": t_warm,
+                                     "solves_per_s": warm_rate,
+                                     "iterations_mean": float(np.mean([r.iterations for r in warm])),
+                                     "max_relative_kkt": float(max(r.relative_kkt for r in warm
+                                                                   if r.status == "optimal"))},
+            "speedup_vs_plain_gpu": warm_rate / plain_rate if plain_rate > 0 else None,
+            "timing": "host wall clock; batched lines include load, the warm line also "
+                      "prediction and the start-KKT gate"}
+
+
 def profile_case(args) -> None:
     """One solve on a transportation LP of the given size: the ncu target."""
     import torch
@@ -283,6 +348,9 @@ def main() -> None:
                     help="config-3 family size for the batched line (0 = skip)")
     ap.add_argument("--plain-instances", type=int, default=16,
                     help="instances of that family solved one at a time for comparison")
+    ap.add_argument("--ws-train", type=int, default=1024,
+                    help="config-4 training solves for the learned warm start (0 = skip)")
+    ap.add_argument("--ws-test", type=int, default=128, help="config-4 held-out instances")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiler target: load the LP and run one solve of --iters-per-step "
                          "iterations, nothing else")
@@ -404,6 +472,7 @@ def main() -> None:
     full_s = time.perf_counter() - t0
 
     batch = batch_line(pkg, eng, args, rank) if args.batch_instances > 0 else None
+    warm = warmstart_line(pkg, eng, args, rank) if args.ws_train > 0 else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -428,6 +497,8 @@ def main() -> None:
     }
     if batch is not None:
         line["batch"] = batch
+    if warm is not None:
+        line["warmstart"] = warm
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prob)
     eng.close()

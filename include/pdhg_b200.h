@@ -188,6 +188,16 @@ int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off,
                     const double* col_hi, const double* row_lo, const double* row_hi);
 int pdhg_solve_batch(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* infos, double* x,
                      double* y, double* rc);
+/* Relative KKT residual of candidate starting points for the loaded batch,
+ * one value per instance: x (n) and y (m) stacked like pdhg_solve_batch's
+ * outputs, original units and sense, NULL = zero vector (the cold start).
+ * PDLP's measure with l2 norms -- max(||primal bound violation of A clamp(x)||
+ * / (1 + ||b||), ||dual sign violations|| / (1 + ||c||), objective gap) -- so a
+ * point near the optimum scores near 0 even where it is not exactly at its
+ * bounds. Engine extension for the learned warm start, which keeps a
+ * predicted start only where it beats the cold start on this measure (the
+ * reference has no warm start: pdhg.cpp:268-270). */
+int pdhg_batch_start_kkt(pdhg_ctx* ctx, const double* x, const double* y, double* kkt);
 
 /* Iteration-kernel shapes in use for the loaded problem in `precision`
  * (PDHG_PREC_MIXED or PDHG_PREC_FP64): out[0] lanes per short row and out[1]

@@ -820,4 +820,23 @@ int batch_solve_abi(BatchCtx& c, const pdhg_options* options, pdhg_info* infos, 
 
 int32_t batch_count(const BatchCtx& c) { return c.loaded ? c.count : 0; }
 
+int batch_point_kkt_abi(BatchCtx& c, const double* x, const double* y, double* kkt) {
+    if (!c.loaded || kkt == nullptr) {
+        c.err = "pdhg_batch_start_kkt: no batch loaded or kkt is NULL";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    BCK(cudaSetDevice(c.device));
+    cudaStream_t s = c.stream;
+    DBuf<double> xd, yd, out;
+    if (x != nullptr) BCK(upload(xd, x, static_cast<size_t>(c.n), s));
+    if (y != nullptr) BCK(upload(yd, y, static_cast<size_t>(c.m), s));
+    BCK(out.alloc(static_cast<size_t>(c.count)));
+    launch_batch_point_kkt(c.view(), x != nullptr ? xd.p : nullptr, y != nullptr ? yd.p : nullptr,
+                           out.p, s);
+    BCK(cudaGetLastError());
+    BCK(cudaMemcpyAsync(kkt, out.p, sizeof(double) * c.count, cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    return PDHG_OK;
+}
+
 }  // namespace pdhg

@@ -646,7 +646,78 @@ __global__ void __launch_bounds__(kBlock) batch_final(BatchView b, Iterates<T> i
     }
 }
 
+// Relative KKT residual of a given point (x, y in original units and sense; a
+// null pointer is the zero vector), per instance, the PDLP way with l2 norms:
+// primal: ||bound violation of A clamp(x)||; dual: sign violations of the row
+// duals and of the reduced costs against the column bounds (a boxed column
+// admits any reduced cost); gap: |primal - dual objective| / (1 + |p| + |d|),
+// infinite bounds dropped from the dual objective (their violations are in the
+// dual term). Internal minimize sense: y and c times the objective sign.
+__global__ void __launch_bounds__(kBlock) batch_point_kkt(BatchView b, const double* x,
+                                                          const double* y, double* out) {
+    const int k = blockIdx.x;
+    const InstState& s = b.is[k];
+    const DevProblem& P = b.P;
+    const double sign = s.obj_sign;
+    const int lane = threadIdx.x & 31;
+    const int groups = kBlock / 32;
+    double rp2 = 0.0, rd2 = 0.0, pobj = 0.0, dobj = 0.0, bn2 = 0.0, cn2 = 0.0;
+    auto xc = [&](int j) {
+        const double v = x != nullptr ? x[j] : 0.0;
+        return clampT<double>(v, P.lo_o[j], P.hi_o[j]);
+    };
+    for (int i = b.row_off[k] + static_cast<int>(threadIdx.x) / 32; i < b.row_off[k + 1];
+         i += groups) {
+        const double act = row_dot64(b.Ao, i, lane, 32, xc);
+        if (lane != 0) continue;
+        const double lo = P.rlo_o[i], hi = P.rhi_o[i];
+        double v = 0.0;
+        if (fb(lo) && act < lo) v = lo - act;
+        if (fb(hi) && act > hi) v = act - hi;
+        rp2 += v * v;
+        const double bb = smax(fb(lo) ? fabs(lo) : 0.0, fb(hi) ? fabs(hi) : 0.0);
+        bn2 += bb * bb;
+        const double yi = y != nullptr ? sign * y[i] : 0.0;
+        double dv = 0.0;
+        if (!fb(lo) && yi > 0.0) dv = yi;   // only an upper bound: y <= 0
+        if (!fb(hi) && yi < 0.0) dv = -yi;  // only a lower bound: y >= 0
+        rd2 += dv * dv;
+        if (yi > 0.0 && fb(lo)) dobj += yi * lo;
+        else if (yi < 0.0 && fb(hi)) dobj += yi * hi;
+    }
+    for (int j = b.col_off[k] + static_cast<int>(threadIdx.x) / 32; j < b.col_off[k + 1];
+         j += groups) {
+        const double aty = row_dot64(b.ATo, j, lane, 32, [y, sign](int i) {
+            return y != nullptr ? sign * y[i] : 0.0;
+        });
+        if (lane != 0) continue;
+        const double cj = sign * P.c_o[j];
+        const double rc = cj - aty;
+        const double lo = P.lo_o[j], hi = P.hi_o[j];
+        pobj += cj * xc(j);
+        cn2 += cj * cj;
+        double dv = 0.0;
+        if (fb(lo) && !fb(hi) && rc < 0.0) dv = -rc;
+        else if (!fb(lo) && fb(hi) && rc > 0.0) dv = rc;
+        else if (!fb(lo) && !fb(hi)) dv = fabs(rc);
+        rd2 += dv * dv;
+        if (rc > 0.0 && fb(lo)) dobj += rc * lo;
+        else if (rc < 0.0 && fb(hi)) dobj += rc * hi;
+    }
+    const double a = block_sum_det(rp2), d2 = block_sum_det(rd2), p = block_sum_det(pobj);
+    const double dd = block_sum_det(dobj), bn = block_sum_det(bn2), cn = block_sum_det(cn2);
+    if (threadIdx.x == 0) {
+        const double gap = fabs(p - dd) / (1.0 + fabs(p) + fabs(dd));
+        out[k] = smax(smax(sqrt(a) / (1.0 + sqrt(bn)), sqrt(d2) / (1.0 + sqrt(cn))), gap);
+    }
+}
+
 }  // namespace
+
+void launch_batch_point_kkt(const BatchView& b, const double* x, const double* y, double* out,
+                            cudaStream_t s) {
+    if (b.count > 0) batch_point_kkt<<<b.count, kBlock, 0, s>>>(b, x, y, out);
+}
 
 // ---------------------------------------------------------------------------
 // Launchers

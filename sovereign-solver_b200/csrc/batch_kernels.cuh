@@ -101,6 +101,11 @@ void launch_batch_scale_vectors(const BatchView& b, double* c_s, double* lo_s, d
                                 double* rlo_s, double* rhi_s, cudaStream_t s);
 void launch_batch_norms(const BatchView& b, cudaStream_t s);
 
+// PDLP-style relative KKT residual of a given point per instance (original
+// units and sense; a null x or y is the zero vector).
+void launch_batch_point_kkt(const BatchView& b, const double* x, const double* y, double* out,
+                            cudaStream_t s);
+
 // Internal status of an instance whose FP32 phase stalled (mixed mode).
 constexpr int kBatchStalled = 100;
 

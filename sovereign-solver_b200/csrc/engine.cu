@@ -1502,6 +1502,21 @@ int pdhg_solve_batch(pdhg_ctx* ctx, const pdhg_options* options, pdhg_info* info
     }
 }
 
+int pdhg_batch_start_kkt(pdhg_ctx* ctx, const double* x, const double* y, double* kkt) {
+    if (ctx == nullptr) return PDHG_ERR_INVALID_ARGUMENT;
+    pdhg::Ctx& cx = ctx->c;
+    if (cx.batch == nullptr || pdhg::batch_count(*cx.batch) == 0) {
+        cx.err = "pdhg_batch_start_kkt: no batch loaded";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        return pdhg::batch_point_kkt_abi(*cx.batch, x, y, kkt);
+    } catch (const std::exception& e) {
+        cx.err = e.what();
+        return PDHG_ERR_BACKEND;
+    }
+}
+
 int pdhg_csr_spmv(int device, int transpose, int32_t m, int32_t n, int64_t nnz,
                   const int32_t* row_ptr, const int32_t* col_idx, const double* values,
                   double alpha, const double* x, double beta, double* y) {

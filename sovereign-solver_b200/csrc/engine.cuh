@@ -342,5 +342,6 @@ int batch_load_abi(BatchCtx& c, int32_t count, const int32_t* row_off, const int
 int batch_solve_abi(BatchCtx& c, const pdhg_options* options, pdhg_info* infos, double* x,
                     double* y, double* rc);
 int32_t batch_count(const BatchCtx& c);
+int batch_point_kkt_abi(BatchCtx& c, const double* x, const double* y, double* kkt);
 
 }  // namespace pdhg

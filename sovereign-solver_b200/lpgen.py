@@ -26,6 +26,7 @@ Families:
 """
 from __future__ import annotations
 
+import dataclasses
 import math
 
 import numpy as np
@@ -125,6 +126,12 @@ def transportation_lp(supplies: int = 2000, demands: int = 5000, seed: int = 100
 
 def badly_scaled_lp(m: int = 200_000, n: int = 500_000, k: int = 8, seed: int = 2000,
                     zipf_s: float = 1.1, ineq_frac: float = 0.3) -> Problem:
+    return _badly_scaled_with_point(m, n, k, seed, zipf_s, ineq_frac)[0]
+
+
+def _badly_scaled_with_point(m: int, n: int, k: int, seed: int, zipf_s: float = 1.1,
+                             ineq_frac: float = 0.3):
+    """badly_scaled_lp and the interior point x0 its b was built from."""
     rng = np.random.default_rng(seed)
     ranks = rng.permutation(m) + 1
     p = ranks.astype(np.float64) ** (-zipf_s)
@@ -148,7 +155,7 @@ def badly_scaled_lp(m: int = 200_000, n: int = 500_000, k: int = 8, seed: int = 
     A.col_lo, A.col_hi = lo, hi
     A.row_lo = np.where(ineq, -INF, b)
     A.row_hi = b
-    return A
+    return A, x0
 
 
 def row_lengths_lp(lengths: list[int], n: int, seed: int = 0) -> Problem:
@@ -172,6 +179,63 @@ def row_lengths_lp(lengths: list[int], n: int, seed: int = 0) -> Problem:
     A.row_hi = b.copy()
     A.c = csr_rmatvec(A, y0) + rng.uniform(0.0, 1.0, n)
     return A
+
+
+@dataclasses.dataclass
+class ParametricFamily:
+    """A parametric LP family over one matrix: b = b0 + B_b theta and
+    c = c0 + B_c theta (theta in R^p), the <= rows of the base staying <=."""
+    base: Problem
+    Bb: np.ndarray      # m x p
+    Bc: np.ndarray      # n x p
+    ineq: np.ndarray    # rows with row_lo = -inf
+    theta_std: float
+
+    @property
+    def n_params(self) -> int:
+        return self.Bb.shape[1]
+
+    def instance(self, theta: np.ndarray) -> Problem:
+        b = self.base.row_hi + self.Bb @ theta
+        c = self.base.c + self.Bc @ theta
+        return dataclasses.replace(self.base, c=c, row_lo=np.where(self.ineq, -INF, b),
+                                   row_hi=b, name=f"{self.base.name}_theta")
+
+    def thetas(self, count: int, seed: int) -> np.ndarray:
+        rng = np.random.default_rng(seed)
+        return rng.normal(0.0, self.theta_std, (count, self.n_params))
+
+
+def parametric_family(m: int = 50_000, n: int = 120_000, k: int = 5, seed: int = 4000,
+                      n_params: int = 64, rel: float = 0.1, theta_std: float = 0.1,
+                      b_mode: str = "feasible", box_frac: float = 0.1) -> ParametricFamily:
+    """Config 4: the base is config-2 structure (power-law rows, log-uniform
+    magnitudes, 30% <= rows, box bounds, b = A x0 (+ slack) for an interior
+    x0); theta ~ N(0, theta_std^2 I). B_c is dense Gaussian with
+    E||B_c theta|| = rel ||c0|| (every c is bounded over the box).
+
+    b_mode "gaussian": B_b dense Gaussian with E||B_b theta|| = rel ||b0||. On
+    badly scaled bases with equality rows and boxes this makes (nearly) every
+    instance infeasible. b_mode "feasible" (default): B_b = A B_x, i.e. b moves
+    with a feasible point x0 + B_x theta, B_x dense Gaussian with each row
+    scaled so the point's coordinate moves with a standard deviation of
+    box_frac times its distance to the nearer bound."""
+    base, x0 = _badly_scaled_with_point(m, n, k, seed)
+    rng = np.random.default_rng(seed + 1)
+    Bc = rng.standard_normal((n, n_params))
+    Bc *= rel * np.linalg.norm(base.c) / (theta_std * np.linalg.norm(Bc))
+    if b_mode == "gaussian":
+        Bb = rng.standard_normal((m, n_params))
+        Bb *= rel * np.linalg.norm(base.row_hi) / (theta_std * np.linalg.norm(Bb))
+    elif b_mode == "feasible":
+        Bx = rng.standard_normal((n, n_params))
+        dist = np.minimum(x0 - base.col_lo, base.col_hi - x0)
+        Bx *= (box_frac * dist / (theta_std * np.linalg.norm(Bx, axis=1)))[:, None]
+        Bb = np.stack([csr_matvec(base, Bx[:, j]) for j in range(n_params)], axis=1)
+    else:
+        raise ValueError(b_mode)
+    ineq = ~np.isfinite(base.row_lo)
+    return ParametricFamily(base=base, Bb=Bb, Bc=Bc, ineq=ineq, theta_std=theta_std)
 
 
 def batch_family(count: int = 4096, seed_base: int = 3000, m_lo: int = 50,

@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
                                       _dp, _dp, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.pdhg_solve_batch.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Info), _dp,
                                        _dp, _dp]
+        L.pdhg_batch_start_kkt.argtypes = [C.c_void_p, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -401,6 +402,28 @@ class Engine:
             r0, r1 = int(b["row_off"][k]), int(b["row_off"][k + 1])
             c0, c1 = int(b["col_off"][k]), int(b["col_off"][k + 1])
             out.append(_result(infos[k], x[c0:c1], y[r0:r1], rc[c0:c1]))
+        return out
+
+    def start_kkt(self, x0: list[np.ndarray] | None = None,
+                  y0: list[np.ndarray] | None = None) -> np.ndarray:
+        """Relative KKT residual of candidate starts for the loaded batch
+        (pdhg_batch_start_kkt); None = the cold start."""
+        if getattr(self, "_batch", None) is None:
+            raise PdhgError(3, "Engine.start_kkt: no batch loaded")
+        b, shapes = self._batch
+        out = np.zeros(len(shapes))
+        keep = []
+        xs = ys = C.cast(None, _dp)
+        if x0 is not None:
+            xa = np.ascontiguousarray(np.concatenate(x0), dtype=np.float64)
+            keep.append(xa)
+            xs = _d(xa)
+        if y0 is not None:
+            ya = np.ascontiguousarray(np.concatenate(y0), dtype=np.float64)
+            keep.append(ya)
+            ys = _d(ya)
+        _check(lib().pdhg_batch_start_kkt(self._h, xs, ys, _d(out)), "pdhg_batch_start_kkt",
+               self._h)
         return out
 
     def scaling(self) -> tuple[np.ndarray, np.ndarray]:
