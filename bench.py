@@ -253,6 +253,43 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
                       "pdhg_solve_batch; per instance pdhg_load_problem + pdhg_solve)"}
 
 
+def precision_line(pkg, eng, args, rank: int) -> dict:
+    """Config 2: the badly scaled LP (200,000 rows, 500,000 columns, 8
+    nonzeros per column at power-law rows, magnitudes log-uniform in
+    [1e-3, 1e3], 30% <= rows, boxes), solved from the cold start under the
+    same iteration budget and 1e-4 relative-KKT rule by the all-FP64 mode, the
+    FP32-bulk / FP64-check mode (FP64 polish once the FP32 phase stalls) and
+    the same without the polish (FP32 iterates to the end). Each arm's
+    objective error is taken against the FP64 run."""
+    p = pkg.lpgen.badly_scaled_lp(200_000, 500_000, 8, seed=2000 + rank)
+    out = {"workload": f"badly scaled LP {p.m:,} x {p.n:,}, {p.nnz:,} nnz (power-law rows, "
+                       f"|a| log-uniform [1e-3, 1e3], 30% <= rows)",
+           "iteration_budget": args.precision_iters}
+    arms = {"fp64": dict(precision="fp64"), "mixed": dict(precision="mixed"),
+            "fp32_only": dict(precision="mixed", polish_iterations=0)}
+    with pkg.Engine(eng.device) as e:
+        e.load(p)
+        for name, kw in arms.items():
+            o = pkg.PdhgOptions(termination_rule="relative_kkt", restart_rule="adaptive",
+                                primal_weight_update=True, tolerance=1e-4,
+                                max_iterations=args.precision_iters, **kw)
+            r = e.solve(o, want_point=False)
+            out[name] = {"status": r.status, "iterations": r.iterations,
+                         "relative_kkt": r.relative_kkt, "objective": r.objective,
+                         "fp64_iterations": r.fp64_iterations,
+                         "device_seconds": r.device_seconds,
+                         "iterations_per_s": r.iterations / r.device_seconds
+                         if r.device_seconds > 0 else None,
+                         "b_spmv_gb_per_s": spmv_bytes(p.m, p.n, p.nnz) * r.iterations
+                         / r.device_seconds / 1e9 if r.device_seconds > 0 else None}
+        out["tuning"] = {"fp64": e.tuning("fp64"), "mixed": e.tuning("mixed")}
+    ref = out["fp64"]["objective"]
+    for name in ("mixed", "fp32_only"):
+        out[name]["objective_error_vs_fp64"] = (abs(out[name]["objective"] - ref)
+                                                / max(1.0, abs(ref)))
+    return out
+
+
 def warmstart_line(pkg, eng, args, rank: int) -> dict:
     """Config 4 at reduced size: a parametric family over a config-2-structure
     base (500 rows, 1,200 columns, 6,000 nonzeros; 64 parameters moving b and
@@ -351,6 +388,8 @@ def main() -> None:
     ap.add_argument("--ws-train", type=int, default=1024,
                     help="config-4 training solves for the learned warm start (0 = skip)")
     ap.add_argument("--ws-test", type=int, default=128, help="config-4 held-out instances")
+    ap.add_argument("--precision-iters", type=int, default=100_000,
+                    help="iteration budget per mode of the config-2 precision study (0 = skip)")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiler target: load the LP and run one solve of --iters-per-step "
                          "iterations, nothing else")
@@ -473,6 +512,7 @@ def main() -> None:
 
     batch = batch_line(pkg, eng, args, rank) if args.batch_instances > 0 else None
     warm = warmstart_line(pkg, eng, args, rank) if args.ws_train > 0 else None
+    prec = precision_line(pkg, eng, args, rank) if args.precision_iters > 0 else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -499,6 +539,8 @@ def main() -> None:
         line["batch"] = batch
     if warm is not None:
         line["warmstart"] = warm
+    if prec is not None:
+        line["precision"] = prec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prob)
     eng.close()

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -38,14 +39,34 @@ struct DBuf {
     }
 };
 
+// Owning storage of a RowItems list.
+struct ItemsDev {
+    DBuf<int4> item;
+    DBuf<int2> split;
+    DBuf<unsigned int> ticket;
+    DBuf<double> part;
+    int32_t n_item = 0;
+    RowItems view() const {
+        RowItems v;
+        v.item = item.p;
+        v.split = split.p;
+        v.ticket = ticket.p;
+        v.part = part.p;
+        v.n_item = n_item;
+        return v;
+    }
+};
+
 struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
-    DBuf<int32_t> rp, ci, long_rows, wrows, mid_rows, huge_rows;
+    DBuf<int32_t> rp, ci, long_rows, wrows, warp_rows0, warp_rows1;
+    ItemsDev items_long, items_huge;
     DBuf<double> v64;
     DBuf<float> v32;
     DBuf<char> tscratch;  // build_transpose scratch when this matrix is a transpose
     int32_t n_long = 0, n_short = 0, n_wrows = 0, n_mid = 0, n_huge = 0;
+    int32_t short_max = kLongRow, n_iter_short = 0, n_warp0 = 0, n_warp1 = 0;
     int vw = 1;
     DevCsr view() const {
         DevCsr d;
@@ -62,10 +83,16 @@ struct MatDev {
         d.vw = vw;
         d.wrows = wrows.p;
         d.n_wrows = n_wrows;
-        d.mid_rows = mid_rows.p;
-        d.huge_rows = huge_rows.p;
+        d.short_max = short_max;
+        d.n_iter_short = n_iter_short;
+        d.warp_rows0 = warp_rows0.p;
+        d.warp_rows1 = warp_rows1.p;
+        d.n_warp0 = n_warp0;
+        d.n_warp1 = n_warp1;
         d.n_mid = n_mid;
         d.n_huge = n_huge;
+        d.items_long = items_long.view();
+        d.items_huge = items_huge.view();
         return d;
     }
 };
@@ -128,36 +155,106 @@ inline int cuda_fail(std::string* err, cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? PDHG_ERR_OUT_OF_MEMORY : PDHG_ERR_BACKEND;
 }
 
+// CTA work items (RowItems) over the rows of `ext` ({row, begin, end, -}, in
+// row order) longer than min_len: one item per row of at most seg entries,
+// else ceil(len / seg) near-equal segments. seg is kSegLen, or more when the
+// rows' entries would make more than two items per CTA slot of the GPU
+// (resident_ctas): rows are split only as far as filling the GPU needs.
+inline int build_items(const std::vector<int4>& ext, int min_len, int resident_ctas, ItemsDev& D,
+                       cudaStream_t s, std::string* err) {
+    int64_t total = 0;
+    for (const int4& r : ext)
+        if (r.z - r.y > min_len) total += static_cast<int64_t>(r.z) - r.y;
+    const int64_t seg = std::max<int64_t>(kSegLen, (total + 2 * resident_ctas - 1) / (2 * resident_ctas));
+    std::vector<int4> items;
+    std::vector<int2> splits;
+    for (const int4& r : ext) {
+        const int64_t len = static_cast<int64_t>(r.z) - r.y;
+        if (len <= min_len) continue;
+        const int64_t nseg = (len + seg - 1) / seg;
+        if (nseg <= 1) {
+            items.push_back(make_int4(r.x, r.y, r.z, -1));
+            continue;
+        }
+        const int sid = static_cast<int>(splits.size());
+        splits.push_back(make_int2(static_cast<int>(items.size()), static_cast<int>(nseg)));
+        for (int64_t k = 0; k < nseg; ++k) {
+            const int b = r.y + static_cast<int>(len * k / nseg);
+            const int e = r.y + static_cast<int>(len * (k + 1) / nseg);
+            items.push_back(make_int4(r.x, b, e, sid));
+        }
+    }
+    D.n_item = static_cast<int32_t>(items.size());
+    cudaError_t e;
+    if ((e = upload(D.item, items.data(), items.size(), s)) != cudaSuccess ||
+        (e = upload(D.split, splits.data(), splits.size(), s)) != cudaSuccess ||
+        (e = D.ticket.alloc(splits.size())) != cudaSuccess ||
+        (e = D.part.alloc(2 * items.size())) != cudaSuccess)
+        return cuda_fail(err, e, "build_items");
+    if (!splits.empty()) cudaMemsetAsync(D.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    // the host vectors are read by the copies above before they go out of scope
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_items");
+    return PDHG_OK;
+}
+
 // Row binning on the device: long-row list, short-row count, lanes per short
-// row (about half the mean short-row length, a power of two in [1, 32]), and
-// the warp-row list of the ordered kernels.
+// row (about half the mean short-row length, a power of two in [1, 32]), the
+// warp-row list of the ordered kernels, and the throughput kernels' tiers:
+// short rows up to short_max, the two warp-row lists and the CTA work items.
 inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     cudaError_t e = M.long_rows.alloc(static_cast<size_t>(M.rows) + 1);
     if (e != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     if ((e = M.wrows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess ||
-        (e = M.mid_rows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess ||
-        (e = M.huge_rows.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
+        (e = M.warp_rows0.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess ||
+        (e = M.warp_rows1.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
         return cuda_fail(err, e, "bin_matrix");
     DBuf<unsigned long long> cnt;
     if ((e = cnt.alloc(8)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s);
     launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
     launch_bin(M.rp.p, M.rows, kWarpRow, M.wrows.p, cnt.p + 3, s);
-    launch_bin_range(M.rp.p, M.rows, kLongRow, kHugeRow, M.mid_rows.p, cnt.p + 6, s);
-    launch_bin_range(M.rp.p, M.rows, kHugeRow, 0x7fffffff, M.huge_rows.p, cnt.p + 7, s);
     unsigned long long h[8];
     cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     M.n_long = static_cast<int32_t>(h[0]);
     M.n_short = static_cast<int32_t>(h[1]);
     M.n_wrows = static_cast<int32_t>(h[3]);
-    M.n_mid = static_cast<int32_t>(h[6]);
-    M.n_huge = static_cast<int32_t>(h[7]);
     const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
     int w = 1;
     while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;
     M.vw = w;
-    return PDHG_OK;
+    // lane groups take rows of up to 16 lanes' worth (a few unrolled rounds
+    // per lane); longer rows go to a warp each
+    M.short_max = std::min(kLongRow, std::max(kWarpRow, 16 * w));
+    launch_bin_range(M.rp.p, M.rows, M.short_max, kLongRow, M.warp_rows0.p, cnt.p + 6, s);
+    launch_bin_range(M.rp.p, M.rows, M.short_max, kHugeRow, M.warp_rows1.p, cnt.p + 7, s);
+    cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+    M.n_warp0 = static_cast<int32_t>(h[6]);
+    M.n_warp1 = static_cast<int32_t>(h[7]);
+
+    // extents of the long rows, in row order (the binning kernels append in
+    // arrival order)
+    std::vector<int4> ext(static_cast<size_t>(M.n_long));
+    if (M.n_long > 0) {
+        DBuf<int4> d_ext;
+        if ((e = d_ext.alloc(ext.size())) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+        launch_row_extents(M.long_rows.p, M.n_long, M.rp.p, d_ext.p, s);
+        cudaMemcpyAsync(ext.data(), d_ext.p, sizeof(int4) * ext.size(), cudaMemcpyDeviceToHost, s);
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+        std::sort(ext.begin(), ext.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
+    }
+    M.n_huge = 0;
+    for (const int4& r : ext) M.n_huge += (r.z - r.y > kHugeRow) ? 1 : 0;
+    M.n_mid = M.n_long - M.n_huge;
+    M.n_iter_short = M.rows - M.n_warp1 - M.n_huge;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int resident = 4 * std::max(sms, 1);  // the long-row kernel's CTAs per SM
+    int rc = build_items(ext, kLongRow, resident, M.items_long, s, err);
+    if (rc != PDHG_OK) return rc;
+    return build_items(ext, kHugeRow, resident, M.items_huge, s, err);
 }
 
 // row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,

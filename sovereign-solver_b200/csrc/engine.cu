@@ -61,6 +61,7 @@ struct Ctx {
     int device = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
+    PassFork fork;  // side stream + events: short- and long-row kernels side by side
     std::string err;
     long long gen = 0;  // bumps on every load / rescale
 
@@ -107,6 +108,9 @@ struct Ctx {
         if (batch != nullptr) batch_delete(batch);
         if (graph != nullptr) cudaGraphExecDestroy(graph);
         if (mail != nullptr) cudaFreeHost(mail);
+        if (fork.fork != nullptr) cudaEventDestroy(fork.fork);
+        if (fork.join != nullptr) cudaEventDestroy(fork.join);
+        if (fork.side != nullptr) cudaStreamDestroy(fork.side);
         if (stream != nullptr) cudaStreamDestroy(stream);
     }
 
@@ -391,11 +395,11 @@ struct Launcher {
             launch_exact_dual(ei, first, s);
             c.launches += 2;
         } else if (prec == PDHG_PREC_MIXED) {
-            c.launches += launch_fast_primal(fi32, first, s);
-            c.launches += launch_fast_dual(fi32, first, s);
+            c.launches += launch_fast_primal(fi32, first, s, &c.fork);
+            c.launches += launch_fast_dual(fi32, first, s, &c.fork);
         } else {
-            c.launches += launch_fast_primal(fi64, first, s);
-            c.launches += launch_fast_dual(fi64, first, s);
+            c.launches += launch_fast_primal(fi64, first, s, &c.fork);
+            c.launches += launch_fast_dual(fi64, first, s, &c.fork);
         }
     }
     void check(long long period, cudaStream_t s) {
@@ -810,8 +814,8 @@ std::string tune_sig(const char* prec, const char* pass, const DevCsr& M) {
 template <class T>
 float time_pass(Ctx& c, FastIter<T>& fi, bool primal, cudaEvent_t e0, cudaEvent_t e1) {
     auto run = [&]() {
-        if (primal) launch_fast_primal(fi, 0, c.stream);
-        else launch_fast_dual(fi, 0, c.stream);
+        if (primal) launch_fast_primal(fi, 0, c.stream, &c.fork);
+        else launch_fast_dual(fi, 0, c.stream, &c.fork);
     };
     run();
     run();
@@ -1228,12 +1232,12 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
     for (int i = 0; i < iters; ++i) {
         CK(cudaEventRecord(ev[3 * i], c.stream));
         if (prec == PDHG_PREC_FP64_EXACT) launch_exact_primal(L.ei, 0, c.stream);
-        else if (prec == PDHG_PREC_MIXED) launch_fast_primal(L.fi32, 0, c.stream);
-        else launch_fast_primal(L.fi64, 0, c.stream);
+        else if (prec == PDHG_PREC_MIXED) launch_fast_primal(L.fi32, 0, c.stream, &c.fork);
+        else launch_fast_primal(L.fi64, 0, c.stream, &c.fork);
         CK(cudaEventRecord(ev[3 * i + 1], c.stream));
         if (prec == PDHG_PREC_FP64_EXACT) launch_exact_dual(L.ei, 0, c.stream);
-        else if (prec == PDHG_PREC_MIXED) launch_fast_dual(L.fi32, 0, c.stream);
-        else launch_fast_dual(L.fi64, 0, c.stream);
+        else if (prec == PDHG_PREC_MIXED) launch_fast_dual(L.fi32, 0, c.stream, &c.fork);
+        else launch_fast_dual(L.fi64, 0, c.stream, &c.fork);
         CK(cudaEventRecord(ev[3 * i + 2], c.stream));
     }
     CK(cudaEventRecord(ev[3 * iters], c.stream));
@@ -1343,7 +1347,10 @@ int pdhg_create(int device, pdhg_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return PDHG_ERR_BACKEND;
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
     if (c.sm_count <= 0) c.sm_count = 148;
-    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c.fork.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.fork.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.fork.join, cudaEventDisableTiming) != cudaSuccess)
         return PDHG_ERR_BACKEND;
     void* mp = nullptr;
     if (cudaHostAlloc(&mp, sizeof(pdhg::Mailbox), cudaHostAllocMapped) != cudaSuccess)

@@ -27,6 +27,29 @@ namespace pdhg {
 
 constexpr int kBlock = 256;  // threads per CTA for every engine kernel
 
+// Row-length tiers of the binning (entries per row).
+constexpr int kLongRow = 512;   // above: a CTA per row (CTA items in the throughput kernels)
+constexpr int kWarpRow = 32;    // ordered kernels: above, one warp per row
+constexpr int kHugeRow = 4096;  // long_mode 1: above, CTA items instead of a warp
+
+// CTA work items over long rows. A row of at most kSegLen entries (more when
+// the long rows hold enough entries to fill the GPU without splitting) is one
+// item; a longer row is cut into near-equal segments, one item each, so that
+// no single CTA walks a row of hundreds of thousands of entries while the rest
+// of the GPU idles. Each segment's CTA stores its
+// partial dot products and takes a ticket; the CTA that draws the row's last
+// ticket adds the partials in segment order (deterministic whatever the
+// arrival order), resets the ticket and runs the row's epilogue.
+constexpr int kSegLen = 4096;
+
+struct RowItems {
+    const int4* item = nullptr;      // {row, begin, end, split}; split -1 = the whole row
+    const int2* split = nullptr;     // per split row: {first item, segments}
+    unsigned int* ticket = nullptr;  // per split row, 0 between launches
+    double* part = nullptr;          // 2 partials per item
+    int32_t n_item = 0;
+};
+
 struct DevCsr {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
@@ -46,21 +69,29 @@ struct DevCsr {
     // list every row runs on one thread.
     const int32_t* wrows = nullptr;
     int32_t n_wrows = 0;
-    // The iteration kernels split the long rows once more: up to kHugeRow
-    // entries one warp per row (mid_rows), longer ones one CTA per row.
-    const int32_t* mid_rows = nullptr;
-    const int32_t* huge_rows = nullptr;
+    // The throughput kernels (iteration and check) bin once more. Rows of at
+    // most short_max entries (16 lanes' worth at the binning's lanes per row,
+    // within [kWarpRow, kLongRow]) run on lane groups, n_iter_short of them;
+    // longer rows one warp per row up to kLongRow entries (warp_rows0:
+    // long_mode 0 and the check) or up to kHugeRow entries (warp_rows1:
+    // long_mode 1), and CTA work items above. n_mid counts the rows of
+    // kLongRow..kHugeRow entries, n_huge those above.
+    int32_t short_max = kLongRow;
+    int32_t n_iter_short = 0;
+    const int32_t* warp_rows0 = nullptr;
+    const int32_t* warp_rows1 = nullptr;
+    int32_t n_warp0 = 0, n_warp1 = 0;
     int32_t n_mid = 0, n_huge = 0;
+    // CTA work items over every row above kLongRow (long_mode 0 and the check
+    // kernel) and over the rows above kHugeRow (long_mode 1).
+    RowItems items_long, items_huge;
     // Iteration-kernel shape (the autotuner's choice): lanes per short row
-    // (0 = vw) and the long-row strategy (0: one CTA per row over long_rows;
-    // 1: one warp per mid row, one CTA per huge row).
+    // (0 = vw) and the long-row strategy (0: warp_rows0 + items_long;
+    // 1: warp_rows1 + items_huge).
     int iter_vw = 0;
     int long_mode = 0;
 };
 
-constexpr int kLongRow = 512;
-constexpr int kWarpRow = 32;
-constexpr int kHugeRow = 16384;
 
 // Accumulator slots (bit patterns of non-negative doubles, combined with
 // atomicMax -- order-independent, so exact).
@@ -190,10 +221,20 @@ struct FastIter {
     Iterates<T> it;
     DevState* st;
 };
+// A pass's short-row and long-row kernels touch disjoint rows and only read
+// the gathered vector, so they may run side by side: with a PassFork the long
+// kernel goes to `side` (fork: s -> side, join: side -> s), else both run in
+// order on s. Inside a stream capture this becomes two parallel graph branches.
+struct PassFork {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
 template <class T>
-int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s);  // kernels launched
+int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s,
+                       const PassFork* f = nullptr);  // kernels launched
 template <class T>
-int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s);
+int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s,
+                     const PassFork* f = nullptr);
 template <class T>
 int fast_launches_per_iteration(const FastIter<T>& a);
 
@@ -308,6 +349,9 @@ void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* 
                       unsigned long long* count, cudaStream_t s);
 void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                 unsigned long long* counters, cudaStream_t s);
+// out[k] = {rows[k], rp[rows[k]], rp[rows[k] + 1], 0} for k < n.
+void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out,
+                        cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
                        double* row_max, double* col_max, double tol, IntakeState* is,
                        cudaStream_t s);

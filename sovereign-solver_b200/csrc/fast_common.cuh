@@ -106,6 +106,50 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
     return am_last;
 }
 
+// One segment of a split row done; every thread of the CTA calls it (block-
+// uniform) with the CTA's two partials. Thread 0 stores them and takes the
+// row's ticket. The CTA that draws the last ticket returns true on every
+// thread with the row's totals: warp 0 reads the segments' partials (lane l
+// takes segments l, l+32, ...) and adds them in a fixed shuffle order, so the
+// result does not depend on which CTA finished when; it also resets the
+// ticket for the next launch. The other CTAs return false.
+__device__ __forceinline__ bool segment_finish(const RowItems& L, int idx, int split, double v0,
+                                               double v1, double* t0, double* t1) {
+    __shared__ int last;
+    __shared__ double tot[2];
+    if (threadIdx.x == 0) {
+        L.part[2 * idx] = v0;
+        L.part[2 * idx + 1] = v1;
+        __threadfence();
+        const int2 sp = __ldg(L.split + split);
+        last = atomicAdd(L.ticket + split, 1u) == static_cast<unsigned>(sp.y - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!last) return false;
+    if (threadIdx.x < 32) {
+        __threadfence();
+        const int2 sp = __ldg(L.split + split);
+        double a = 0.0, b = 0.0;
+        for (int k = sp.x + static_cast<int>(threadIdx.x); k < sp.x + sp.y; k += 32) {
+            a += __ldcg(L.part + 2 * k);
+            b += __ldcg(L.part + 2 * k + 1);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (threadIdx.x == 0) {
+            tot[0] = a;
+            tot[1] = b;
+            L.ticket[split] = 0u;
+        }
+    }
+    __syncthreads();
+    *t0 = tot[0];
+    *t1 = tot[1];
+    return true;
+}
+
 // Long-row dot product: 128-bit loads of values and column indices on the
 // aligned body, scalar head and tail. The matrix is streamed (evict-first,
 // ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go

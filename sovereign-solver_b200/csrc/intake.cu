@@ -120,6 +120,13 @@ __global__ void k_bin(const int32_t* rp, int32_t rows, int long_threshold, int32
     }
 }
 
+__global__ void k_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= n) return;
+    const int32_t r = rows[k];
+    out[k] = make_int4(r, rp[r], rp[r + 1], 0);
+}
+
 // Rows with lo < length <= hi appended to `list` (grid-stride; one atomic per
 // warp that has any).
 __global__ void k_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
@@ -417,6 +424,11 @@ void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* lo
                 unsigned long long* counters, cudaStream_t s) {
     const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
     if (rows > 0) k_bin<<<g, kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+}
+
+void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out,
+                        cudaStream_t s) {
+    if (n > 0) k_row_extents<<<nblocks(n), kBlock, 0, s>>>(rows, n, rp, out);
 }
 
 void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,

@@ -9,12 +9,15 @@
 //           y += sigma (s_bar - A x_bar), Cesaro sum.
 //
 // Work split by row length (one or two launches per pass, see below):
-//   rows with <= kLongRow nonzeros    VW lanes per row (VW = power of two ~
-//                                     mean length), lanes stride the row,
-//                                     shuffle reduction;
-//   rows of kLongRow..kHugeRow        one warp per row, 128-bit vector loads
-//                                     of values and indices, shuffle reduction;
-//   longer rows                       one CTA per row, block reduction.
+//   rows of <= short_max nonzeros     VW lanes per row (VW = power of two ~
+//                                     mean length), lanes stride the row in
+//                                     rounds of four loads, shuffle reduction;
+//   rows of short_max..kLongRow       one warp per row, 128-bit vector loads
+//   (mode 1: ..kHugeRow)              of values and indices, shuffle reduction;
+//   longer rows                       CTA work items of at most kSegLen
+//                                     entries (a row of more is split into
+//                                     segments whose partials the last CTA
+//                                     adds in segment order), block reduction.
 // The epilogue of a short row runs on the group's lane 0, so consecutive
 // groups touch consecutive vector entries (coalesced).
 //
@@ -31,7 +34,9 @@
 
 // CTAs per SM the iteration kernels are compiled to fit (register budget);
 // build knobs, 1 = no constraint. The short-row kernel is lean: eight CTAs
-// (32 registers) fit in FP32, six in FP64 without spills.
+// (32 registers) fit in FP32, six in FP64 without spills. The long-row kernel
+// with only CTA items fits six; with the warp-row path as well, four (64
+// registers; a few bytes of spill in FP32).
 #ifndef PDHG_SHORT_MIN_CTAS
 #define PDHG_SHORT_MIN_CTAS 8
 #endif
@@ -55,10 +60,10 @@ namespace {
 //
 // One SpMV-plus-update pass is split by row length into two kernels, so the
 // short-row kernel keeps its registers (and occupancy) low:
-//   fast_iter       rows of at most kLongRow entries, groups of VW lanes;
-//   fast_iter_long  rows longer than kLongRow: one CTA each (long_mode 0), or
-//                   one warp each up to kHugeRow entries and one CTA each
-//                   above (long_mode 1).
+//   fast_iter       rows of at most short_max entries, groups of VW lanes;
+//   fast_iter_long  longer rows: one warp each up to kLongRow entries and CTA
+//                   work items above (long_mode 0), or one warp each up to
+//                   kHugeRow entries and CTA work items above (long_mode 1).
 // `reset` is set on the first kernel of a period's first pass: it clears the
 // flags the previous period's restart kernel consumed.
 
@@ -88,16 +93,32 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     EpiIn<T> in{};
     if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
     const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
-    if (e - b > kLongRow) return;  // fast_iter_long handles it
+    if (e - b > M.short_max) return;  // fast_iter_long handles it
+    // rounds of four entries per lane: the index and value loads of a round
+    // are all in flight before its gathers, the gathers before the adds
     T acc = T(0);
-    for (int k = b + lane; k < e; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
+    for (int k0 = b + lane; k0 < e; k0 += 4 * VW) {
+        int c[4];
+        T v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * VW;
+            c[u] = k < e ? __ldcs(M.ci + k) : 0;
+            v[u] = k < e ? __ldcs(vals + k) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * VW < e) acc += v[u] * __ldg(xg + c[u]);
+    }
     if (VW > 1) acc = group_sum(acc, VW);
     if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
 }
 
-template <class T, bool PRIMAL, int MODE>
-__global__ void __launch_bounds__(kBlock, MODE == 0 ? PDHG_LONG_MIN_CTAS : PDHG_WARPROW_MIN_CTAS)
-    fast_iter_long(FastIter<T> a, int first, int reset, int mid_blocks) {
+// WARPS = false: the pass has no warp rows in this mode, only CTA items (the
+// warp path is compiled out, so more CTAs fit per SM).
+template <class T, bool PRIMAL, int MODE, bool WARPS>
+__global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_LONG_MIN_CTAS)
+    fast_iter_long(FastIter<T> a, int first, int reset, int warp_blocks) {
     DevState* st = a.st;
     iter_reset(st, reset);
     if (st->done) return;
@@ -107,25 +128,33 @@ __global__ void __launch_bounds__(kBlock, MODE == 0 ? PDHG_LONG_MIN_CTAS : PDHG_
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    if (MODE == 1 && static_cast<int>(blockIdx.x) < mid_blocks) {
-        // one warp per row
+    if (WARPS && static_cast<int>(blockIdx.x) < warp_blocks) {
+        // one warp per row: rows above short_max up to kLongRow (mode 0) or
+        // kHugeRow (mode 1) entries
         const int w = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-        if (w >= M.n_mid) return;
-        const int r = __ldg(M.mid_rows + w);
+        if (w >= (MODE == 0 ? M.n_warp0 : M.n_warp1)) return;
+        const int r = __ldg((MODE == 0 ? M.warp_rows0 : M.warp_rows1) + w);
         const int lane = threadIdx.x & 31;
         EpiIn<T> in{};
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
         const T acc = warp_row_dot<T>(M.ci, vals, xg, __ldg(M.rp + r), __ldg(M.rp + r + 1));
         if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     } else {
-        // one CTA per row: every long row (mode 0) or those above kHugeRow
-        const int r = MODE == 0 ? __ldg(M.long_rows + blockIdx.x)
-                                : __ldg(M.huge_rows + (blockIdx.x - mid_blocks));
+        // CTA work items: rows above kLongRow (mode 0) or kHugeRow (mode 1),
+        // those above kSegLen entries in segments
+        const RowItems& L = MODE == 0 ? M.items_long : M.items_huge;
+        const int idx = static_cast<int>(blockIdx.x) - warp_blocks;
+        const int4 w = __ldg(L.item + idx);
         EpiIn<T> in{};
-        if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
-        const int b = __ldg(M.rp + r), e = __ldg(M.rp + r + 1);
-        const T acc = long_row_dot<T>(M.ci, vals, xg, b, e);
-        if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
+        if (threadIdx.x == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+        T acc = long_row_dot<T>(M.ci, vals, xg, w.y, w.z);
+        if (w.w >= 0) {  // block-uniform
+            double tot, unused;
+            if (!segment_finish(L, idx, w.w, static_cast<double>(acc), 0.0, &tot, &unused)) return;
+            acc = static_cast<T>(tot);
+            if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+        }
+        if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
     }
 }
 
@@ -139,19 +168,19 @@ __global__ void k_clear_flags(DevState* st) {
 inline int iter_lanes(const DevCsr& M) { return M.iter_vw > 0 ? M.iter_vw : M.vw; }
 
 inline int short_blocks_for(const DevCsr& M) {
-    if (M.n_short == 0) return 0;
+    if (M.n_iter_short == 0) return 0;
     return static_cast<int>((static_cast<int64_t>(M.rows) * iter_lanes(M) + kBlock - 1) / kBlock);
 }
 
 // Kernels one pass over M launches besides the flag reset.
 inline int pass_launches(const DevCsr& M) {
     if (M.rows == 0) return 0;
-    return (short_blocks_for(M) > 0 ? 1 : 0) + (M.n_long > 0 ? 1 : 0);
+    return (short_blocks_for(M) > 0 ? 1 : 0) + (M.rows > M.n_iter_short ? 1 : 0);
 }
 
 // Returns the number of kernels launched.
 template <class T, bool PRIMAL>
-int launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
+int launch_iter(const FastIter<T>& a, int first, cudaStream_t s, const PassFork* f) {
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     if (M.rows == 0) {
         if (PRIMAL && first) {
@@ -162,10 +191,27 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
     }
     const int sb = short_blocks_for(M);
     const int mode = M.long_mode;
-    const int mb = mode == 1 ? (M.n_mid + kBlock / 32 - 1) / (kBlock / 32) : 0;
-    const int lb = mode == 1 ? mb + M.n_huge : M.n_long;
+    const int nw = mode == 1 ? M.n_warp1 : M.n_warp0;
+    const int mb = (nw + kBlock / 32 - 1) / (kBlock / 32);
+    const int lb = mb + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
     const int reset_short = (PRIMAL && first) ? 1 : 0;
     const int reset_long = (PRIMAL && first && sb == 0) ? 1 : 0;
+    const bool fork = f != nullptr && f->side != nullptr && sb > 0 && lb > 0;
+    cudaStream_t ls = s;
+    if (fork) {
+        cudaEventRecord(f->fork, s);
+        cudaStreamWaitEvent(f->side, f->fork, 0);
+        ls = f->side;
+    }
+    if (lb > 0) {
+        if (mb == 0) {
+            if (mode == 1) fast_iter_long<T, PRIMAL, 1, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);
+            else fast_iter_long<T, PRIMAL, 0, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);
+        } else {
+            if (mode == 1) fast_iter_long<T, PRIMAL, 1, true><<<lb, kBlock, 0, ls>>>(a, first, reset_long, mb);
+            else fast_iter_long<T, PRIMAL, 0, true><<<lb, kBlock, 0, ls>>>(a, first, reset_long, mb);
+        }
+    }
     if (sb > 0) {
         switch (iter_lanes(M)) {
             case 1: fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
@@ -176,9 +222,9 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s) {
             default: fast_iter<T, 32, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
         }
     }
-    if (lb > 0) {
-        if (mode == 1) fast_iter_long<T, PRIMAL, 1><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb);
-        else fast_iter_long<T, PRIMAL, 0><<<lb, kBlock, 0, s>>>(a, first, reset_long, mb);
+    if (fork) {
+        cudaEventRecord(f->join, f->side);
+        cudaStreamWaitEvent(s, f->join, 0);
     }
     return (sb > 0 ? 1 : 0) + (lb > 0 ? 1 : 0);
 }
@@ -260,91 +306,100 @@ __device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
     __syncthreads();
 }
 
-// Grid-stride over virtual blocks [row short | row long | col short | col long];
-// the grid itself is capped (a few CTAs per SM), so each CTA sums its rows into
-// per-thread running terms and takes part in one reduction.
+// Products of entries [k, e) (stride `step`) of a row of A (ROWS: with the
+// current x and the Cesaro average of x) or of A^T (with y and its average).
+template <class T, bool ROWS>
+__device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr& M, int k, int e,
+                                             int step, double inv, double& ac, double& aa) {
+    for (; k < e; k += step) {
+        const int j = M.ci[k];
+        const double v = M.v64[k];
+        if (ROWS) {
+            ac += v * static_cast<double>(a.it.x[j]);
+            aa += v * avg_x(a.it, j, inv);
+        } else {
+            ac += v * static_cast<double>(a.it.y[j]);
+            aa += v * avg_y(a.it, j, inv);
+        }
+    }
+}
+
+template <class T, bool ROWS>
+__device__ __forceinline__ void row_or_col_terms(const FastCheck<T>& a, int r, double ac, double aa,
+                                                 double inv, Terms& t) {
+    if (ROWS) row_terms(a, r, ac, aa, inv, t);
+    else col_terms(a, r, ac, aa, inv, t);
+}
+
+// Virtual block vb of one matrix's part [short | warp rows | CTA items]:
+// short rows on groups of M.vw lanes, rows up to kLongRow one warp each
+// (warp_rows0), longer ones as CTA items (items_long). Block-uniform.
+template <class T, bool ROWS>
+__device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int sb, int wb,
+                           double inv, Terms& t) {
+    double ac = 0.0, aa = 0.0;
+    if (vb < sb) {
+        const int vw = M.vw;
+        const int lane = threadIdx.x & (vw - 1);
+        const int r = (vb * kBlock + threadIdx.x) / vw;
+        if (r >= M.rows) return;
+        const int b = M.rp[r], e = M.rp[r + 1];
+        if (e - b > M.short_max) return;
+        row_products<T, ROWS>(a, M, b + lane, e, vw, inv, ac, aa);
+        ac = group_sum(ac, vw);
+        aa = group_sum(aa, vw);
+        if (lane == 0) row_or_col_terms<T, ROWS>(a, r, ac, aa, inv, t);
+    } else if (vb < sb + wb) {
+        const int w = (vb - sb) * (kBlock / 32) + (threadIdx.x >> 5);
+        if (w >= M.n_warp0) return;
+        const int r = M.warp_rows0[w];
+        const int lane = threadIdx.x & 31;
+        row_products<T, ROWS>(a, M, M.rp[r] + lane, M.rp[r + 1], 32, inv, ac, aa);
+        for (int o = 16; o > 0; o >>= 1) {
+            ac += __shfl_xor_sync(0xffffffffu, ac, o);
+            aa += __shfl_xor_sync(0xffffffffu, aa, o);
+        }
+        if (lane == 0) row_or_col_terms<T, ROWS>(a, r, ac, aa, inv, t);
+    } else {
+        const int idx = vb - sb - wb;
+        const int4 w = M.items_long.item[idx];
+        row_products<T, ROWS>(a, M, w.y + threadIdx.x, w.z, kBlock, inv, ac, aa);
+        ac = block_total(ac);
+        aa = block_total(aa);
+        if (w.w >= 0 && !segment_finish(M.items_long, idx, w.w, ac, aa, &ac, &aa)) return;
+        if (threadIdx.x == 0) row_or_col_terms<T, ROWS>(a, w.x, ac, aa, inv, t);
+    }
+}
+
+// Virtual blocks of the check over one matrix: short-row blocks (M.vw lanes
+// per row), warp-row blocks, CTA items.
+__host__ __device__ inline int check_short_blocks(const DevCsr& M) {
+    if (M.n_iter_short == 0) return 0;
+    return static_cast<int>((static_cast<int64_t>(M.rows) * M.vw + kBlock - 1) / kBlock);
+}
+__host__ __device__ inline int check_warp_blocks(const DevCsr& M) { return (M.n_warp0 + kBlock / 32 - 1) / (kBlock / 32); }
+inline int check_blocks(const DevCsr& M) {
+    return check_short_blocks(M) + check_warp_blocks(M) + M.items_long.n_item;
+}
+
+// Grid-stride over the virtual blocks of A (act = A x, current and average)
+// then of A^T (aty = A^T y); the grid itself is capped (a few CTAs per SM),
+// so each CTA sums its rows into per-thread running terms and takes part in
+// one reduction.
 template <class T>
-__global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_blocks, int cs_blocks) {
+__global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a) {
     DevState* st = a.st;
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
     const double inv = 1.0 / static_cast<double>(k_avg);
     Terms t;
-    const int b0 = rs_blocks, b1 = b0 + a.A.n_long, b2 = b1 + cs_blocks, b3 = b2 + a.AT.n_long;
-    for (int bid = blockIdx.x; bid < b3; bid += gridDim.x) {
-        if (bid < b1) {
-            // rows of A: act = A x (current and average)
-            const DevCsr& M = a.A;
-            if (bid < b0) {
-                const int vw = M.vw;
-                const int lane = threadIdx.x & (vw - 1);
-                const int r = (bid * kBlock + threadIdx.x) / vw;
-                if (r < M.rows) {
-                    const int b = M.rp[r], e = M.rp[r + 1];
-                    if (e - b <= kLongRow) {
-                        double ac = 0.0, aa = 0.0;
-                        for (int k = b + lane; k < e; k += vw) {
-                            const int j = M.ci[k];
-                            const double v = M.v64[k];
-                            ac += v * static_cast<double>(a.it.x[j]);
-                            aa += v * avg_x(a.it, j, inv);
-                        }
-                        ac = group_sum(ac, vw);
-                        aa = group_sum(aa, vw);
-                        if (lane == 0) row_terms(a, r, ac, aa, inv, t);
-                    }
-                }
-            } else {
-                const int r = M.long_rows[bid - b0];
-                const int b = M.rp[r], e = M.rp[r + 1];
-                double ac = 0.0, aa = 0.0;
-                for (int k = b + threadIdx.x; k < e; k += kBlock) {
-                    const int j = M.ci[k];
-                    const double v = M.v64[k];
-                    ac += v * static_cast<double>(a.it.x[j]);
-                    aa += v * avg_x(a.it, j, inv);
-                }
-                ac = block_total(ac);
-                aa = block_total(aa);
-                if (threadIdx.x == 0) row_terms(a, r, ac, aa, inv, t);
-            }
-        } else {
-            // rows of A^T: aty = A^T y (current and average)
-            const DevCsr& M = a.AT;
-            if (bid < b2) {
-                const int vw = M.vw;
-                const int lane = threadIdx.x & (vw - 1);
-                const int r = ((bid - b1) * kBlock + threadIdx.x) / vw;
-                if (r < M.rows) {
-                    const int b = M.rp[r], e = M.rp[r + 1];
-                    if (e - b <= kLongRow) {
-                        double ac = 0.0, aa = 0.0;
-                        for (int k = b + lane; k < e; k += vw) {
-                            const int i = M.ci[k];
-                            const double v = M.v64[k];
-                            ac += v * static_cast<double>(a.it.y[i]);
-                            aa += v * avg_y(a.it, i, inv);
-                        }
-                        ac = group_sum(ac, vw);
-                        aa = group_sum(aa, vw);
-                        if (lane == 0) col_terms(a, r, ac, aa, inv, t);
-                    }
-                }
-            } else {
-                const int r = M.long_rows[bid - b2];
-                const int b = M.rp[r], e = M.rp[r + 1];
-                double ac = 0.0, aa = 0.0;
-                for (int k = b + threadIdx.x; k < e; k += kBlock) {
-                    const int i = M.ci[k];
-                    const double v = M.v64[k];
-                    ac += v * static_cast<double>(a.it.y[i]);
-                    aa += v * avg_y(a.it, i, inv);
-                }
-                ac = block_total(ac);
-                aa = block_total(aa);
-                if (threadIdx.x == 0) col_terms(a, r, ac, aa, inv, t);
-            }
-        }
+    const int sbA = check_short_blocks(a.A), wbA = check_warp_blocks(a.A);
+    const int sbT = check_short_blocks(a.AT), wbT = check_warp_blocks(a.AT);
+    const int nA = sbA + wbA + a.A.items_long.n_item;
+    const int nT = sbT + wbT + a.AT.items_long.n_item;
+    for (int bid = blockIdx.x; bid < nA + nT; bid += gridDim.x) {
+        if (bid < nA) check_part<T, true>(a, a.A, bid, sbA, wbA, inv, t);
+        else check_part<T, false>(a, a.AT, bid - nA, sbT, wbT, inv, t);
     }
     block_max_terms(t, st->acc);
     if (a.termination_rule == 1) {
@@ -357,7 +412,16 @@ __global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_bloc
             p[0] = s0; p[1] = s1; p[2] = s2; p[3] = s3;
         }
     }
-    if (!last_block(&st->ticket[TK_FAST]) || threadIdx.x != 0) return;
+    if (!last_block(&st->ticket[TK_FAST])) return;
+    // the objectives' per-CTA partial sums, added by the whole last CTA in a
+    // fixed order (strided, then a tree)
+    double obj[4] = {0.0, 0.0, 0.0, 0.0};
+    if (a.termination_rule == 1) {
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock)
+            for (int q = 0; q < 4; ++q) obj[q] += __ldcg(a.cs.part + 4 * b + q);
+        for (int q = 0; q < 4; ++q) obj[q] = block_sum_det(obj[q]);
+    }
+    if (threadIdx.x != 0) return;
 
     // ---- decision (one thread) ----
     const double cp = acc_read(&st->acc[ACC_CUR_P]), cd = acc_read(&st->acc[ACC_CUR_D]);
@@ -393,13 +457,7 @@ __global__ void __launch_bounds__(kBlock) fast_check(FastCheck<T> a, int rs_bloc
         } else {
             double rel = 0.0;
             if (a.termination_rule == 1) {
-                double ps = 0.0, ds = 0.0;
-                const volatile double* part = a.cs.part;
-                const int off = ab ? 2 : 0;
-                for (unsigned b = 0; b < gridDim.x; ++b) {
-                    ps += part[4 * b + off];
-                    ds += part[4 * b + off + 1];
-                }
+                double ps = ab ? obj[2] : obj[0], ds = ab ? obj[3] : obj[1];
                 ps += a.P.obj_sign * a.P.obj_const;  // the constant shifts both objectives
                 ds += a.P.obj_sign * a.P.obj_const;
                 const double gap = fabs(ps - ds) / (1.0 + fabs(ps) + fabs(ds));
@@ -537,14 +595,16 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
         a.cs.part[2 * blockIdx.x] = bx;
         a.cs.part[2 * blockIdx.x + 1] = by;
     }
-    if (!last_block(&st->ticket[TK_RESTART]) || threadIdx.x != 0) return;
-    st->ticket[TK_RESTART] = 0u;
-    double sx = 0.0, sy = 0.0;
-    const volatile double* part = a.cs.part;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-        sx += part[2 * b];
-        sy += part[2 * b + 1];
+    if (!last_block(&st->ticket[TK_RESTART])) return;
+    double sx = 0.0, sy = 0.0;  // the whole last CTA, fixed order
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock) {
+        sx += __ldcg(a.cs.part + 2 * b);
+        sy += __ldcg(a.cs.part + 2 * b + 1);
     }
+    sx = block_sum_det(sx);
+    sy = block_sum_det(sy);
+    if (threadIdx.x != 0) return;
+    st->ticket[TK_RESTART] = 0u;
     const double dx = sqrt(sx), dy = sqrt(sy);
     if (dx > 1e-10 && dy > 1e-10) {
         // omega <- exp(0.5 log(dy/dx) + 0.5 log(omega))
@@ -557,12 +617,12 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
 }  // namespace
 
 template <class T>
-int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s) {
-    return launch_iter<T, true>(a, first, s);
+int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s, const PassFork* f) {
+    return launch_iter<T, true>(a, first, s, f);
 }
 template <class T>
-int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s) {
-    return launch_iter<T, false>(a, first, s);
+int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s, const PassFork* f) {
+    return launch_iter<T, false>(a, first, s, f);
 }
 template <class T>
 int fast_launches_per_iteration(const FastIter<T>& a) {
@@ -571,12 +631,10 @@ int fast_launches_per_iteration(const FastIter<T>& a) {
 
 template <class T>
 void launch_fast_check(const FastCheck<T>& a, cudaStream_t s) {
-    const int rsb = short_blocks_for(a.A);
-    const int csb = short_blocks_for(a.AT);
-    int grid = rsb + a.A.n_long + csb + a.AT.n_long;
+    int grid = check_blocks(a.A) + check_blocks(a.AT);
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid == 0) grid = 1;
-    fast_check<T><<<grid, kBlock, 0, s>>>(a, rsb, csb);
+    fast_check<T><<<grid, kBlock, 0, s>>>(a);
     if (a.want_candidate) {
         const int32_t nmax = a.P.n > a.P.m ? a.P.n : a.P.m;
         if (nmax > 0) fast_candidate<T><<<(nmax + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
@@ -590,13 +648,13 @@ void launch_fast_restart(const FastCheck<T>& a, cudaStream_t s) {
 
 // Upper bound on check-kernel CTAs (partial-sum buffer sizing).
 int fast_check_grid(const DevCsr& A, const DevCsr& AT) {
-    return short_blocks_for(A) + A.n_long + short_blocks_for(AT) + AT.n_long + 1;
+    return check_blocks(A) + check_blocks(AT) + 1;
 }
 
-template int launch_fast_primal<float>(const FastIter<float>&, int, cudaStream_t);
-template int launch_fast_primal<double>(const FastIter<double>&, int, cudaStream_t);
-template int launch_fast_dual<float>(const FastIter<float>&, int, cudaStream_t);
-template int launch_fast_dual<double>(const FastIter<double>&, int, cudaStream_t);
+template int launch_fast_primal<float>(const FastIter<float>&, int, cudaStream_t, const PassFork*);
+template int launch_fast_primal<double>(const FastIter<double>&, int, cudaStream_t, const PassFork*);
+template int launch_fast_dual<float>(const FastIter<float>&, int, cudaStream_t, const PassFork*);
+template int launch_fast_dual<double>(const FastIter<double>&, int, cudaStream_t, const PassFork*);
 template int fast_launches_per_iteration<float>(const FastIter<float>&);
 template int fast_launches_per_iteration<double>(const FastIter<double>&);
 template void launch_fast_check<float>(const FastCheck<float>&, cudaStream_t);

@@ -1,0 +1,86 @@
+"""Long rows cut into CTA segments.
+
+Rows of more than 4,096 entries are summed by several CTAs; the CTA that
+finishes a row's last segment adds the segments' partials in segment order and
+runs the row's update. Both long-row strategies of the throughput kernels (a
+CTA work item per long row, or a warp per row up to 4,096 entries and CTA
+items above) are pinned in turn through the tuning-cache file, on an LP with
+rows of 300,000 / 100,000 / 20,000 / 4,097 entries (74, 25, 5 and 2
+segments) beside warp-sized and short rows. In each:
+
+* the FP64 iterates stay within 1e-10 (relative, floor 1) of the exact
+  kernels' over the first 100 iterations (no check among them, so no restart
+  decision can flip);
+* repeated solves, FP64 and FP32-mixed, give bit-identical results (the
+  segment order fixes the sum order whatever order the CTAs finish in).
+"""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+SNIPPET = """
+import importlib, json, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+pkg = importlib.import_module("sovereign-solver_b200")
+lengths = [300_000, 100_000, 20_000, 4_097] + [5_000] * 10 + [3_000] * 50 + [1_000] * 400 \\
+    + [600] * 200 + [8] * 3000
+p = pkg.lpgen.row_lengths_lp(lengths, 400_000, seed=7)
+assert p.nnz >= 1 << 20  # large enough for the tuner (and its cache) to be used
+
+def rel_err(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+kw = dict(max_iterations=300, tolerance=1e-12, restart_check_period=150, trace_iters=100)
+with pkg.Engine(0) as e:
+    e.load(p)
+    ex = e.solve(pkg.PdhgOptions(**kw))
+    f1 = e.solve(pkg.PdhgOptions(precision="fp64", **kw))
+    f2 = e.solve(pkg.PdhgOptions(precision="fp64", **kw))
+    mk = dict(precision="mixed", termination_rule="relative_kkt", restart_rule="adaptive",
+              max_iterations=600, restart_check_period=40)
+    m1 = e.solve(pkg.PdhgOptions(**mk))
+    m2 = e.solve(pkg.PdhgOptions(**mk))
+    out = dict(
+        fp64=e.tuning("fp64"), mixed=e.tuning("mixed"),
+        err=max(max(rel_err(f1.trace_x[k], ex.trace_x[k]), rel_err(f1.trace_y[k], ex.trace_y[k]))
+                for k in range(100)),
+        fp64_repeat=bool(np.array_equal(f1.primal, f2.primal) and np.array_equal(f1.dual, f2.dual)
+                         and np.array_equal(f1.trace_x, f2.trace_x)),
+        mixed_repeat=bool(np.array_equal(m1.primal, m2.primal) and np.array_equal(m1.dual, m2.dual)
+                          and m1.objective == m2.objective),
+        iterations=[ex.iterations, f1.iterations, m1.iterations])
+    print(json.dumps(out))
+"""
+
+
+def run(cache, mode=None):
+    if mode is not None:
+        entries = json.loads(cache.read_text())
+        cache.write_text(json.dumps({k: [v[0], mode] for k, v in entries.items()}))
+    env = dict(os.environ, PDHG_B200_TUNE_CACHE=str(cache))
+    r = subprocess.run([sys.executable, "-c", SNIPPET.format(root=ROOT)], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-4000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_split_rows_in_both_long_row_strategies(tmp_path):
+    cache = tmp_path / "tune.json"
+    runs = [(None, run(cache))]  # the tuner times the shapes and writes the file
+    assert any(k.startswith("f64/dual/") for k in json.loads(cache.read_text()))
+    runs += [(mode, run(cache, mode)) for mode in (0, 1)]
+    for mode, out in runs:
+        assert out["err"] <= 1e-10, (mode, out)
+        assert out["fp64_repeat"] and out["mixed_repeat"], (mode, out)
+        if mode is not None:
+            assert out["fp64"]["dual_long_mode"] == mode, out
+            assert out["mixed"]["dual_long_mode"] == mode, out
