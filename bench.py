@@ -356,18 +356,28 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
 
 
 def profile_case(args) -> None:
-    """One solve on a transportation LP of the given size: the ncu target."""
+    """One mixed-precision solve of --iters-per-step iterations: the ncu target.
+    --profile-lp transportation: the transportation LP of --supplies x
+    --demands; badly_scaled: the 200,000 x 500,000 badly scaled LP (FP32 to the
+    end, no polish)."""
     import torch
     torch.cuda.set_device(0)
     pkg = importlib.import_module("sovereign-solver_b200")
-    prob = pkg.lpgen.transportation_lp(args.supplies, args.demands, seed=1000)
+    if args.profile_lp == "badly_scaled":
+        prob = pkg.lpgen.badly_scaled_lp(200_000, 500_000, 8, seed=2000)
+        name = "badly scaled 200000x500000"
+    else:
+        prob = pkg.lpgen.transportation_lp(args.supplies, args.demands, seed=1000)
+        name = f"transportation {args.supplies}x{args.demands}"
     with pkg.Engine(0) as eng:
         eng.load(prob)
         r = eng.solve(pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
-                                      restart_rule="adaptive", tolerance=1e-12,
+                                      restart_rule="adaptive", primal_weight_update=True,
+                                      tolerance=1e-12, polish_iterations=0,
                                       max_iterations=args.iters_per_step), want_point=False)
-    print(json.dumps({"profile_case": f"transportation {args.supplies}x{args.demands}",
-                      "iterations": r.iterations, "status": r.status}))
+        tuning = eng.tuning("mixed")
+    print(json.dumps({"profile_case": name, "iterations": r.iterations, "status": r.status,
+                      "tuning": tuning}))
 
 
 def main() -> None:
@@ -390,6 +400,9 @@ def main() -> None:
     ap.add_argument("--ws-test", type=int, default=128, help="config-4 held-out instances")
     ap.add_argument("--precision-iters", type=int, default=100_000,
                     help="iteration budget per mode of the config-2 precision study (0 = skip)")
+    ap.add_argument("--profile-lp", default="transportation",
+                    choices=["transportation", "badly_scaled"],
+                    help="the LP of --profile-case")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiler target: load the LP and run one solve of --iters-per-step "
                          "iterations, nothing else")
