@@ -201,8 +201,10 @@ int pdhg_batch_start_kkt(pdhg_ctx* ctx, const double* x, const double* y, double
 
 /* Iteration-kernel shapes in use for the loaded problem in `precision`
  * (PDHG_PREC_MIXED or PDHG_PREC_FP64): out[0] lanes per short row and out[1]
- * long-row strategy (0: one CTA per row; 1: one warp per row up to 16,384
- * entries) of the primal pass (rows of A^T), out[2], out[3] the same for the
+ * long-row strategy (0: a warp per row up to 512 entries, CTA work items
+ * above; 1: a warp per row up to 4,096 entries, CTA items above; 2: warp work
+ * items for every row past the short ones; rows longer than a work item are
+ * split into segments) of the primal pass (rows of A^T), out[2], out[3] the same for the
  * dual pass (rows of A), out[4] = 1 when chosen by timing, 0 for the defaults
  * (no solve yet, autotune off, or a small LP). Engine extension: the autotuner
  * times the candidates once per matrix shape and precision, and keeps the

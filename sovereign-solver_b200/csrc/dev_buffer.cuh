@@ -61,7 +61,7 @@ struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
     DBuf<int32_t> rp, ci, long_rows, wrows, warp_rows0, warp_rows1;
-    ItemsDev items_long, items_huge;
+    ItemsDev items_long, items_huge, items_warp;
     DBuf<double> v64;
     DBuf<float> v32;
     DBuf<char> tscratch;  // build_transpose scratch when this matrix is a transpose
@@ -93,6 +93,7 @@ struct MatDev {
         d.n_huge = n_huge;
         d.items_long = items_long.view();
         d.items_huge = items_huge.view();
+        d.items_warp = items_warp.view();
         return d;
     }
 };
@@ -155,17 +156,17 @@ inline int cuda_fail(std::string* err, cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? PDHG_ERR_OUT_OF_MEMORY : PDHG_ERR_BACKEND;
 }
 
-// CTA work items (RowItems) over the rows of `ext` ({row, begin, end, -}, in
-// row order) longer than min_len: one item per row of at most seg entries,
-// else ceil(len / seg) near-equal segments. seg is kSegLen, or more when the
-// rows' entries would make more than two items per CTA slot of the GPU
-// (resident_ctas): rows are split only as far as filling the GPU needs.
-inline int build_items(const std::vector<int4>& ext, int min_len, int resident_ctas, ItemsDev& D,
-                       cudaStream_t s, std::string* err) {
+// Work items (RowItems) over the rows of `ext` ({row, begin, end, -}, in row
+// order) longer than min_len: one item per row of at most seg entries, else
+// ceil(len / seg) near-equal segments. seg is min_seg, or more when the rows'
+// entries would make more than two items per resident CTA (or warp) of the
+// GPU (`resident`): rows are split only as far as filling the GPU needs.
+inline int build_items(const std::vector<int4>& ext, int min_len, int min_seg, int resident,
+                       ItemsDev& D, cudaStream_t s, std::string* err) {
     int64_t total = 0;
     for (const int4& r : ext)
         if (r.z - r.y > min_len) total += static_cast<int64_t>(r.z) - r.y;
-    const int64_t seg = std::max<int64_t>(kSegLen, (total + 2 * resident_ctas - 1) / (2 * resident_ctas));
+    const int64_t seg = std::max<int64_t>(min_seg, (total + 2 * resident - 1) / (2 * resident));
     std::vector<int4> items;
     std::vector<int2> splits;
     for (const int4& r : ext) {
@@ -233,13 +234,14 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     M.n_warp0 = static_cast<int32_t>(h[6]);
     M.n_warp1 = static_cast<int32_t>(h[7]);
 
-    // extents of the long rows, in row order (the binning kernels append in
-    // arrival order)
-    std::vector<int4> ext(static_cast<size_t>(M.n_long));
-    if (M.n_long > 0) {
+    // extents of every row above short_max (warp_rows0 + long rows), in row
+    // order (the binning kernels append in arrival order)
+    std::vector<int4> ext(static_cast<size_t>(M.n_long) + static_cast<size_t>(M.n_warp0));
+    if (!ext.empty()) {
         DBuf<int4> d_ext;
         if ((e = d_ext.alloc(ext.size())) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
         launch_row_extents(M.long_rows.p, M.n_long, M.rp.p, d_ext.p, s);
+        launch_row_extents(M.warp_rows0.p, M.n_warp0, M.rp.p, d_ext.p + M.n_long, s);
         cudaMemcpyAsync(ext.data(), d_ext.p, sizeof(int4) * ext.size(), cudaMemcpyDeviceToHost, s);
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
         std::sort(ext.begin(), ext.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
@@ -251,10 +253,13 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int resident = 4 * std::max(sms, 1);  // the long-row kernel's CTAs per SM
-    int rc = build_items(ext, kLongRow, resident, M.items_long, s, err);
+    sms = std::max(sms, 1);
+    const int resident = 4 * sms;  // the long-row kernel's CTAs per SM
+    int rc = build_items(ext, kLongRow, kSegLen, resident, M.items_long, s, err);
     if (rc != PDHG_OK) return rc;
-    return build_items(ext, kHugeRow, resident, M.items_huge, s, err);
+    rc = build_items(ext, kHugeRow, kSegLen, resident, M.items_huge, s, err);
+    if (rc != PDHG_OK) return rc;
+    return build_items(ext, M.short_max, kWarpSegLen, 32 * sms, M.items_warp, s, err);
 }
 
 // row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,

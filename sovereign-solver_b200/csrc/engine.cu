@@ -272,6 +272,10 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     c.gen += 1;
     c.tuning[0] = Ctx::Tuning{};  // new matrices: shapes are chosen again
     c.tuning[1] = Ctx::Tuning{};
+    rbuf.release();
+    cbuf.release();
+    part.release();
+    pc.mark("scale: free scratch");
     return PDHG_OK;
 }
 
@@ -742,8 +746,9 @@ __global__ void k_restart_state(DevState* st) {
 // ---- autotuner of the iteration kernels ----------------------------------------
 //
 // For each pass (primal over A^T, dual over A) the candidates are the lanes
-// per short row around the binning's choice (vw/2, vw, 2vw) and, when the
-// matrix has rows longer than kLongRow, both long-row strategies. Each is
+// per short row around the binning's choice (vw/2, vw, 2vw) and, for the rows
+// past the short ones, the long-row strategies that differ on this matrix
+// (1 only when it has rows of kLongRow..kHugeRow entries). Each is
 // timed with CUDA events on the engine's stream (2 launches to warm, 5
 // timed) and replaces the current best only when faster by more than 5%, so
 // noise does not flip the choice. LPs below kTuneMinNnz nonzeros are
@@ -783,7 +788,7 @@ void tune_read_file() {
         int a = 0, b = 0;
         const size_t lb = txt.find('[', end);
         if (lb != std::string::npos && std::sscanf(txt.c_str() + lb, "[%d , %d]", &a, &b) == 2 &&
-            a >= 1 && a <= 32 && (a & (a - 1)) == 0 && (b == 0 || b == 1))
+            a >= 1 && a <= 32 && (a & (a - 1)) == 0 && b >= 0 && b <= 2)
             g_tune_cache[key] = {a, b};
         pos = end + 1;
     }
@@ -859,6 +864,7 @@ void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* 
     for (int vw : vws) {
         if (vw != M.vw) cand.push_back({vw, 0});
         if (M.n_mid > 0) cand.push_back({vw, 1});
+        if (M.items_warp.n_item > 0) cand.push_back({vw, 2});
     }
     // two rounds over all candidates, each keeping its faster time, so no
     // candidate is judged on a cold GPU (clocks ramping, first launches)

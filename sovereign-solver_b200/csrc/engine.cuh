@@ -41,6 +41,7 @@ constexpr int kHugeRow = 4096;  // long_mode 1: above, CTA items instead of a wa
 // ticket adds the partials in segment order (deterministic whatever the
 // arrival order), resets the ticket and runs the row's epilogue.
 constexpr int kSegLen = 4096;
+constexpr int kWarpSegLen = 1024;  // the same for warp work items (long_mode 2)
 
 struct RowItems {
     const int4* item = nullptr;      // {row, begin, end, split}; split -1 = the whole row
@@ -83,11 +84,12 @@ struct DevCsr {
     int32_t n_warp0 = 0, n_warp1 = 0;
     int32_t n_mid = 0, n_huge = 0;
     // CTA work items over every row above kLongRow (long_mode 0 and the check
-    // kernel) and over the rows above kHugeRow (long_mode 1).
-    RowItems items_long, items_huge;
+    // kernel) and over the rows above kHugeRow (long_mode 1); warp work items
+    // over every row above short_max (long_mode 2).
+    RowItems items_long, items_huge, items_warp;
     // Iteration-kernel shape (the autotuner's choice): lanes per short row
     // (0 = vw) and the long-row strategy (0: warp_rows0 + items_long;
-    // 1: warp_rows1 + items_huge).
+    // 1: warp_rows1 + items_huge; 2: items_warp).
     int iter_vw = 0;
     int long_mode = 0;
 };

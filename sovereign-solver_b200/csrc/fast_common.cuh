@@ -150,6 +150,32 @@ __device__ __forceinline__ bool segment_finish(const RowItems& L, int idx, int s
     return true;
 }
 
+// The same for a segment summed by one warp (every lane calls it, warp-
+// uniform; no block barrier): lane 0 stores the warp's partial and takes the
+// row's ticket; the warp drawing the last ticket returns true on every lane
+// with the row's total (lane l adds segments l, l+32, ..., then a fixed
+// shuffle tree) and resets the ticket.
+__device__ __forceinline__ bool warp_segment_finish(const RowItems& L, int idx, int split,
+                                                    double v, double* t) {
+    const int lane = threadIdx.x & 31;
+    const int2 sp = __ldg(L.split + split);
+    int last = 0;
+    if (lane == 0) {
+        L.part[2 * idx] = v;
+        __threadfence();
+        last = atomicAdd(L.ticket + split, 1u) == static_cast<unsigned>(sp.y - 1) ? 1 : 0;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return false;
+    __threadfence();
+    double a = 0.0;
+    for (int k = sp.x + lane; k < sp.x + sp.y; k += 32) a += __ldcg(L.part + 2 * k);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) L.ticket[split] = 0u;
+    *t = a;
+    return true;
+}
+
 // Long-row dot product: 128-bit loads of values and column indices on the
 // aligned body, scalar head and tail. The matrix is streamed (evict-first,
 // ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go

@@ -49,6 +49,9 @@
 #ifndef PDHG_WARPROW_MIN_CTAS
 #define PDHG_WARPROW_MIN_CTAS 4
 #endif
+#ifndef PDHG_WARPITEM_MIN_CTAS
+#define PDHG_WARPITEM_MIN_CTAS 4
+#endif
 
 namespace pdhg {
 
@@ -63,7 +66,8 @@ namespace {
 //   fast_iter       rows of at most short_max entries, groups of VW lanes;
 //   fast_iter_long  longer rows: one warp each up to kLongRow entries and CTA
 //                   work items above (long_mode 0), or one warp each up to
-//                   kHugeRow entries and CTA work items above (long_mode 1).
+//                   kHugeRow entries and CTA work items above (long_mode 1);
+//   fast_iter_witems  or all of them as warp work items (long_mode 2).
 // `reset` is set on the first kernel of a period's first pass: it clears the
 // flags the previous period's restart kernel consumed.
 
@@ -158,6 +162,38 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
     }
 }
 
+// long_mode 2: every row above short_max as warp work items (a whole row, or
+// a segment of a longer one); no block barrier anywhere, each warp finishes
+// on its own.
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
+    fast_iter_witems(FastIter<T> a, int first, int reset) {
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const RowItems& L = M.items_warp;
+    const int idx = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    if (idx >= L.n_item) return;
+    const T* __restrict__ vals = mvals<T>(M);
+    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
+    const PV<T> pv = pvec<T>(a.P);
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const int lane = threadIdx.x & 31;
+    const int4 w = __ldg(L.item + idx);
+    EpiIn<T> in{};
+    if (lane == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+    T acc = warp_row_dot<T>(M.ci, vals, xg, w.y, w.z);
+    if (w.w >= 0) {  // warp-uniform
+        double tot;
+        if (!warp_segment_finish(L, idx, w.w, static_cast<double>(acc), &tot)) return;
+        acc = static_cast<T>(tot);
+        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+    }
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+}
+
 __global__ void k_clear_flags(DevState* st) {
     if (threadIdx.x == 0) {
         st->restart = 0;
@@ -191,9 +227,9 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s, const PassFork*
     }
     const int sb = short_blocks_for(M);
     const int mode = M.long_mode;
-    const int nw = mode == 1 ? M.n_warp1 : M.n_warp0;
+    const int nw = mode == 2 ? M.items_warp.n_item : mode == 1 ? M.n_warp1 : M.n_warp0;
     const int mb = (nw + kBlock / 32 - 1) / (kBlock / 32);
-    const int lb = mb + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
+    const int lb = mode == 2 ? mb : mb + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
     const int reset_short = (PRIMAL && first) ? 1 : 0;
     const int reset_long = (PRIMAL && first && sb == 0) ? 1 : 0;
     const bool fork = f != nullptr && f->side != nullptr && sb > 0 && lb > 0;
@@ -203,7 +239,9 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s, const PassFork*
         cudaStreamWaitEvent(f->side, f->fork, 0);
         ls = f->side;
     }
-    if (lb > 0) {
+    if (lb > 0 && mode == 2) {
+        fast_iter_witems<T, PRIMAL><<<lb, kBlock, 0, ls>>>(a, first, reset_long);
+    } else if (lb > 0) {
         if (mb == 0) {
             if (mode == 1) fast_iter_long<T, PRIMAL, 1, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);
             else fast_iter_long<T, PRIMAL, 0, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);

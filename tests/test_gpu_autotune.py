@@ -26,7 +26,7 @@ def test_autotune_picks_valid_shapes_and_keeps_the_optimum(pkg):
         assert t["timed"]
         for k in ("primal_lanes", "dual_lanes"):
             assert t[k] in (1, 2, 4, 8, 16, 32)
-        assert t["primal_long_mode"] in (0, 1) and t["dual_long_mode"] in (0, 1)
+        assert t["primal_long_mode"] in (0, 1, 2) and t["dual_long_mode"] in (0, 1, 2)
         fixed = e.solve(pkg.PdhgOptions(autotune=False, **KW))
     assert tuned.status == fixed.status == "optimal"
     assert abs(tuned.objective - fixed.objective) <= 2e-3 * abs(fixed.objective)

@@ -1,12 +1,13 @@
 """Long rows cut into CTA segments.
 
-Rows of more than 4,096 entries are summed by several CTAs; the CTA that
-finishes a row's last segment adds the segments' partials in segment order and
-runs the row's update. Both long-row strategies of the throughput kernels (a
-CTA work item per long row, or a warp per row up to 4,096 entries and CTA
-items above) are pinned in turn through the tuning-cache file, on an LP with
-rows of 300,000 / 100,000 / 20,000 / 4,097 entries (74, 25, 5 and 2
-segments) beside warp-sized and short rows. In each:
+Rows longer than a work item are summed by several CTAs (or warps); the one
+that finishes a row's last segment adds the segments' partials in segment
+order and runs the row's update. The three long-row strategies of the
+throughput kernels (CTA items above 512 entries, CTA items above 4,096, warp
+items above the short rows) are pinned in turn through the tuning-cache file,
+on an LP with rows of 300,000 / 100,000 / 20,000 / 4,097 entries (74, 25, 5
+and 2 CTA segments; more as warp segments) beside warp-sized and short rows.
+In each:
 
 * the FP64 iterates stay within 1e-10 (relative, floor 1) of the exact
   kernels' over the first 100 iterations (no check among them, so no restart
@@ -77,7 +78,7 @@ def test_split_rows_in_both_long_row_strategies(tmp_path):
     cache = tmp_path / "tune.json"
     runs = [(None, run(cache))]  # the tuner times the shapes and writes the file
     assert any(k.startswith("f64/dual/") for k in json.loads(cache.read_text()))
-    runs += [(mode, run(cache, mode)) for mode in (0, 1)]
+    runs += [(mode, run(cache, mode)) for mode in (0, 1, 2)]
     for mode, out in runs:
         assert out["err"] <= 1e-10, (mode, out)
         assert out["fp64_repeat"] and out["mixed_repeat"], (mode, out)
