@@ -57,11 +57,59 @@ struct ItemsDev {
     }
 };
 
+// Owning storage of a LongTiers set.
+struct TiersDev {
+    DBuf<int32_t> warp_rows0, warp_rows1;
+    int32_t n_warp0 = 0, n_warp1 = 0;
+    ItemsDev items_long, items_huge, items_warp;
+    LongTiers view() const {
+        LongTiers t;
+        t.warp_rows0 = warp_rows0.p;
+        t.warp_rows1 = warp_rows1.p;
+        t.n_warp0 = n_warp0;
+        t.n_warp1 = n_warp1;
+        t.items_long = items_long.view();
+        t.items_huge = items_huge.view();
+        t.items_warp = items_warp.view();
+        return t;
+    }
+};
+
+// Owning storage of RowSlices.
+struct SlicesDev {
+    DBuf<int4> slice, item;
+    DBuf<int2> split;
+    DBuf<int32_t> row, rlen, col;
+    DBuf<float> v32;
+    DBuf<double> v64, part;
+    DBuf<unsigned int> ticket;
+    int32_t n_slice = 0, n_item = 0;
+    RowSlices view() const {
+        RowSlices v;
+        v.n_slice = n_slice;
+        v.n_item = n_item;
+        v.slice = slice.p;
+        v.row = row.p;
+        v.rlen = rlen.p;
+        v.col = col.p;
+        v.v32 = v32.p;
+        v.v64 = v64.p;
+        v.item = item.p;
+        v.split = split.p;
+        v.ticket = ticket.p;
+        v.part = part.p;
+        return v;
+    }
+};
+
 struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
     DBuf<int32_t> rp, ci, long_rows, wrows, warp_rows0, warp_rows1;
     ItemsDev items_long, items_huge, items_warp;
+    std::vector<int4> ext;  // host: {row, begin, end, -} of every row above short_max, row order
+    SlicesDev slices;
+    TiersDev no_slice_tiers;
     DBuf<double> v64;
     DBuf<float> v32;
     DBuf<char> tscratch;  // build_transpose scratch when this matrix is a transpose
@@ -94,6 +142,8 @@ struct MatDev {
         d.items_long = items_long.view();
         d.items_huge = items_huge.view();
         d.items_warp = items_warp.view();
+        d.slices = slices.view();
+        d.no_slice_tiers = no_slice_tiers.view();
         return d;
     }
 };
@@ -246,6 +296,9 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
         std::sort(ext.begin(), ext.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
     }
+    M.ext = ext;
+    M.slices.n_slice = 0;
+    M.slices.n_item = 0;
     M.n_huge = 0;
     for (const int4& r : ext) M.n_huge += (r.z - r.y > kHugeRow) ? 1 : 0;
     M.n_mid = M.n_long - M.n_huge;
@@ -262,7 +315,178 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
     return build_items(ext, M.short_max, kWarpSegLen, 32 * sms, M.items_warp, s, err);
 }
 
-// row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,
+// The long-row tiers over the rows of `ext` (row order, all above short_max),
+// built on the host: warp-row lists and the three item lists.
+inline int build_tiers(const std::vector<int4>& ext, int short_max, int sms, TiersDev& T,
+                       cudaStream_t s, std::string* err) {
+    std::vector<int32_t> w0, w1;
+    for (const int4& r : ext) {
+        const int len = r.z - r.y;
+        if (len > short_max && len <= kLongRow) w0.push_back(r.x);
+        if (len > short_max && len <= kHugeRow) w1.push_back(r.x);
+    }
+    T.n_warp0 = static_cast<int32_t>(w0.size());
+    T.n_warp1 = static_cast<int32_t>(w1.size());
+    cudaError_t e;
+    if ((e = upload(T.warp_rows0, w0, s)) != cudaSuccess ||
+        (e = upload(T.warp_rows1, w1, s)) != cudaSuccess)
+        return cuda_fail(err, e, "build_tiers");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_tiers");
+    int rc = build_items(ext, kLongRow, kSegLen, 4 * sms, T.items_long, s, err);
+    if (rc != PDHG_OK) return rc;
+    rc = build_items(ext, kHugeRow, kSegLen, 4 * sms, T.items_huge, s, err);
+    if (rc != PDHG_OK) return rc;
+    return build_items(ext, short_max, kWarpSegLen, 32 * sms, T.items_warp, s, err);
+}
+
+// Distinct 128-byte lines (32 four-byte entries) among 32 column indices.
+inline int lines_of(const int32_t* c) {
+    int32_t l[32];
+    for (int i = 0; i < 32; ++i) l[i] = c[i] >> 5;
+    std::sort(l, l + 32);
+    return static_cast<int>(std::unique(l, l + 32) - l);
+}
+
+constexpr int kSliceMinLen = 256;  // rows shorter than this are not worth a slice
+
+// Row slices of a scaled matrix (after bin_matrix, values in v64 and v32).
+// Candidates: runs of 32 consecutive rows of M.ext whose lengths are within
+// 5% of each other and at least kSliceMinLen. For each, column indices are
+// sampled at four positions k: across the 32 rows at k (slice order) and
+// along the first row from k (row order); a candidate becomes a slice when a
+// 32-wide gather in slice order touches at most a quarter of the 128-byte
+// lines it touches in row order. Then the lane-interleaved copy, the warp
+// items (k-chunks, split like rows when a slice needs several) and the long-
+// row tiers of the remaining rows.
+inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
+    SlicesDev& S = M.slices;
+    S.n_slice = 0;
+    S.n_item = 0;
+    const std::vector<int4>& ext = M.ext;
+    std::vector<size_t> cand;
+    std::vector<int> cand_lo;
+    for (size_t i = 0; i + 32 <= ext.size();) {
+        int lo = 0x7fffffff, hi = 0;
+        for (size_t j = i; j < i + 32; ++j) {
+            const int len = ext[j].z - ext[j].y;
+            lo = std::min(lo, len);
+            hi = std::max(hi, len);
+        }
+        if (lo >= kSliceMinLen && static_cast<int64_t>(lo) * 20 >= static_cast<int64_t>(hi) * 19) {
+            cand.push_back(i);
+            cand_lo.push_back(lo);
+            i += 32;
+        } else {
+            ++i;
+        }
+    }
+    if (cand.empty()) return PDHG_OK;
+    // sampled positions: per candidate, 4 x (32 across rows + 32 along row 0)
+    constexpr int kSamples = 4;
+    std::vector<int64_t> pos;
+    pos.reserve(cand.size() * kSamples * 64);
+    for (size_t c = 0; c < cand.size(); ++c) {
+        const int lo = cand_lo[c];
+        for (int q = 0; q < kSamples; ++q) {
+            const int k = static_cast<int>(static_cast<int64_t>(lo - 32) * q / (kSamples - 1));
+            for (int l = 0; l < 32; ++l) pos.push_back(static_cast<int64_t>(ext[cand[c] + l].y) + k);
+            for (int l = 0; l < 32; ++l) pos.push_back(static_cast<int64_t>(ext[cand[c]].y) + k + l);
+        }
+    }
+    std::vector<int32_t> cols(pos.size());
+    {
+        DBuf<int64_t> d_pos;
+        DBuf<int32_t> d_cols;
+        cudaError_t e;
+        if ((e = upload(d_pos, pos, s)) != cudaSuccess || (e = d_cols.alloc(pos.size())) != cudaSuccess)
+            return cuda_fail(err, e, "build_slices");
+        launch_gather_cols(M.ci.p, d_pos.p, static_cast<int32_t>(pos.size()), d_cols.p, s);
+        cudaMemcpyAsync(cols.data(), d_cols.p, sizeof(int32_t) * cols.size(), cudaMemcpyDeviceToHost, s);
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");
+    }
+    std::vector<size_t> chosen;
+    for (size_t c = 0; c < cand.size(); ++c) {
+        int across = 0, along = 0;
+        for (int q = 0; q < kSamples; ++q) {
+            const int32_t* b = cols.data() + (c * kSamples + q) * 64;
+            across += lines_of(b);
+            along += lines_of(b + 32);
+        }
+        if (4 * across <= along) chosen.push_back(cand[c]);
+    }
+    if (chosen.empty()) return PDHG_OK;
+
+    // slice metadata and the lane-interleaved copy
+    const int ns = static_cast<int>(chosen.size());
+    std::vector<int4> meta(static_cast<size_t>(ns));
+    std::vector<int32_t> row(32 * static_cast<size_t>(ns)), rlen(32 * static_cast<size_t>(ns));
+    int64_t total = 0, ksteps = 0;
+    for (int sl = 0; sl < ns; ++sl) {
+        int len = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int4& r = ext[chosen[static_cast<size_t>(sl)] + static_cast<size_t>(l)];
+            row[32 * static_cast<size_t>(sl) + l] = r.x;
+            rlen[32 * static_cast<size_t>(sl) + l] = r.z - r.y;
+            len = std::max(len, r.z - r.y);
+        }
+        if (total + 32 * static_cast<int64_t>(len) > 0x7fffffffLL) break;  // int offsets
+        meta[static_cast<size_t>(sl)] = make_int4(len, static_cast<int>(total), 32, 0);
+        total += 32 * static_cast<int64_t>(len);
+        ksteps += len;
+        S.n_slice = sl + 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = std::max(sms, 1);
+    // warp items: k-chunks of at least 64 steps, about two per resident warp
+    const int64_t resident = 32LL * sms;
+    int64_t chunk = std::max<int64_t>(64, (ksteps + 2 * resident - 1) / (2 * resident));
+    chunk = (chunk + 7) / 8 * 8;
+    std::vector<int4> items;
+    std::vector<int2> splits;
+    for (int sl = 0; sl < S.n_slice; ++sl) {
+        const int len = meta[static_cast<size_t>(sl)].x;
+        const int nchunk = static_cast<int>((len + chunk - 1) / chunk);
+        if (nchunk <= 1) {
+            items.push_back(make_int4(sl, 0, len, -1));
+            continue;
+        }
+        const int sid = static_cast<int>(splits.size());
+        splits.push_back(make_int2(static_cast<int>(items.size()), nchunk));
+        for (int q = 0; q < nchunk; ++q)
+            items.push_back(make_int4(sl, static_cast<int>(q * chunk),
+                                      static_cast<int>(std::min<int64_t>(len, (q + 1) * chunk)), sid));
+    }
+    S.n_item = static_cast<int32_t>(items.size());
+    cudaError_t e;
+    meta.resize(static_cast<size_t>(S.n_slice));
+    row.resize(32 * static_cast<size_t>(S.n_slice));
+    rlen.resize(32 * static_cast<size_t>(S.n_slice));
+    if ((e = upload(S.slice, meta, s)) != cudaSuccess || (e = upload(S.row, row, s)) != cudaSuccess ||
+        (e = upload(S.rlen, rlen, s)) != cudaSuccess || (e = S.col.alloc(static_cast<size_t>(total))) != cudaSuccess ||
+        (e = S.v32.alloc(static_cast<size_t>(total))) != cudaSuccess ||
+        (e = S.v64.alloc(static_cast<size_t>(total))) != cudaSuccess ||
+        (e = upload(S.item, items, s)) != cudaSuccess || (e = upload(S.split, splits, s)) != cudaSuccess ||
+        (e = S.ticket.alloc(splits.size())) != cudaSuccess ||
+        (e = S.part.alloc(32 * items.size())) != cudaSuccess)
+        return cuda_fail(err, e, "build_slices");
+    if (!splits.empty()) cudaMemsetAsync(S.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    launch_fill_slices(M.view(), S.view(), S.col.p, S.v32.p, S.v64.p, total, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");
+
+    // the long-row tiers without the rows of the slices kept
+    std::vector<char> in_slice(ext.size(), 0);
+    for (int sl = 0; sl < S.n_slice; ++sl)
+        for (size_t l = 0; l < 32; ++l) in_slice[chosen[static_cast<size_t>(sl)] + l] = 1;
+    std::vector<int4> rest;
+    rest.reserve(ext.size());
+    for (size_t i = 0; i < ext.size(); ++i)
+        if (!in_slice[i]) rest.push_back(ext[i]);
+    return build_tiers(rest, M.short_max, sms, M.no_slice_tiers, s, err);
+}
+
+// row_ptr structure on the host// row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,
 // non-decreasing. Every device kernel that walks rows relies on it.
 inline bool row_ptr_ok(int32_t rows, int64_t nnz, const int32_t* rp) {
     if (rp[0] != 0 || rp[rows] != nnz) return false;

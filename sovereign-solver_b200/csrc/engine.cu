@@ -109,8 +109,10 @@ struct Ctx {
         if (graph != nullptr) cudaGraphExecDestroy(graph);
         if (mail != nullptr) cudaFreeHost(mail);
         if (fork.fork != nullptr) cudaEventDestroy(fork.fork);
-        if (fork.join != nullptr) cudaEventDestroy(fork.join);
-        if (fork.side != nullptr) cudaStreamDestroy(fork.side);
+        for (int i = 0; i < 2; ++i) {
+            if (fork.join[i] != nullptr) cudaEventDestroy(fork.join[i]);
+            if (fork.side[i] != nullptr) cudaStreamDestroy(fork.side[i]);
+        }
         if (stream != nullptr) cudaStreamDestroy(stream);
     }
 
@@ -242,6 +244,10 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     int rc = bin_matrix(c.As, s, &c.err);
     if (rc != PDHG_OK) return rc;
     rc = bin_matrix(c.ATs, s, &c.err);
+    if (rc != PDHG_OK) return rc;
+    rc = build_slices(c.As, s, &c.err);
+    if (rc != PDHG_OK) return rc;
+    rc = build_slices(c.ATs, s, &c.err);
     if (rc != PDHG_OK) return rc;
     const double sign = c.lp.maximize ? -1.0 : 1.0;
     CK(c.c_s.alloc(static_cast<size_t>(n) + 1));
@@ -441,9 +447,11 @@ template <class T>
 void apply_tuning(const Ctx::Tuning& t, FastIter<T>& fi) {
     if (!t.have) return;
     fi.AT.iter_vw = t.shape[0];
-    fi.AT.long_mode = t.shape[1];
+    fi.AT.long_mode = t.shape[1] & 3;
+    fi.AT.use_slices = t.shape[1] >> 2;
     fi.A.iter_vw = t.shape[2];
-    fi.A.long_mode = t.shape[3];
+    fi.A.long_mode = t.shape[3] & 3;
+    fi.A.use_slices = t.shape[3] >> 2;
 }
 
 Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candidate) {
@@ -788,7 +796,7 @@ void tune_read_file() {
         int a = 0, b = 0;
         const size_t lb = txt.find('[', end);
         if (lb != std::string::npos && std::sscanf(txt.c_str() + lb, "[%d , %d]", &a, &b) == 2 &&
-            a >= 1 && a <= 32 && (a & (a - 1)) == 0 && b >= 0 && b <= 2)
+            a >= 1 && a <= 32 && (a & (a - 1)) == 0 && b >= 0 && b <= 6 && (b & 3) <= 2)
             g_tune_cache[key] = {a, b};
         pos = end + 1;
     }
@@ -810,9 +818,9 @@ void tune_write_file() {
 
 std::string tune_sig(const char* prec, const char* pass, const DevCsr& M) {
     char b[256];
-    std::snprintf(b, sizeof b, "%s/%s/rows%d/cols%d/nnz%lld/short%d/long%d/mid%d/huge%d/vw%d",
+    std::snprintf(b, sizeof b, "%s/%s/rows%d/cols%d/nnz%lld/short%d/long%d/mid%d/huge%d/vw%d/sl%d",
                   prec, pass, M.rows, M.cols, static_cast<long long>(M.nnz), M.n_short, M.n_long,
-                  M.n_mid, M.n_huge, M.vw);
+                  M.n_mid, M.n_huge, M.vw, M.slices.n_slice);
     return b;
 }
 
@@ -833,13 +841,15 @@ float time_pass(Ctx& c, FastIter<T>& fi, bool primal, cudaEvent_t e0, cudaEvent_
     return ms;
 }
 
-// Chooses {lanes, mode} for one pass; fi's matrix fields are set to the choice.
+// Chooses {lanes, mode} for one pass (mode = long-row strategy + 4 when the
+// row slices are used); fi's matrix fields are set to the choice.
 template <class T>
 void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* lanes,
                int* mode, cudaEvent_t e0, cudaEvent_t e1) {
     DevCsr& M = primal ? fi.AT : fi.A;
     M.iter_vw = M.vw;
     M.long_mode = 0;
+    M.use_slices = 0;
     *lanes = M.vw;
     *mode = 0;
     if (M.rows == 0 || M.nnz < kTuneMinNnz) return;
@@ -850,7 +860,9 @@ void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* 
         const auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
             M.iter_vw = *lanes = it->second.first;
-            M.long_mode = *mode = it->second.second;
+            *mode = it->second.second;
+            M.long_mode = *mode & 3;
+            M.use_slices = (*mode >> 2) != 0 && M.slices.n_item > 0 ? 1 : 0;
             return;
         }
     }
@@ -882,6 +894,26 @@ void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* 
     *mode = cand[pick].second;
     M.iter_vw = *lanes;
     M.long_mode = *mode;
+    if (M.slices.n_item > 0) {
+        // the row slices on top of the best shape, each strategy over the
+        // remaining long rows
+        float best = t[pick];
+        int best_mode = *mode;
+        M.use_slices = 1;
+        for (int m = 0; m <= 2; ++m) {
+            if (m == 1 && M.n_mid == 0) continue;
+            M.long_mode = m;
+            float ts = 3.0e38f;
+            for (int round = 0; round < 2; ++round) ts = std::min(ts, time_pass(c, fi, primal, e0, e1));
+            if (ts < 0.95f * best) {
+                best = ts;
+                best_mode = m + 4;
+            }
+        }
+        *mode = best_mode;
+        M.long_mode = best_mode & 3;
+        M.use_slices = best_mode >> 2;
+    }
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tune_cache[key] = {*lanes, *mode};
     tune_write_file();
@@ -1354,9 +1386,11 @@ int pdhg_create(int device, pdhg_ctx** out) {
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
     if (c.sm_count <= 0) c.sm_count = 148;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c.fork.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c.fork.side[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c.fork.side[1], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c.fork.fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c.fork.join, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c.fork.join[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.fork.join[1], cudaEventDisableTiming) != cudaSuccess)
         return PDHG_ERR_BACKEND;
     void* mp = nullptr;
     if (cudaHostAlloc(&mp, sizeof(pdhg::Mailbox), cudaHostAllocMapped) != cudaSuccess)

@@ -51,6 +51,37 @@ struct RowItems {
     int32_t n_item = 0;
 };
 
+// Row slices: 32 long rows of about the same length stored lane-interleaved
+// (entry k of lane l at off + 32 k + l). Chosen for rows whose gathers
+// coalesce across rows but not along a row -- consecutive entries of a row
+// far apart in the gathered vector, the k-th entries of the 32 rows next to
+// each other (the demand rows of a transportation LP). A warp item covers
+// entries [k0, k1) of one slice, lane l summing row l, so the value, index
+// and gather loads of a step are each one or two lines. A slice cut into
+// several items combines per lane like a split row (ticket per slice, 32
+// partials per item, added in item order by the last warp).
+struct RowSlices {
+    int32_t n_slice = 0, n_item = 0;
+    const int4* slice = nullptr;     // {len (longest lane), off, rows in use, -}
+    const int32_t* row = nullptr;    // 32 per slice: row id, -1 for an unused lane
+    const int32_t* rlen = nullptr;   // 32 per slice: the lane's row length
+    const int32_t* col = nullptr;    // lane-interleaved column indices (scaled matrix)
+    const float* v32 = nullptr;      // lane-interleaved scaled values, FP32 and FP64
+    const double* v64 = nullptr;
+    const int4* item = nullptr;      // {slice, k0, k1, split}; split -1 = the whole slice
+    const int2* split = nullptr;     // per split slice: {first item, items}
+    unsigned int* ticket = nullptr;  // per split slice, 0 between launches
+    double* part = nullptr;          // 32 partials per item
+};
+
+// The long-row tiers of the throughput kernels (see DevCsr).
+struct LongTiers {
+    const int32_t* warp_rows0 = nullptr;
+    const int32_t* warp_rows1 = nullptr;
+    int32_t n_warp0 = 0, n_warp1 = 0;
+    RowItems items_long, items_huge, items_warp;
+};
+
 struct DevCsr {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
@@ -87,11 +118,17 @@ struct DevCsr {
     // kernel) and over the rows above kHugeRow (long_mode 1); warp work items
     // over every row above short_max (long_mode 2).
     RowItems items_long, items_huge, items_warp;
+    // Row slices (iteration kernels only) and the long-row tiers without the
+    // slices' rows, which replace the fields above when use_slices is set.
+    RowSlices slices;
+    LongTiers no_slice_tiers;
     // Iteration-kernel shape (the autotuner's choice): lanes per short row
-    // (0 = vw) and the long-row strategy (0: warp_rows0 + items_long;
-    // 1: warp_rows1 + items_huge; 2: items_warp).
+    // (0 = vw), the long-row strategy (0: warp_rows0 + items_long;
+    // 1: warp_rows1 + items_huge; 2: items_warp) and whether the row slices
+    // take their rows.
     int iter_vw = 0;
     int long_mode = 0;
+    int use_slices = 0;
 };
 
 
@@ -223,13 +260,14 @@ struct FastIter {
     Iterates<T> it;
     DevState* st;
 };
-// A pass's short-row and long-row kernels touch disjoint rows and only read
-// the gathered vector, so they may run side by side: with a PassFork the long
-// kernel goes to `side` (fork: s -> side, join: side -> s), else both run in
-// order on s. Inside a stream capture this becomes two parallel graph branches.
+// A pass's short-row, long-row and row-slice kernels touch disjoint rows and
+// only read the gathered vector, so they may run side by side: with a
+// PassFork the long-row kernel goes to side[0] and the slice kernel to side[1]
+// (fork: s -> sides, join: sides -> s), else all run in order on s. Inside a
+// stream capture these become parallel graph branches.
 struct PassFork {
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };
 template <class T>
 int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s,
@@ -354,6 +392,14 @@ void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* lo
 // out[k] = {rows[k], rp[rows[k]], rp[rows[k] + 1], 0} for k < n.
 void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out,
                         cudaStream_t s);
+// Column indices of sampled entries: out[q] = ci[pos[q]] for q < n.
+void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_t* out,
+                        cudaStream_t s);
+// Lane-interleaved copy of the slices' rows: for slice s, lane l, entry k <
+// rlen: col/v32/v64[off + 32 k + l] = the row's k-th entry; padding entries
+// get column 0 and value 0.
+void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,
+                        int64_t total, cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,
                        double* row_max, double* col_max, double tol, IntakeState* is,
                        cudaStream_t s);

@@ -127,6 +127,38 @@ __global__ void k_row_extents(const int32_t* rows, int32_t n, const int32_t* rp,
     out[k] = make_int4(r, rp[r], rp[r + 1], 0);
 }
 
+__global__ void k_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_t* out) {
+    const int q = blockIdx.x * kBlock + threadIdx.x;
+    if (q < n) out[q] = ci[pos[q]];
+}
+
+// One CTA per slice (grid-stride over slices): entry k of lane l from the
+// CSR row S.row[32 s + l], or padding (column 0, value 0) past the row's end.
+__global__ void k_fill_slices(const int32_t* rp, const int32_t* ci, const double* v64,
+                              const float* v32, RowSlices S, int32_t* col, float* o32,
+                              double* o64) {
+    for (int sl = blockIdx.x; sl < S.n_slice; sl += gridDim.x) {
+        const int4 d = S.slice[sl];
+        const int64_t n = static_cast<int64_t>(d.x) * 32;
+        for (int64_t e = threadIdx.x; e < n; e += kBlock) {
+            const int l = static_cast<int>(e & 31);
+            const int k = static_cast<int>(e >> 5);
+            const int r = S.row[32 * sl + l];
+            const int64_t dst = d.y + e;
+            if (r >= 0 && k < S.rlen[32 * sl + l]) {
+                const int64_t src = rp[r] + k;
+                col[dst] = ci[src];
+                o32[dst] = v32[src];
+                o64[dst] = v64[src];
+            } else {
+                col[dst] = 0;
+                o32[dst] = 0.f;
+                o64[dst] = 0.0;
+            }
+        }
+    }
+}
+
 // Rows with lo < length <= hi appended to `list` (grid-stride; one atomic per
 // warp that has any).
 __global__ void k_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
@@ -429,6 +461,18 @@ void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* lo
 void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out,
                         cudaStream_t s) {
     if (n > 0) k_row_extents<<<nblocks(n), kBlock, 0, s>>>(rows, n, rp, out);
+}
+
+void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_t* out,
+                        cudaStream_t s) {
+    if (n > 0) k_gather_cols<<<nblocks(n), kBlock, 0, s>>>(ci, pos, n, out);
+}
+
+void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,
+                        int64_t total, cudaStream_t s) {
+    if (S.n_slice == 0 || total == 0) return;
+    const int g = S.n_slice < kGridCap ? S.n_slice : kGridCap;
+    k_fill_slices<<<g, kBlock, 0, s>>>(M.rp, M.ci, M.v64, M.v32, S, col, v32, v64);
 }
 
 void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,

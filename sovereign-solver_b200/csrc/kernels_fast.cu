@@ -52,6 +52,9 @@
 #ifndef PDHG_WARPITEM_MIN_CTAS
 #define PDHG_WARPITEM_MIN_CTAS 4
 #endif
+#ifndef PDHG_SLICE_MIN_CTAS
+#define PDHG_SLICE_MIN_CTAS 4
+#endif
 
 namespace pdhg {
 
@@ -194,6 +197,82 @@ __global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
     if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
 }
 
+template <class T>
+__device__ __forceinline__ const T* slice_vals(const RowSlices& S);
+template <>
+__device__ __forceinline__ const float* slice_vals<float>(const RowSlices& S) { return S.v32; }
+template <>
+__device__ __forceinline__ const double* slice_vals<double>(const RowSlices& S) { return S.v64; }
+
+// Row slices (RowSlices): a warp item is entries [k0, k1) of one slice, lane
+// l on the slice's row l, in rounds of eight steps; each step is one
+// coalesced index load, one coalesced value load and one gather per lane.
+// A slice cut into several items: every lane stores its partial, lane 0 takes
+// the slice's ticket, and the last warp adds each lane's partials in item
+// order (four interleaved sums, fixed) before the 32 rows' updates.
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
+    fast_iter_slices(FastIter<T> a, int first, int reset) {
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const RowSlices& S = M.slices;
+    const int idx = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    if (idx >= S.n_item) return;
+    const int lane = threadIdx.x & 31;
+    const int4 w = __ldg(S.item + idx);
+    const int4 d = __ldg(S.slice + w.x);
+    const int row = __ldg(S.row + 32 * w.x + lane);
+    const int kend = min(w.z, __ldg(S.rlen + 32 * w.x + lane));
+    const int32_t* __restrict__ col = S.col + d.y + lane;
+    const T* __restrict__ val = slice_vals<T>(S) + d.y + lane;
+    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
+    T acc = T(0);
+    for (int k0 = w.y; k0 < w.z; k0 += 8) {
+        int c[8];
+        T v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = k0 + u;
+            c[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
+            v[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (k0 + u < kend) acc += v[u] * __ldg(xg + c[u]);
+    }
+    if (w.w >= 0) {
+        S.part[32 * static_cast<int64_t>(idx) + lane] = static_cast<double>(acc);
+        __threadfence();
+        __syncwarp();
+        const int2 sp = __ldg(S.split + w.w);
+        int last = 0;
+        if (lane == 0) last = atomicAdd(S.ticket + w.w, 1u) == static_cast<unsigned>(sp.y - 1) ? 1 : 0;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) return;
+        __threadfence();
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+        int q = sp.x;
+        const int qe = sp.x + sp.y;
+        for (; q + 4 <= qe; q += 4) {
+            t0 += __ldcg(S.part + 32 * static_cast<int64_t>(q) + lane);
+            t1 += __ldcg(S.part + 32 * static_cast<int64_t>(q + 1) + lane);
+            t2 += __ldcg(S.part + 32 * static_cast<int64_t>(q + 2) + lane);
+            t3 += __ldcg(S.part + 32 * static_cast<int64_t>(q + 3) + lane);
+        }
+        for (; q < qe; ++q) t0 += __ldcg(S.part + 32 * static_cast<int64_t>(q) + lane);
+        if (lane == 0) S.ticket[w.w] = 0u;
+        acc = static_cast<T>((t0 + t1) + (t2 + t3));
+    }
+    if (row < 0) return;
+    const PV<T> pv = pvec<T>(a.P);
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, row, first, fresh);
+    epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma);
+}
+
 __global__ void k_clear_flags(DevState* st) {
     if (threadIdx.x == 0) {
         st->restart = 0;
@@ -208,49 +287,91 @@ inline int short_blocks_for(const DevCsr& M) {
     return static_cast<int>((static_cast<int64_t>(M.rows) * iter_lanes(M) + kBlock - 1) / kBlock);
 }
 
+// The matrix a pass runs on: with the row slices in use, the long-row tiers
+// without the slices' rows replace the full ones.
+inline DevCsr pass_matrix(const DevCsr& M) {
+    if (!M.use_slices || M.slices.n_item == 0) return M;
+    DevCsr X = M;
+    const LongTiers& t = M.no_slice_tiers;
+    X.warp_rows0 = t.warp_rows0;
+    X.warp_rows1 = t.warp_rows1;
+    X.n_warp0 = t.n_warp0;
+    X.n_warp1 = t.n_warp1;
+    X.items_long = t.items_long;
+    X.items_huge = t.items_huge;
+    X.items_warp = t.items_warp;
+    return X;
+}
+
+// CTAs of a pass's kernels: short rows, the long-row kernel (of which the
+// first `warp` run warp rows), the row slices.
+struct PassPlan {
+    int shrt = 0, warp = 0, lng = 0, slc = 0;
+};
+inline PassPlan pass_plan(const DevCsr& M) {
+    PassPlan p;
+    if (M.rows == 0) return p;
+    p.shrt = short_blocks_for(M);
+    const int mode = M.long_mode;
+    const int nw = mode == 2 ? M.items_warp.n_item : mode == 1 ? M.n_warp1 : M.n_warp0;
+    p.warp = (nw + kBlock / 32 - 1) / (kBlock / 32);
+    p.lng = mode == 2 ? p.warp : p.warp + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
+    if (M.use_slices) p.slc = (M.slices.n_item + kBlock / 32 - 1) / (kBlock / 32);
+    return p;
+}
+
 // Kernels one pass over M launches besides the flag reset.
-inline int pass_launches(const DevCsr& M) {
-    if (M.rows == 0) return 0;
-    return (short_blocks_for(M) > 0 ? 1 : 0) + (M.rows > M.n_iter_short ? 1 : 0);
+inline int pass_launches(const DevCsr& M0) {
+    const PassPlan p = pass_plan(pass_matrix(M0));
+    return (p.shrt > 0 ? 1 : 0) + (p.lng > 0 ? 1 : 0) + (p.slc > 0 ? 1 : 0);
 }
 
 // Returns the number of kernels launched.
 template <class T, bool PRIMAL>
-int launch_iter(const FastIter<T>& a, int first, cudaStream_t s, const PassFork* f) {
-    const DevCsr& M = PRIMAL ? a.AT : a.A;
-    if (M.rows == 0) {
+int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork* f) {
+    const DevCsr& M0 = PRIMAL ? a0.AT : a0.A;
+    if (M0.rows == 0) {
         if (PRIMAL && first) {
-            k_clear_flags<<<1, 32, 0, s>>>(a.st);
+            k_clear_flags<<<1, 32, 0, s>>>(a0.st);
             return 1;
         }
         return 0;
     }
-    const int sb = short_blocks_for(M);
+    FastIter<T> a = a0;
+    DevCsr& M = PRIMAL ? a.AT : a.A;
+    M = pass_matrix(M0);
+    const PassPlan p = pass_plan(M);
     const int mode = M.long_mode;
-    const int nw = mode == 2 ? M.items_warp.n_item : mode == 1 ? M.n_warp1 : M.n_warp0;
-    const int mb = (nw + kBlock / 32 - 1) / (kBlock / 32);
-    const int lb = mode == 2 ? mb : mb + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
-    const int reset_short = (PRIMAL && first) ? 1 : 0;
-    const int reset_long = (PRIMAL && first && sb == 0) ? 1 : 0;
-    const bool fork = f != nullptr && f->side != nullptr && sb > 0 && lb > 0;
-    cudaStream_t ls = s;
+    // the flag reset rides on the first kernel of the period's first pass
+    const int rs = PRIMAL && first ? 1 : 0;
+    const int reset_short = rs;
+    const int reset_long = rs && p.shrt == 0 ? 1 : 0;
+    const int reset_slc = rs && p.shrt == 0 && p.lng == 0 ? 1 : 0;
+    const int kernels = (p.shrt > 0) + (p.lng > 0) + (p.slc > 0);
+    const bool fork = f != nullptr && f->side[0] != nullptr && kernels > 1;
+    cudaStream_t ls = s, ss = s;
     if (fork) {
         cudaEventRecord(f->fork, s);
-        cudaStreamWaitEvent(f->side, f->fork, 0);
-        ls = f->side;
+        cudaStreamWaitEvent(f->side[0], f->fork, 0);
+        if (p.slc > 0) cudaStreamWaitEvent(f->side[1], f->fork, 0);
+        ls = f->side[0];
+        ss = f->side[1];
     }
-    if (lb > 0 && mode == 2) {
-        fast_iter_witems<T, PRIMAL><<<lb, kBlock, 0, ls>>>(a, first, reset_long);
-    } else if (lb > 0) {
+    if (p.lng > 0 && mode == 2) {
+        fast_iter_witems<T, PRIMAL><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long);
+    } else if (p.lng > 0) {
+        const int mb = p.warp;
         if (mb == 0) {
-            if (mode == 1) fast_iter_long<T, PRIMAL, 1, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);
-            else fast_iter_long<T, PRIMAL, 0, false><<<lb, kBlock, 0, ls>>>(a, first, reset_long, 0);
+            if (mode == 1) fast_iter_long<T, PRIMAL, 1, false><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long, 0);
+            else fast_iter_long<T, PRIMAL, 0, false><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long, 0);
         } else {
-            if (mode == 1) fast_iter_long<T, PRIMAL, 1, true><<<lb, kBlock, 0, ls>>>(a, first, reset_long, mb);
-            else fast_iter_long<T, PRIMAL, 0, true><<<lb, kBlock, 0, ls>>>(a, first, reset_long, mb);
+            if (mode == 1) fast_iter_long<T, PRIMAL, 1, true><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long, mb);
+            else fast_iter_long<T, PRIMAL, 0, true><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long, mb);
         }
     }
-    if (sb > 0) {
+    if (p.slc > 0) fast_iter_slices<T, PRIMAL><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
+    if (p.shrt > 0) {
+        const int sb = p.shrt;
         switch (iter_lanes(M)) {
             case 1: fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 2: fast_iter<T, 2, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
@@ -261,10 +382,14 @@ int launch_iter(const FastIter<T>& a, int first, cudaStream_t s, const PassFork*
         }
     }
     if (fork) {
-        cudaEventRecord(f->join, f->side);
-        cudaStreamWaitEvent(s, f->join, 0);
+        cudaEventRecord(f->join[0], f->side[0]);
+        cudaStreamWaitEvent(s, f->join[0], 0);
+        if (p.slc > 0) {
+            cudaEventRecord(f->join[1], f->side[1]);
+            cudaStreamWaitEvent(s, f->join[1], 0);
+        }
     }
-    return (sb > 0 ? 1 : 0) + (lb > 0 ? 1 : 0);
+    return kernels;
 }
 
 // ---------------------------------------------------------------------------

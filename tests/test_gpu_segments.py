@@ -85,3 +85,72 @@ def test_split_rows_in_both_long_row_strategies(tmp_path):
         if mode is not None:
             assert out["fp64"]["dual_long_mode"] == mode, out
             assert out["mixed"]["dual_long_mode"] == mode, out
+
+
+SLICE_SNIPPET = """
+import importlib, json, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+pkg = importlib.import_module("sovereign-solver_b200")
+p = pkg.lpgen.transportation_lp(600, 900, seed=1000)  # 1.08M nonzeros: the tuner runs
+assert p.nnz >= 1 << 20
+
+def rel_err(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+kw = dict(max_iterations=300, tolerance=1e-12, restart_check_period=150, trace_iters=100)
+with pkg.Engine(0) as e:
+    e.load(p)
+    ex = e.solve(pkg.PdhgOptions(**kw))
+    f1 = e.solve(pkg.PdhgOptions(precision="fp64", **kw))
+    f2 = e.solve(pkg.PdhgOptions(precision="fp64", **kw))
+    mk = dict(precision="mixed", termination_rule="relative_kkt", restart_rule="adaptive",
+              max_iterations=200_000)
+    m1 = e.solve(pkg.PdhgOptions(**mk))
+    m2 = e.solve(pkg.PdhgOptions(**mk))
+    f64 = e.solve(pkg.PdhgOptions(**dict(mk, precision="fp64")))
+    out = dict(
+        fp64=e.tuning("fp64"), mixed=e.tuning("mixed"),
+        err=max(max(rel_err(f1.trace_x[k], ex.trace_x[k]), rel_err(f1.trace_y[k], ex.trace_y[k]))
+                for k in range(100)),
+        fp64_repeat=bool(np.array_equal(f1.primal, f2.primal) and np.array_equal(f1.dual, f2.dual)),
+        mixed_repeat=bool(np.array_equal(m1.primal, m2.primal) and m1.objective == m2.objective),
+        status=[m1.status, f64.status],
+        obj_gap=abs(m1.objective - f64.objective) / max(1.0, abs(f64.objective)))
+    print(json.dumps(out))
+"""
+
+
+def test_row_slices_on_a_transportation_lp(tmp_path):
+    """The demand rows of a transportation LP (600 entries, consecutive rows
+    gathering consecutive columns) become lane-interleaved row slices; with
+    the slices pinned on (each long-row strategy for the remaining rows) and
+    off, the FP64 iterates track the exact kernels, repeated solves are
+    bit-identical and the mixed mode stops like the FP64 mode (at the FP64
+    optimum when both converge)."""
+    cache = tmp_path / "tune.json"
+    env = dict(os.environ, PDHG_B200_TUNE_CACHE=str(cache))
+    code = SLICE_SNIPPET.format(root=ROOT)
+
+    def go(mode=None):
+        if mode is not None:
+            entries = json.loads(cache.read_text())
+            cache.write_text(json.dumps(
+                {k: [v[0], mode if "/dual/" in k else v[1]] for k, v in entries.items()}))
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True,
+                           text=True, timeout=900)
+        assert r.returncode == 0, r.stderr[-4000:]
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    first = go()
+    keys = json.loads(cache.read_text())
+    assert any("/dual/" in k and not k.endswith("/sl0") for k in keys), keys
+    for mode, out in [(None, first)] + [(m, go(m)) for m in (0, 4, 5, 6)]:
+        assert out["err"] <= 1e-10, (mode, out)
+        assert out["fp64_repeat"] and out["mixed_repeat"], (mode, out)
+        assert out["status"][0] == out["status"][1], (mode, out)
+        if out["status"][0] == "optimal":
+            assert out["obj_gap"] <= 2e-3, (mode, out)
+        if mode is not None:
+            assert out["fp64"]["dual_long_mode"] == mode, out
