@@ -204,7 +204,9 @@ int pdhg_batch_start_kkt(pdhg_ctx* ctx, const double* x, const double* y, double
  * long-row strategy (0: a warp per row up to 512 entries, CTA work items
  * above; 1: a warp per row up to 4,096 entries, CTA items above; 2: warp work
  * items for every row past the short ones; rows longer than a work item are
- * split into segments) of the primal pass (rows of A^T), out[2], out[3] the same for the
+ * split into segments; plus 4 when row slices -- lane-interleaved copies of
+ * runs of 32 equal-length rows whose gathers coalesce across rows -- take
+ * their rows) of the primal pass (rows of A^T), out[2], out[3] the same for the
  * dual pass (rows of A), out[4] = 1 when chosen by timing, 0 for the defaults
  * (no solve yet, autotune off, or a small LP). Engine extension: the autotuner
  * times the candidates once per matrix shape and precision, and keeps the
