@@ -43,7 +43,7 @@ struct DBuf {
 struct ItemsDev {
     DBuf<int4> item;
     DBuf<int2> split;
-    DBuf<unsigned int> ticket;
+    DBuf<unsigned int> ticket, fetch;
     DBuf<double> part;
     int32_t n_item = 0;
     RowItems view() const {
@@ -52,6 +52,7 @@ struct ItemsDev {
         v.split = split.p;
         v.ticket = ticket.p;
         v.part = part.p;
+        v.fetch = fetch.p;
         v.n_item = n_item;
         return v;
     }
@@ -82,7 +83,7 @@ struct SlicesDev {
     DBuf<int32_t> row, rlen, col;
     DBuf<float> v32;
     DBuf<double> v64, part;
-    DBuf<unsigned int> ticket;
+    DBuf<unsigned int> ticket, fetch;
     int32_t n_slice = 0, n_item = 0;
     RowSlices view() const {
         RowSlices v;
@@ -98,6 +99,7 @@ struct SlicesDev {
         v.split = split.p;
         v.ticket = ticket.p;
         v.part = part.p;
+        v.fetch = fetch.p;
         return v;
     }
 };
@@ -240,9 +242,11 @@ inline int build_items(const std::vector<int4>& ext, int min_len, int min_seg, i
     if ((e = upload(D.item, items.data(), items.size(), s)) != cudaSuccess ||
         (e = upload(D.split, splits.data(), splits.size(), s)) != cudaSuccess ||
         (e = D.ticket.alloc(splits.size())) != cudaSuccess ||
-        (e = D.part.alloc(2 * items.size())) != cudaSuccess)
+        (e = D.part.alloc(2 * items.size())) != cudaSuccess ||
+        (e = D.fetch.alloc(2)) != cudaSuccess)
         return cuda_fail(err, e, "build_items");
     if (!splits.empty()) cudaMemsetAsync(D.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    cudaMemsetAsync(D.fetch.p, 0, 2 * sizeof(unsigned int), s);
     // the host vectors are read by the copies above before they go out of scope
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_items");
     return PDHG_OK;
@@ -439,9 +443,10 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     sms = std::max(sms, 1);
-    // warp items: k-chunks of at least 64 steps, about two per resident warp
+    // warp items: k-chunks of at least 32 steps, about four per resident warp
+    // (the slice kernel is persistent and claims items one by one)
     const int64_t resident = 32LL * sms;
-    int64_t chunk = std::max<int64_t>(64, (ksteps + 2 * resident - 1) / (2 * resident));
+    int64_t chunk = std::max<int64_t>(32, (ksteps + 4 * resident - 1) / (4 * resident));
     chunk = (chunk + 7) / 8 * 8;
     std::vector<int4> items;
     std::vector<int2> splits;
@@ -469,9 +474,11 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
         (e = S.v64.alloc(static_cast<size_t>(total))) != cudaSuccess ||
         (e = upload(S.item, items, s)) != cudaSuccess || (e = upload(S.split, splits, s)) != cudaSuccess ||
         (e = S.ticket.alloc(splits.size())) != cudaSuccess ||
-        (e = S.part.alloc(32 * items.size())) != cudaSuccess)
+        (e = S.part.alloc(32 * items.size())) != cudaSuccess ||
+        (e = S.fetch.alloc(2)) != cudaSuccess)
         return cuda_fail(err, e, "build_slices");
     if (!splits.empty()) cudaMemsetAsync(S.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    cudaMemsetAsync(S.fetch.p, 0, 2 * sizeof(unsigned int), s);
     launch_fill_slices(M.view(), S.view(), S.col.p, S.v32.p, S.v64.p, total, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");
 

@@ -1385,6 +1385,7 @@ int pdhg_create(int device, pdhg_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return PDHG_ERR_BACKEND;
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
     if (c.sm_count <= 0) c.sm_count = 148;
+    if (pdhg::init_fast_kernels(device) != 0) return PDHG_ERR_BACKEND;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c.fork.side[0], cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c.fork.side[1], cudaStreamNonBlocking) != cudaSuccess ||

@@ -48,6 +48,7 @@ struct RowItems {
     const int2* split = nullptr;     // per split row: {first item, segments}
     unsigned int* ticket = nullptr;  // per split row, 0 between launches
     double* part = nullptr;          // 2 partials per item
+    unsigned int* fetch = nullptr;   // persistent kernels: {next item, exits}, 0 between launches
     int32_t n_item = 0;
 };
 
@@ -72,6 +73,7 @@ struct RowSlices {
     const int2* split = nullptr;     // per split slice: {first item, items}
     unsigned int* ticket = nullptr;  // per split slice, 0 between launches
     double* part = nullptr;          // 32 partials per item
+    unsigned int* fetch = nullptr;   // {next item, exits}, 0 between launches
 };
 
 // The long-row tiers of the throughput kernels (see DevCsr).
@@ -277,6 +279,10 @@ int launch_fast_dual(const FastIter<T>& a, int first, cudaStream_t s,
                      const PassFork* f = nullptr);
 template <class T>
 int fast_launches_per_iteration(const FastIter<T>& a);
+// Once per device, before the first launch and outside any stream capture:
+// records how many CTAs of the persistent iteration kernels are resident per
+// device (their grids). 0 on success.
+int init_fast_kernels(int device);
 
 // Restart rules: 0 = the reference's (restart to the average when its residual
 // is <= restart_decrease x the residual at the last restart, pdhg.cpp:391-408);

@@ -106,6 +106,45 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
     return am_last;
 }
 
+// Persistent kernels claim work items from a counter pair {next, exits}:
+// cta_fetch (every thread of the CTA calls it) returns the next item index to
+// all threads, warp_fetch the same for one warp. Each CTA (warp) that ran the
+// loop reports its exit once; the last of the grid resets both counters for
+// the next launch (launches on a stream are ordered, so nobody claims in
+// between). Nothing ever waits on another CTA.
+__device__ __forceinline__ int cta_fetch(unsigned int* fetch) {
+    __shared__ int next;
+    if (threadIdx.x == 0) next = static_cast<int>(atomicAdd(fetch, 1u));
+    __syncthreads();
+    const int v = next;
+    __syncthreads();
+    return v;
+}
+
+__device__ __forceinline__ void cta_exit(unsigned int* fetch) {
+    if (threadIdx.x != 0) return;
+    __threadfence();
+    if (atomicAdd(fetch + 1, 1u) == gridDim.x - 1) {
+        fetch[0] = 0u;
+        fetch[1] = 0u;
+    }
+}
+
+__device__ __forceinline__ int warp_fetch(unsigned int* fetch) {
+    int v = 0;
+    if ((threadIdx.x & 31) == 0) v = static_cast<int>(atomicAdd(fetch, 1u));
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__device__ __forceinline__ void warp_exit(unsigned int* fetch) {
+    if ((threadIdx.x & 31) != 0) return;
+    __threadfence();
+    if (atomicAdd(fetch + 1, 1u) == gridDim.x * (blockDim.x / 32) - 1) {
+        fetch[0] = 0u;
+        fetch[1] = 0u;
+    }
+}
+
 // One segment of a split row done; every thread of the CTA calls it (block-
 // uniform) with the CTA's two partials. Thread 0 stores them and takes the
 // row's ticket. The CTA that draws the last ticket returns true on every

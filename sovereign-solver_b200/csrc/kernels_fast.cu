@@ -27,6 +27,7 @@
 // (original_space_residual, pdhg.cpp:145-199) derived elementwise from the
 // scaled products: A_o x_o = D_r^-1 (A_s x_s) and (c - A^T y)_o = r_s / D_c.
 // Its last CTA takes the candidate / termination / restart decision.
+#include <algorithm>
 #include <type_traits>
 
 #include "engine.cuh"
@@ -121,8 +122,33 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
 }
 
-// WARPS = false: the pass has no warp rows in this mode, only CTA items (the
-// warp path is compiled out, so more CTAs fit per SM).
+// One CTA work item of L (block-uniform): the dot of its entries, then for a
+// whole row its update, for a segment its partial and ticket (and the row's
+// update when this CTA completes the row).
+template <class T, bool PRIMAL>
+__device__ __forceinline__ void cta_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
+                                         int idx, int first, bool fresh, T tau, T sigma) {
+    const T* __restrict__ vals = mvals<T>(M);
+    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
+    const PV<T> pv = pvec<T>(a.P);
+    const int4 w = __ldg(L.item + idx);
+    EpiIn<T> in{};
+    if (threadIdx.x == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+    T acc = long_row_dot<T>(M.ci, vals, xg, w.y, w.z);
+    if (w.w >= 0) {  // block-uniform
+        double tot, unused;
+        if (!segment_finish(L, idx, w.w, static_cast<double>(acc), 0.0, &tot, &unused)) return;
+        acc = static_cast<T>(tot);
+        if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+    }
+    if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+}
+
+// WARPS = true: the first warp_blocks CTAs take the warp rows, one CTA per
+// item after them. WARPS = false (the pass has no warp rows in this mode):
+// a persistent grid (the resident CTAs) claims items one by one from L.fetch,
+// so no wave of CTAs ends half empty; the warp path is compiled out, so more
+// CTAs fit per SM.
 template <class T, bool PRIMAL, int MODE, bool WARPS>
 __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_LONG_MIN_CTAS)
     fast_iter_long(FastIter<T> a, int first, int reset, int warp_blocks) {
@@ -130,38 +156,36 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
     iter_reset(st, reset);
     if (st->done) return;
     const DevCsr& M = PRIMAL ? a.AT : a.A;
-    const T* __restrict__ vals = mvals<T>(M);
-    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
-    const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    if (WARPS && static_cast<int>(blockIdx.x) < warp_blocks) {
+    const RowItems& L = MODE == 0 ? M.items_long : M.items_huge;
+    if (!WARPS) {
+        for (;;) {
+            const int idx = cta_fetch(L.fetch);
+            if (idx >= L.n_item) break;
+            cta_item<T, PRIMAL>(a, M, L, idx, first, fresh, tau, sigma);
+        }
+        cta_exit(L.fetch);
+        return;
+    }
+    if (static_cast<int>(blockIdx.x) < warp_blocks) {
         // one warp per row: rows above short_max up to kLongRow (mode 0) or
         // kHugeRow (mode 1) entries
         const int w = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
         if (w >= (MODE == 0 ? M.n_warp0 : M.n_warp1)) return;
         const int r = __ldg((MODE == 0 ? M.warp_rows0 : M.warp_rows1) + w);
         const int lane = threadIdx.x & 31;
+        const PV<T> pv = pvec<T>(a.P);
         EpiIn<T> in{};
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
-        const T acc = warp_row_dot<T>(M.ci, vals, xg, __ldg(M.rp + r), __ldg(M.rp + r + 1));
+        const T acc = warp_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? a.it.y : a.it.xbar,
+                                      __ldg(M.rp + r), __ldg(M.rp + r + 1));
         if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
     } else {
         // CTA work items: rows above kLongRow (mode 0) or kHugeRow (mode 1),
-        // those above kSegLen entries in segments
-        const RowItems& L = MODE == 0 ? M.items_long : M.items_huge;
-        const int idx = static_cast<int>(blockIdx.x) - warp_blocks;
-        const int4 w = __ldg(L.item + idx);
-        EpiIn<T> in{};
-        if (threadIdx.x == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
-        T acc = long_row_dot<T>(M.ci, vals, xg, w.y, w.z);
-        if (w.w >= 0) {  // block-uniform
-            double tot, unused;
-            if (!segment_finish(L, idx, w.w, static_cast<double>(acc), 0.0, &tot, &unused)) return;
-            acc = static_cast<T>(tot);
-            if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
-        }
-        if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+        // those above the segment length in segments
+        cta_item<T, PRIMAL>(a, M, L, static_cast<int>(blockIdx.x) - warp_blocks, first, fresh,
+                            tau, sigma);
     }
 }
 
@@ -204,22 +228,17 @@ __device__ __forceinline__ const float* slice_vals<float>(const RowSlices& S) { 
 template <>
 __device__ __forceinline__ const double* slice_vals<double>(const RowSlices& S) { return S.v64; }
 
-// Row slices (RowSlices): a warp item is entries [k0, k1) of one slice, lane
-// l on the slice's row l, in rounds of eight steps; each step is one
-// coalesced index load, one coalesced value load and one gather per lane.
-// A slice cut into several items: every lane stores its partial, lane 0 takes
-// the slice's ticket, and the last warp adds each lane's partials in item
-// order (four interleaved sums, fixed) before the 32 rows' updates.
+// One warp item of the row slices (warp-uniform): entries [k0, k1) of one
+// slice, lane l on the slice's row l, in rounds of eight steps; each step is
+// one coalesced index load, one coalesced value load and one gather per lane.
+// The next round's index and value loads are issued before this round's
+// gathers, so the matrix stream and the gathers overlap. A slice cut into
+// several items: every lane stores its partial, lane 0 takes the slice's
+// ticket, and the last warp adds each lane's partials in item order (four
+// interleaved sums, fixed) before the 32 rows' updates.
 template <class T, bool PRIMAL>
-__global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
-    fast_iter_slices(FastIter<T> a, int first, int reset) {
-    DevState* st = a.st;
-    iter_reset(st, reset);
-    if (st->done) return;
-    const DevCsr& M = PRIMAL ? a.AT : a.A;
-    const RowSlices& S = M.slices;
-    const int idx = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-    if (idx >= S.n_item) return;
+__device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices& S, int idx,
+                                           int first, bool fresh, T tau, T sigma) {
     const int lane = threadIdx.x & 31;
     const int4 w = __ldg(S.item + idx);
     const int4 d = __ldg(S.slice + w.x);
@@ -229,18 +248,31 @@ __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     const T* __restrict__ val = slice_vals<T>(S) + d.y + lane;
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     T acc = T(0);
+    int c[8];
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int k = w.y + u;
+        c[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
+        v[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+    }
     for (int k0 = w.y; k0 < w.z; k0 += 8) {
-        int c[8];
-        T v[8];
+        int cn[8];
+        T vn[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const int k = k0 + u;
-            c[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
-            v[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+            const int k = k0 + 8 + u;
+            cn[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
+            vn[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u)
             if (k0 + u < kend) acc += v[u] * __ldg(xg + c[u]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            c[u] = cn[u];
+            v[u] = vn[u];
+        }
     }
     if (w.w >= 0) {
         S.part[32 * static_cast<int64_t>(idx) + lane] = static_cast<double>(acc);
@@ -267,10 +299,28 @@ __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     }
     if (row < 0) return;
     const PV<T> pv = pvec<T>(a.P);
-    const bool fresh = first && st->fresh;
-    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
     const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, row, first, fresh);
     epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma);
+}
+
+// The row-slice kernel: a persistent grid (the resident CTAs) whose warps
+// claim slice items one by one from S.fetch.
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
+    fast_iter_slices(FastIter<T> a, int first, int reset) {
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const RowSlices& S = M.slices;
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    for (;;) {
+        const int idx = warp_fetch(S.fetch);
+        if (idx >= S.n_item) break;
+        slice_item<T, PRIMAL>(a, S, idx, first, fresh, tau, sigma);
+    }
+    warp_exit(S.fetch);
 }
 
 __global__ void k_clear_flags(DevState* st) {
@@ -308,21 +358,35 @@ inline DevCsr pass_matrix(const DevCsr& M) {
 struct PassPlan {
     int shrt = 0, warp = 0, lng = 0, slc = 0;
 };
-inline PassPlan pass_plan(const DevCsr& M) {
+
+// Resident CTAs per device of the persistent kernels ([0] FP32, [1] FP64): the
+// CTA-item kernel without warp rows and the row-slice kernel. Their grids are
+// capped at these (set by init_fast_kernels from the occupancy calculator).
+int g_cap_long[2] = {148 * PDHG_LONG_MIN_CTAS, 148 * PDHG_LONG_MIN_CTAS};
+int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};
+
+inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
     PassPlan p;
     if (M.rows == 0) return p;
     p.shrt = short_blocks_for(M);
     const int mode = M.long_mode;
     const int nw = mode == 2 ? M.items_warp.n_item : mode == 1 ? M.n_warp1 : M.n_warp0;
     p.warp = (nw + kBlock / 32 - 1) / (kBlock / 32);
-    p.lng = mode == 2 ? p.warp : p.warp + (mode == 1 ? M.items_huge.n_item : M.items_long.n_item);
-    if (M.use_slices) p.slc = (M.slices.n_item + kBlock / 32 - 1) / (kBlock / 32);
+    if (mode == 2) {
+        p.lng = p.warp;
+    } else {
+        const int items = mode == 1 ? M.items_huge.n_item : M.items_long.n_item;
+        // without warp rows the CTA-item kernel is persistent: resident CTAs only
+        p.lng = p.warp > 0 ? p.warp + items : std::min(items, std::max(cap_long, 1));
+    }
+    if (M.use_slices && M.slices.n_item > 0)
+        p.slc = std::min((M.slices.n_item + kBlock / 32 - 1) / (kBlock / 32), std::max(cap_slice, 1));
     return p;
 }
 
 // Kernels one pass over M launches besides the flag reset.
 inline int pass_launches(const DevCsr& M0) {
-    const PassPlan p = pass_plan(pass_matrix(M0));
+    const PassPlan p = pass_plan(pass_matrix(M0), 1, 1);
     return (p.shrt > 0 ? 1 : 0) + (p.lng > 0 ? 1 : 0) + (p.slc > 0 ? 1 : 0);
 }
 
@@ -340,7 +404,8 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
     FastIter<T> a = a0;
     DevCsr& M = PRIMAL ? a.AT : a.A;
     M = pass_matrix(M0);
-    const PassPlan p = pass_plan(M);
+    const int pi = sizeof(T) == 4 ? 0 : 1;
+    const PassPlan p = pass_plan(M, g_cap_long[pi], g_cap_slice[pi]);
     const int mode = M.long_mode;
     // the flag reset rides on the first kernel of the period's first pass
     const int rs = PRIMAL && first ? 1 : 0;
@@ -778,6 +843,29 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
 }
 
 }  // namespace
+
+template <class K>
+int resident_per_sm(K kernel) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBlock, 0) != cudaSuccess) return 0;
+    return n;
+}
+
+int init_fast_kernels(int device) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+        return 1;
+    const int l32 = resident_per_sm(fast_iter_long<float, false, 0, false>);
+    const int l64 = resident_per_sm(fast_iter_long<double, false, 0, false>);
+    const int s32 = resident_per_sm(fast_iter_slices<float, false>);
+    const int s64 = resident_per_sm(fast_iter_slices<double, false>);
+    if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0) return 1;
+    g_cap_long[0] = l32 * sms;
+    g_cap_long[1] = l64 * sms;
+    g_cap_slice[0] = s32 * sms;
+    g_cap_slice[1] = s64 * sms;
+    return 0;
+}
 
 template <class T>
 int launch_fast_primal(const FastIter<T>& a, int first, cudaStream_t s, const PassFork* f) {
