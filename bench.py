@@ -45,7 +45,19 @@ sys.path.insert(0, ROOT)
 METRIC = "LPs solved/s at 1e-4 rel KKT: learned+batched vs plain GPU PDHG; SpMV HBM GB/s"
 UNIT = "GB/s"
 SUPPLIES, DEMANDS = 2000, 5000
-WORKLOAD = "transportation LP 2,000 x 5,000 (10M columns, 7,000 rows, 20M nnz), FP32-bulk/FP64-check PDHG"
+
+
+def workload_name(supplies: int, demands: int) -> str:
+    return (f"transportation LP {supplies:,} x {demands:,} ({supplies * demands:,} columns, "
+            f"{supplies + demands:,} rows, {2 * supplies * demands:,} nnz), FP32-bulk/FP64-check PDHG")
+
+
+WORKLOAD = workload_name(SUPPLIES, DEMANDS)
+
+
+def replica_problem(pkg, rank: int, supplies: int = SUPPLIES, demands: int = DEMANDS):
+    """The LP one replica solves: the same shape on every rank, its own seed."""
+    return pkg.lpgen.transportation_lp(supplies, demands, seed=1000 + rank)
 
 
 def spmv_bytes(m: int, n: int, nnz: int) -> float:
@@ -124,24 +136,23 @@ def dist_env():
     return rank, world, local
 
 
-def max_over_ranks(v: float, world: int) -> float:
-    if world == 1:
-        return v
+def _reduce(v: float, op: str) -> float:
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    """The largest v of all ranks (the job's time is its slowest rank's)."""
+    return v if world == 1 else _reduce(v, "max")
 
 
 def sum_over_ranks(v: float, world: int) -> float:
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """The sum of v over all ranks (whole-job units)."""
+    return v if world == 1 else _reduce(v, "sum")
 
 
 def barrier(world: int):
@@ -187,7 +198,7 @@ def run_reference(args) -> None:
                           "unavailable": "oracle/_ref/libsovref.so not built (needs the reference sources)"}))
         return
     pkg = importlib.import_module("sovereign-solver_b200")
-    prob = pkg.lpgen.transportation_lp(SUPPLIES, DEMANDS, seed=1000)
+    prob = replica_problem(pkg, 0, args.supplies, args.demands)
     per_step = args.ref_iters_per_step
     total = (args.warmup + args.steps) * per_step + 1
     t = np.zeros(total)
@@ -204,7 +215,8 @@ def run_reference(args) -> None:
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded transportation LP)",
-        "config": {"workload": WORKLOAD, "iterations_per_step": per_step,
+        "config": {"workload": workload_name(args.supplies, args.demands),
+                   "iterations_per_step": per_step,
                    "implementation": "reference sov::Pdhg::solve, Host backend (single-threaded)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
@@ -426,7 +438,7 @@ def main() -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     pkg = importlib.import_module("sovereign-solver_b200")
-    prob = pkg.lpgen.transportation_lp(SUPPLIES, DEMANDS, seed=1000 + rank)
+    prob = replica_problem(pkg, rank)
     m, n, nnz = prob.m, prob.n, prob.nnz
     b_spmv = spmv_bytes(m, n, nnz)
     eng = pkg.Engine(local)
