@@ -44,6 +44,10 @@ struct BatchCtx {
 
     MatDev Ao, ATo, As, ATs;
     DBuf<int32_t> row_off_d, col_off_d, row_inst, col_inst;
+    DBuf<int4> chk_item;
+    DBuf<double> chk_part;
+    DBuf<unsigned int> chk_ticket;
+    int32_t n_chk = 0;
     DBuf<double> c_o, lo_o, hi_o, rlo_o, rhi_o, c_s, lo_s, hi_s, rlo_s, rhi_s, rs_d, cs_d;
     DBuf<float> c32, lo32, hi32, rlo32, rhi32;
     DBuf<InstState> is;
@@ -83,6 +87,10 @@ struct BatchCtx {
         b.col_off = col_off_d.p;
         b.row_inst = row_inst.p;
         b.col_inst = col_inst.p;
+        b.chk_item = chk_item.p;
+        b.n_chk = n_chk;
+        b.chk_part = chk_part.p;
+        b.chk_ticket = chk_ticket.p;
         b.A = As.view();
         b.AT = ATs.view();
         b.Ao = Ao.view();
@@ -320,6 +328,26 @@ int batch_load(BatchCtx& c, int32_t count, const int32_t* row_off, const int32_t
     BCK(c.col_inst.alloc(static_cast<size_t>(n) + 1));
     launch_batch_fill_inst(c.row_off_d.p, count, c.row_inst.p, s);
     launch_batch_fill_inst(c.col_off_d.p, count, c.col_inst.p, s);
+    {
+        // the check's CTA items: about kCheckWork units (entries of both
+        // matrices plus rows and columns) per part, at most kCheckParts parts
+        constexpr int64_t kCheckWork = 16384;
+        constexpr int64_t kCheckParts = 64;
+        std::vector<int4> items;
+        for (int32_t k = 0; k < count; ++k) {
+            const int64_t nnz_k = static_cast<int64_t>(rp[row_off[k + 1]]) - rp[row_off[k]];
+            const int64_t work = 2 * nnz_k + (row_off[k + 1] - row_off[k]) + (col_off[k + 1] - col_off[k]);
+            const int parts = static_cast<int>(
+                std::min<int64_t>(kCheckParts, std::max<int64_t>(1, (work + kCheckWork - 1) / kCheckWork)));
+            for (int j = 0; j < parts; ++j) items.push_back(make_int4(k, j, parts, 0));
+        }
+        c.n_chk = static_cast<int32_t>(items.size());
+        BCK(upload(c.chk_item, items, s));
+        BCK(c.chk_part.alloc(12 * items.size()));
+        BCK(c.chk_ticket.alloc(static_cast<size_t>(count)));
+        BCK(cudaMemsetAsync(c.chk_ticket.p, 0, sizeof(unsigned int) * count, s));
+        BCK(cudaStreamSynchronize(s));  // the host vector is read by the copy above
+    }
     BCK(upload(c.c_o, cv, static_cast<size_t>(n), s));
     BCK(upload(c.lo_o, col_lo, static_cast<size_t>(n), s));
     BCK(upload(c.hi_o, col_hi, static_cast<size_t>(n), s));

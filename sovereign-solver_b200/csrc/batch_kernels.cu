@@ -135,14 +135,17 @@ __device__ __forceinline__ void inst_col_terms(const BatchView& b, const Iterate
 // current point and the average in one pass.
 template <class T, bool COLS>
 __device__ __forceinline__ void inst_pass(const BatchView& b, const Iterates<T>& it,
-                                          const BatchParams& p, int k, double inv, double sign,
-                                          Terms& t) {
+                                          const BatchParams& p, int k, int part, int parts,
+                                          double inv, double sign, Terms& t) {
     const DevCsr& M = COLS ? b.AT : b.A;
     const int vw = M.vw;
     const int lane = threadIdx.x & (vw - 1);
     const int groups = kBlock / vw;
-    const int r0 = COLS ? b.col_off[k] : b.row_off[k];
-    const int r1 = COLS ? b.col_off[k + 1] : b.row_off[k + 1];
+    const int q0 = COLS ? b.col_off[k] : b.row_off[k];
+    const int q1 = COLS ? b.col_off[k + 1] : b.row_off[k + 1];
+    // part `part` of `parts` of the instance's rows (columns)
+    const int r0 = q0 + static_cast<int>(static_cast<int64_t>(q1 - q0) * part / parts);
+    const int r1 = q0 + static_cast<int>(static_cast<int64_t>(q1 - q0) * (part + 1) / parts);
     for (int r = r0 + static_cast<int>(threadIdx.x) / vw; r < r1; r += groups) {
         double ac = 0.0, aa = 0.0;
         for (int q = M.rp[r] + lane; q < M.rp[r + 1]; q += vw) {
@@ -172,27 +175,51 @@ __device__ void finish_instance(const BatchView& b, InstState& s) {
 
 template <class T>
 __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> it, BatchParams p) {
-    const int k = blockIdx.x;
+    const int4 item = b.chk_item[blockIdx.x];
+    const int k = item.x, part = item.y, parts = item.z;
     InstState& s = b.is[k];
-    // uniform per CTA: only this CTA writes s.done, after its reductions. (The
-    // global done flag is written by other CTAs of this launch, so it must not
-    // decide an early exit here; when it is set every instance is done anyway.)
+    // uniform per CTA. Only the instance's last CTA writes s.done, and only
+    // after every CTA of the instance has taken its ticket -- each read this
+    // flag before that -- so all parts of an instance agree. (The global done
+    // flag is written by other CTAs of this launch, so it must not decide an
+    // early exit here; when it is set every instance is done anyway.)
     if (s.done) return;
     const long long k_avg = s.since_restart + p.period;
     const double inv = 1.0 / static_cast<double>(k_avg);
     Terms t;
-    inst_pass<T, false>(b, it, p, k, inv, s.obj_sign, t);
-    inst_pass<T, true>(b, it, p, k, inv, s.obj_sign, t);
-    const double cp = bmax(t.cp), cd = bmax(t.cd), ap = bmax(t.ap), ad = bmax(t.ad);
-    const double ocp = bmax(t.ocp), ocd = bmax(t.ocd), oap = bmax(t.oap), oad = bmax(t.oad);
-    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    inst_pass<T, false>(b, it, p, k, part, parts, inv, s.obj_sign, t);
+    inst_pass<T, true>(b, it, p, k, part, parts, inv, s.obj_sign, t);
+    double v[12];
+    v[0] = bmax(t.cp); v[1] = bmax(t.cd); v[2] = bmax(t.ap); v[3] = bmax(t.ad);
+    v[4] = bmax(t.ocp); v[5] = bmax(t.ocd); v[6] = bmax(t.oap); v[7] = bmax(t.oad);
+    v[8] = v[9] = v[10] = v[11] = 0.0;
     if (p.termination_rule == 1) {
-        s0 = block_sum_det(t.pobj_c);
-        s1 = block_sum_det(t.dobj_c);
-        s2 = block_sum_det(t.pobj_a);
-        s3 = block_sum_det(t.dobj_a);
+        v[8] = block_sum_det(t.pobj_c);
+        v[9] = block_sum_det(t.dobj_c);
+        v[10] = block_sum_det(t.pobj_a);
+        v[11] = block_sum_det(t.dobj_a);
     }
     if (threadIdx.x != 0) return;
+    if (parts > 1) {
+        // store this part, take the instance's ticket; the last part merges
+        // (maxima order-free, sums in part order) and goes on to the decision
+        double* mine = b.chk_part + 12 * static_cast<int64_t>(blockIdx.x);
+        for (int q = 0; q < 12; ++q) mine[q] = v[q];
+        __threadfence();
+        if (atomicAdd(b.chk_ticket + k, 1u) != static_cast<unsigned>(parts - 1)) return;
+        __threadfence();
+        const double* first = b.chk_part + 12 * (static_cast<int64_t>(blockIdx.x) - part);
+        for (int q = 0; q < 12; ++q) v[q] = q < 8 ? 0.0 : __ldcg(first + q);
+        for (int j = 0; j < parts; ++j) {
+            for (int q = 0; q < 8; ++q) v[q] = smax(v[q], __ldcg(first + 12 * j + q));
+            if (j > 0)
+                for (int q = 8; q < 12; ++q) v[q] += __ldcg(first + 12 * j + q);
+        }
+        b.chk_ticket[k] = 0u;
+    }
+    const double cp = v[0], cd = v[1], ap = v[2], ad = v[3];
+    const double ocp = v[4], ocd = v[5], oap = v[6], oad = v[7];
+    const double s0 = v[8], s1 = v[9], s2 = v[10], s3 = v[11];
     // ---- the instance's decision (as the single engine's check) ----
     const double cur = smax(cp, cd), avg = smax(ap, ad);
     s.cur_res = cur;
@@ -749,7 +776,7 @@ void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, i
 template <class T>
 void launch_batch_check(const BatchView& b, const Iterates<T>& it, const BatchParams& p,
                         cudaStream_t s) {
-    if (b.count > 0) batch_check<T><<<b.count, kBlock, 0, s>>>(b, it, p);
+    if (b.n_chk > 0) batch_check<T><<<b.n_chk, kBlock, 0, s>>>(b, it, p);
 }
 
 template <class T>

@@ -56,6 +56,15 @@ struct BatchView {
     InstState* is = nullptr;
     BatchGlobal* g = nullptr;
     Mailbox* mail = nullptr;
+    // The check's CTA items: instance k's rows and columns in C parts, part j
+    // of C = {k, j, C, -} (C by the instance's size, so that no single CTA
+    // sums a large instance while the rest of the GPU waits). A CTA stores its
+    // partial maxima and sums (12 per item) and takes the instance's ticket;
+    // the last CTA of the instance merges them in item order and decides.
+    const int4* chk_item = nullptr;
+    int32_t n_chk = 0;
+    double* chk_part = nullptr;
+    unsigned int* chk_ticket = nullptr;  // per instance, 0 between launches
 };
 
 struct BatchParams {

@@ -156,3 +156,22 @@ def test_many_uneven_instances(pkg, orc, engine):
         o = orc.oracle_solve(ps[k], termination_rule=1, restart_rule=1, tolerance=1e-7,
                              max_iterations=200_000)
         assert abs(rs[k].objective - o.objective) <= 2e-3 * max(1.0, abs(o.objective))
+
+
+def test_large_instances_checked_in_parts_match_the_single_engine(pkg, engine):
+    # instances of 1,500 x 4,000 and 3,000 x 7,500 (20k and 45k nonzeros): the
+    # check sums each in several CTA parts merged by the instance's last part
+    ps = [pkg.lpgen.random_equality_lp(1500, 4000, 5, seed=21),
+          pkg.lpgen.random_equality_lp(40, 100, 4, seed=23),
+          pkg.lpgen.random_equality_lp(3000, 7500, 6, seed=22)]
+    opt = pkg.PdhgOptions(precision="fp64", max_iterations=60_000, **ADAPTIVE)
+    single = []
+    for p in ps:
+        engine.load(p)
+        single.append(engine.solve(opt))
+    engine.load_batch(ps)
+    for k, (r, s) in enumerate(zip(engine.solve_batch(opt), single)):
+        assert r.status == s.status, (k, r.status, s.status)
+        assert abs(r.iterations - s.iterations) <= 80, (k, r.iterations, s.iterations)
+        assert abs(r.objective - s.objective) <= 1e-6 * max(1.0, abs(s.objective)), \
+            (k, r.objective, s.objective)
