@@ -37,7 +37,10 @@ __device__ double bmax(double v) {
 // Iterations: the single engine's fused kernels with a per-row instance lookup
 // ---------------------------------------------------------------------------
 
-template <class T, int VW, bool PRIMAL>
+// LONG = false: the matrix has no row above kLongRow; the CTA-per-row path is
+// compiled out, which keeps the registers (and the occupancy) of the
+// lane-group path.
+template <class T, int VW, bool PRIMAL, bool LONG>
 __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it, int first,
                                                      int short_blk) {
     if (b.g->done) return;
@@ -46,7 +49,7 @@ __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? it.y : it.xbar;
     const PV<T> pv = pvec<T>(b.P);
-    if (static_cast<int>(blockIdx.x) < short_blk) {
+    if (!LONG || static_cast<int>(blockIdx.x) < short_blk) {
         const int lane = threadIdx.x & (VW - 1);
         const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
         if (r >= M.rows) return;
@@ -58,8 +61,22 @@ __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it
         if (lane == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
         const int rb = __ldcs(M.rp + r), re = __ldcs(M.rp + r + 1);
         if (re - rb > kLongRow) return;
+        // rounds of four entries per lane: the index and value loads of a
+        // round are all in flight before its gathers
         T acc = T(0);
-        for (int k = rb + lane; k < re; k += VW) acc += __ldcs(vals + k) * __ldg(xg + __ldcs(M.ci + k));
+        for (int k0 = rb + lane; k0 < re; k0 += 4 * VW) {
+            int c[4];
+            T v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * VW;
+                c[u] = k < re ? __ldcs(M.ci + k) : 0;
+                v[u] = k < re ? __ldcs(vals + k) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u * VW < re) acc += v[u] * __ldg(xg + c[u]);
+        }
         if (VW > 1) acc = group_sum(acc, VW);
         if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
     } else {
@@ -76,8 +93,9 @@ __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it
 }
 
 // ---------------------------------------------------------------------------
-// Check: one CTA per instance (kkt_residual, original_space_residual,
-// candidate, termination, restart rule: pdhg.cpp:333-408)
+// Check: each instance in one or more CTA parts, the last part of an instance
+// merging and deciding (kkt_residual, original_space_residual, candidate,
+// termination, restart rule: pdhg.cpp:333-408)
 // ---------------------------------------------------------------------------
 
 template <class T>
@@ -757,10 +775,15 @@ void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, i
     if (M.rows == 0) return;
     const int sb = short_blocks(M);
     const int grid = sb + M.n_long;
-#define PDHG_BATCH_ITER(VW)                                                              \
-    do {                                                                                 \
-        if (primal) batch_iter<T, VW, true><<<grid, kBlock, 0, s>>>(b, it, first, sb);   \
-        else batch_iter<T, VW, false><<<grid, kBlock, 0, s>>>(b, it, first, sb);         \
+#define PDHG_BATCH_ITER(VW)                                                                      \
+    do {                                                                                         \
+        if (M.n_long > 0) {                                                                      \
+            if (primal) batch_iter<T, VW, true, true><<<grid, kBlock, 0, s>>>(b, it, first, sb); \
+            else batch_iter<T, VW, false, true><<<grid, kBlock, 0, s>>>(b, it, first, sb);      \
+        } else {                                                                                 \
+            if (primal) batch_iter<T, VW, true, false><<<grid, kBlock, 0, s>>>(b, it, first, sb);\
+            else batch_iter<T, VW, false, false><<<grid, kBlock, 0, s>>>(b, it, first, sb);     \
+        }                                                                                        \
     } while (0)
     switch (M.vw) {
         case 1: PDHG_BATCH_ITER(1); break;
