@@ -48,6 +48,8 @@ struct BatchCtx {
     DBuf<double> chk_part;
     DBuf<unsigned int> chk_ticket;
     int32_t n_chk = 0;
+    DBuf<int32_t> blk_list_a, blk_list_t;
+    DBuf<unsigned char> blk_flag_a, blk_flag_t;
     DBuf<double> c_o, lo_o, hi_o, rlo_o, rhi_o, c_s, lo_s, hi_s, rlo_s, rhi_s, rs_d, cs_d;
     DBuf<float> c32, lo32, hi32, rlo32, rhi32;
     DBuf<InstState> is;
@@ -91,6 +93,10 @@ struct BatchCtx {
         b.n_chk = n_chk;
         b.chk_part = chk_part.p;
         b.chk_ticket = chk_ticket.p;
+        b.blk_list[0] = blk_list_a.p;
+        b.blk_list[1] = blk_list_t.p;
+        b.blk_flag[0] = blk_flag_a.p;
+        b.blk_flag[1] = blk_flag_t.p;
         b.A = As.view();
         b.AT = ATs.view();
         b.Ao = Ao.view();
@@ -257,6 +263,15 @@ int batch_intake(BatchCtx& c, const pdhg_options& o) {
     if (rc != PDHG_OK) return rc;
     rc = bin_matrix(c.ATs, s, &c.err);
     if (rc != PDHG_OK) return rc;
+    {
+        // active block lists of the iteration kernels (one entry per lane-group block)
+        const size_t nba = static_cast<size_t>((static_cast<int64_t>(c.As.rows) * c.As.vw + kBlock - 1) / kBlock) + 1;
+        const size_t nbt = static_cast<size_t>((static_cast<int64_t>(c.ATs.rows) * c.ATs.vw + kBlock - 1) / kBlock) + 1;
+        BCK(c.blk_list_a.alloc(nba));
+        BCK(c.blk_flag_a.alloc(nba));
+        BCK(c.blk_list_t.alloc(nbt));
+        BCK(c.blk_flag_t.alloc(nbt));
+    }
     BCK(c.c_s.alloc(static_cast<size_t>(c.n) + 1));
     BCK(c.lo_s.alloc(static_cast<size_t>(c.n) + 1));
     BCK(c.hi_s.alloc(static_cast<size_t>(c.n) + 1));
@@ -432,6 +447,7 @@ void batch_period(BatchCtx& c, const BatchParams& p, long long iters, bool with_
     if (with_check) {
         launch_batch_check<T>(b, it, p, s);
         launch_batch_restart<T>(b, it, p, s);
+        launch_batch_compact(b, s);
         launch_batch_tick(b, iters, budget, h, use_h, s);
     }
 }
@@ -489,6 +505,7 @@ int batch_run(BatchCtx& c, const pdhg_options& o, std::chrono::steady_clock::tim
     p.y_last = c.y_last.p;
     p.act_avg = c.act_avg.p;
     p.allow_switch = allow_switch ? 1 : 0;
+    launch_batch_compact(c.view(), s);  // the block lists of the instances now active
     const long long span = last > iter0 ? last - iter0 : 0;
     const long long n_periods = span / p.period;
     const long long tail = span % p.period;
@@ -626,6 +643,7 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
     BCK(cudaMemcpy(c.is.p, h.data(), sizeof(InstState) * c.count, cudaMemcpyHostToDevice));
     BatchGlobal gh{};
     gh.active = active;
+    gh.dirty = 1;  // the block lists are rebuilt before the first iteration
     gh.done = active == 0 ? 1 : 0;
     BCK(cudaMemcpy(c.g.p, &gh, sizeof gh, cudaMemcpyHostToDevice));
     std::memset(const_cast<Mailbox*>(c.mail), 0, sizeof(Mailbox));
@@ -718,6 +736,7 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
             if (stalled > 0 && last > gh.iter) {
                 any_polished = true;
                 gh.active = stalled;
+                gh.dirty = 1;
                 gh.done = 0;
                 BCK(cudaMemcpy(c.is.p, h.data(), sizeof(InstState) * c.count, cudaMemcpyHostToDevice));
                 BCK(cudaMemcpy(c.g.p, &gh, sizeof gh, cudaMemcpyHostToDevice));

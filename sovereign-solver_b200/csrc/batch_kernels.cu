@@ -1,4 +1,5 @@
 // batch_kernels.cu -- kernels of the batched engine; see batch_kernels.cuh.
+#include <algorithm>
 #include <cmath>
 
 #include "batch_kernels.cuh"
@@ -37,57 +38,72 @@ __device__ double bmax(double v) {
 // Iterations: the single engine's fused kernels with a per-row instance lookup
 // ---------------------------------------------------------------------------
 
-// LONG = false: the matrix has no row above kLongRow; the CTA-per-row path is
-// compiled out, which keeps the registers (and the occupancy) of the
-// lane-group path.
-template <class T, int VW, bool PRIMAL, bool LONG>
-__global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it, int first,
-                                                     int short_blk) {
-    if (b.g->done) return;
+// One lane-group block of rows (kBlock / VW rows, groups of VW lanes): the
+// rows of instances still iterating, rows above kLongRow left to the CTA path.
+template <class T, int VW, bool PRIMAL>
+__device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T>& it, int first,
+                                            int blk) {
     const DevCsr& M = PRIMAL ? b.AT : b.A;
     const int32_t* inst_of = PRIMAL ? b.col_inst : b.row_inst;
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? it.y : it.xbar;
     const PV<T> pv = pvec<T>(b.P);
-    if (!LONG || static_cast<int>(blockIdx.x) < short_blk) {
-        const int lane = threadIdx.x & (VW - 1);
-        const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
-        if (r >= M.rows) return;
-        const InstState& s = b.is[inst_of[r]];
-        if (s.done) return;  // uniform within the row's lane group
-        const bool fresh = first && s.fresh;
-        const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
-        EpiIn<T> in{};
-        if (lane == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
-        const int rb = __ldcs(M.rp + r), re = __ldcs(M.rp + r + 1);
-        if (re - rb > kLongRow) return;
-        // rounds of four entries per lane: the index and value loads of a
-        // round are all in flight before its gathers
-        T acc = T(0);
-        for (int k0 = rb + lane; k0 < re; k0 += 4 * VW) {
-            int c[4];
-            T v[4];
+    const int lane = threadIdx.x & (VW - 1);
+    const int r = (blk * kBlock + threadIdx.x) / VW;
+    if (r >= M.rows) return;
+    const InstState& s = b.is[inst_of[r]];
+    if (s.done) return;  // uniform within the row's lane group
+    const bool fresh = first && s.fresh;
+    const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
+    EpiIn<T> in{};
+    if (lane == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
+    const int rb = __ldcs(M.rp + r), re = __ldcs(M.rp + r + 1);
+    if (re - rb > kLongRow) return;
+    // rounds of four entries per lane: the index and value loads of a round
+    // are all in flight before its gathers
+    T acc = T(0);
+    for (int k0 = rb + lane; k0 < re; k0 += 4 * VW) {
+        int c[4];
+        T v[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int k = k0 + u * VW;
-                c[u] = k < re ? __ldcs(M.ci + k) : 0;
-                v[u] = k < re ? __ldcs(vals + k) : T(0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (k0 + u * VW < re) acc += v[u] * __ldg(xg + c[u]);
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * VW;
+            c[u] = k < re ? __ldcs(M.ci + k) : 0;
+            v[u] = k < re ? __ldcs(vals + k) : T(0);
         }
-        if (VW > 1) acc = group_sum(acc, VW);
-        if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * VW < re) acc += v[u] * __ldg(xg + c[u]);
+    }
+    if (VW > 1) acc = group_sum(acc, VW);
+    if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
+}
+
+// The first short_grid CTAs take one block each of the active block list (the
+// grid covers every block; CTAs past the list's length exit at once); with
+// LONG, one CTA per row above kLongRow follows. LONG = false (no such row)
+// compiles the CTA-per-row path out, which keeps the registers of the
+// lane-group path.
+template <class T, int VW, bool PRIMAL, bool LONG>
+__global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it, int first,
+                                                     int short_grid) {
+    if (b.g->done) return;
+    if (!LONG || static_cast<int>(blockIdx.x) < short_grid) {
+        const int pi = PRIMAL ? 1 : 0;
+        if (static_cast<int>(blockIdx.x) >= b.g->nblk[pi]) return;
+        batch_block<T, VW, PRIMAL>(b, it, first, b.blk_list[pi][blockIdx.x]);
     } else {
-        const int r = M.long_rows[blockIdx.x - short_blk];
+        const DevCsr& M = PRIMAL ? b.AT : b.A;
+        const int32_t* inst_of = PRIMAL ? b.col_inst : b.row_inst;
+        const int r = M.long_rows[blockIdx.x - short_grid];
         const InstState& s = b.is[inst_of[r]];
         if (s.done) return;  // uniform within the CTA
+        const PV<T> pv = pvec<T>(b.P);
         const bool fresh = first && s.fresh;
         const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
         EpiIn<T> in{};
         if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
-        const T acc = long_row_dot<T>(M.ci, vals, xg, M.rp[r], M.rp[r + 1]);
+        const T acc = long_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? it.y : it.xbar, M.rp[r], M.rp[r + 1]);
         if (threadIdx.x == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
     }
 }
@@ -189,6 +205,7 @@ __device__ __forceinline__ void inst_pass(const BatchView& b, const Iterates<T>&
 __device__ void finish_instance(const BatchView& b, InstState& s) {
     const int left = atomicSub(&b.g->active, 1);
     if (left == 1) b.g->done = 1;
+    b.g->dirty = 1;
 }
 
 template <class T>
@@ -412,6 +429,77 @@ __global__ void batch_tick(BatchView b, long long period, long long budget_iters
         __threadfence_system();
     }
     if (use_handle) cudaGraphSetConditional(handle, cont ? 1u : 0u);
+}
+
+constexpr int kCompactThreads = 1024;
+
+// Exclusive scan of one int per thread over the CTA (kCompactThreads); every
+// thread gets its offset and the total.
+__device__ int cta_scan(int v, int* total) {
+    __shared__ int warp_tot[kCompactThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kCompactThreads / 32 ? warp_tot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kCompactThreads / 32) warp_tot[lane] = w;  // inclusive warp totals
+    }
+    __syncthreads();
+    const int before = warp > 0 ? warp_tot[warp - 1] : 0;
+    *total = warp_tot[kCompactThreads / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+// One CTA: when g->dirty, for A's rows and A^T's rows, flag the lane-group
+// blocks holding a row of an instance not done (an instance's rows [r0, r1)
+// span blocks r0 vw / kBlock .. (r1 vw - 1) / kBlock; a block shared by two
+// instances is flagged once), then write the flagged blocks in order into the
+// list and their number into g->nblk. Clears g->dirty.
+__global__ void __launch_bounds__(kCompactThreads) batch_compact(BatchView b, int nb_a, int nb_t) {
+    __shared__ int dirty;
+    if (threadIdx.x == 0) dirty = b.g->dirty;
+    __syncthreads();
+    if (!dirty) return;
+    for (int mat = 0; mat < 2; ++mat) {
+        const int nb = mat == 0 ? nb_a : nb_t;
+        const int vw = mat == 0 ? b.A.vw : b.AT.vw;
+        const int32_t* off = mat == 0 ? b.row_off : b.col_off;
+        unsigned char* flag = b.blk_flag[mat];
+        int32_t* list = b.blk_list[mat];
+        for (int i = threadIdx.x; i < nb; i += kCompactThreads) flag[i] = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < b.count; k += kCompactThreads) {
+            if (b.is[k].done) continue;
+            const int r0 = off[k], r1 = off[k + 1];
+            if (r1 <= r0) continue;
+            const int b0 = static_cast<int>(static_cast<int64_t>(r0) * vw / kBlock);
+            const int b1 = static_cast<int>((static_cast<int64_t>(r1) * vw - 1) / kBlock);
+            for (int q = b0; q <= b1 && q < nb; ++q) flag[q] = 1;
+        }
+        __syncthreads();
+        int base = 0;
+        for (int start = 0; start < nb; start += kCompactThreads) {
+            const int i = start + static_cast<int>(threadIdx.x);
+            const int f = i < nb ? flag[i] : 0;
+            int total = 0;
+            const int pos = cta_scan(f, &total);
+            if (f) list[base + pos] = i;
+            base += total;
+        }
+        if (threadIdx.x == 0) b.g->nblk[mat] = base;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) b.g->dirty = 0;
 }
 
 __global__ void batch_fill_inst(const int32_t* off, int32_t* out) {
@@ -794,6 +882,10 @@ void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, i
         default: PDHG_BATCH_ITER(32); break;
     }
 #undef PDHG_BATCH_ITER
+}
+
+void launch_batch_compact(const BatchView& b, cudaStream_t s) {
+    batch_compact<<<1, kCompactThreads, 0, s>>>(b, short_blocks(b.A), short_blocks(b.AT));
 }
 
 template <class T>

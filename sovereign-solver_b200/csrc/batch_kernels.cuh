@@ -44,6 +44,8 @@ struct BatchGlobal {
     int active;        // instances still iterating
     long long iter;    // iterations completed before the current period
     long long checks;
+    int dirty;         // an instance finished (or restarted): rebuild the block lists
+    int nblk[2];       // active lane-group blocks of A's rows [0] and A^T's rows [1]
 };
 
 struct BatchView {
@@ -65,6 +67,13 @@ struct BatchView {
     int32_t n_chk = 0;
     double* chk_part = nullptr;
     unsigned int* chk_ticket = nullptr;  // per instance, 0 between launches
+    // Active block lists of the iteration kernels' lane-group path ([0] rows
+    // of A, [1] rows of A^T): the blocks (kBlock / vw rows each) holding a row
+    // of an instance still iterating, rebuilt by batch_compact whenever an
+    // instance finishes, so that finished instances stop costing CTAs. flag is
+    // the rebuild's scratch (one byte per block).
+    int32_t* blk_list[2] = {nullptr, nullptr};
+    unsigned char* blk_flag[2] = {nullptr, nullptr};
 };
 
 struct BatchParams {
@@ -89,6 +98,8 @@ void launch_batch_restart(const BatchView& b, const Iterates<T>& it, const Batch
                           cudaStream_t s);
 void launch_batch_tick(const BatchView& b, long long period, long long budget_iters,
                        cudaGraphConditionalHandle handle, int use_handle, cudaStream_t s);
+// Rebuilds the active block lists when g->dirty is set (one CTA; a no-op otherwise).
+void launch_batch_compact(const BatchView& b, cudaStream_t s);
 void launch_batch_fill_inst(const int32_t* off, int32_t count, int32_t* out, cudaStream_t s);
 void launch_batch_warm(const BatchView& b, double* x0, double* y0, cudaStream_t s);
 
