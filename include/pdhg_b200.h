@@ -64,6 +64,11 @@ typedef enum {
     PDHG_PREC_FP64 = 2
 } pdhg_precision;
 
+/* Checkpoint (pdhg.hpp:121-134): at every check, on the solving thread, the
+ * candidate in original units and its original-space residual. x_original and
+ * y_original are valid only during the call (the engine reuses the buffers).
+ * While the callback runs the GPU already works on the next check period; a
+ * stop request (cancellation, time limit) is honoured at the check after it. */
 typedef void (*pdhg_checkpoint_fn)(void* user, long long iteration, const double* x_original,
                                    const double* y_original, double original_residual);
 

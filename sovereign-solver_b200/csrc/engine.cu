@@ -94,6 +94,13 @@ struct Ctx {
     GraphSig graph_sig;
     long long launches = 0;
 
+    // Checkpoint feed: two pinned slots, each the candidate (x: n, y: m, original
+    // units) and the solver state of one period, copied on the stream behind
+    // the period so that the callback reads them while the next period runs.
+    double* cb_pin = nullptr;
+    DevState* cb_state = nullptr;
+    size_t cb_cap = 0;  // doubles per slot
+
     BatchCtx* batch = nullptr;  // pdhg_load_batch / pdhg_solve_batch
 
     // Iteration-kernel shapes per fast precision ([0] MIXED, [1] FP64):
@@ -108,6 +115,8 @@ struct Ctx {
         if (batch != nullptr) batch_delete(batch);
         if (graph != nullptr) cudaGraphExecDestroy(graph);
         if (mail != nullptr) cudaFreeHost(mail);
+        if (cb_pin != nullptr) cudaFreeHost(cb_pin);
+        if (cb_state != nullptr) cudaFreeHost(cb_state);
         if (fork.fork != nullptr) cudaEventDestroy(fork.fork);
         for (int i = 0; i < 2; ++i) {
             if (fork.join[i] != nullptr) cudaEventDestroy(fork.join[i]);
@@ -562,33 +571,62 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
     const long long n_periods = budget / period;
     const long long tail = budget % period;
     const bool want_cb = o.checkpoint != nullptr;
-    const int lookahead = (want_cb || o.verbose) ? 1 : kLookahead;
+    // With a checkpoint callback two periods are in flight and each hands its
+    // candidate over through a pinned slot (the callback runs while the next
+    // period computes); verbose output reads the mailbox, one period at a time.
+    const int lookahead = o.verbose ? 1 : want_cb ? 2 : kLookahead;
+    const bool feed = want_cb && lookahead == 2;
+    if (feed) {
+        const size_t need = static_cast<size_t>(c.lp.n) + static_cast<size_t>(c.lp.m) + 1;
+        if (c.cb_cap < need) {
+            if (c.cb_pin != nullptr) cudaFreeHost(c.cb_pin);
+            c.cb_pin = nullptr;
+            c.cb_cap = 0;
+            CK(cudaHostAlloc(reinterpret_cast<void**>(&c.cb_pin), 2 * need * sizeof(double),
+                             cudaHostAllocDefault));
+            c.cb_cap = need;
+        }
+        if (c.cb_state == nullptr)
+            CK(cudaHostAlloc(reinterpret_cast<void**>(&c.cb_state), 2 * sizeof(DevState),
+                             cudaHostAllocDefault));
+    }
     long long seen_checks = c.mail->checks;
     bool stop_sent = false;
     int stop_code = 0;
     double best = kInf;
     long long since_improve = 0;
 
-    auto on_check = [&](void) -> int {
-        // called after a period's event completed (lookahead 1 when callbacks are on)
-        const long long checks = c.mail->checks;
+    // Called after a period's event completed. slot >= 0: the period's pinned
+    // snapshot (checkpoint feed); slot < 0: the mailbox and a synchronous copy.
+    auto on_check = [&](int slot) -> int {
+        const DevState* snap = slot >= 0 ? c.cb_state + slot : nullptr;
+        const long long checks = snap ? snap->checks : static_cast<long long>(c.mail->checks);
         if (checks == seen_checks) return PDHG_OK;
         seen_checks = checks;
-        const bool failed = c.mail->done && c.mail->status == PDHG_STATUS_NUMERICAL_FAILURE;
+        const bool done = snap ? snap->done != 0 : c.mail->done != 0;
+        const int status = snap ? snap->status : c.mail->status;
+        const bool failed = done && status == PDHG_STATUS_NUMERICAL_FAILURE;
+        const long long it = snap ? snap->iter : static_cast<long long>(c.mail->iter);
+        const double orig_res = snap ? snap->orig_res : static_cast<double>(c.mail->orig_res);
+        const double rel_kkt = snap ? snap->rel_kkt : static_cast<double>(c.mail->rel_kkt);
         if (o.verbose && c.mail->restarted && !failed)
-            std::fprintf(stderr, "  [pdhg] restart at iter %lld, residual %.3g\n",
-                         static_cast<long long>(c.mail->iter), static_cast<double>(c.mail->avg_res));
+            std::fprintf(stderr, "  [pdhg] restart at iter %lld, residual %.3g\n", it,
+                         static_cast<double>(c.mail->avg_res));
         if (want_cb && !failed) {
             const int32_t n = c.lp.n, m = c.lp.m;
-            std::vector<double> hx(static_cast<size_t>(n)), hy(static_cast<size_t>(m));
-            if (n) CK(cudaMemcpyAsync(hx.data(), c.cand_xo.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
-            if (m) CK(cudaMemcpyAsync(hy.data(), c.cand_yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
-            CK(cudaStreamSynchronize(c.stream));
-            o.checkpoint(o.checkpoint_user, static_cast<long long>(c.mail->iter) - 1, hx.data(),
-                         hy.data(), c.mail->orig_res);
+            if (snap) {
+                const double* hx = c.cb_pin + static_cast<size_t>(slot) * c.cb_cap;
+                o.checkpoint(o.checkpoint_user, it - 1, hx, hx + n, orig_res);
+            } else {
+                std::vector<double> hx(static_cast<size_t>(n)), hy(static_cast<size_t>(m));
+                if (n) CK(cudaMemcpyAsync(hx.data(), c.cand_xo.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+                if (m) CK(cudaMemcpyAsync(hy.data(), c.cand_yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+                CK(cudaStreamSynchronize(c.stream));
+                o.checkpoint(o.checkpoint_user, it - 1, hx.data(), hy.data(), orig_res);
+            }
         }
-        if (allow_switch && !c.mail->done) {
-            const double r = o.termination_rule == 1 ? c.mail->rel_kkt : c.mail->orig_res;
+        if (allow_switch && !done) {
+            const double r = o.termination_rule == 1 ? rel_kkt : orig_res;
             if (r < 0.98 * best) {
                 best = r;
                 since_improve = 0;
@@ -629,7 +667,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         L.check(period, c.stream);
         CK(cudaStreamSynchronize(c.stream));
         ++p;
-        int rc = on_check();
+        int rc = on_check(-1);
         if (rc != PDHG_OK) return rc;
     }
     if (p < n_periods && !c.mail->done) {
@@ -646,7 +684,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         sig.gen = c.gen;
         int rc = build_graph(c, L, period, sig);
         if (rc != PDHG_OK) return rc;
-        std::deque<cudaEvent_t> inflight;
+        std::deque<std::pair<cudaEvent_t, int>> inflight;  // event, pool slot
         std::vector<cudaEvent_t> pool;
         for (int i = 0; i < lookahead; ++i) {
             cudaEvent_t e;
@@ -661,17 +699,28 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
                 poll_stop();
                 CK(cudaGraphLaunch(c.graph, c.stream));
                 c.launches += per;
-                cudaEvent_t e = pool[next_ev];
+                const int slot = next_ev;
+                if (feed) {
+                    // this period's candidate and state into its pinned slot
+                    // (reused two launches later, after this slot's callback)
+                    const int32_t n = c.lp.n, m = c.lp.m;
+                    double* hx = c.cb_pin + static_cast<size_t>(slot) * c.cb_cap;
+                    if (n) CK(cudaMemcpyAsync(hx, c.cand_xo.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+                    if (m) CK(cudaMemcpyAsync(hx + n, c.cand_yo.p, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+                    CK(cudaMemcpyAsync(c.cb_state + slot, c.st.p, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream));
+                }
+                cudaEvent_t e = pool[slot];
                 next_ev = (next_ev + 1) % lookahead;
                 CK(cudaEventRecord(e, c.stream));
-                inflight.push_back(e);
+                inflight.push_back({e, slot});
                 ++p;
                 continue;
             }
             if (inflight.empty()) break;
-            CK(cudaEventSynchronize(inflight.front()));
+            const std::pair<cudaEvent_t, int> front = inflight.front();
+            CK(cudaEventSynchronize(front.first));
             inflight.pop_front();
-            int rc2 = on_check();
+            int rc2 = on_check(feed ? front.second : -1);
             if (rc2 != PDHG_OK) return rc2;
         }
         for (cudaEvent_t e : pool) cudaEventDestroy(e);

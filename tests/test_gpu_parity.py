@@ -316,3 +316,24 @@ def test_warm_start_from_the_solution_converges_immediately(pkg, engine):
                  max_iterations=200_000, x0=cold.primal, y0=cold.dual)
     assert warm.status == "optimal"
     assert warm.iterations < cold.iterations
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_feed_matches_the_synchronous_copies(pkg, engine, precision):
+    # with a callback the engine keeps two periods in flight and hands each
+    # candidate over through a pinned slot; verbose output keeps one period in
+    # flight and copies synchronously: both must deliver the same calls
+    p = pkg.lpgen.random_equality_lp(300, 800, 5, seed=31)
+    runs = []
+    for verbose in (False, True):
+        seen = []
+        r = solve(pkg, engine, p, precision=precision, max_iterations=2000, tolerance=1e-7,
+                  termination_rule="relative_kkt", restart_rule="adaptive", verbose=verbose,
+                  checkpoint=lambda it, x, y, res: seen.append((it, x, y, res)))
+        runs.append((r, seen))
+    (r1, s1), (r2, s2) = runs
+    assert [s[0] for s in s1] == [s[0] for s in s2] and len(s1) > 5
+    assert [s[0] for s in s1] == list(range(39, 40 * len(s1), 40))
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[3] == b[3]
+    assert (r1.status, r1.iterations, r1.objective) == (r2.status, r2.iterations, r2.objective)
