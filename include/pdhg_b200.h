@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define PDHG_B200_ABI_VERSION 2
+#define PDHG_B200_ABI_VERSION 3
 
 /* Return codes: the order and meaning of sov::Status (status.hpp:25-34). */
 typedef enum {
@@ -48,7 +48,13 @@ typedef enum {
     PDHG_STATUS_TIME_LIMIT = 2,
     PDHG_STATUS_NUMERICAL_FAILURE = 3,
     PDHG_STATUS_NOT_SOLVED = 4,
-    PDHG_STATUS_CANCELLED = 5
+    PDHG_STATUS_CANCELLED = 5,
+    /* engine extension (option infeasibility_detection): a certificate proves
+     * that no x meets the row and column bounds; pdhg_solve writes its row
+     * multipliers to y (the reference's FarkasCertificate, duals.hpp:47-70,
+     * which the reference's PDHG never produces: its verdict there stays
+     * iteration_limit) */
+    PDHG_STATUS_PRIMAL_INFEASIBLE = 6
 } pdhg_status;
 
 /* Arithmetic of the iteration kernels. */
@@ -115,6 +121,13 @@ typedef struct pdhg_options {
     int autotune;            /* 1 (default): MIXED / FP64 time the iteration kernels' shapes
                                 on the first solve of a loaded LP with >= 2^20 nonzeros and
                                 keep the fastest (see pdhg_get_tuning); 0 = fixed defaults */
+    int infeasibility_detection; /* 0 (default) = reference behaviour. 1 (MIXED / FP64): at
+                                every check the change of y since the previous check (original
+                                units) is tested as a FarkasCertificate (duals.cpp:36-79): when
+                                the ranges the row bounds and the column bounds force on
+                                sum_i y_i (Ax)_i are disjoint by more than 1e-6 relative, the
+                                solve stops with PDHG_STATUS_PRIMAL_INFEASIBLE and y receives
+                                the multipliers, scaled to max |y_i| = 1 */
 } pdhg_options;
 
 /* sov::PdhgResult (pdhg.hpp:136-153) minus the vectors, which pdhg_solve

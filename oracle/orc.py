@@ -129,6 +129,7 @@ def ref_lib() -> C.CDLL:
                                     C.POINTER(C.c_int), _dp]
     lib.ref_model_arrays.argtypes = [C.c_void_p, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp]
     lib.ref_model_free.argtypes = [C.c_void_p]
+    lib.ref_certifies.argtypes = [C.POINTER(OrcProblem), _dp, C.c_double, _dp]
     return lib
 
 
@@ -305,3 +306,30 @@ def reference_read_model(text: str, is_mps: bool = False) -> dict:
     return {"m": mm, "n": nn, "row_ptr": rp, "col_idx": ci[:k], "val": va[:k], "c": c[:nn],
             "col_lo": cl[:nn], "col_hi": ch[:nn], "row_lo": rl[:mm], "row_hi": rh[:mm],
             "obj_const": oc.value, "maximize": bool(mx.value)}
+
+
+def _certifies(which: str, p, y, slack: float = 1e-6):
+    keep: list = []
+    prob = _problem(p, keep)
+    yv = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
+    ranges = np.zeros(4)
+    if which == "oracle":
+        lib = orc_lib()
+        lib.orc_certifies.argtypes = [C.POINTER(OrcProblem), _dp, C.c_double, _dp]
+        ok = lib.orc_certifies(C.byref(prob), _d(yv), slack, _d(ranges))
+    else:
+        ok = ref_lib().ref_certifies(C.byref(prob), _d(yv), slack, _d(ranges))
+        if ok < 0:
+            raise RuntimeError("ref_certifies raised")
+    return bool(ok), ranges
+
+
+def oracle_certifies(p, y, slack: float = 1e-6):
+    """FarkasCertificate{y}.certifies_infeasibility(p, slack) restated
+    (src/l1/duals.cpp:16-79): (certified, [row lo, row hi, col lo, col hi])."""
+    return _certifies("oracle", p, y, slack)
+
+
+def reference_certifies(p, y, slack: float = 1e-6):
+    """The reference's own FarkasCertificate checker (compiled duals.cpp)."""
+    return _certifies("reference", p, y, slack)

@@ -795,3 +795,59 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
     free_scaled(&s);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------
+ * FarkasCertificate (src/l1/duals.cpp:16-79)
+ * ------------------------------------------------------------------------- */
+
+/* term_range (duals.cpp:16-20): mult * [lo, hi], reversed for a negative
+ * multiplier, exactly {0} for a zero one. */
+static void term_range(double mult, double lo, double hi, double* tlo, double* thi) {
+    if (mult == 0.0) {
+        *tlo = 0.0;
+        *thi = 0.0;
+    } else if (mult > 0.0) {
+        *tlo = mult * lo;
+        *thi = mult * hi;
+    } else {
+        *tlo = mult * hi;
+        *thi = mult * lo;
+    }
+}
+
+int orc_certifies(const orc_problem* p, const double* y, double slack, double* ranges) {
+    /* row_side_range (duals.cpp:36-43): rows in order */
+    double rlo = 0.0, rhi = 0.0;
+    for (int32_t i = 0; i < p->m; ++i) {
+        double tlo, thi;
+        term_range(y[i], p->row_lo[i], p->row_hi[i], &tlo, &thi);
+        rlo = rlo + tlo;
+        rhi = rhi + thi;
+    }
+    /* column_side_range (duals.cpp:45-69): d = A^T y by a row-major scatter
+     * (zero multipliers skipped), then columns in order */
+    double* d = (double*)calloc((size_t)p->n + 1, sizeof(double));
+    for (int32_t r = 0; r < p->m; ++r) {
+        const double yr = y[r];
+        if (yr == 0.0) continue;
+        for (int32_t k = p->row_ptr[r]; k < p->row_ptr[r + 1]; ++k) d[p->col_idx[k]] += yr * p->val[k];
+    }
+    double clo = 0.0, chi = 0.0;
+    for (int32_t j = 0; j < p->n; ++j) {
+        double tlo, thi;
+        term_range(d[j], p->col_lo[j], p->col_hi[j], &tlo, &thi);
+        clo = clo + tlo;
+        chi = chi + thi;
+    }
+    free(d);
+    if (ranges != NULL) {
+        ranges[0] = rlo;
+        ranges[1] = rhi;
+        ranges[2] = clo;
+        ranges[3] = chi;
+    }
+    /* certifies_infeasibility (duals.cpp:71-79): NaN never certifies;
+     * Range::disjoint_from (duals.hpp) */
+    if (isnan(rlo) || isnan(rhi) || isnan(clo) || isnan(chi)) return 0;
+    return (rhi < clo - slack || chi < rlo - slack) ? 1 : 0;
+}

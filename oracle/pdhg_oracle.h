@@ -141,6 +141,13 @@ void orc_spmv_transpose(int32_t m, int32_t n, const int32_t* row_ptr, const int3
 void orc_project_box(int32_t n, const double* lo, const double* hi, double* x);
 double orc_pairwise_dot(const double* x, const double* y, int64_t n);
 
+/* FarkasCertificate{y}.certifies_infeasibility(problem, slack)
+ * (src/l1/duals.cpp:16-79): the row-side range of S = sum_i y_i (Ax)_i forced
+ * by the row bounds, the column-side range forced by the column bounds through
+ * d = A^T y, and whether they are disjoint by more than `slack`. ranges (4,
+ * optional) = row lo, row hi, column lo, column hi. Returns 1 or 0. */
+int orc_certifies(const orc_problem* p, const double* y, double slack, double* ranges);
+
 /* The power iteration of estimate_operator_norm (src/l1/pdhg.cpp:48-79) on a
  * CSR matrix as given. */
 double orc_operator_norm(int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col_idx,

@@ -19,6 +19,7 @@
 
 #include "pdhg_oracle.h"  // the shared orc_problem / orc_options / orc_info structs
 #include "sovereign/backend.hpp"
+#include "sovereign/duals.hpp"
 #include "sovereign/io.hpp"
 #include "sovereign/pdhg.hpp"
 #include "sovereign/problem.hpp"
@@ -217,6 +218,29 @@ int ref_pdhg_solve(const orc_problem* p, const orc_options* o, orc_info* info, d
     } catch (const std::exception& e) {
         std::snprintf(info->message, sizeof info->message, "exception: %s", e.what());
         return 1;
+    }
+}
+
+// FarkasCertificate{y}.certifies_infeasibility(problem, slack) and its two
+// ranges (src/l1/duals.cpp:36-79): ranges[0..3] = row-side lo, hi, column-side
+// lo, hi. Returns 1 when the ranges are disjoint by more than `slack`, 0 when
+// not, -1 on an exception.
+int ref_certifies(const orc_problem* p, const double* y, double slack, double* ranges) {
+    try {
+        const sov::Problem problem = build_problem(p);
+        sov::FarkasCertificate cert;
+        cert.row_multipliers.assign(y, y + p->m);
+        const auto rr = cert.row_side_range(problem);
+        const auto cr = cert.column_side_range(problem);
+        if (ranges != nullptr) {
+            ranges[0] = rr.lo;
+            ranges[1] = rr.hi;
+            ranges[2] = cr.lo;
+            ranges[3] = cr.hi;
+        }
+        return cert.certifies_infeasibility(problem, slack) ? 1 : 0;
+    } catch (const std::exception&) {
+        return -1;
     }
 }
 

@@ -574,10 +574,12 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
         c.err = "pdhg_solve_batch: the batched engine runs in precision mixed or fp64";
         return PDHG_ERR_UNSUPPORTED;
     }
-    if (o.checkpoint != nullptr || o.trace_iters > 0 || o.restart_check_period < 1 ||
+    if (o.checkpoint != nullptr || o.trace_iters > 0 || o.infeasibility_detection != 0 ||
+        o.restart_check_period < 1 ||
         o.termination_rule < 0 || o.termination_rule > 1 || o.restart_rule < 0 ||
         o.restart_rule > 1 || o.power_iterations < 0) {
-        c.err = "pdhg_solve_batch: invalid options (no checkpoint / trace in batches)";
+        c.err = "pdhg_solve_batch: invalid options (no checkpoint / trace / infeasibility "
+                "detection in batches)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     BCK(cudaSetDevice(c.device));

@@ -46,12 +46,12 @@ struct GraphSig {
     long long period = 0;
     int cand = 0;
     double tol = 0, bt = 0, dec = 0;
-    int rule = 0, restart_rule = 0, pw = 0;
+    int rule = 0, restart_rule = 0, pw = 0, infeas = 0;
     long long gen = -1;
     bool operator==(const GraphSig& o) const {
         return prec == o.prec && period == o.period && cand == o.cand && tol == o.tol &&
                bt == o.bt && dec == o.dec && rule == o.rule && restart_rule == o.restart_rule &&
-               pw == o.pw && gen == o.gen;
+               pw == o.pw && infeas == o.infeas && gen == o.gen;
     }
 };
 
@@ -86,6 +86,7 @@ struct Ctx {
     DBuf<double> act_avg, cand_xo, cand_yo, part, bx, by, xo, yo, rc, trow, tcol;
     DBuf<double> pw_u, pw_v, pw_w, pw_part, pw_out, x0s, y0s;
     DBuf<double> x_last, y_last;  // restart points (primal-weight update)
+    DBuf<double> ray_yp, ray_atyp, ray_y;  // infeasibility test: previous y, A^T y; dy (original)
     DBuf<DevState> st;
     Mailbox* mail = nullptr;
     Mailbox* mail_dev = nullptr;
@@ -387,7 +388,7 @@ int alloc_iterates(Ctx& c, bool f32) {
     const int g = std::max({fast_check_grid(c.As.view(), c.ATs.view()),
                             exact_check_grid(c.As.view(), c.ATs.view()),
                             exact_check_grid(c.Ao.view(), c.ATo.view())}) + 1;
-    CK(c.part.alloc(static_cast<size_t>(g) * 4 + 4));
+    CK(c.part.alloc(static_cast<size_t>(g) * 8 + 8));
     CK(c.bx.alloc(n));
     CK(c.by.alloc(m));
     CK(c.xo.alloc(n));
@@ -489,6 +490,12 @@ Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candid
                                o.restart_check_period, o.termination_rule,
                                want_candidate ? 1 : 0, c.st.p, c.mail_dev, o.restart_rule,
                                o.primal_weight_update, c.x_last.p, c.y_last.p, 8 * c.sm_count};
+    if (o.infeasibility_detection) {
+        L.fc32.infeas = L.fc64.infeas = 1;
+        L.fc32.ray_y_prev = L.fc64.ray_y_prev = c.ray_yp.p;
+        L.fc32.ray_aty_prev = L.fc64.ray_aty_prev = c.ray_atyp.p;
+        L.fc32.ray_y = L.fc64.ray_y = c.ray_y.p;
+    }
     return L;
 }
 
@@ -681,6 +688,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         sig.rule = o.termination_rule;
         sig.restart_rule = o.restart_rule;
         sig.pw = o.primal_weight_update;
+        sig.infeas = o.infeasibility_detection;
         sig.gen = c.gen;
         int rc = build_graph(c, L, period, sig);
         if (rc != PDHG_OK) return rc;
@@ -1012,6 +1020,12 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
                 "mixed or fp64 (fp64_exact reproduces the reference, which has neither)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
+    if (o.infeasibility_detection < 0 || o.infeasibility_detection > 1 ||
+        (o.precision == PDHG_PREC_FP64_EXACT && o.infeasibility_detection)) {
+        c.err = "pdhg_solve: infeasibility_detection is 0 or 1 and needs precision mixed or "
+                "fp64 (fp64_exact reproduces the reference, which never reports infeasible)";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
     CK(cudaSetDevice(c.device));
     ScalingParams sp;
     sp.ruiz_iterations = o.ruiz_iterations;
@@ -1041,6 +1055,15 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     int prec = o.precision;
     rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
     if (rc != PDHG_OK) return rc;
+    if (o.infeasibility_detection) {
+        // the first check only stores its y and A^T y (DevState.ray_base = 0)
+        CK(c.ray_yp.alloc(static_cast<size_t>(c.lp.m) + 1));
+        CK(c.ray_atyp.alloc(static_cast<size_t>(c.lp.n) + 1));
+        CK(c.ray_y.alloc(static_cast<size_t>(c.lp.m) + 1));
+        CK(cudaMemsetAsync(c.ray_yp.p, 0, sizeof(double) * c.ray_yp.n, c.stream));
+        CK(cudaMemsetAsync(c.ray_atyp.p, 0, sizeof(double) * c.ray_atyp.n, c.stream));
+        CK(cudaMemsetAsync(c.ray_y.p, 0, sizeof(double) * c.ray_y.n, c.stream));
+    }
     CK(c.st.alloc(1));
     if (prec != PDHG_PREC_FP64_EXACT && o.autotune) {
         Ctx::Tuning& t = c.tuning[prec == PDHG_PREC_MIXED ? 0 : 1];
@@ -1163,6 +1186,22 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
                       iterations);
         info->has_point = 0;
         info->kernel_launches = c.launches;
+        return PDHG_OK;
+    }
+    if (status == PDHG_STATUS_PRIMAL_INFEASIBLE) {  // engine extension: a certificate
+        info->status = status;
+        info->has_point = 0;
+        info->kernel_launches = c.launches;
+        std::snprintf(info->message, sizeof info->message,
+                      "primal infeasible at iteration %lld: the row multipliers in y force "
+                      "sum_i y_i (Ax)_i into [%.6g, %.6g] through the row bounds and into "
+                      "[%.6g, %.6g] through the column bounds",
+                      iterations, h.ray_ranges[0], h.ray_ranges[1], h.ray_ranges[2],
+                      h.ray_ranges[3]);
+        if (y != nullptr && m > 0) {
+            CK(cudaMemcpy(y, c.ray_y.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+            for (int32_t i = 0; i < m; ++i) y[i] *= h.ray_scale;
+        }
         return PDHG_OK;
     }
     if (status == PDHG_STATUS_NOT_SOLVED) status = PDHG_STATUS_ITERATION_LIMIT;
@@ -1389,6 +1428,7 @@ void pdhg_default_options(pdhg_options* o) {
     o->termination_rule = 0;
     o->polish_iterations = -1;
     o->autotune = 1;
+    o->infeasibility_detection = 0;
 }
 
 const char* pdhg_status_string(int s) {
@@ -1399,6 +1439,7 @@ const char* pdhg_status_string(int s) {
         case PDHG_STATUS_NUMERICAL_FAILURE: return "numerical_failure";
         case PDHG_STATUS_NOT_SOLVED: return "not_solved";
         case PDHG_STATUS_CANCELLED: return "cancelled";
+        case PDHG_STATUS_PRIMAL_INFEASIBLE: return "primal_infeasible";  // engine extension
     }
     return "unknown";
 }

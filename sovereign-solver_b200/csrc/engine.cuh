@@ -141,6 +141,7 @@ enum Acc {
     ACC_ORIG_P, ACC_ORIG_D,                               // exact mode: candidate, original space
     ACC_OC_P, ACC_OC_D, ACC_OA_P, ACC_OA_D,               // fast mode: cur / avg, original space
     ACC_FIN_PINF, ACC_FIN_DINF,                           // final result
+    ACC_RAY,                                              // infeasibility test: max |dy| (original)
     ACC_COUNT = 16
 };
 
@@ -170,6 +171,9 @@ struct DevState {
     double res_prev_cand;     // adaptive rule: candidate residual at the previous check
     int restart_to_avg;       // adaptive rule: restart point is the average (else current)
     int gap_finite;
+    int ray_base;             // infeasibility test: the previous check's y / A^T y are stored
+    double ray_scale;         // 1 / max |dy| of the certifying check
+    double ray_ranges[4];     // its row-side lo, hi and column-side lo, hi (scaled by ray_scale)
     unsigned long long acc[ACC_COUNT];
     unsigned int ticket[TK_COUNT];
 };
@@ -306,6 +310,12 @@ struct FastCheck {
     double* x_last;            // scaled point of the last restart (n)
     double* y_last;            // (m)
     int grid_cap;              // CTAs of the (grid-stride) check kernel: SMs x 8
+    // infeasibility test (option infeasibility_detection): y and A^T y of the
+    // previous check (scaled; m, n) and the change of y in original units (m)
+    int infeas = 0;
+    double* ray_y_prev = nullptr;
+    double* ray_aty_prev = nullptr;
+    double* ray_y = nullptr;
 };
 template <class T>
 void launch_fast_check(const FastCheck<T>& a, cudaStream_t s);

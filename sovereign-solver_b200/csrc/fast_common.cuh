@@ -421,7 +421,25 @@ struct Terms {
     double cp = 0, cd = 0, ap = 0, ad = 0;         // scaled: cur / avg, primal / dual
     double ocp = 0, ocd = 0, oap = 0, oad = 0;     // original space
     double pobj_c = 0, dobj_c = 0, pobj_a = 0, dobj_a = 0;
+    // infeasibility test: row-side and column-side ranges of the change of y
+    // (FarkasCertificate::row_side_range / column_side_range), max |dy|
+    double rlo = 0, rhi = 0, clo = 0, chi = 0, raymax = 0;
 };
+
+// term_range of the reference's certificate checker (duals.cpp:16-20):
+// mult * [lo, hi] (reversed for a negative multiplier, exactly {0} for a zero
+// one), added into the running range [lo_acc, hi_acc].
+__device__ __forceinline__ void ray_term(double mult, double lo, double hi, double& lo_acc,
+                                         double& hi_acc) {
+    if (mult == 0.0) return;
+    if (mult > 0.0) {
+        lo_acc += mult * lo;
+        hi_acc += mult * hi;
+    } else {
+        lo_acc += mult * hi;
+        hi_acc += mult * lo;
+    }
+}
 
 template <class T>
 __device__ __forceinline__ double avg_x(const Iterates<T>& it, int j, double inv) {

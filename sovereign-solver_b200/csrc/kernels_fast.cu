@@ -485,6 +485,13 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
         t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
     }
+    if (a.infeas) {  // the change of y since the previous check, original units
+        const double dy = P.obj_sign * rs * (yc - a.ray_y_prev[i]);
+        a.ray_y_prev[i] = yc;
+        a.ray_y[i] = dy;
+        ray_term(dy, lo_o, hi_o, t.rlo, t.rhi);
+        t.raymax = smax(t.raymax, fabs(dy));
+    }
 }
 
 template <class T>
@@ -508,26 +515,32 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
         t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ra / cs, lo_o, hi_o);
     }
+    if (a.infeas) {  // d = A_o^T dy_o = sign (A_s^T dy_s) / cs, by linearity
+        const double dd = P.obj_sign * (aty_c - a.ray_aty_prev[j]) / cs;
+        a.ray_aty_prev[j] = aty_c;
+        ray_term(dd, lo_o, hi_o, t.clo, t.chi);
+    }
 }
 
 // Block maxima of the 8 residual terms, one atomicMax per CTA and slot.
 __device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
-    __shared__ double sh[8][kBlock / 32];
-    double v[8] = {t.cp, t.cd, t.ap, t.ad, t.ocp, t.ocd, t.oap, t.oad};
+    __shared__ double sh[9][kBlock / 32];
+    double v[9] = {t.cp, t.cd, t.ap, t.ad, t.ocp, t.ocd, t.oap, t.oad, t.raymax};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 9; ++q) {
         double x = v[q];
         for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
         if (lane == 0) sh[q][warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x < 8) {
+    if (threadIdx.x < 9) {
         double x = 0.0;
         for (int w = 0; w < kBlock / 32; ++w) x = fmax(x, sh[threadIdx.x][w]);
-        // v[0..3] -> ACC_CUR_P..ACC_AVG_D, v[4..7] -> ACC_OC_P..ACC_OA_D
-        const int slot = threadIdx.x < 4 ? ACC_CUR_P + static_cast<int>(threadIdx.x)
-                                         : ACC_OC_P + static_cast<int>(threadIdx.x) - 4;
+        // v[0..3] -> ACC_CUR_P..ACC_AVG_D, v[4..7] -> ACC_OC_P..ACC_OA_D, v[8] -> ACC_RAY
+        const int slot = threadIdx.x < 4   ? ACC_CUR_P + static_cast<int>(threadIdx.x)
+                         : threadIdx.x < 8 ? ACC_OC_P + static_cast<int>(threadIdx.x) - 4
+                                           : ACC_RAY;
         if (x > 0.0)
             atomicMax(&acc[slot], static_cast<unsigned long long>(__double_as_longlong(x)));
     }
@@ -632,24 +645,35 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
         else check_part<T, false>(a, a.AT, bid - nA, sbT, wbT, inv, t);
     }
     block_max_terms(t, st->acc);
-    if (a.termination_rule == 1) {
-        const double s0 = block_sum_det(t.pobj_c);
-        const double s1 = block_sum_det(t.dobj_c);
-        const double s2 = block_sum_det(t.pobj_a);
-        const double s3 = block_sum_det(t.dobj_a);
-        if (threadIdx.x == 0) {
-            double* p = a.cs.part + 4 * blockIdx.x;
-            p[0] = s0; p[1] = s1; p[2] = s2; p[3] = s3;
+    // per-CTA partial sums, 8 per CTA: the objectives [0..3] (relative-KKT
+    // rule), the infeasibility test's ranges [4..7]
+    const bool sum_obj = a.termination_rule == 1, sum_ray = a.infeas != 0;
+    if (sum_obj || sum_ray) {
+        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (sum_obj) {
+            v[0] = block_sum_det(t.pobj_c);
+            v[1] = block_sum_det(t.dobj_c);
+            v[2] = block_sum_det(t.pobj_a);
+            v[3] = block_sum_det(t.dobj_a);
         }
+        if (sum_ray) {
+            v[4] = block_sum_det(t.rlo);
+            v[5] = block_sum_det(t.rhi);
+            v[6] = block_sum_det(t.clo);
+            v[7] = block_sum_det(t.chi);
+        }
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 8; ++q) a.cs.part[8 * blockIdx.x + q] = v[q];
     }
     if (!last_block(&st->ticket[TK_FAST])) return;
-    // the objectives' per-CTA partial sums, added by the whole last CTA in a
-    // fixed order (strided, then a tree)
-    double obj[4] = {0.0, 0.0, 0.0, 0.0};
-    if (a.termination_rule == 1) {
+    // the per-CTA partial sums, added by the whole last CTA in a fixed order
+    // (strided, then a tree)
+    double obj[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (sum_obj || sum_ray) {
         for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock)
-            for (int q = 0; q < 4; ++q) obj[q] += __ldcg(a.cs.part + 4 * b + q);
-        for (int q = 0; q < 4; ++q) obj[q] = block_sum_det(obj[q]);
+            for (int q = 0; q < 8; ++q) obj[q] += __ldcg(a.cs.part + 8 * b + q);
+        for (int q = 0; q < 8; ++q)
+            if (q < 4 ? sum_obj : sum_ray) obj[q] = block_sum_det(obj[q]);
     }
     if (threadIdx.x != 0) return;
 
@@ -658,7 +682,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
     const double ap = acc_read(&st->acc[ACC_AVG_P]), ad = acc_read(&st->acc[ACC_AVG_D]);
     const double ocp = acc_read(&st->acc[ACC_OC_P]), ocd = acc_read(&st->acc[ACC_OC_D]);
     const double oap = acc_read(&st->acc[ACC_OA_P]), oad = acc_read(&st->acc[ACC_OA_D]);
+    const double ray_max = acc_read(&st->acc[ACC_RAY]);
     for (int q = ACC_CUR_P; q <= ACC_OA_D; ++q) st->acc[q] = 0ull;
+    st->acc[ACC_RAY] = 0ull;
     st->ticket[TK_FAST] = 0u;
     const double cur = smax(cp, cd), avg = smax(ap, ad);
     st->cur_res = cur;
@@ -695,7 +721,35 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
             }
             st->rel_kkt = rel;
             const bool conv = (a.termination_rule == 1) ? (rel < a.tol) : (orig < a.tol);
-            if (conv) {  // pdhg.cpp:383-389
+            // Infeasibility test (engine extension): the change of y since the
+            // previous check as a FarkasCertificate (duals.cpp:36-79), scaled
+            // to max |dy| = 1; certified when the row-side and column-side
+            // ranges are disjoint by more than 1e-6 x (1 + their finite ends).
+            bool infeasible = false;
+            if (a.infeas) {
+                if (st->ray_base && !conv && ray_max > 0.0 && isfinite(ray_max)) {
+                    const double k = 1.0 / ray_max;
+                    const double r[4] = {obj[4] * k, obj[5] * k, obj[6] * k, obj[7] * k};
+                    double ref = 1.0;
+                    bool nan = false;
+                    for (int q = 0; q < 4; ++q) {
+                        if (isfinite(r[q])) ref += fabs(r[q]);
+                        nan = nan || isnan(r[q]);
+                    }
+                    const double slack = 1e-6 * ref;
+                    if (!nan && (r[1] < r[2] - slack || r[3] < r[0] - slack)) {
+                        infeasible = true;
+                        st->ray_scale = k;
+                        for (int q = 0; q < 4; ++q) st->ray_ranges[q] = r[q];
+                    }
+                }
+                st->ray_base = 1;  // this check's y and A^T y are stored
+            }
+            if (infeasible) {
+                st->done = 1;
+                st->status = PDHG_STATUS_PRIMAL_INFEASIBLE;
+                st->stop_iter = it_idx + 1;
+            } else if (conv) {  // pdhg.cpp:383-389
                 st->done = 1;
                 st->converged = 1;
                 st->status = kStatusOptimal;
@@ -739,6 +793,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
                     st->stop_iter = it_idx + 1;
                 }
             }
+            // a restart moves y: the next check has no base to difference with
+            if (a.infeas && st->restart) st->ray_base = 0;
         }
     }
     st->iter += a.period_iters;

@@ -24,7 +24,7 @@ from .problem import Problem
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpdhg_b200.so")
 
 STATUS = ["optimal", "iteration_limit", "time_limit", "numerical_failure", "not_solved",
-          "cancelled"]
+          "cancelled", "primal_infeasible"]
 PREC = {"fp64_exact": 0, "mixed": 1, "fp64": 2}
 
 _dp = C.POINTER(C.c_double)
@@ -45,7 +45,7 @@ class _Options(C.Structure):
                 ("x0", _dp), ("y0", _dp), ("checkpoint", CHECKPOINT_FN),
                 ("checkpoint_user", C.c_void_p), ("cancel_flag", C.POINTER(C.c_int)),
                 ("trace_iters", C.c_int), ("trace_x", _dp), ("trace_y", _dp),
-                ("autotune", C.c_int)]
+                ("autotune", C.c_int), ("infeasibility_detection", C.c_int)]
 
 
 class _Info(C.Structure):
@@ -154,6 +154,10 @@ class PdhgOptions:
     checkpoint: Optional[Callable[[int, np.ndarray, np.ndarray, float], None]] = None
     trace_iters: int = 0
     autotune: bool = True
+    # engine extension (MIXED / FP64): stop with status "primal_infeasible" and a
+    # certificate (PdhgResult.farkas) when the change of y between two checks
+    # proves that no x meets the bounds
+    infeasibility_detection: bool = False
 
 
 @dataclass
@@ -178,6 +182,9 @@ class PdhgResult:
     device_seconds: float = 0.0
     trace_x: Optional[np.ndarray] = None
     trace_y: Optional[np.ndarray] = None
+    # status "primal_infeasible": the certificate's row multipliers
+    # (sov::FarkasCertificate::row_multipliers, duals.hpp:47-70), max |y_i| = 1
+    farkas: Optional[np.ndarray] = None
 
 
 class CancellationToken:
@@ -236,7 +243,9 @@ def _c_start(o: _Options, keep: list, cancel, x0, y0) -> None:
 
 def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray) -> PdhgResult:
     hp = bool(info.has_point)
+    certified = STATUS[info.status] == "primal_infeasible"
     return PdhgResult(
+        farkas=y.copy() if certified else None,
         status=STATUS[info.status], objective=info.objective,
         primal=x.copy() if hp else np.zeros(0), dual=y.copy() if hp else np.zeros(0),
         reduced_costs=rc.copy() if hp else np.zeros(0),

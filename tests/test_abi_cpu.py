@@ -47,7 +47,8 @@ def test_defaults_are_the_reference_defaults(pkg):
     assert o.pock_chambolle_alpha == 1.0 and o.apply_ruiz == 1 and o.apply_pock_chambolle == 1
     assert o.precision == 0 and o.termination_rule == 0
     assert o.autotune == 1  # an engine extension; it never applies to fp64_exact
-    assert lib.pdhg_abi_version() == 2
+    assert o.infeasibility_detection == 0  # extension, off: the reference never reports it
+    assert lib.pdhg_abi_version() == 3
     d = pkg.PdhgOptions()
     assert d.tolerance == o.tolerance and d.max_iterations == o.max_iterations
 
@@ -57,6 +58,7 @@ def test_status_and_error_strings(pkg):
     assert [lib.pdhg_status_string(i).decode() for i in range(6)] == [
         "optimal", "iteration_limit", "time_limit", "numerical_failure", "not_solved",
         "cancelled"]
+    assert lib.pdhg_status_string(6).decode() == "primal_infeasible"  # engine extension
     assert lib.pdhg_error_string(3).decode() == "invalid argument"
     assert lib.pdhg_error_string(6).decode() == "backend error"
 

@@ -90,3 +90,39 @@ def test_scaling_and_spmv_match(pkg, orc):
                           orc.reference_spmv(p, -1.0, x, 0.0, np.zeros(p.m)))
     assert np.array_equal(orc.oracle_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True),
                           orc.reference_spmv(p, 0.5, y, 2.0, np.ones(p.n), transpose=True))
+
+
+def _same_ranges(a, b):
+    for u, v in zip(a, b):
+        assert u == v or (np.isnan(u) and np.isnan(v)), (a, b)
+
+
+def test_certificate_checker_is_the_reference(pkg, orc):
+    # FarkasCertificate{y}.certifies_infeasibility (src/l1/duals.cpp:16-79):
+    # verdict and both ranges, bit for bit, on the reference's infeasible
+    # smoke model (x >= 0, x >= 2, x <= 1: y = (1, -1) certifies it) and on
+    # random multipliers over random LPs (zero multipliers included)
+    _ref_or_skip(orc)
+    p = golden_problem(pkg, load_golden("smoke_tiny_infeasible"))
+    for y, expect in (([1.0, -1.0], True), ([1.0, 1.0], False), ([0.0, 0.0], False)):
+        a, ra = orc.oracle_certifies(p, y)
+        b, rb = orc.reference_certifies(p, y)
+        assert a == b == expect
+        _same_ranges(ra, rb)
+    rng = np.random.default_rng(5)
+    for seed in range(4):
+        q = pkg.lpgen.badly_scaled_lp(40, 90, 4, seed=seed)
+        for _ in range(5):
+            y = rng.standard_normal(q.m) * (rng.random(q.m) < 0.7)
+            a, ra = orc.oracle_certifies(q, y)
+            b, rb = orc.reference_certifies(q, y)
+            assert a == b
+            _same_ranges(ra, rb)
+    # with the lower bound of the first row dropped the row side becomes
+    # (-inf, inf): nothing is certified
+    q = golden_problem(pkg, load_golden("smoke_tiny_infeasible"))
+    q.row_lo = np.array([-np.inf, -np.inf])
+    a, ra = orc.oracle_certifies(q, [1.0, -1.0])
+    b, rb = orc.reference_certifies(q, [1.0, -1.0])
+    assert a == b is False
+    _same_ranges(ra, rb)
