@@ -54,7 +54,12 @@ typedef enum {
      * multipliers to y (the reference's FarkasCertificate, duals.hpp:47-70,
      * which the reference's PDHG never produces: its verdict there stays
      * iteration_limit) */
-    PDHG_STATUS_PRIMAL_INFEASIBLE = 6
+    PDHG_STATUS_PRIMAL_INFEASIBLE = 6,
+    /* engine extension (option infeasibility_detection): a ray d in x proves
+     * that the dual has no solution, so the LP is unbounded if it is feasible
+     * (the reference's simplex names this outcome Unbounded, simplex.hpp:42);
+     * pdhg_solve writes the ray to x */
+    PDHG_STATUS_DUAL_INFEASIBLE = 7
 } pdhg_status;
 
 /* Arithmetic of the iteration kernels. */
@@ -127,7 +132,13 @@ typedef struct pdhg_options {
                                 the ranges the row bounds and the column bounds force on
                                 sum_i y_i (Ax)_i are disjoint by more than 1e-6 relative, the
                                 solve stops with PDHG_STATUS_PRIMAL_INFEASIBLE and y receives
-                                the multipliers, scaled to max |y_i| = 1 */
+                                the multipliers, scaled to max |y_i| = 1. Else the change of x,
+                                scaled to d with max |d_j| = 1, is tested as a ray: when the
+                                objective falls along it (c^T d < 0 in the minimize sense) and
+                                it leaves the recession cones of the column and row bounds (a
+                                finite lower end allows no decrease of x_j or (Ad)_i, a finite
+                                upper end no increase) by at most 1e-6 and 1e-6 |c^T d|, the
+                                solve stops with PDHG_STATUS_DUAL_INFEASIBLE and x receives d */
 } pdhg_options;
 
 /* sov::PdhgResult (pdhg.hpp:136-153) minus the vectors, which pdhg_solve

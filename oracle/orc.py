@@ -333,3 +333,38 @@ def oracle_certifies(p, y, slack: float = 1e-6):
 def reference_certifies(p, y, slack: float = 1e-6):
     """The reference's own FarkasCertificate checker (compiled duals.cpp)."""
     return _certifies("reference", p, y, slack)
+
+
+def ray_certifies(p, d, eps: float = 1e-6):
+    """The engine's ray test for dual infeasibility, restated in numpy. It has
+    no reference counterpart: the reference's PDHG never reports an outcome
+    other than those of sov::PdhgStatus (pdhg.hpp:74-81), and its simplex
+    reports Unbounded (simplex.hpp:42) without a ray. d, scaled to max |d_j| = 1,
+    certifies when c^T d < 0 in the minimize sense and d and A d leave the
+    recession cones of the column and row bounds (a finite lower end allows no
+    decrease, a finite upper end no increase) by at most eps and eps |c^T d|.
+    Returns (certified, c^T d, violation), both for the scaled d."""
+    d = np.asarray(d, dtype=np.float64)
+    big = np.max(np.abs(d)) if d.size else 0.0
+    if not np.isfinite(big) or big == 0.0:
+        return False, float("nan"), float("nan")
+    d = d / big
+    rp = np.asarray(p.row_ptr, dtype=np.int64)
+    ci = np.asarray(p.col_idx, dtype=np.int64)
+    val = np.asarray(p.val, dtype=np.float64)
+    rows = np.repeat(np.arange(p.m), np.diff(rp))
+    ad = np.zeros(p.m)
+    np.add.at(ad, rows, val * d[ci])
+    sign = -1.0 if p.maximize else 1.0
+    obj = float(sign * np.dot(np.asarray(p.c, dtype=np.float64), d))
+
+    def cone(v, lo, hi):
+        lo = np.asarray(lo, dtype=np.float64)
+        hi = np.asarray(hi, dtype=np.float64)
+        down = np.where((v < 0) & np.isfinite(lo), -v, 0.0)
+        up = np.where((v > 0) & np.isfinite(hi), v, 0.0)
+        return float(max(down.max(initial=0.0), up.max(initial=0.0)))
+
+    viol = max(cone(d, p.col_lo, p.col_hi), cone(ad, p.row_lo, p.row_hi))
+    ok = obj < 0.0 and viol <= eps and viol <= eps * -obj
+    return ok, obj, viol

@@ -87,6 +87,7 @@ struct Ctx {
     DBuf<double> pw_u, pw_v, pw_w, pw_part, pw_out, x0s, y0s;
     DBuf<double> x_last, y_last;  // restart points (primal-weight update)
     DBuf<double> ray_yp, ray_atyp, ray_y;  // infeasibility test: previous y, A^T y; dy (original)
+    DBuf<double> xray_xp, xray_d0, xray_d1;  // ray test: previous x; two projected rays (scaled)
     DBuf<DevState> st;
     Mailbox* mail = nullptr;
     Mailbox* mail_dev = nullptr;
@@ -388,7 +389,7 @@ int alloc_iterates(Ctx& c, bool f32) {
     const int g = std::max({fast_check_grid(c.As.view(), c.ATs.view()),
                             exact_check_grid(c.As.view(), c.ATs.view()),
                             exact_check_grid(c.Ao.view(), c.ATo.view())}) + 1;
-    CK(c.part.alloc(static_cast<size_t>(g) * 8 + 8));
+    CK(c.part.alloc(static_cast<size_t>(g) * kCheckSums + kCheckSums));
     CK(c.bx.alloc(n));
     CK(c.by.alloc(m));
     CK(c.xo.alloc(n));
@@ -432,16 +433,17 @@ struct Launcher {
             fc32.period_iters = period;
             launch_fast_check(fc32, s);
             launch_fast_restart(fc32, s);
-            c.launches += 2 + (fc32.want_candidate ? 1 : 0);
+            c.launches += 2 + (fc32.want_candidate ? 1 : 0) + fc32.infeas;
         } else {
             fc64.period_iters = period;
             launch_fast_check(fc64, s);
             launch_fast_restart(fc64, s);
-            c.launches += 2 + (fc64.want_candidate ? 1 : 0);
+            c.launches += 2 + (fc64.want_candidate ? 1 : 0) + fc64.infeas;
         }
     }
     long long launches_per_period(long long period) const {
-        const long long chk = prec == PDHG_PREC_FP64_EXACT ? 3 : 2 + (fc32.want_candidate ? 1 : 0);
+        const long long chk =
+            prec == PDHG_PREC_FP64_EXACT ? 3 : 2 + (fc32.want_candidate ? 1 : 0) + fc32.infeas;
         long long per_iter = 2;
         long long clear = 0;  // the flag reset when the primal pass has no rows
         if (prec != PDHG_PREC_FP64_EXACT) {
@@ -495,6 +497,9 @@ Launcher make_launcher(Ctx& c, int prec, const pdhg_options& o, bool want_candid
         L.fc32.ray_y_prev = L.fc64.ray_y_prev = c.ray_yp.p;
         L.fc32.ray_aty_prev = L.fc64.ray_aty_prev = c.ray_atyp.p;
         L.fc32.ray_y = L.fc64.ray_y = c.ray_y.p;
+        L.fc32.xray_x_prev = L.fc64.xray_x_prev = c.xray_xp.p;
+        L.fc32.xray_d[0] = L.fc64.xray_d[0] = c.xray_d0.p;
+        L.fc32.xray_d[1] = L.fc64.xray_d[1] = c.xray_d1.p;
     }
     return L;
 }
@@ -1056,13 +1061,16 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
     if (rc != PDHG_OK) return rc;
     if (o.infeasibility_detection) {
-        // the first check only stores its y and A^T y (DevState.ray_base = 0)
-        CK(c.ray_yp.alloc(static_cast<size_t>(c.lp.m) + 1));
-        CK(c.ray_atyp.alloc(static_cast<size_t>(c.lp.n) + 1));
-        CK(c.ray_y.alloc(static_cast<size_t>(c.lp.m) + 1));
-        CK(cudaMemsetAsync(c.ray_yp.p, 0, sizeof(double) * c.ray_yp.n, c.stream));
-        CK(cudaMemsetAsync(c.ray_atyp.p, 0, sizeof(double) * c.ray_atyp.n, c.stream));
-        CK(cudaMemsetAsync(c.ray_y.p, 0, sizeof(double) * c.ray_y.n, c.stream));
+        // the first check only stores its x, A x, y and A^T y (DevState.ray_base = 0)
+        const size_t m1 = static_cast<size_t>(c.lp.m) + 1, n1 = static_cast<size_t>(c.lp.n) + 1;
+        CK(c.ray_yp.alloc(m1));
+        CK(c.ray_atyp.alloc(n1));
+        CK(c.ray_y.alloc(m1));
+        CK(c.xray_xp.alloc(n1));
+        CK(c.xray_d0.alloc(n1));
+        CK(c.xray_d1.alloc(n1));
+        for (DBuf<double>* b : {&c.ray_yp, &c.ray_atyp, &c.ray_y, &c.xray_xp, &c.xray_d0, &c.xray_d1})
+            CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, c.stream));
     }
     CK(c.st.alloc(1));
     if (prec != PDHG_PREC_FP64_EXACT && o.autotune) {
@@ -1204,6 +1212,24 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
         }
         return PDHG_OK;
     }
+    if (status == PDHG_STATUS_DUAL_INFEASIBLE) {  // engine extension: a ray in x
+        info->status = status;
+        info->has_point = 0;
+        info->kernel_launches = c.launches;
+        std::snprintf(info->message, sizeof info->message,
+                      "dual infeasible (unbounded if feasible) at iteration %lld: along the ray "
+                      "d in x (max |d_j| = 1) the objective falls by %.6g (minimize sense) and "
+                      "the bounds are left by at most %.3g",
+                      iterations, -h.xray_obj, h.xray_viol);
+        if (x != nullptr && n > 0) {  // original units: d_o = d_s * cs, then max |d_j| = 1
+            std::vector<double> cs(static_cast<size_t>(n));
+            CK(cudaMemcpy(x, h.xray_buf ? c.xray_d1.p : c.xray_d0.p, sizeof(double) * n,
+                          cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(cs.data(), P.cs, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            for (int32_t j = 0; j < n; ++j) x[j] = x[j] * cs[j] * h.xray_scale;
+        }
+        return PDHG_OK;
+    }
     if (status == PDHG_STATUS_NOT_SOLVED) status = PDHG_STATUS_ITERATION_LIMIT;
     info->status = status;
 
@@ -1240,6 +1266,13 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     info->has_point = 1;
     info->kernel_launches = c.launches;
     info->seconds = elapsed_since(t0);
+    if (o.infeasibility_detection && status != PDHG_STATUS_OPTIMAL)
+        std::snprintf(info->message, sizeof info->message,
+                      "no certificate; at the last test the multipliers' ranges were [%.6g, %.6g] "
+                      "(rows) and [%.6g, %.6g] (columns), the ray's c^T d %.6g with cone "
+                      "violation %.3g",
+                      h.ray_ranges[0], h.ray_ranges[1], h.ray_ranges[2], h.ray_ranges[3],
+                      h.xray_obj, h.xray_viol);
     return PDHG_OK;
 }
 
@@ -1440,6 +1473,7 @@ const char* pdhg_status_string(int s) {
         case PDHG_STATUS_NOT_SOLVED: return "not_solved";
         case PDHG_STATUS_CANCELLED: return "cancelled";
         case PDHG_STATUS_PRIMAL_INFEASIBLE: return "primal_infeasible";  // engine extension
+        case PDHG_STATUS_DUAL_INFEASIBLE: return "dual_infeasible";      // engine extension
     }
     return "unknown";
 }

@@ -142,10 +142,15 @@ enum Acc {
     ACC_OC_P, ACC_OC_D, ACC_OA_P, ACC_OA_D,               // fast mode: cur / avg, original space
     ACC_FIN_PINF, ACC_FIN_DINF,                           // final result
     ACC_RAY,                                              // infeasibility test: max |dy| (original)
+    ACC_XRAY_MAX, ACC_XRAY_V,                             // ray test: max |d|, rows' cone violation
     ACC_COUNT = 16
 };
 
 enum Ticket { TK_CHECK1 = 0, TK_CHECK2, TK_FAST, TK_RESTART, TK_COUNT = 4 };
+
+// Per-CTA partial sums of the fast check kernel: the objectives (4), the
+// Farkas ranges (4), c^T dx of the ray test (1).
+constexpr int kCheckSums = 9;
 
 struct DevState {
     int done;         // 1 = every later kernel returns at once
@@ -174,6 +179,10 @@ struct DevState {
     int ray_base;             // infeasibility test: the previous check's y / A^T y are stored
     double ray_scale;         // 1 / max |dy| of the certifying check
     double ray_ranges[4];     // its row-side lo, hi and column-side lo, hi (scaled by ray_scale)
+    int xray_pending;         // ray test: a projected ray awaits its rows' test
+    int xray_buf;             // which of the two ray buffers holds it
+    double xray_scale;        // its 1 / max |d_j| (original units)
+    double xray_obj, xray_viol;  // its c^T d (minimize sense) and cone violation, max |d| = 1
     unsigned long long acc[ACC_COUNT];
     unsigned int ticket[TK_COUNT];
 };
@@ -311,11 +320,15 @@ struct FastCheck {
     double* y_last;            // (m)
     int grid_cap;              // CTAs of the (grid-stride) check kernel: SMs x 8
     // infeasibility test (option infeasibility_detection): y and A^T y of the
-    // previous check (scaled; m, n) and the change of y in original units (m)
+    // previous check (scaled; m, n) and the change of y in original units (m);
+    // the ray test: x of the previous check (scaled; n) and two buffers for
+    // the change of x projected onto the columns' recession cones (scaled; n)
     int infeas = 0;
     double* ray_y_prev = nullptr;
     double* ray_aty_prev = nullptr;
     double* ray_y = nullptr;
+    double* xray_x_prev = nullptr;
+    double* xray_d[2] = {nullptr, nullptr};
 };
 template <class T>
 void launch_fast_check(const FastCheck<T>& a, cudaStream_t s);

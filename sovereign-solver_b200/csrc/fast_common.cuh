@@ -424,7 +424,18 @@ struct Terms {
     // infeasibility test: row-side and column-side ranges of the change of y
     // (FarkasCertificate::row_side_range / column_side_range), max |dy|
     double rlo = 0, rhi = 0, clo = 0, chi = 0, raymax = 0;
+    // ray test: max |d| and c^T d of the projected change of x
+    double xmax = 0, xobj = 0;
 };
+
+// How far a change d of a bounded quantity leaves the recession cone of
+// [lo, hi]: a finite lower end allows no decrease, a finite upper end no
+// increase.
+__device__ __forceinline__ double cone_violation(double d, double lo, double hi) {
+    if (d < 0.0 && fb(lo)) return -d;
+    if (d > 0.0 && fb(hi)) return d;
+    return 0.0;
+}
 
 // term_range of the reference's certificate checker (duals.cpp:16-20):
 // mult * [lo, hi] (reversed for a negative multiplier, exactly {0} for a zero

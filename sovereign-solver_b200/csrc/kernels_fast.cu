@@ -461,8 +461,10 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
 // Check kernel
 // ---------------------------------------------------------------------------
 
-// Per-row terms, merged into the thread's running maxima / sums.
-template <class T>
+// Per-row terms, merged into the thread's running maxima / sums. INF: with
+// the infeasibility tests (option infeasibility_detection), a separate
+// instance so that the plain check keeps its registers.
+template <class T, bool INF>
 __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double act_c,
                                           double act_a, double inv, Terms& t) {
     const DevProblem& P = a.P;
@@ -485,7 +487,7 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
         t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
     }
-    if (a.infeas) {  // the change of y since the previous check, original units
+    if (INF) {  // the change of y since the previous check, original units
         const double dy = P.obj_sign * rs * (yc - a.ray_y_prev[i]);
         a.ray_y_prev[i] = yc;
         a.ray_y[i] = dy;
@@ -494,7 +496,7 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
     }
 }
 
-template <class T>
+template <class T, bool INF>
 __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double aty_c,
                                           double aty_a, double inv, Terms& t) {
     const DevProblem& P = a.P;
@@ -515,32 +517,47 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
         t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ra / cs, lo_o, hi_o);
     }
-    if (a.infeas) {  // d = A_o^T dy_o = sign (A_s^T dy_s) / cs, by linearity
+    if (INF) {  // d = A_o^T dy_o = sign (A_s^T dy_s) / cs, by linearity
         const double dd = P.obj_sign * (aty_c - a.ray_aty_prev[j]) / cs;
         a.ray_aty_prev[j] = aty_c;
         ray_term(dd, lo_o, hi_o, t.clo, t.chi);
+        // ray test: the change of x since the previous check, projected onto
+        // the recession cone of the column's bounds (no decrease at a finite
+        // lower end, no increase at a finite upper end), into the buffer the
+        // pending ray does not hold
+        const double dxs = xc - a.xray_x_prev[j];
+        a.xray_x_prev[j] = xc;
+        const double ds = cone_violation(dxs, lo_o, hi_o) > 0.0 ? 0.0 : dxs;  // cs > 0
+        (a.st->xray_buf ? a.xray_d[0] : a.xray_d[1])[j] = ds;
+        const double dx = ds * cs;
+        t.xmax = smax(t.xmax, fabs(dx));
+        t.xobj += P.obj_sign * P.c_o[j] * dx;
     }
 }
 
-// Block maxima of the 8 residual terms, one atomicMax per CTA and slot.
+// Block maxima of the 8 residual terms (and with INF the 2 of the
+// infeasibility tests), one atomicMax per CTA and slot.
+template <bool INF>
 __device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
-    __shared__ double sh[9][kBlock / 32];
-    double v[9] = {t.cp, t.cd, t.ap, t.ad, t.ocp, t.ocd, t.oap, t.oad, t.raymax};
+    constexpr int K = INF ? 10 : 8;
+    __shared__ double sh[K][kBlock / 32];
+    double v[10] = {t.cp, t.cd, t.ap, t.ad, t.ocp, t.ocd, t.oap, t.oad, t.raymax, t.xmax};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
+    for (int q = 0; q < K; ++q) {
         double x = v[q];
         for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
         if (lane == 0) sh[q][warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x < 9) {
+    if (threadIdx.x < K) {
         double x = 0.0;
         for (int w = 0; w < kBlock / 32; ++w) x = fmax(x, sh[threadIdx.x][w]);
-        // v[0..3] -> ACC_CUR_P..ACC_AVG_D, v[4..7] -> ACC_OC_P..ACC_OA_D, v[8] -> ACC_RAY
+        // v[0..3] -> ACC_CUR_P..ACC_AVG_D, v[4..7] -> ACC_OC_P..ACC_OA_D,
+        // v[8..9] -> ACC_RAY, ACC_XRAY_MAX
         const int slot = threadIdx.x < 4   ? ACC_CUR_P + static_cast<int>(threadIdx.x)
                          : threadIdx.x < 8 ? ACC_OC_P + static_cast<int>(threadIdx.x) - 4
-                                           : ACC_RAY;
+                                           : ACC_RAY + static_cast<int>(threadIdx.x) - 8;
         if (x > 0.0)
             atomicMax(&acc[slot], static_cast<unsigned long long>(__double_as_longlong(x)));
     }
@@ -565,17 +582,17 @@ __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr
     }
 }
 
-template <class T, bool ROWS>
+template <class T, bool ROWS, bool INF>
 __device__ __forceinline__ void row_or_col_terms(const FastCheck<T>& a, int r, double ac, double aa,
                                                  double inv, Terms& t) {
-    if (ROWS) row_terms(a, r, ac, aa, inv, t);
-    else col_terms(a, r, ac, aa, inv, t);
+    if (ROWS) row_terms<T, INF>(a, r, ac, aa, inv, t);
+    else col_terms<T, INF>(a, r, ac, aa, inv, t);
 }
 
 // Virtual block vb of one matrix's part [short | warp rows | CTA items]:
 // short rows on groups of M.vw lanes, rows up to kLongRow one warp each
 // (warp_rows0), longer ones as CTA items (items_long). Block-uniform.
-template <class T, bool ROWS>
+template <class T, bool ROWS, bool INF>
 __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int sb, int wb,
                            double inv, Terms& t) {
     double ac = 0.0, aa = 0.0;
@@ -589,7 +606,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         row_products<T, ROWS>(a, M, b + lane, e, vw, inv, ac, aa);
         ac = group_sum(ac, vw);
         aa = group_sum(aa, vw);
-        if (lane == 0) row_or_col_terms<T, ROWS>(a, r, ac, aa, inv, t);
+        if (lane == 0) row_or_col_terms<T, ROWS, INF>(a, r, ac, aa, inv, t);
     } else if (vb < sb + wb) {
         const int w = (vb - sb) * (kBlock / 32) + (threadIdx.x >> 5);
         if (w >= M.n_warp0) return;
@@ -600,7 +617,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
             ac += __shfl_xor_sync(0xffffffffu, ac, o);
             aa += __shfl_xor_sync(0xffffffffu, aa, o);
         }
-        if (lane == 0) row_or_col_terms<T, ROWS>(a, r, ac, aa, inv, t);
+        if (lane == 0) row_or_col_terms<T, ROWS, INF>(a, r, ac, aa, inv, t);
     } else {
         const int idx = vb - sb - wb;
         const int4 w = M.items_long.item[idx];
@@ -608,7 +625,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         ac = block_total(ac);
         aa = block_total(aa);
         if (w.w >= 0 && !segment_finish(M.items_long, idx, w.w, ac, aa, &ac, &aa)) return;
-        if (threadIdx.x == 0) row_or_col_terms<T, ROWS>(a, w.x, ac, aa, inv, t);
+        if (threadIdx.x == 0) row_or_col_terms<T, ROWS, INF>(a, w.x, ac, aa, inv, t);
     }
 }
 
@@ -628,9 +645,12 @@ inline int check_blocks(const DevCsr& M) {
 // so each CTA sums its rows into per-thread running terms and takes part in
 // one reduction. Compiled to fit four CTAs per SM in FP32 (64 registers) and
 // three in FP64 (80), both without spills; unbounded it took 109-118
-// registers and two CTAs per SM.
-template <class T>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(FastCheck<T> a) {
+// registers and two CTAs per SM. The instance with the infeasibility tests
+// (INF) carries 11 more running terms: three CTAs per SM in FP32 (80) and two
+// in FP64 (122), also without spills.
+template <class T, bool INF>
+__global__ void __launch_bounds__(kBlock, INF ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 4 : 3))
+    fast_check(FastCheck<T> a) {
     DevState* st = a.st;
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
@@ -641,15 +661,16 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
     const int nA = sbA + wbA + a.A.items_long.n_item;
     const int nT = sbT + wbT + a.AT.items_long.n_item;
     for (int bid = blockIdx.x; bid < nA + nT; bid += gridDim.x) {
-        if (bid < nA) check_part<T, true>(a, a.A, bid, sbA, wbA, inv, t);
-        else check_part<T, false>(a, a.AT, bid - nA, sbT, wbT, inv, t);
+        if (bid < nA) check_part<T, true, INF>(a, a.A, bid, sbA, wbA, inv, t);
+        else check_part<T, false, INF>(a, a.AT, bid - nA, sbT, wbT, inv, t);
     }
-    block_max_terms(t, st->acc);
-    // per-CTA partial sums, 8 per CTA: the objectives [0..3] (relative-KKT
-    // rule), the infeasibility test's ranges [4..7]
-    const bool sum_obj = a.termination_rule == 1, sum_ray = a.infeas != 0;
+    block_max_terms<INF>(t, st->acc);
+    // per-CTA partial sums, kCheckSums per CTA: the objectives [0..3]
+    // (relative-KKT rule), the infeasibility test's ranges [4..7], the ray
+    // test's c^T dx [8]
+    const bool sum_obj = a.termination_rule == 1, sum_ray = INF;
     if (sum_obj || sum_ray) {
-        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double v[kCheckSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (sum_obj) {
             v[0] = block_sum_det(t.pobj_c);
             v[1] = block_sum_det(t.dobj_c);
@@ -661,18 +682,19 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
             v[5] = block_sum_det(t.rhi);
             v[6] = block_sum_det(t.clo);
             v[7] = block_sum_det(t.chi);
+            v[8] = block_sum_det(t.xobj);
         }
         if (threadIdx.x == 0)
-            for (int q = 0; q < 8; ++q) a.cs.part[8 * blockIdx.x + q] = v[q];
+            for (int q = 0; q < kCheckSums; ++q) a.cs.part[kCheckSums * blockIdx.x + q] = v[q];
     }
     if (!last_block(&st->ticket[TK_FAST])) return;
     // the per-CTA partial sums, added by the whole last CTA in a fixed order
     // (strided, then a tree)
-    double obj[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double obj[kCheckSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (sum_obj || sum_ray) {
         for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock)
-            for (int q = 0; q < 8; ++q) obj[q] += __ldcg(a.cs.part + 8 * b + q);
-        for (int q = 0; q < 8; ++q)
+            for (int q = 0; q < kCheckSums; ++q) obj[q] += __ldcg(a.cs.part + kCheckSums * b + q);
+        for (int q = 0; q < kCheckSums; ++q)
             if (q < 4 ? sum_obj : sum_ray) obj[q] = block_sum_det(obj[q]);
     }
     if (threadIdx.x != 0) return;
@@ -683,8 +705,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
     const double ocp = acc_read(&st->acc[ACC_OC_P]), ocd = acc_read(&st->acc[ACC_OC_D]);
     const double oap = acc_read(&st->acc[ACC_OA_P]), oad = acc_read(&st->acc[ACC_OA_D]);
     const double ray_max = acc_read(&st->acc[ACC_RAY]);
+    const double xray_v = acc_read(&st->acc[ACC_XRAY_V]), xray_max = acc_read(&st->acc[ACC_XRAY_MAX]);
     for (int q = ACC_CUR_P; q <= ACC_OA_D; ++q) st->acc[q] = 0ull;
-    st->acc[ACC_RAY] = 0ull;
+    st->acc[ACC_RAY] = st->acc[ACC_XRAY_V] = st->acc[ACC_XRAY_MAX] = 0ull;
     st->ticket[TK_FAST] = 0u;
     const double cur = smax(cp, cd), avg = smax(ap, ad);
     st->cur_res = cur;
@@ -725,8 +748,14 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
             // previous check as a FarkasCertificate (duals.cpp:36-79), scaled
             // to max |dy| = 1; certified when the row-side and column-side
             // ranges are disjoint by more than 1e-6 x (1 + their finite ends).
-            bool infeasible = false;
-            if (a.infeas) {
+            // Else the ray test: the change of x at the previous check,
+            // projected onto the columns' recession cones and scaled to
+            // max |d| = 1, certifies dual infeasibility when c^T d < 0
+            // (minimize sense) and A d leaves the rows' recession cones by at
+            // most 1e-6 and 1e-6 |c^T d| (fast_xray_rows measured it after
+            // that check). This check's change becomes the next candidate.
+            bool infeasible = false, unbounded = false;
+            if (INF) {
                 if (st->ray_base && !conv && ray_max > 0.0 && isfinite(ray_max)) {
                     const double k = 1.0 / ray_max;
                     const double r[4] = {obj[4] * k, obj[5] * k, obj[6] * k, obj[7] * k};
@@ -737,17 +766,29 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
                         nan = nan || isnan(r[q]);
                     }
                     const double slack = 1e-6 * ref;
-                    if (!nan && (r[1] < r[2] - slack || r[3] < r[0] - slack)) {
-                        infeasible = true;
-                        st->ray_scale = k;
-                        for (int q = 0; q < 4; ++q) st->ray_ranges[q] = r[q];
+                    infeasible = !nan && (r[1] < r[2] - slack || r[3] < r[0] - slack);
+                    st->ray_scale = k;  // the last test's figures, reported either way
+                    for (int q = 0; q < 4; ++q) st->ray_ranges[q] = r[q];
+                }
+                if (st->xray_pending && !conv && !infeasible) {
+                    const double ob = st->xray_obj, vi = xray_v * st->xray_scale;
+                    unbounded = ob < 0.0 && vi <= 1e-6 && vi <= 1e-6 * -ob;
+                    st->xray_viol = vi;
+                }
+                if (!unbounded) {  // this check's projected change: the next candidate
+                    const bool ok = st->ray_base && xray_max > 0.0 && isfinite(xray_max);
+                    st->xray_pending = ok ? 1 : 0;
+                    if (ok) {
+                        st->xray_buf ^= 1;
+                        st->xray_scale = 1.0 / xray_max;
+                        st->xray_obj = obj[8] * st->xray_scale;
                     }
                 }
-                st->ray_base = 1;  // this check's y and A^T y are stored
+                st->ray_base = 1;  // this check's x, A x, y and A^T y are stored
             }
-            if (infeasible) {
+            if (infeasible || unbounded) {
                 st->done = 1;
-                st->status = PDHG_STATUS_PRIMAL_INFEASIBLE;
+                st->status = infeasible ? PDHG_STATUS_PRIMAL_INFEASIBLE : PDHG_STATUS_DUAL_INFEASIBLE;
                 st->stop_iter = it_idx + 1;
             } else if (conv) {  // pdhg.cpp:383-389
                 st->done = 1;
@@ -793,8 +834,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 4 : 3) fast_check(Fas
                     st->stop_iter = it_idx + 1;
                 }
             }
-            // a restart moves y: the next check has no base to difference with
-            if (a.infeas && st->restart) st->ray_base = 0;
+            // a restart moves x and y: the next check has no base to difference with
+            if (INF && st->restart) st->ray_base = 0;
         }
     }
     st->iter += a.period_iters;
@@ -938,12 +979,45 @@ int fast_launches_per_iteration(const FastIter<T>& a) {
     return pass_launches(a.AT) + pass_launches(a.A);
 }
 
+// Ray test, rows' half: after a check that left a pending ray d (projected
+// onto the columns' recession cones, scaled units), the largest amount by
+// which A_o d_o = (A_s d_s) / rs leaves a row's recession cone, one warp per
+// row (original-space values, FP64), into ACC_XRAY_V for the next check.
+// It runs even when that check ended the solve: a solve that goes on (the
+// mixed mode's FP64 phase) tests the ray at its first check. Measuring the
+// same ray again leaves the maximum as it was.
+template <class T>
+__global__ void __launch_bounds__(kBlock) fast_xray_rows(FastCheck<T> a) {
+    const DevState* st = a.st;
+    if (!st->xray_pending) return;
+    const double* d = st->xray_buf ? a.xray_d[1] : a.xray_d[0];
+    const DevCsr& M = a.A;
+    const int lane = threadIdx.x & 31;
+    double v = 0.0;
+    for (int r = (blockIdx.x * kBlock + threadIdx.x) >> 5; r < M.rows; r += (gridDim.x * kBlock) >> 5) {
+        double s = 0.0;
+        for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) s += M.v64[k] * d[M.ci[k]];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        v = smax(v, cone_violation(s / a.P.rs[r], a.P.rlo_o[r], a.P.rhi_o[r]));
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0 && v > 0.0)
+        atomicMax(&a.st->acc[ACC_XRAY_V], static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
 template <class T>
 void launch_fast_check(const FastCheck<T>& a, cudaStream_t s) {
     int grid = check_blocks(a.A) + check_blocks(a.AT);
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid == 0) grid = 1;
-    fast_check<T><<<grid, kBlock, 0, s>>>(a);
+    if (a.infeas) {
+        fast_check<T, true><<<grid, kBlock, 0, s>>>(a);
+        const int rows_grid = (a.A.rows + kBlock / 32 - 1) / (kBlock / 32);
+        const int xg = rows_grid < a.grid_cap || a.grid_cap <= 0 ? rows_grid : a.grid_cap;
+        fast_xray_rows<T><<<xg > 0 ? xg : 1, kBlock, 0, s>>>(a);
+    } else {
+        fast_check<T, false><<<grid, kBlock, 0, s>>>(a);
+    }
     if (a.want_candidate) {
         const int32_t nmax = a.P.n > a.P.m ? a.P.n : a.P.m;
         if (nmax > 0) fast_candidate<T><<<(nmax + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);

@@ -24,7 +24,7 @@ from .problem import Problem
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpdhg_b200.so")
 
 STATUS = ["optimal", "iteration_limit", "time_limit", "numerical_failure", "not_solved",
-          "cancelled", "primal_infeasible"]
+          "cancelled", "primal_infeasible", "dual_infeasible"]
 PREC = {"fp64_exact": 0, "mixed": 1, "fp64": 2}
 
 _dp = C.POINTER(C.c_double)
@@ -156,7 +156,9 @@ class PdhgOptions:
     autotune: bool = True
     # engine extension (MIXED / FP64): stop with status "primal_infeasible" and a
     # certificate (PdhgResult.farkas) when the change of y between two checks
-    # proves that no x meets the bounds
+    # proves that no x meets the bounds, or with status "dual_infeasible" and a
+    # ray (PdhgResult.ray) when the change of x between two checks is a
+    # direction of unbounded descent
     infeasibility_detection: bool = False
 
 
@@ -185,6 +187,9 @@ class PdhgResult:
     # status "primal_infeasible": the certificate's row multipliers
     # (sov::FarkasCertificate::row_multipliers, duals.hpp:47-70), max |y_i| = 1
     farkas: Optional[np.ndarray] = None
+    # status "dual_infeasible": the ray d in x, max |d_j| = 1, along which the
+    # objective falls without leaving the bounds (unbounded if feasible)
+    ray: Optional[np.ndarray] = None
 
 
 class CancellationToken:
@@ -243,9 +248,10 @@ def _c_start(o: _Options, keep: list, cancel, x0, y0) -> None:
 
 def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray) -> PdhgResult:
     hp = bool(info.has_point)
-    certified = STATUS[info.status] == "primal_infeasible"
+    farkas = STATUS[info.status] == "primal_infeasible"
+    ray = STATUS[info.status] == "dual_infeasible"
     return PdhgResult(
-        farkas=y.copy() if certified else None,
+        farkas=y.copy() if farkas else None, ray=x.copy() if ray else None,
         status=STATUS[info.status], objective=info.objective,
         primal=x.copy() if hp else np.zeros(0), dual=y.copy() if hp else np.zeros(0),
         reduced_costs=rc.copy() if hp else np.zeros(0),

@@ -59,6 +59,7 @@ def test_status_and_error_strings(pkg):
         "optimal", "iteration_limit", "time_limit", "numerical_failure", "not_solved",
         "cancelled"]
     assert lib.pdhg_status_string(6).decode() == "primal_infeasible"  # engine extension
+    assert lib.pdhg_status_string(7).decode() == "dual_infeasible"  # engine extension
     assert lib.pdhg_error_string(3).decode() == "invalid argument"
     assert lib.pdhg_error_string(6).decode() == "backend error"
 

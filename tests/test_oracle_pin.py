@@ -126,3 +126,31 @@ def test_certificate_checker_is_the_reference(pkg, orc):
     b, rb = orc.reference_certifies(q, [1.0, -1.0])
     assert a == b is False
     _same_ranges(ra, rb)
+
+
+def test_ray_checker_on_known_rays(pkg, orc):
+    # the engine's dual-infeasibility ray test (no reference counterpart),
+    # restated in numpy, on the reference's unbounded smoke model
+    # (min -x1, x1 - x2 <= 5, x >= 0: d = (1, 1) keeps every bound and the
+    # objective falls by 1 along it)
+    p = golden_problem(pkg, load_golden("smoke_tiny_unbounded"))
+    ok, obj, viol = orc.ray_certifies(p, [2.0, 2.0])  # scaled to max |d| = 1
+    assert ok and obj == -1.0 and viol == 0.0
+    ok, obj, viol = orc.ray_certifies(p, [1.0, 0.0])  # x1 - x2 grows past its upper end
+    assert not ok and viol == 1.0
+    ok, obj, viol = orc.ray_certifies(p, [-1.0, -1.0])  # leaves x >= 0, objective rises
+    assert not ok and obj == 1.0
+    assert not orc.ray_certifies(p, [0.0, 0.0])[0]
+    assert not orc.ray_certifies(p, [np.nan, 1.0])[0]
+    # within eps of the cone (1e-7 above the row's end, objective -1): certified
+    assert orc.ray_certifies(p, [1.0, 1.0 - 1e-7])[0]
+    assert not orc.ray_certifies(p, [1.0, 1.0 - 1e-5])[0]
+    # maximize: max x1 is the same ray
+    q = golden_problem(pkg, load_golden("smoke_tiny_unbounded"))
+    q.c, q.maximize = np.array([1.0, 0.0]), True
+    ok, obj, _ = orc.ray_certifies(q, [1.0, 1.0])
+    assert ok and obj == -1.0
+    # a bounded LP (columns boxed) has no ray
+    b = pkg.lpgen.random_equality_lp(30, 70, 3, seed=5)
+    rng = np.random.default_rng(3)
+    assert not any(orc.ray_certifies(b, rng.standard_normal(b.n))[0] for _ in range(20))
