@@ -333,6 +333,76 @@ int pdhg_scaling(int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
  * to pdhg_scaling's. Host buffers of m and n doubles. */
 int pdhg_get_scaling(pdhg_ctx* ctx, double* row_scale, double* col_scale);
 
+/* ---- MPS reader ----------------------------------------------------------
+ * sov::read_mps_string / sov::read_mps (include/sovereign/io.hpp:57-59,
+ * src/io/mps_reader.cpp): the same dialect, the same model (rows and columns
+ * in file order, the CSR of Problem::Builder::finish with duplicates summed
+ * and zeros dropped, bounds, integrality, names), the same warnings and
+ * error messages, the same fixed-column retry. Host only (no device). */
+
+/* sov::MpsOptions (io.hpp:46-54) + threads. */
+typedef struct pdhg_mps_options {
+    int negative_upper_bound; /* 0 (default) = LowerBecomesMinusInfinity, 1 = KeepLowerAtZero */
+    int keep_free_rows;       /* 1 (default) = non-objective N rows stay as free rows */
+    int threads;              /* host threads; 0 (default) = all hardware threads */
+} pdhg_mps_options;
+
+typedef struct pdhg_model pdhg_model; /* sov::ReadResult (io.hpp:29-33) */
+
+typedef struct pdhg_model_info {
+    int32_t m, n;
+    int64_t nnz;
+    double obj_const;   /* Problem::objective_constant */
+    int maximize;       /* Problem::sense */
+    int32_t warnings;   /* ReadResult::warnings.size() */
+    int fixed_format;   /* 1 when the free-form read failed and the fixed-column one succeeded */
+} pdhg_model_info;
+
+/* MpsOptions{} (io.hpp:46-54): the defaults above. */
+void pdhg_default_mps_options(pdhg_mps_options* options);
+
+/* read_mps_string(text, options, origin) (io.hpp:58-59, mps_reader.cpp:538-564):
+ * MPS text of len bytes (need not be NUL-terminated); origin names it in
+ * messages (NULL = "<string>"). On a malformed model: PDHG_ERR_INVALID_ARGUMENT,
+ * *out = NULL and err (err_cap bytes, may be NULL) gets the reference's
+ * sov::Error message. */
+int pdhg_read_mps(const char* text, size_t len, const char* origin,
+                  const pdhg_mps_options* options, pdhg_model** out, char* err, size_t err_cap);
+/* read_mps(path, options) (io.hpp:57, mps_reader.cpp:566-572): the file's bytes
+ * as they are (no decompression, like the reference), origin = path;
+ * "cannot open '<path>'" when it cannot be read. */
+int pdhg_read_mps_file(const char* path, const pdhg_mps_options* options, pdhg_model** out,
+                       char* err, size_t err_cap);
+/* Frees a model (the ReadResult, io.hpp:29-33). */
+void pdhg_model_free(pdhg_model* model);
+/* Problem::num_rows / num_cols / num_nonzeros / objective_constant / sense
+ * (problem.hpp:52-64) and ReadResult::warnings.size() (io.hpp:31). */
+int pdhg_model_get_info(const pdhg_model* model, pdhg_model_info* info);
+/* Problem::matrix / objective / row and column bounds / col_kind
+ * (problem.hpp:56-78), as pointers into the model (valid until
+ * pdhg_model_free), any may be NULL: CSR (m + 1, nnz, nnz), c (n), bounds
+ * (n, n, m, m), is_integer (n, 0 / 1). They go straight into pdhg_load_problem. */
+int pdhg_model_arrays(const pdhg_model* model, const int32_t** row_ptr, const int32_t** col_idx,
+                      const double** values, const double** c, const double** col_lo,
+                      const double** col_hi, const double** row_lo, const double** row_hi,
+                      const uint8_t** is_integer);
+/* Problem::name (problem.hpp:83): the NAME card. */
+const char* pdhg_model_name(const pdhg_model* model);
+/* Problem::objective_name (problem.hpp:84): the first N row. */
+const char* pdhg_model_objective_name(const pdhg_model* model);
+/* Problem::row_names()[i] (problem.hpp:85); NULL when out of range. */
+const char* pdhg_model_row_name(const pdhg_model* model, int32_t i);
+/* Problem::col_names()[j] (problem.hpp:86); NULL when out of range. */
+const char* pdhg_model_col_name(const pdhg_model* model, int32_t j);
+/* Problem::row_names / col_names (problem.hpp:85-86) at once: row (columns = 0)
+ * or column (columns = 1) name k is the NUL-terminated string at
+ * chars + offsets[k]; offsets has count + 1 entries. */
+int pdhg_model_name_table(const pdhg_model* model, int columns, const char** chars,
+                          const int64_t** offsets);
+/* ReaderWarning k (io.hpp:23-27): line (0 for the layout note), section, text. */
+int pdhg_model_warning(const pdhg_model* model, int32_t k, int64_t* line, const char** section,
+                       const char** message);
+
 #ifdef __cplusplus
 }
 #endif

@@ -368,3 +368,62 @@ def ray_certifies(p, d, eps: float = 1e-6):
     viol = max(cone(d, p.col_lo, p.col_hi), cone(ad, p.row_lo, p.row_hi))
     ok = obj < 0.0 and viol <= eps and viol <= eps * -obj
     return ok, obj, viol
+
+
+def reference_read_mps(text, origin: str = "<string>", keep_lower_at_zero: bool = False,
+                       keep_free_rows: bool = True) -> dict:
+    """The reference's own read_mps_string(text, MpsOptions, origin)
+    (src/io/mps_reader.cpp:506-533) -> the model's arrays, names, integrality
+    and warnings; {"error": message} when it throws."""
+    lib = ref_lib()
+    if not getattr(lib, "_mps_declared", False):
+        vp = C.c_void_p
+        lib.ref_read_mps.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_int, C.c_int,
+                                     C.c_char_p, C.c_size_t]
+        lib.ref_read_mps.restype = vp
+        lib.ref_model_kinds.argtypes = [vp, C.POINTER(C.c_uint8)]
+        for f in ("ref_model_name", "ref_model_objective_name"):
+            getattr(lib, f).argtypes = [vp]
+            getattr(lib, f).restype = C.c_char_p
+        for f in ("ref_model_row_name", "ref_model_col_name"):
+            getattr(lib, f).argtypes = [vp, C.c_int32]
+            getattr(lib, f).restype = C.c_char_p
+        lib.ref_model_n_warnings.argtypes = [vp]
+        lib.ref_model_n_warnings.restype = C.c_int32
+        lib.ref_model_warning.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]
+        lib._mps_declared = True
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    err = C.create_string_buffer(4096)
+    h = lib.ref_read_mps(data, len(data), origin.encode(), int(keep_lower_at_zero),
+                         int(keep_free_rows), err, len(err))
+    if not h:
+        return {"error": err.value.decode(errors="replace")}
+    try:
+        m, n, nnz, mx, oc = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int(), C.c_double()
+        lib.ref_model_shape(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(oc))
+        M, N, K = m.value, n.value, nnz.value
+        rp = np.zeros(M + 1, dtype=np.int32)
+        ci = np.zeros(max(K, 1), dtype=np.int32)
+        va = np.zeros(max(K, 1))
+        c, cl, ch = np.zeros(max(N, 1)), np.zeros(max(N, 1)), np.zeros(max(N, 1))
+        rl, rh = np.zeros(max(M, 1)), np.zeros(max(M, 1))
+        lib.ref_model_arrays(h, _i(rp), _i(ci), _d(va), _d(c), _d(cl), _d(ch), _d(rl), _d(rh))
+        kinds = np.zeros(max(N, 1), dtype=np.uint8)
+        lib.ref_model_kinds(h, kinds.ctypes.data_as(C.POINTER(C.c_uint8)))
+        warnings = []
+        for k in range(lib.ref_model_n_warnings(h)):
+            line, sec, msg = C.c_int64(), C.c_char_p(), C.c_char_p()
+            lib.ref_model_warning(h, k, C.byref(line), C.byref(sec), C.byref(msg))
+            warnings.append((line.value, sec.value.decode(), msg.value.decode()))
+        return {"m": M, "n": N, "row_ptr": rp, "col_idx": ci[:K], "val": va[:K], "c": c[:N],
+                "col_lo": cl[:N], "col_hi": ch[:N], "row_lo": rl[:M], "row_hi": rh[:M],
+                "obj_const": oc.value, "maximize": bool(mx.value),
+                "is_integer": kinds[:N].astype(bool),
+                "name": lib.ref_model_name(h).decode(),
+                "objective_name": lib.ref_model_objective_name(h).decode(),
+                "row_names": [lib.ref_model_row_name(h, i).decode() for i in range(M)],
+                "col_names": [lib.ref_model_col_name(h, j).decode() for j in range(N)],
+                "warnings": warnings}
+    finally:
+        lib.ref_model_free(h)

@@ -171,6 +171,7 @@ sov::PdhgOptions to_options(const orc_options* o) {
 
 struct Loaded {
     sov::Problem problem;
+    std::vector<sov::ReaderWarning> warnings;
 };
 
 }  // namespace
@@ -295,10 +296,57 @@ int ref_backend_spmv(int transpose, int32_t m, int32_t n, int64_t nnz, const int
 void* ref_read_model_string(const char* text, int is_mps) {
     try {
         sov::ReadResult r = is_mps ? sov::read_mps_string(text) : sov::read_lp_string(text);
-        return new Loaded{std::move(r.problem)};
+        return new Loaded{std::move(r.problem), std::move(r.warnings)};
     } catch (const std::exception&) {
         return nullptr;
     }
+}
+
+// read_mps_string(text, MpsOptions, origin) with the options spelled out; on
+// an error the handle is null and err gets e.what().
+void* ref_read_mps(const char* text, size_t len, const char* origin, int keep_lower_at_zero,
+                   int keep_free_rows, char* err, size_t err_cap) {
+    err[0] = '\0';
+    try {
+        sov::MpsOptions o;
+        o.negative_upper_bound = keep_lower_at_zero
+                                     ? sov::NegativeUpperBoundRule::KeepLowerAtZero
+                                     : sov::NegativeUpperBoundRule::LowerBecomesMinusInfinity;
+        o.keep_free_rows = keep_free_rows != 0;
+        sov::ReadResult r = sov::read_mps_string(std::string(text, len), o, origin);
+        return new Loaded{std::move(r.problem), std::move(r.warnings)};
+    } catch (const std::exception& e) {
+        std::strncpy(err, e.what(), err_cap - 1);
+        err[err_cap - 1] = '\0';
+        return nullptr;
+    }
+}
+
+void ref_model_kinds(void* h, uint8_t* is_integer) {
+    const sov::Problem& p = static_cast<Loaded*>(h)->problem;
+    for (sov::Idx j = 0; j < p.num_cols(); ++j)
+        is_integer[j] = p.col_kind()[j] == sov::VarKind::Integer ? 1 : 0;
+}
+
+const char* ref_model_name(void* h) { return static_cast<Loaded*>(h)->problem.name().c_str(); }
+const char* ref_model_objective_name(void* h) {
+    return static_cast<Loaded*>(h)->problem.objective_name().c_str();
+}
+const char* ref_model_row_name(void* h, int32_t i) {
+    return static_cast<Loaded*>(h)->problem.row_names()[i].c_str();
+}
+const char* ref_model_col_name(void* h, int32_t j) {
+    return static_cast<Loaded*>(h)->problem.col_names()[j].c_str();
+}
+int32_t ref_model_n_warnings(void* h) {
+    return static_cast<int32_t>(static_cast<Loaded*>(h)->warnings.size());
+}
+void ref_model_warning(void* h, int32_t k, int64_t* line, const char** section,
+                       const char** message) {
+    const sov::ReaderWarning& w = static_cast<Loaded*>(h)->warnings[static_cast<size_t>(k)];
+    *line = w.line;
+    *section = w.section.c_str();
+    *message = w.message.c_str();
 }
 
 void ref_model_shape(void* h, int32_t* m, int32_t* n, int64_t* nnz, int* maximize,
