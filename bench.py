@@ -392,6 +392,63 @@ def profile_case(args) -> None:
                       "tuning": tuning}))
 
 
+def mps_reader_line(args) -> None:
+    """Read throughput of the MPS reader (host threads, no device): the
+    transportation LP of --supplies x --demands written as MPS text, read by
+    pdhg_read_mps with all host threads and with one; the reference's
+    read_mps_string (oracle/_ref, one thread, as it is written) on the same
+    model at --mps-ref-supplies supplies. Bytes of text per second."""
+    import ctypes as C
+    pkg = importlib.import_module("sovereign-solver_b200")
+    L = pkg.mps._lib()
+
+    def text_of(supplies):
+        p = pkg.lpgen.transportation_lp(supplies, args.demands, seed=1000)
+        return pkg.mps.write_mps(p).encode(), p
+
+    def ours(text, threads):
+        o = pkg.mps._MpsOptions(0, 1, threads)
+        h, err = C.c_void_p(), C.create_string_buffer(4096)
+        t = time.perf_counter()
+        rc = L.pdhg_read_mps(text, len(text), None, C.byref(o), C.byref(h), err, len(err))
+        dt = time.perf_counter() - t
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        L.pdhg_model_free(h)
+        return dt
+
+    text, p = text_of(args.supplies)
+    cores = os.cpu_count() or 1
+    all_t = min(ours(text, 0) for _ in range(3))
+    one_t = ours(text, 1)
+    line = {"metric": "mps_read_throughput", "value": round(len(text) / all_t / 1e6, 1),
+            "unit": "MB/s", "higher_is_better": True, "threads": cores,
+            "seconds": round(all_t, 3), "single_thread_MBps": round(len(text) / one_t / 1e6, 1),
+            "config": {"workload": f"transportation {args.supplies}x{args.demands} as MPS text",
+                       "bytes": len(text), "rows": p.m, "columns": p.n, "nonzeros": p.nnz},
+            "data": "synthetic"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc  # the reference reader, where oracle/_ref is built
+    if orc.ref_available() and args.mps_ref_supplies > 0:
+        rtext, rp = text_of(args.mps_ref_supplies)
+        R = orc.ref_lib()
+        orc.reference_read_mps("ROWS\n N c\n")  # declares the entry points
+        err = C.create_string_buffer(4096)
+        t = time.perf_counter()
+        h = R.ref_read_mps(rtext, len(rtext), b"<string>", 0, 1, err, len(err))
+        rt = time.perf_counter() - t
+        R.ref_model_free(h)
+        ours_same = min(ours(rtext, 0) for _ in range(3))
+        line["reference"] = {"value": round(len(rtext) / rt / 1e6, 1), "unit": "MB/s", "cores": 1,
+                             "kind": "reference", "seconds": round(rt, 3),
+                             "sample": f"transportation {args.mps_ref_supplies}x{args.demands} "
+                                       f"({len(rtext)} bytes, {rp.nnz} nonzeros)",
+                             "ours_on_the_sample_MBps": round(len(rtext) / ours_same / 1e6, 1)}
+    else:
+        line["reference"] = {"unavailable": "oracle/_ref not built"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -420,7 +477,14 @@ def main() -> None:
                          "iterations, nothing else")
     ap.add_argument("--supplies", type=int, default=SUPPLIES)
     ap.add_argument("--demands", type=int, default=DEMANDS)
+    ap.add_argument("--mps-reader", action="store_true",
+                    help="measure the MPS reader instead (host only, one JSON line)")
+    ap.add_argument("--mps-ref-supplies", type=int, default=200,
+                    help="supplies of the model the reference's reader is timed on")
     args = ap.parse_args()
+    if args.mps_reader:
+        mps_reader_line(args)
+        return
     if args.profile_case:
         profile_case(args)
         return

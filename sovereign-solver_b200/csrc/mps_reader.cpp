@@ -879,82 +879,130 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     const int64_t F = base[T];
     std::vector<std::string_view> fname(static_cast<size_t>(F));  // by flat id
     std::vector<uint64_t> fhash(static_cast<size_t>(F));
+    const int S = std::max(1, threads_);
+    // flat ids of each chunk, bucketed by shard (file order inside a bucket)
+    std::vector<std::vector<std::vector<int64_t>>> bucket(static_cast<size_t>(T));
     parallel_for(threads_, T, [&](int, int64_t cb0, int64_t ce) {
-        for (int64_t c = cb0; c < ce; ++c)
+        for (int64_t c = cb0; c < ce; ++c) {
+            auto& bk = bucket[static_cast<size_t>(c)];
+            bk.assign(static_cast<size_t>(S), {});
             for (int32_t l = 0; l < ch[c].names.size(); ++l) {
-                fname[base[c] + l] = ch[c].names.get(l);
-                fhash[base[c] + l] = ch[c].hash[static_cast<size_t>(l)];
+                const int64_t f = base[c] + l;
+                const uint64_t h = ch[c].hash[static_cast<size_t>(l)];
+                fname[f] = ch[c].names.get(l);
+                fhash[f] = h;
+                bk[(h >> 40) % static_cast<uint64_t>(S)].push_back(f);
             }
+        }
     });
     clk.mark("merge: flat ids");
     auto name_of = [&](int64_t f) { return fname[static_cast<size_t>(f)]; };
     auto hash_of = [&](int64_t f) { return fhash[static_cast<size_t>(f)]; };
     std::vector<int64_t> src(static_cast<size_t>(F));
-    const int S = std::max(1, threads_);
     const bool have_cols = b.col_names.size() > 0;
     parallel_for(S, S, [&](int, int64_t sb, int64_t se) {
         for (int64_t sh = sb; sh < se; ++sh) {
-            std::vector<int64_t> mine;
-            const uint64_t* hv = fhash.data();
-            for (int64_t f = 0; f < F; ++f)
-                if (static_cast<int64_t>((hv[f] >> 40) % static_cast<uint64_t>(S)) == sh) mine.push_back(f);
+            size_t count = 0;
+            for (int c = 0; c < T; ++c) count += bucket[c][static_cast<size_t>(sh)].size();
             size_t cap = 16;
-            while (cap < 2 * mine.size()) cap <<= 1;
+            while (cap < 2 * count) cap <<= 1;
             std::vector<int64_t> table(cap, -1);
             const uint64_t mask = cap - 1;
-            for (int64_t f : mine) {
-                const uint64_t h = hash_of(f);
-                const std::string_view nm = name_of(f);
-                if (have_cols) {
-                    const int32_t j = b.col_idx.find(nm, h);
-                    if (j >= 0) {
-                        src[f] = j;
-                        continue;
+            for (int c = 0; c < T; ++c) {
+                for (int64_t f : bucket[c][static_cast<size_t>(sh)]) {
+                    const uint64_t h = hash_of(f);
+                    const std::string_view nm = name_of(f);
+                    if (have_cols) {
+                        const int32_t j = b.col_idx.find(nm, h);
+                        if (j >= 0) {
+                            src[f] = j;
+                            continue;
+                        }
                     }
-                }
-                uint64_t q = h & mask;
-                for (;;) {
-                    const int64_t g = table[q];
-                    if (g < 0) {
-                        table[q] = f;
-                        src[f] = -1;
-                        break;
+                    uint64_t q = h & mask;
+                    for (;;) {
+                        const int64_t g = table[q];
+                        if (g < 0) {
+                            table[q] = f;
+                            src[f] = -1;
+                            break;
+                        }
+                        if (name_of(g) == nm) {
+                            src[f] = -2 - g;
+                            break;
+                        }
+                        q = (q + 1) & mask;
                     }
-                    if (name_of(g) == nm) {
-                        src[f] = -2 - g;
-                        break;
-                    }
-                    q = (q + 1) & mask;
                 }
             }
         }
     });
+    bucket.clear();
     clk.mark("merge: shards");
-    // numbering in file order (sequential, integers only)
+    // numbering in file order: first appearances counted per block, a prefix
+    // over the blocks, then each block numbers its own; repeats take the
+    // number of the first appearance they point at
     const int64_t n0 = b.col_names.size();
     std::vector<int32_t> id(static_cast<size_t>(F));
-    std::vector<int64_t> fresh;  // flat ids of the new columns, in order
-    for (int64_t f = 0; f < F; ++f) {
-        const int64_t v = src[f];
-        if (v == -1) {
-            id[f] = static_cast<int32_t>(n0 + static_cast<int64_t>(fresh.size()));
-            fresh.push_back(f);
-        } else if (v >= 0) {
-            id[f] = static_cast<int32_t>(v);
-        } else {
-            id[f] = id[-2 - v];
+    const int64_t NB = std::max<int64_t>(1, std::min<int64_t>(F / 65536 + 1, 4 * threads_));
+    std::vector<int64_t> firsts(static_cast<size_t>(NB) + 1, 0);
+    parallel_for(threads_, NB, [&](int, int64_t bb, int64_t be) {
+        for (int64_t q = bb; q < be; ++q) {
+            int64_t k = 0;
+            for (int64_t f = F * q / NB; f < F * (q + 1) / NB; ++f) k += src[f] == -1;
+            firsts[q + 1] = k;
         }
-    }
-    clk.mark("merge: numbering");
-    const int64_t nn = static_cast<int64_t>(fresh.size());
+    });
+    for (int64_t q = 0; q < NB; ++q) firsts[q + 1] += firsts[q];
+    const int64_t nn = firsts[NB];
     if (n0 + nn > std::numeric_limits<int32_t>::max() - 1)
         throw ReadError{"too many rows or columns for 32-bit indices"};
-    // new names into the arena (offsets in order, bytes by threads) and the index
+    std::vector<int64_t> fresh(static_cast<size_t>(nn));  // flat ids of the new columns, in order
+    parallel_for(threads_, NB, [&](int, int64_t bb, int64_t be) {
+        for (int64_t q = bb; q < be; ++q) {
+            int64_t k = firsts[q];
+            for (int64_t f = F * q / NB; f < F * (q + 1) / NB; ++f) {
+                if (src[f] == -1) {
+                    id[f] = static_cast<int32_t>(n0 + k);
+                    fresh[k++] = f;
+                } else if (src[f] >= 0) {
+                    id[f] = static_cast<int32_t>(src[f]);
+                }
+            }
+        }
+    });
+    parallel_for(threads_, NB, [&](int, int64_t bb, int64_t be) {
+        for (int64_t q = bb; q < be; ++q)
+            for (int64_t f = F * q / NB; f < F * (q + 1) / NB; ++f)
+                if (src[f] <= -2) id[f] = id[-2 - src[f]];
+    });
+    clk.mark("merge: numbering");
+    // new names into the arena (offsets by a blocked prefix, bytes by
+    // threads) and into the index
     Arena& A = b.col_names;
     std::vector<int64_t>& off = A.off;
     off.resize(static_cast<size_t>(n0 + nn) + 1);
-    for (int64_t k = 0; k < nn; ++k)
-        off[n0 + k + 1] = off[n0 + k] + static_cast<int64_t>(name_of(fresh[k]).size()) + 1;
+    const int64_t NK = std::max<int64_t>(1, std::min<int64_t>(nn / 65536 + 1, 4 * threads_));
+    std::vector<int64_t> boff(static_cast<size_t>(NK) + 1, 0);
+    parallel_for(threads_, NK, [&](int, int64_t bb, int64_t be) {
+        for (int64_t q = bb; q < be; ++q) {
+            int64_t t = 0;
+            for (int64_t k = nn * q / NK; k < nn * (q + 1) / NK; ++k)
+                t += static_cast<int64_t>(name_of(fresh[k]).size()) + 1;
+            boff[q + 1] = t;
+        }
+    });
+    boff[0] = off[n0];
+    for (int64_t q = 0; q < NK; ++q) boff[q + 1] += boff[q];
+    parallel_for(threads_, NK, [&](int, int64_t bb, int64_t be) {
+        for (int64_t q = bb; q < be; ++q) {
+            int64_t o = boff[q];
+            for (int64_t k = nn * q / NK; k < nn * (q + 1) / NK; ++k) {
+                o += static_cast<int64_t>(name_of(fresh[k]).size()) + 1;
+                off[n0 + k + 1] = o;
+            }
+        }
+    });
     A.chars.resize(static_cast<size_t>(off[n0 + nn]));
     b.col_idx.reserve(static_cast<size_t>(n0 + nn));
     int32_t* slots = b.col_idx.slot.data();
