@@ -189,24 +189,14 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
     }
 }
 
-// long_mode 2: every row above short_max as warp work items (a whole row, or
-// a segment of a longer one); no block barrier anywhere, each warp finishes
-// on its own.
+// One warp work item of long_mode 2 (warp-uniform): a whole row, or a segment
+// of a longer one whose last warp adds the segments in order.
 template <class T, bool PRIMAL>
-__global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
-    fast_iter_witems(FastIter<T> a, int first, int reset) {
-    DevState* st = a.st;
-    iter_reset(st, reset);
-    if (st->done) return;
-    const DevCsr& M = PRIMAL ? a.AT : a.A;
-    const RowItems& L = M.items_warp;
-    const int idx = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-    if (idx >= L.n_item) return;
+__device__ __forceinline__ void warp_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
+                                          int idx, int first, bool fresh, T tau, T sigma) {
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     const PV<T> pv = pvec<T>(a.P);
-    const bool fresh = first && st->fresh;
-    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
     const int lane = threadIdx.x & 31;
     const int4 w = __ldg(L.item + idx);
     EpiIn<T> in{};
@@ -219,6 +209,22 @@ __global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
     }
     if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+}
+
+// long_mode 2: every row above short_max as warp work items; no block barrier
+// anywhere, each warp finishes on its own.
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
+    fast_iter_witems(FastIter<T> a, int first, int reset) {
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const int idx = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    if (idx >= M.items_warp.n_item) return;
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    warp_item<T, PRIMAL>(a, M, M.items_warp, idx, first, fresh, tau, sigma);
 }
 
 template <class T>
@@ -304,8 +310,10 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
 }
 
 // The row-slice kernel: a persistent grid (the resident CTAs) whose warps
-// claim slice items one by one from S.fetch.
-template <class T, bool PRIMAL>
+// claim items one by one from S.fetch. With long_mode 2 (WITEMS) the queue
+// goes on past the slice items into the warp items of the other long rows, so
+// one kernel and one tail cover every long row of the pass.
+template <class T, bool PRIMAL, bool WITEMS>
 __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     fast_iter_slices(FastIter<T> a, int first, int reset) {
     DevState* st = a.st;
@@ -315,10 +323,13 @@ __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     const RowSlices& S = M.slices;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const int ns = S.n_item;
+    const int nt = ns + (WITEMS ? M.items_warp.n_item : 0);
     for (;;) {
         const int idx = warp_fetch(S.fetch);
-        if (idx >= S.n_item) break;
-        slice_item<T, PRIMAL>(a, S, idx, first, fresh, tau, sigma);
+        if (idx >= nt) break;
+        if (!WITEMS || idx < ns) slice_item<T, PRIMAL>(a, S, idx, first, fresh, tau, sigma);
+        else warp_item<T, PRIMAL>(a, M, M.items_warp, idx - ns, first, fresh, tau, sigma);
     }
     warp_exit(S.fetch);
 }
@@ -370,8 +381,15 @@ inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
     if (M.rows == 0) return p;
     p.shrt = short_blocks_for(M);
     const int mode = M.long_mode;
+    const bool sliced = M.use_slices && M.slices.n_item > 0;
     const int nw = mode == 2 ? M.items_warp.n_item : mode == 1 ? M.n_warp1 : M.n_warp0;
     p.warp = (nw + kBlock / 32 - 1) / (kBlock / 32);
+    if (mode == 2 && sliced) {
+        // the slice kernel takes the warp items too (fast_iter_slices)
+        p.warp = 0;
+        p.slc = std::min((M.slices.n_item + nw + kBlock / 32 - 1) / (kBlock / 32), std::max(cap_slice, 1));
+        return p;
+    }
     if (mode == 2) {
         p.lng = p.warp;
     } else {
@@ -434,7 +452,10 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
             else fast_iter_long<T, PRIMAL, 0, true><<<p.lng, kBlock, 0, ls>>>(a, first, reset_long, mb);
         }
     }
-    if (p.slc > 0) fast_iter_slices<T, PRIMAL><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
+    if (p.slc > 0 && mode == 2)
+        fast_iter_slices<T, PRIMAL, true><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
+    else if (p.slc > 0)
+        fast_iter_slices<T, PRIMAL, false><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
     if (p.shrt > 0) {
         const int sb = p.shrt;
         switch (iter_lanes(M)) {
@@ -956,8 +977,8 @@ int init_fast_kernels(int device) {
         return 1;
     const int l32 = resident_per_sm(fast_iter_long<float, false, 0, false>);
     const int l64 = resident_per_sm(fast_iter_long<double, false, 0, false>);
-    const int s32 = resident_per_sm(fast_iter_slices<float, false>);
-    const int s64 = resident_per_sm(fast_iter_slices<double, false>);
+    const int s32 = resident_per_sm(fast_iter_slices<float, false, false>);
+    const int s64 = resident_per_sm(fast_iter_slices<double, false, false>);
     if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0) return 1;
     g_cap_long[0] = l32 * sms;
     g_cap_long[1] = l64 * sms;
