@@ -82,8 +82,8 @@ struct SlicesDev {
     DBuf<int2> split;
     DBuf<int32_t> row, rlen, col;
     DBuf<float> v32;
-    DBuf<double> v64, part;
-    DBuf<unsigned int> ticket, fetch;
+    DBuf<double> v64, part, cpart;
+    DBuf<unsigned int> ticket, fetch, cticket;
     int32_t n_slice = 0, n_item = 0;
     RowSlices view() const {
         RowSlices v;
@@ -100,6 +100,8 @@ struct SlicesDev {
         v.ticket = ticket.p;
         v.part = part.p;
         v.fetch = fetch.p;
+        v.cticket = cticket.p;
+        v.cpart = cpart.p;
         return v;
     }
 };
@@ -475,9 +477,14 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
         (e = upload(S.item, items, s)) != cudaSuccess || (e = upload(S.split, splits, s)) != cudaSuccess ||
         (e = S.ticket.alloc(splits.size())) != cudaSuccess ||
         (e = S.part.alloc(32 * items.size())) != cudaSuccess ||
+        (e = S.cticket.alloc(splits.size())) != cudaSuccess ||
+        (e = S.cpart.alloc(64 * items.size())) != cudaSuccess ||
         (e = S.fetch.alloc(2)) != cudaSuccess)
         return cuda_fail(err, e, "build_slices");
-    if (!splits.empty()) cudaMemsetAsync(S.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    if (!splits.empty()) {
+        cudaMemsetAsync(S.ticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+        cudaMemsetAsync(S.cticket.p, 0, sizeof(unsigned int) * splits.size(), s);
+    }
     cudaMemsetAsync(S.fetch.p, 0, 2 * sizeof(unsigned int), s);
     launch_fill_slices(M.view(), S.view(), S.col.p, S.v32.p, S.v64.p, total, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");

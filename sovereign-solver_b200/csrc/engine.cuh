@@ -74,6 +74,8 @@ struct RowSlices {
     unsigned int* ticket = nullptr;  // per split slice, 0 between launches
     double* part = nullptr;          // 32 partials per item
     unsigned int* fetch = nullptr;   // {next item, exits}, 0 between launches
+    unsigned int* cticket = nullptr; // the check's: per split slice, 0 between launches
+    double* cpart = nullptr;         // the check's: 64 partials per item (current, average)
 };
 
 // The long-row tiers of the throughput kernels (see DevCsr).

@@ -650,27 +650,121 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
     }
 }
 
+// The check over row slices: a virtual block is up to 8 slice items, one per
+// warp, lane l on the slice's row l, so the index, FP64 value and gather loads
+// of a step are coalesced where the rows gather consecutive columns (the
+// demand rows of a transportation LP). Each lane sums in k order; a slice cut
+// into several items combines each lane's two sums in item order through the
+// check's own ticket and partials.
+template <class T, bool ROWS, bool INF>
+__device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, double inv, Terms& t) {
+    const RowSlices& S = M.slices;
+    const int idx = vb * (kBlock / 32) + (threadIdx.x >> 5);
+    if (idx >= S.n_item) return;  // warp-uniform
+    const int lane = threadIdx.x & 31;
+    const int4 w = __ldg(S.item + idx);
+    const int4 d = __ldg(S.slice + w.x);
+    const int row = __ldg(S.row + 32 * w.x + lane);
+    const int kend = min(w.z, __ldg(S.rlen + 32 * w.x + lane));
+    const int32_t* __restrict__ col = S.col + d.y + lane;
+    const double* __restrict__ val = S.v64 + d.y + lane;
+    double ac = 0.0, aa = 0.0;
+    int k = w.y;
+    for (; k + 2 <= kend; k += 2) {
+        int j[2];
+        double v[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            j[u] = __ldcs(col + 32 * static_cast<int64_t>(k + u));
+            v[u] = __ldcs(val + 32 * static_cast<int64_t>(k + u));
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (ROWS) {
+                ac += v[u] * static_cast<double>(a.it.x[j[u]]);
+                aa += v[u] * avg_x(a.it, j[u], inv);
+            } else {
+                ac += v[u] * static_cast<double>(a.it.y[j[u]]);
+                aa += v[u] * avg_y(a.it, j[u], inv);
+            }
+        }
+    }
+    for (; k < kend; ++k) {
+        const int j = __ldcs(col + 32 * static_cast<int64_t>(k));
+        const double v = __ldcs(val + 32 * static_cast<int64_t>(k));
+        if (ROWS) {
+            ac += v * static_cast<double>(a.it.x[j]);
+            aa += v * avg_x(a.it, j, inv);
+        } else {
+            ac += v * static_cast<double>(a.it.y[j]);
+            aa += v * avg_y(a.it, j, inv);
+        }
+    }
+    if (w.w >= 0) {  // warp-uniform
+        S.cpart[64 * static_cast<int64_t>(idx) + lane] = ac;
+        S.cpart[64 * static_cast<int64_t>(idx) + 32 + lane] = aa;
+        __threadfence();
+        __syncwarp();
+        const int2 sp = __ldg(S.split + w.w);
+        int last = 0;
+        if (lane == 0) last = atomicAdd(S.cticket + w.w, 1u) == static_cast<unsigned>(sp.y - 1) ? 1 : 0;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) return;
+        __threadfence();
+        double sc = 0.0, sa = 0.0;
+        for (int q = sp.x; q < sp.x + sp.y; ++q) {
+            sc += __ldcg(S.cpart + 64 * static_cast<int64_t>(q) + lane);
+            sa += __ldcg(S.cpart + 64 * static_cast<int64_t>(q) + 32 + lane);
+        }
+        if (lane == 0) S.cticket[w.w] = 0u;
+        ac = sc;
+        aa = sa;
+    }
+    if (row >= 0) row_or_col_terms<T, ROWS, INF>(a, row, ac, aa, inv, t);
+}
+
 // Virtual blocks of the check over one matrix: short-row blocks (M.vw lanes
-// per row), warp-row blocks, CTA items.
+// per row), warp-row blocks, CTA items, slice blocks (8 slice items each).
 __host__ __device__ inline int check_short_blocks(const DevCsr& M) {
     if (M.n_iter_short == 0) return 0;
     return static_cast<int>((static_cast<int64_t>(M.rows) * M.vw + kBlock - 1) / kBlock);
 }
 __host__ __device__ inline int check_warp_blocks(const DevCsr& M) { return (M.n_warp0 + kBlock / 32 - 1) / (kBlock / 32); }
+__host__ __device__ inline int check_slice_blocks(const DevCsr& M) {
+    return M.slices.n_item > 0 ? (M.slices.n_item + kBlock / 32 - 1) / (kBlock / 32) : 0;
+}
 inline int check_blocks(const DevCsr& M) {
-    return check_short_blocks(M) + check_warp_blocks(M) + M.items_long.n_item;
+    return check_short_blocks(M) + check_warp_blocks(M) + M.items_long.n_item + check_slice_blocks(M);
+}
+
+// The matrix the check walks: where the matrix has row slices (whether or
+// not the iteration passes use them), the long-row tiers without the slices'
+// rows, the slices covering those rows.
+inline DevCsr check_view(const DevCsr& M) {
+    if (M.slices.n_item == 0) return M;
+    DevCsr X = M;
+    const LongTiers& t = M.no_slice_tiers;
+    X.warp_rows0 = t.warp_rows0;
+    X.warp_rows1 = t.warp_rows1;
+    X.n_warp0 = t.n_warp0;
+    X.n_warp1 = t.n_warp1;
+    X.items_long = t.items_long;
+    X.items_huge = t.items_huge;
+    X.items_warp = t.items_warp;
+    return X;
 }
 
 // Grid-stride over the virtual blocks of A (act = A x, current and average)
 // then of A^T (aty = A^T y); the grid itself is capped (a few CTAs per SM),
 // so each CTA sums its rows into per-thread running terms and takes part in
-// one reduction. Compiled to fit four CTAs per SM in FP32 (64 registers) and
-// three in FP64 (80), both without spills; unbounded it took 109-118
-// registers and two CTAs per SM. The instance with the infeasibility tests
-// (INF) carries 11 more running terms: three CTAs per SM in FP32 (80) and two
-// in FP64 (122), also without spills.
+// one reduction. FP64 fits three CTAs per SM (80 registers, no spills). FP32
+// keeps four (64 registers): with the slice walk that spills about 140 bytes,
+// yet on the 10M-column transportation LP it ran 416 us against 517 at three
+// CTAs without spills (and 484 before the slice walk). Unbounded it took
+// 109-118 registers and two CTAs per SM. The instance with the infeasibility
+// tests (INF) carries 11 more running terms: two CTAs per SM.
 template <class T, bool INF>
-__global__ void __launch_bounds__(kBlock, INF ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 4 : 3))
+__global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
     fast_check(FastCheck<T> a) {
     DevState* st = a.st;
     if (st->done) return;
@@ -679,11 +773,14 @@ __global__ void __launch_bounds__(kBlock, INF ? (sizeof(T) == 4 ? 3 : 2) : (size
     Terms t;
     const int sbA = check_short_blocks(a.A), wbA = check_warp_blocks(a.A);
     const int sbT = check_short_blocks(a.AT), wbT = check_warp_blocks(a.AT);
-    const int nA = sbA + wbA + a.A.items_long.n_item;
-    const int nT = sbT + wbT + a.AT.items_long.n_item;
+    const int pA = sbA + wbA + a.A.items_long.n_item, pT = sbT + wbT + a.AT.items_long.n_item;
+    const int nA = pA + check_slice_blocks(a.A);
+    const int nT = pT + check_slice_blocks(a.AT);
     for (int bid = blockIdx.x; bid < nA + nT; bid += gridDim.x) {
-        if (bid < nA) check_part<T, true, INF>(a, a.A, bid, sbA, wbA, inv, t);
-        else check_part<T, false, INF>(a, a.AT, bid - nA, sbT, wbT, inv, t);
+        if (bid < pA) check_part<T, true, INF>(a, a.A, bid, sbA, wbA, inv, t);
+        else if (bid < nA) check_slices<T, true, INF>(a, a.A, bid - pA, inv, t);
+        else if (bid < nA + pT) check_part<T, false, INF>(a, a.AT, bid - nA, sbT, wbT, inv, t);
+        else check_slices<T, false, INF>(a, a.AT, bid - nA - pT, inv, t);
     }
     block_max_terms<INF>(t, st->acc);
     // per-CTA partial sums, kCheckSums per CTA: the objectives [0..3]
@@ -1027,7 +1124,10 @@ __global__ void __launch_bounds__(kBlock) fast_xray_rows(FastCheck<T> a) {
 }
 
 template <class T>
-void launch_fast_check(const FastCheck<T>& a, cudaStream_t s) {
+void launch_fast_check(const FastCheck<T>& a0, cudaStream_t s) {
+    FastCheck<T> a = a0;
+    a.A = check_view(a0.A);
+    a.AT = check_view(a0.AT);
     int grid = check_blocks(a.A) + check_blocks(a.AT);
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid == 0) grid = 1;
@@ -1052,7 +1152,7 @@ void launch_fast_restart(const FastCheck<T>& a, cudaStream_t s) {
 
 // Upper bound on check-kernel CTAs (partial-sum buffer sizing).
 int fast_check_grid(const DevCsr& A, const DevCsr& AT) {
-    return check_blocks(A) + check_blocks(AT) + 1;
+    return check_blocks(check_view(A)) + check_blocks(check_view(AT)) + 1;
 }
 
 template int launch_fast_primal<float>(const FastIter<float>&, int, cudaStream_t, const PassFork*);

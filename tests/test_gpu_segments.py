@@ -154,3 +154,56 @@ def test_row_slices_on_a_transportation_lp(tmp_path):
             assert out["obj_gap"] <= 2e-3, (mode, out)
         if mode is not None:
             assert out["fp64"]["dual_long_mode"] == mode, out
+
+
+def _orig_residual(p, x, y, bt):
+    """The check's original-space residual of a candidate (x, y), restated in
+    numpy: max over rows of the bound violation of A x and of the
+    complementary-slackness term of y, and over columns of that of the
+    reduced cost c - A^T y (a finite end within bt of the value is active)."""
+    import numpy as np
+    rows = np.repeat(np.arange(p.m), np.diff(p.row_ptr))
+    act = np.zeros(p.m)
+    np.add.at(act, rows, p.val * x[p.col_idx])
+    aty = np.zeros(p.n)
+    np.add.at(aty, p.col_idx, p.val * y[rows])
+    rc = p.c - aty
+
+    def cs(v, a, lo, hi):
+        at_lo = np.isfinite(lo) & (np.abs(a - lo) < bt)
+        at_hi = np.isfinite(hi) & (np.abs(a - hi) < bt)
+        out = np.abs(v)
+        out = np.where(at_lo & ~at_hi, np.maximum(0.0, -v), out)
+        out = np.where(at_hi & ~at_lo, np.maximum(0.0, v), out)
+        return np.where(at_lo & at_hi, 0.0, out)
+
+    with np.errstate(invalid="ignore"):
+        op = np.maximum(np.where(np.isfinite(p.row_lo), p.row_lo - act, 0.0),
+                        np.where(np.isfinite(p.row_hi), act - p.row_hi, 0.0))
+    return max(float(np.max(np.maximum(op, 0.0), initial=0.0)),
+               float(np.max(cs(y, act, p.row_lo, p.row_hi), initial=0.0)),
+               float(np.max(cs(rc, x, p.col_lo, p.col_hi), initial=0.0)))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_check_over_row_slices_matches_the_candidates_residual(pkg, precision):
+    """The check walks the demand rows of a transportation LP through their
+    row slices; at every check the residual it reports for its candidate
+    (the checkpoint callback's point and residual) must be the one numpy
+    computes from that point."""
+    import numpy as np
+    p = pkg.lpgen.transportation_lp(600, 900, seed=1000)
+    seen = []
+
+    def cb(it, x, y, res):
+        seen.append((it, x.copy(), y.copy(), res))
+
+    with pkg.Engine(0) as e:
+        e.load(p)
+        e.solve(pkg.PdhgOptions(precision=precision, termination_rule="relative_kkt",
+                                restart_rule="adaptive", max_iterations=400, tolerance=1e-4,
+                                checkpoint=cb))
+    assert len(seen) >= 5
+    for it, x, y, res in seen:
+        want = _orig_residual(p, x, y, 1e-4)
+        assert res == pytest.approx(want, rel=1e-9, abs=1e-12), (it, res, want)
