@@ -79,7 +79,7 @@ struct TiersDev {
 // Owning storage of RowSlices.
 struct SlicesDev {
     DBuf<int4> slice, item;
-    DBuf<int2> split;
+    DBuf<int2> split, affine;
     DBuf<int32_t> row, rlen, col;
     DBuf<float> v32;
     DBuf<double> v64, part, cpart;
@@ -102,6 +102,7 @@ struct SlicesDev {
         v.fetch = fetch.p;
         v.cticket = cticket.p;
         v.cpart = cpart.p;
+        v.affine = affine.p;
         return v;
     }
 };
@@ -487,6 +488,9 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
     }
     cudaMemsetAsync(S.fetch.p, 0, 2 * sizeof(unsigned int), s);
     launch_fill_slices(M.view(), S.view(), S.col.p, S.v32.p, S.v64.p, total, s);
+    if ((e = S.affine.alloc(static_cast<size_t>(S.n_slice))) != cudaSuccess)
+        return cuda_fail(err, e, "build_slices");
+    launch_affine_slices(S.view(), S.affine.p, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");
 
     // the long-row tiers without the rows of the slices kept

@@ -74,6 +74,7 @@ struct RowSlices {
     unsigned int* ticket = nullptr;  // per split slice, 0 between launches
     double* part = nullptr;          // 32 partials per item
     unsigned int* fetch = nullptr;   // {next item, exits}, 0 between launches
+    const int2* affine = nullptr;    // per slice {base, stride}: column base + l + k stride, or {0, 0}
     unsigned int* cticket = nullptr; // the check's: per split slice, 0 between launches
     double* cpart = nullptr;         // the check's: 64 partials per item (current, average)
 };
@@ -429,6 +430,7 @@ void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_
 // Lane-interleaved copy of the slices' rows: for slice s, lane l, entry k <
 // rlen: col/v32/v64[off + 32 k + l] = the row's k-th entry; padding entries
 // get column 0 and value 0.
+void launch_affine_slices(const RowSlices& S, int2* affine, cudaStream_t s);
 void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,
                         int64_t total, cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,

@@ -159,6 +159,33 @@ __global__ void k_fill_slices(const int32_t* rp, const int32_t* ci, const double
     }
 }
 
+// Affine slices: where every entry of a slice (lane l, step k, k below the
+// lane's row length) is column base + l + k * stride, the slice kernel
+// computes the columns instead of loading them. {base, stride}, or {0, 0} for
+// a slice with any other entry; every entry is compared.
+__global__ void k_affine_slices(RowSlices S, int2* affine) {
+    __shared__ int ok;
+    for (int sl = blockIdx.x; sl < S.n_slice; sl += gridDim.x) {
+        const int4 d = S.slice[sl];
+        const int64_t base = S.col[d.y];
+        const int64_t stride = d.x > 1 ? static_cast<int64_t>(S.col[d.y + 32]) - base : 0;
+        if (threadIdx.x == 0) ok = stride > 0 ? 1 : 0;
+        __syncthreads();
+        const int64_t n = static_cast<int64_t>(d.x) * 32;
+        bool bad = false;
+        for (int64_t e = threadIdx.x; e < n; e += kBlock) {
+            const int l = static_cast<int>(e & 31);
+            const int k = static_cast<int>(e >> 5);
+            if (k < S.rlen[32 * sl + l] && S.col[d.y + e] != base + l + k * stride) bad = true;
+        }
+        if (bad) ok = 0;  // every writer writes 0
+        __syncthreads();
+        if (threadIdx.x == 0)
+            affine[sl] = ok ? make_int2(static_cast<int>(base), static_cast<int>(stride)) : make_int2(0, 0);
+        __syncthreads();
+    }
+}
+
 // Rows with lo < length <= hi appended to `list` (grid-stride; one atomic per
 // warp that has any).
 __global__ void k_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
@@ -466,6 +493,11 @@ void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4*
 void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_t* out,
                         cudaStream_t s) {
     if (n > 0) k_gather_cols<<<nblocks(n), kBlock, 0, s>>>(ci, pos, n, out);
+}
+
+void launch_affine_slices(const RowSlices& S, int2* affine, cudaStream_t s) {
+    if (S.n_slice == 0) return;
+    k_affine_slices<<<S.n_slice < 4096 ? S.n_slice : 4096, kBlock, 0, s>>>(S, affine);
 }
 
 void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,

@@ -234,6 +234,49 @@ __device__ __forceinline__ const float* slice_vals<float>(const RowSlices& S) { 
 template <>
 __device__ __forceinline__ const double* slice_vals<double>(const RowSlices& S) { return S.v64; }
 
+// Lane l's dot product over steps [k0, k1) of a slice (k below kend), in
+// rounds of eight: the next round's index and value loads are issued before
+// this round's gathers. AFF: the slice's columns are base + l + k * stride
+// (checked entry by entry at load), computed instead of loaded.
+template <class T, bool AFF>
+__device__ __forceinline__ T slice_dot(const RowSlices& S, int off, int k0s, int k1, int kend, int lane,
+                                       const T* __restrict__ xg, int2 af) {
+    const int32_t* __restrict__ col = S.col + off + lane;
+    const T* __restrict__ val = slice_vals<T>(S) + off + lane;
+    const int abase = af.x + lane;
+    auto colk = [&](int k) -> int {
+        return AFF ? abase + k * af.y : __ldcs(col + 32 * static_cast<int64_t>(k));
+    };
+    T acc = T(0);
+    int c[8];
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int k = k0s + u;
+        c[u] = k < kend ? colk(k) : 0;
+        v[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+    }
+    for (int k0 = k0s; k0 < k1; k0 += 8) {
+        int cn[8];
+        T vn[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = k0 + 8 + u;
+            cn[u] = k < kend ? colk(k) : 0;
+            vn[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (k0 + u < kend) acc += v[u] * __ldg(xg + c[u]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            c[u] = cn[u];
+            v[u] = vn[u];
+        }
+    }
+    return acc;
+}
+
 // One warp item of the row slices (warp-uniform): entries [k0, k1) of one
 // slice, lane l on the slice's row l, in rounds of eight steps; each step is
 // one coalesced index load, one coalesced value load and one gather per lane.
@@ -250,36 +293,11 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
     const int4 d = __ldg(S.slice + w.x);
     const int row = __ldg(S.row + 32 * w.x + lane);
     const int kend = min(w.z, __ldg(S.rlen + 32 * w.x + lane));
-    const int32_t* __restrict__ col = S.col + d.y + lane;
-    const T* __restrict__ val = slice_vals<T>(S) + d.y + lane;
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
-    T acc = T(0);
-    int c[8];
-    T v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int k = w.y + u;
-        c[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
-        v[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
-    }
-    for (int k0 = w.y; k0 < w.z; k0 += 8) {
-        int cn[8];
-        T vn[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int k = k0 + 8 + u;
-            cn[u] = k < kend ? __ldcs(col + 32 * static_cast<int64_t>(k)) : 0;
-            vn[u] = k < kend ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-            if (k0 + u < kend) acc += v[u] * __ldg(xg + c[u]);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            c[u] = cn[u];
-            v[u] = vn[u];
-        }
-    }
+    // an affine slice's columns are computed, not loaded (warp-uniform)
+    const int2 af = __ldg(S.affine + w.x);
+    T acc = af.y > 0 ? slice_dot<T, true>(S, d.y, w.y, w.z, kend, lane, xg, af)
+                     : slice_dot<T, false>(S, d.y, w.y, w.z, kend, lane, xg, af);
     if (w.w >= 0) {
         S.part[32 * static_cast<int64_t>(idx) + lane] = static_cast<double>(acc);
         __threadfence();
