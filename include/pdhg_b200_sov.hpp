@@ -14,6 +14,14 @@
  * sov::Status, like the reference's backend errors; solver outcomes come back
  * in PdhgResult::status and ::message, never as exceptions (pdhg.cpp:223-237).
  * Validation messages name rows and columns by the problem's own names.
+ *
+ * sov::MpsModelB200 is the MPS reader over the engine's pdhg_read_mps: the
+ * model sov::read_mps / read_mps_string (include/sovereign/io.hpp:57-59) would
+ * build, with the same warnings and errors (sov::Error with the reference's
+ * message). to_read_result() rebuilds it as a sov::ReadResult through
+ * sov::Problem::Builder for code that needs a sov::Problem;
+ * PdhgB200::solve(model, ...) hands the reader's arrays to the engine without
+ * that rebuild.
  */
 #pragma once
 
@@ -27,11 +35,100 @@
 
 #include "pdhg_b200.h"
 #include "sovereign/cancellation.hpp"
+#include "sovereign/io.hpp"
 #include "sovereign/pdhg.hpp"
 #include "sovereign/problem.hpp"
 #include "sovereign/status.hpp"
 
 namespace sov {
+
+class MpsModelB200 {
+public:
+    // read_mps_string(text, options, origin) (io.hpp:58-59); threads 0 = all.
+    static MpsModelB200 read_string(const std::string& text, const MpsOptions& options = {},
+                                    const std::string& origin = "<string>", int threads = 0) {
+        pdhg_mps_options o = convert(options, threads);
+        pdhg_model* raw = nullptr;
+        char err[4096];
+        if (pdhg_read_mps(text.data(), text.size(), origin.c_str(), &o, &raw, err, sizeof err) !=
+            PDHG_OK)
+            throw Error(std::string(err));
+        return MpsModelB200(raw);
+    }
+    // read_mps(path, options) (io.hpp:57).
+    static MpsModelB200 read_file(const std::string& path, const MpsOptions& options = {},
+                                  int threads = 0) {
+        pdhg_mps_options o = convert(options, threads);
+        pdhg_model* raw = nullptr;
+        char err[4096];
+        if (pdhg_read_mps_file(path.c_str(), &o, &raw, err, sizeof err) != PDHG_OK)
+            throw Error(std::string(err));
+        return MpsModelB200(raw);
+    }
+
+    const pdhg_model* get() const noexcept { return model_.get(); }
+    const pdhg_model_info& info() const noexcept { return info_; }
+    std::string row_name(int32_t i) const { return pdhg_model_row_name(model_.get(), i); }
+    std::string col_name(int32_t j) const { return pdhg_model_col_name(model_.get(), j); }
+
+    std::vector<ReaderWarning> warnings() const {
+        std::vector<ReaderWarning> out;
+        for (int32_t k = 0; k < info_.warnings; ++k) {
+            int64_t line = 0;
+            const char* section = nullptr;
+            const char* message = nullptr;
+            pdhg_model_warning(model_.get(), k, &line, &section, &message);
+            out.push_back(ReaderWarning{static_cast<int>(line), section, message});
+        }
+        return out;
+    }
+
+    // The same model as a sov::ReadResult, through sov::Problem::Builder in
+    // file order (rows, then columns with bounds, kinds and costs, then the
+    // matrix row by row).
+    ReadResult to_read_result() const {
+        const int32_t *rp = nullptr, *ci = nullptr;
+        const double *v = nullptr, *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr,
+                     *ru = nullptr;
+        const uint8_t* integer = nullptr;
+        pdhg_model_arrays(model_.get(), &rp, &ci, &v, &c, &cl, &cu, &rl, &ru, &integer);
+        Problem::Builder b;
+        b.set_name(pdhg_model_name(model_.get()));
+        b.set_sense(info_.maximize ? ObjSense::Maximize : ObjSense::Minimize);
+        b.set_objective_name(pdhg_model_objective_name(model_.get()));
+        b.set_objective_constant(info_.obj_const);
+        for (int32_t i = 0; i < info_.m; ++i) b.add_row(row_name(i), rl[i], ru[i]);
+        for (int32_t j = 0; j < info_.n; ++j) {
+            const Idx col = b.add_column(col_name(j));
+            b.set_column_bounds(col, cl[j], cu[j]);
+            if (integer[j]) b.set_column_kind(col, VarKind::Integer);
+            b.set_objective_coefficient(col, c[j]);
+        }
+        for (int32_t i = 0; i < info_.m; ++i)
+            for (int32_t k = rp[i]; k < rp[i + 1]; ++k) b.add_coefficient(i, ci[k], v[k]);
+        ReadResult r;
+        r.problem = b.finish();
+        r.warnings = warnings();
+        r.format = "mps";
+        return r;
+    }
+
+private:
+    explicit MpsModelB200(pdhg_model* m) : model_(m, pdhg_model_free) {
+        pdhg_model_get_info(m, &info_);
+    }
+    static pdhg_mps_options convert(const MpsOptions& options, int threads) {
+        pdhg_mps_options o;
+        pdhg_default_mps_options(&o);
+        o.negative_upper_bound =
+            options.negative_upper_bound == NegativeUpperBoundRule::KeepLowerAtZero ? 1 : 0;
+        o.keep_free_rows = options.keep_free_rows ? 1 : 0;
+        o.threads = threads;
+        return o;
+    }
+    std::shared_ptr<pdhg_model> model_;
+    pdhg_model_info info_{};
+};
 
 class PdhgB200 {
 public:
@@ -65,6 +162,45 @@ public:
                                 problem.col_lower().data(), problem.col_upper().data(),
                                 problem.row_lower().data(), problem.row_upper().data()),
               ctx.get(), "pdhg_load_problem");
+        return run(ctx.get(), m, n, cancel, [&](bool column, long idx) -> std::string {
+            const auto names = column ? problem.col_names() : problem.row_names();
+            return idx >= 0 && static_cast<std::size_t>(idx) < names.size()
+                       ? names[static_cast<std::size_t>(idx)]
+                       : std::string();
+        });
+    }
+
+    // The model read by MpsModelB200, its arrays loaded as they are (no
+    // sov::Problem in between); messages name rows and columns as the file does.
+    PdhgResult solve(const MpsModelB200& model, Backend& /*backend*/,
+                     const CancellationToken* cancel = nullptr) const {
+        pdhg_ctx* raw = nullptr;
+        check(pdhg_create(device_, &raw), nullptr, "pdhg_create");
+        std::unique_ptr<pdhg_ctx, int (*)(pdhg_ctx*)> ctx(raw, pdhg_destroy);
+        const pdhg_model_info& mi = model.info();
+        const int32_t *rp = nullptr, *ci = nullptr;
+        const double *v = nullptr, *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr,
+                     *ru = nullptr;
+        pdhg_model_arrays(model.get(), &rp, &ci, &v, &c, &cl, &cu, &rl, &ru, nullptr);
+        check(pdhg_load_problem(ctx.get(), mi.m, mi.n, mi.nnz, rp, ci, v, c, mi.obj_const,
+                                mi.maximize, cl, cu, rl, ru),
+              ctx.get(), "pdhg_load_problem");
+        return run(ctx.get(), mi.m, mi.n, cancel, [&](bool column, long idx) -> std::string {
+            const long count = column ? mi.n : mi.m;
+            if (idx < 0 || idx >= count) return std::string();
+            return column ? model.col_name(static_cast<int32_t>(idx))
+                          : model.row_name(static_cast<int32_t>(idx));
+        });
+    }
+
+    const PdhgOptions& options() const noexcept { return options_; }
+
+private:
+    // Options, cancellation, checkpoints, the solve and the result, for a
+    // problem already loaded into ctx; name(column?, index) for messages.
+    template <class NameFn>
+    PdhgResult run(pdhg_ctx* ctx, int32_t m, int32_t n, const CancellationToken* cancel,
+                   NameFn&& name) const {
 
         pdhg_options o;
         pdhg_default_options(&o);
@@ -102,11 +238,11 @@ public:
         r.dual.resize(static_cast<std::size_t>(m));
         r.reduced_costs.resize(static_cast<std::size_t>(n));
         pdhg_info info;
-        const int rc = pdhg_solve(ctx.get(), &o, &info, r.primal.data(), r.dual.data(),
+        const int rc = pdhg_solve(ctx, &o, &info, r.primal.data(), r.dual.data(),
                                   r.reduced_costs.data());
         running.store(false);
         if (watcher.joinable()) watcher.join();
-        check(rc, ctx.get(), "pdhg_solve");
+        check(rc, ctx, "pdhg_solve");
         if (!info.has_point) {
             r.primal.clear();
             r.dual.clear();
@@ -121,13 +257,10 @@ public:
         r.restarts = info.restarts;
         r.seconds = info.seconds;
         r.operator_norm_estimate = info.operator_norm_estimate;
-        r.message = with_names(problem, info.message);
+        r.message = with_names(info.message, name);
         return r;
     }
 
-    const PdhgOptions& options() const noexcept { return options_; }
-
-private:
     // std::function checkpoint behind the C callback (same thread, same cadence).
     struct Bridge {
         const PdhgOptions* opt;
@@ -148,7 +281,8 @@ private:
     }
 
     // The ABI names rows R<i> and columns C<j>; put the problem's names back.
-    static std::string with_names(const Problem& p, const char* msg) {
+    template <class NameFn>
+    static std::string with_names(const char* msg, NameFn&& name) {
         std::string s(msg);
         const struct {
             const char* word;
@@ -162,9 +296,8 @@ private:
             while (end < s.size() && s[end] >= '0' && s[end] <= '9') ++end;
             if (end == num) continue;
             const long idx = std::stol(s.substr(num, end - num));
-            const auto names = k.tag == 'C' ? p.col_names() : p.row_names();
-            if (idx >= 0 && static_cast<std::size_t>(idx) < names.size())
-                s.replace(num - 1, end - num + 1, names[static_cast<std::size_t>(idx)]);
+            const std::string nm = name(k.tag == 'C', idx);
+            if (!nm.empty()) s.replace(num - 1, end - num + 1, nm);
         }
         return s;
     }

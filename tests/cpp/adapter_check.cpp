@@ -5,7 +5,9 @@
 // with sov::PdhgB200 (the B200 engine behind the same interface, exact mode),
 // and requires identical results: status, message, iterations, restarts,
 // objective, infeasibilities, gap, operator-norm estimate, x, y, reduced
-// costs; the same checkpoint calls; cancellation before the first iteration.
+// costs; the same checkpoint calls; cancellation before the first iteration;
+// and an MPS model read by the reference (read_mps_string, then Pdhg) and by
+// sov::MpsModelB200 (its arrays straight to the engine).
 // Built by oracle/Makefile (target ref) against the reference's headers and
 // its compiled PDHG path; prints one line per case and exits non-zero on any
 // difference. Test infrastructure only.
@@ -17,6 +19,7 @@
 
 #include "pdhg_b200_sov.hpp"
 #include "sovereign/backend.hpp"
+#include "sovereign/io.hpp"
 
 namespace {
 
@@ -169,6 +172,46 @@ int main() {
         compare("checkpoint_result", ref, b200);
         report("checkpoint_calls", it_r == it_g && same_vec(x_r, x_g),
                std::to_string(it_r.size()) + " calls");
+    }
+    // an MPS model: the reference reads it and solves the Problem; the B200
+    // reader's model goes to the engine without a sov::Problem in between.
+    // Ranges, bounds of several types, a second N row and an objective
+    // constant; and a crossed bound, whose message names the file's column.
+    {
+        const std::string text =
+            "NAME          MPSCASE\n"
+            "ROWS\n N  COST\n L  CAP\n G  NEED\n E  BAL\n N  SPARE\n"
+            "COLUMNS\n"
+            "    X1   COST  1.0   CAP  1.0\n    X1   NEED  1.0   SPARE  3.0\n"
+            "    X2   COST  2.0   CAP  1.0\n    X2   BAL  -1.0\n"
+            "    X3   COST  -1.0  BAL  1.0\n    X3   NEED  0.5\n"
+            "    X4   COST  0.25  CAP  2.0\n    X4   BAL   1.0\n"
+            "RHS\n    RHS  COST  -3.5\n    RHS  CAP  8.0   NEED  1.0\n    RHS  BAL  2.0\n"
+            "RANGES\n    RNG  CAP  6.0   BAL  -1.0\n"
+            "BOUNDS\n UP BND  X1  4.0\n LO BND  X3  -5.0\n UP BND  X3  5.0\n UP BND  X4  3.0\n"
+            "ENDATA\n";
+        const sov::ReadResult rr = sov::read_mps_string(text);
+        const sov::MpsModelB200 model = sov::MpsModelB200::read_string(text);
+        sov::PdhgOptions o = opt;
+        o.max_iterations = 5000;
+        compare("mps_model", sov::Pdhg(o).solve(rr.problem, *host),
+                sov::PdhgB200(o).solve(model, *host));
+        std::string crossed = text;
+        crossed.replace(crossed.find(" UP BND  X4  3.0"), 16, " UP BND  X4 -3.0");
+        sov::MpsOptions literal;
+        literal.negative_upper_bound = sov::NegativeUpperBoundRule::KeepLowerAtZero;
+        std::string ref_err, our_err;
+        try {
+            sov::read_mps_string(crossed, literal);
+        } catch (const sov::Error& e) {
+            ref_err = e.what();
+        }
+        try {
+            sov::MpsModelB200::read_string(crossed, literal);
+        } catch (const sov::Error& e) {
+            our_err = e.what();
+        }
+        report("mps_crossed_bound_message", !ref_err.empty() && ref_err == our_err, our_err);
     }
     std::printf("%s\n", failures == 0 ? "ALL OK" : "FAILURES");
     return failures == 0 ? 0 : 1;
