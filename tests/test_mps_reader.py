@@ -449,3 +449,24 @@ def test_cpp_reader_adapter_matches_the_reference(tmp_path):
         files.append(str(f))
     r = subprocess.run([exe] + files, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "ALL OK" in r.stdout, r.stdout[-3000:] + r.stderr[-2000:]
+
+
+def test_bench_mps_reader_line():
+    """bench.py --mps-reader prints one JSON line: the reader's throughput on a
+    written transportation model, one thread and all, and the reference's
+    reader on a sample when oracle/_ref is built."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--mps-reader",
+                        "--supplies", "30", "--demands", "60", "--mps-ref-supplies", "10"],
+                       capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-3000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["metric"] == "mps_read_throughput" and line["unit"] == "MB/s"
+    assert line["value"] > 0 and line["single_thread_MBps"] > 0
+    assert line["config"]["nonzeros"] == 2 * 30 * 60 and line["config"]["columns"] == 30 * 60
+    ref = line["reference"]
+    assert "unavailable" in ref or (ref["value"] > 0 and ref["kind"] == "reference")
