@@ -941,7 +941,7 @@ void tune_pass(Ctx& c, FastIter<T>& fi, bool primal, const char* prec_tag, int* 
         if (M.items_warp.n_item > 0) cand.push_back({vw, 2});
     }
     // two rounds over all candidates, each keeping its faster time, so no
-    // candidate is judged on a cold GPU (clocks ramping, first launches)
+    // candidate is timed only on a cold GPU (clocks ramping, first launches)
     std::vector<float> t(cand.size(), 3.0e38f);
     for (int round = 0; round < 2; ++round)
         for (size_t i = 0; i < cand.size(); ++i) {

@@ -12,7 +12,7 @@ c = c0 + B_c theta over one matrix).
    its relative KKT residual (PDLP's l2 measure, evaluated on the device by
    ``Engine.start_kkt``) is below the cold start's; otherwise the instance
    starts cold. Plain PDHG is
-   therefore both the fallback and the judge, and every solve is held to the
+   therefore both the fallback and the gate, and every solve is held to the
    same termination tolerance.
 """
 from __future__ import annotations
