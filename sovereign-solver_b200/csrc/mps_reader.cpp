@@ -456,6 +456,7 @@ private:
     void apply_range(int32_t row, double range);
     void sequential(const char* b, const char* e, int64_t first_line, bool* stop);
     void columns_parallel(const char* b, const char* e, int64_t first_line);
+    void bounds_parallel(const char* b, const char* e, int64_t first_line);
 
     pdhg_mps_options opt_;
     std::string origin_;
@@ -1058,6 +1059,156 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     clk.mark("columns: triplets");
 }
 
+// ---- BOUNDS by chunks -------------------------------------------------------------------
+
+enum BoundType : int8_t { kUP, kLO, kFX, kFR, kMI, kPL, kBV, kLI, kUI };
+
+// One parsed BOUNDS card: its column (or, for a column COLUMNS never named,
+// the name, resolved in file order), type and value.
+struct BoundCard {
+    int32_t col;               // -1: look the name up when applied
+    int8_t type;
+    double value;
+    int64_t line;              // local line ordinal (1-based) in the chunk
+    std::string_view name;
+};
+
+struct BoundChunk {
+    const char* b = nullptr;
+    const char* e = nullptr;
+    int64_t lines = 0;
+    std::vector<BoundCard> cards;
+    bool failed = false;
+    int64_t err_line = 0;
+    std::string err_msg;
+};
+
+// The cards of [lb, le) parsed by threads (every error that does not depend
+// on earlier cards found there: card shape, type, value), then applied in
+// file order exactly as handle_bounds / apply_bound do, with their warnings.
+void Reader::bounds_parallel(const char* lb, const char* le, int64_t first_line) {
+    const size_t bytes = static_cast<size_t>(le - lb);
+    const int T = static_cast<int>(std::min<size_t>(static_cast<size_t>(threads_) * 4, bytes / (1u << 18) + 1));
+    std::vector<BoundChunk> ch(T);
+    const char* prev = lb;
+    for (int t = 0; t < T; ++t) {
+        const char* e = t + 1 == T ? le : lb + bytes * (t + 1) / T;
+        if (e < le && e > prev) {
+            const char* nl = static_cast<const char*>(std::memchr(e - 1, '\n', static_cast<size_t>(le - (e - 1))));
+            e = nl ? nl + 1 : le;
+        }
+        if (e < prev) e = prev;
+        ch[t].b = prev;
+        ch[t].e = e;
+        prev = e;
+    }
+    const NameIndex& cols = b.col_idx;
+    std::atomic<int> next{0};
+    parallel_for(threads_, threads_, [&](int, int64_t, int64_t) {
+        std::vector<std::string_view> t;
+        for (int c = next.fetch_add(1); c < T; c = next.fetch_add(1)) {
+            BoundChunk& k = ch[c];
+            int64_t ord = 0;
+            for_lines(k.b, k.e, [&](std::string_view line) {
+                ++ord;
+                if (line.empty() || line[0] == '*') return true;
+                auto fail = [&](std::string msg) {
+                    k.failed = true;
+                    k.err_line = ord;
+                    k.err_msg = std::move(msg);
+                    return false;
+                };
+                if (!is_space(line[0])) return fail("internal: header inside a BOUNDS range");
+                if (fixed_) tokenize_fixed(line, t);
+                else tokenize_free(line, t);
+                if (t.empty()) return true;
+                if (t.size() < 2) return fail("BOUNDS card needs a type and a column");
+                const std::string type = upper_copy(t[0]);
+                const bool valueless = type == "FR" || type == "MI" || type == "PL" || type == "BV";
+                if (!valueless && t.size() < 3) return fail("BOUNDS card of type " + type + " needs a value");
+                const size_t col_pos = valueless ? t.size() - 1 : t.size() - 2;
+                BoundCard card{-1, 0, 0.0, ord, t[col_pos]};
+                static const char* const kNames[] = {"UP", "LO", "FX", "FR", "MI", "PL", "BV", "LI", "UI"};
+                int code = -1;
+                for (int q = 0; q < 9; ++q)
+                    if (type == kNames[q]) code = q;
+                if (type == "SC") return fail("semi-continuous bounds (SC) are not supported");
+                if (code < 0) return fail("unknown bound type '" + type + "'");
+                card.type = static_cast<int8_t>(code);
+                if (!valueless) {
+                    const std::string_view tok = t[col_pos + 1];
+                    double v = 0.0;
+                    if (!infinite_token(tok, &v) && !parse_real(tok, &v))
+                        return fail("expected a number, got '" + std::string(tok) + "'");
+                    card.value = v;
+                }
+                card.col = cols.find(card.name);
+                k.cards.push_back(card);
+                return true;
+            });
+            int64_t n = 0;
+            for (const char* p = k.b; p < k.e;) {
+                const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(k.e - p)));
+                ++n;
+                p = nl ? nl + 1 : k.e;
+            }
+            k.lines = n;
+        }
+    });
+    // the first error in file order ends the read; else the cards apply in order
+    int64_t line_base = first_line - 1;
+    for (int c = 0; c < T; ++c) {
+        BoundChunk& k = ch[c];
+        if (k.failed) {
+            line_no_ = line_base + k.err_line;
+            error(k.err_msg);
+        }
+        line_base += k.lines;
+    }
+    line_base = first_line - 1;
+    for (int c = 0; c < T; ++c) {
+        for (const BoundCard& card : ch[c].cards) {
+            line_no_ = line_base + card.line;
+            int32_t col = card.col;
+            if (col < 0) {  // a column COLUMNS never named: made by its first bound
+                const uint64_t h = hash_name(card.name);
+                col = b.col_idx.find(card.name, h);
+                if (col < 0) {
+                    warn("BOUNDS", "bound on column '" + std::string(card.name) + "' which has no coefficients");
+                    col = b.add_column(card.name, h);
+                }
+            }
+            const double lo = b.col_lo[col], v = card.value;
+            switch (card.type) {
+                case kUP:
+                    b.col_hi[col] = v;
+                    if (v < 0.0 && lo == 0.0) {
+                        if (opt_.negative_upper_bound == 0) {
+                            b.col_lo[col] = -kInf;
+                            warn("BOUNDS", "negative UP bound on a column with the default lower bound 0; "
+                                           "lower bound set to -infinity (the established-solver "
+                                           "convention; see MpsOptions::negative_upper_bound)");
+                        } else {
+                            warn("BOUNDS", "negative UP bound leaves crossed bounds (literal reading)");
+                        }
+                    }
+                    break;
+                case kLO: b.col_lo[col] = v; break;
+                case kFX: b.col_lo[col] = v; b.col_hi[col] = v; break;
+                case kFR: b.col_lo[col] = -kInf; b.col_hi[col] = kInf; break;
+                case kMI: b.col_lo[col] = -kInf; break;
+                case kPL: b.col_hi[col] = kInf; break;
+                case kBV: b.col_lo[col] = 0.0; b.col_hi[col] = 1.0; b.is_int[col] = 1; break;
+                case kLI: b.col_lo[col] = v; b.is_int[col] = 1; break;
+                case kUI: b.col_hi[col] = v; b.is_int[col] = 1; break;
+                default: break;
+            }
+        }
+        line_base += ch[c].lines;
+    }
+    line_no_ = line_base;
+}
+
 void Reader::read(const char* buf, size_t len, const std::vector<Header>& headers) {
     bool stop = false;
     // lines before the first header
@@ -1072,6 +1223,8 @@ void Reader::read(const char* buf, size_t len, const std::vector<Header>& header
         if (stop) break;
         if (section_ == Section::Columns && (buf + he) - data > (1 << 20) && threads_ > 1)
             columns_parallel(data, buf + he, headers[h].line + 1);
+        else if (section_ == Section::Bounds && (buf + he) - data > (1 << 20) && threads_ > 1)
+            bounds_parallel(data, buf + he, headers[h].line + 1);
         else
             sequential(data, buf + he, headers[h].line + 1, &stop);
     }

@@ -285,7 +285,7 @@ def fmt(rng, v):
     return NUM_FORMS[rng.integers(len(NUM_FORMS))].format(v)
 
 
-def write_random_mps(seed, m=30, n=60, big=False):
+def write_random_mps(seed, m=30, n=60, big=False, bounds_p=0.4, ghosts=0):
     """A random model in free MPS with the dialect's quirks; when big, many
     columns (a COLUMNS section of several MB) for the chunked parse."""
     rng = np.random.default_rng(seed)
@@ -342,7 +342,10 @@ def write_random_mps(seed, m=30, n=60, big=False):
     L.append("BOUNDS")
     kinds = ["UP", "LO", "FX", "FR", "MI", "PL", "BV", "LI", "UI", "up"]
     for j in range(n):
-        if rng.random() < 0.4:
+        if ghosts and rng.random() < ghosts / n:  # columns COLUMNS never named, some twice
+            g = int(rng.integers(ghosts))
+            L.append(f" UP BND ghost{g} {fmt(rng, float(rng.integers(0, 9)))}")
+        if rng.random() < bounds_p:
             t = kinds[int(rng.integers(len(kinds)))]
             if t in ("FR", "MI", "PL", "BV"):
                 L.append(f" {t} BND x{j}")
@@ -470,3 +473,38 @@ def test_bench_mps_reader_line():
     assert line["config"]["nonzeros"] == 2 * 30 * 60 and line["config"]["columns"] == 30 * 60
     ref = line["reference"]
     assert "unavailable" in ref or (ref["value"] > 0 and ref["kind"] == "reference")
+
+
+@pytest.mark.parametrize("seed", [200, 201])
+def test_large_bounds_sections_parse_in_chunks(pkg, orc, seed):
+    # a BOUNDS card on every column (a section of more than 1 MB) goes to the
+    # threads in chunks and is applied in file order: bounds on columns COLUMNS
+    # never named (the first makes the column and warns), negative UP bounds
+    # under both rules, every bound type
+    text = write_random_mps(seed, m=300, n=60_000, bounds_p=1.0, ghosts=40)
+    assert len(text.partition("BOUNDS")[2]) > 1_100_000
+    for lit in (False, True):
+        a = same_as_reference(pkg, orc, text, keep_lower_at_zero=lit, threads=8)
+        one = ours(pkg, text, threads=1,
+                   negative_upper_bound="keep_lower_at_zero" if lit else "minus_infinity")
+        if isinstance(a, str):
+            assert one == a
+            continue
+        assert any(w[2].startswith("bound on column 'ghost") for w in a.warnings)
+        for f in ARRAYS:
+            assert np.array_equal(getattr(one.problem, f), getattr(a.problem, f))
+        assert one.col_names == a.col_names and one.warnings == a.warnings
+        assert np.array_equal(one.is_integer, a.is_integer)
+
+
+def test_chunked_bounds_report_the_first_error_with_its_line(pkg, orc):
+    text = write_random_mps(9, m=100, n=60_000, bounds_p=1.0)
+    head, _, rest = text.partition("BOUNDS")
+    lines = rest.split("\n")
+    k1, k2 = len(lines) * 2 // 3, len(lines) * 5 // 6
+    lines[k1] = " UP BND x5 notanumber"
+    lines[k2] = " XX BND x6 1"
+    text = head + "BOUNDS" + "\n".join(lines)
+    r = same_as_reference(pkg, orc, text, threads=8)
+    assert r == ours(pkg, text, threads=1)
+    assert isinstance(r, str) and "expected a number, got 'notanumber'" in r
