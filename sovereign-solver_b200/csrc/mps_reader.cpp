@@ -40,9 +40,11 @@
 #include <exception>
 #include <limits>
 #include <memory>
+#include <new>
 #include <string>
 #include <string_view>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/pdhg_b200.h"
@@ -58,6 +60,31 @@ constexpr double kNumericZero = 1e-14;  // tol::numeric_zero (numeric.hpp:95)
 struct ReadError {
     std::string what;
 };
+
+// std::vector storage whose resize() leaves new elements of a trivial type
+// uninitialised: the large arrays below are written in full by threads right
+// after sizing, and zero-filling them first would be a serial pass over
+// hundreds of MB.
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(args)...);
+    }
+};
+template <class T>
+using bigvec = std::vector<T, NoInit<T>>;
 
 // With PDHG_B200_PHASE_TIMES=1 in the environment, each phase's wall time on
 // stderr.
@@ -292,7 +319,7 @@ struct Builder {
     std::vector<uint8_t> is_int;
     std::vector<char> row_sense;     // L G E N, by row
     std::vector<double> row_rhs;     // the last RHS value, by row
-    std::vector<Triplet> entries;    // file order
+    bigvec<Triplet> entries;         // file order
     Arena dropped_names;             // free rows dropped (keep_free_rows = 0)
     NameIndex dropped_idx{&dropped_names};
 
@@ -879,7 +906,7 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     for (int c = 0; c < T; ++c) base[c + 1] = base[c] + ch[c].names.size();
     const int64_t F = base[T];
     std::vector<std::string_view> fname(static_cast<size_t>(F));  // by flat id
-    std::vector<uint64_t> fhash(static_cast<size_t>(F));
+    bigvec<uint64_t> fhash(static_cast<size_t>(F));
     const int S = std::max(1, threads_);
     // flat ids of each chunk, bucketed by shard (file order inside a bucket)
     std::vector<std::vector<std::vector<int64_t>>> bucket(static_cast<size_t>(T));
@@ -899,7 +926,7 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     clk.mark("merge: flat ids");
     auto name_of = [&](int64_t f) { return fname[static_cast<size_t>(f)]; };
     auto hash_of = [&](int64_t f) { return fhash[static_cast<size_t>(f)]; };
-    std::vector<int64_t> src(static_cast<size_t>(F));
+    bigvec<int64_t> src(static_cast<size_t>(F));
     const bool have_cols = b.col_names.size() > 0;
     parallel_for(S, S, [&](int, int64_t sb, int64_t se) {
         for (int64_t sh = sb; sh < se; ++sh) {
@@ -944,7 +971,7 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     // over the blocks, then each block numbers its own; repeats take the
     // number of the first appearance they point at
     const int64_t n0 = b.col_names.size();
-    std::vector<int32_t> id(static_cast<size_t>(F));
+    bigvec<int32_t> id(static_cast<size_t>(F));
     const int64_t NB = std::max<int64_t>(1, std::min<int64_t>(F / 65536 + 1, 4 * threads_));
     std::vector<int64_t> firsts(static_cast<size_t>(NB) + 1, 0);
     parallel_for(threads_, NB, [&](int, int64_t bb, int64_t be) {
@@ -958,7 +985,7 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
     const int64_t nn = firsts[NB];
     if (n0 + nn > std::numeric_limits<int32_t>::max() - 1)
         throw ReadError{"too many rows or columns for 32-bit indices"};
-    std::vector<int64_t> fresh(static_cast<size_t>(nn));  // flat ids of the new columns, in order
+    bigvec<int64_t> fresh(static_cast<size_t>(nn));  // flat ids of the new columns, in order
     parallel_for(threads_, NB, [&](int, int64_t bb, int64_t be) {
         for (int64_t q = bb; q < be; ++q) {
             int64_t k = firsts[q];
@@ -1241,8 +1268,10 @@ struct Model {
     bool maximize = false;
     double obj_const = 0.0;
     int32_t m = 0, n = 0;
-    std::vector<int32_t> rp, ci;
-    std::vector<double> v, c, col_lo, col_hi, row_lo, row_hi;
+    std::vector<int32_t> rp;
+    bigvec<int32_t> ci;
+    bigvec<double> v;
+    std::vector<double> c, col_lo, col_hi, row_lo, row_hi;
     std::vector<uint8_t> is_int;
     Arena row_names, col_names;
     std::vector<Warning> warnings;
@@ -1253,7 +1282,7 @@ namespace {
 
 // CsrMatrix::from_triplets (sparse.cpp:30-70): rows by a stable counting sort,
 // each row by column with duplicates summed in file order, |sum| <= 1e-14 dropped.
-void build_csr(int32_t m, std::vector<Triplet>& ent, int threads, Model* out) {
+void build_csr(int32_t m, bigvec<Triplet>& ent, int threads, Model* out) {
     for (const Triplet& e : ent)
         if (!std::isfinite(e.v)) throw ReadError{"from_triplets: non-finite coefficient"};
     const int64_t nnz = static_cast<int64_t>(ent.size());
@@ -1274,8 +1303,8 @@ void build_csr(int32_t m, std::vector<Triplet>& ent, int threads, Model* out) {
         }
         start[r + 1] = s;
     }
-    std::vector<int32_t> col(static_cast<size_t>(nnz));
-    std::vector<double> val(static_cast<size_t>(nnz));
+    bigvec<int32_t> col(static_cast<size_t>(nnz));
+    bigvec<double> val(static_cast<size_t>(nnz));
     parallel_for(T, T, [&](int, int64_t tb, int64_t te) {
         for (int64_t t = tb; t < te; ++t)
             for (int64_t k = nnz * t / T; k < nnz * (t + 1) / T; ++k) {
@@ -1284,7 +1313,7 @@ void build_csr(int32_t m, std::vector<Triplet>& ent, int threads, Model* out) {
                 val[p] = ent[k].v;
             }
     });
-    std::vector<Triplet>().swap(ent);
+    bigvec<Triplet>().swap(ent);
     cnt.clear();
     // order, sum and drop inside each row; keep[r] = entries kept
     std::vector<int64_t> keep(static_cast<size_t>(m) + 1, 0);
