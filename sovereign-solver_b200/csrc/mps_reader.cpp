@@ -873,14 +873,9 @@ void Reader::columns_parallel(const char* lb, const char* le, int64_t first_line
                 }
                 return true;
             });
-            // lines in the chunk (for the numbers of later chunks' lines)
-            int64_t n = 0;
-            for (const char* p = k.b; p < k.e;) {
-                const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(k.e - p)));
-                ++n;
-                p = nl ? nl + 1 : k.e;
-            }
-            k.lines = n;
+            // lines in the chunk, for the numbers of later chunks' lines (a
+            // chunk that stopped early failed, and its count is never used)
+            k.lines = ord;
             k.state_out = state;
         }
     };
@@ -1173,13 +1168,7 @@ void Reader::bounds_parallel(const char* lb, const char* le, int64_t first_line)
                 k.cards.push_back(card);
                 return true;
             });
-            int64_t n = 0;
-            for (const char* p = k.b; p < k.e;) {
-                const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(k.e - p)));
-                ++n;
-                p = nl ? nl + 1 : k.e;
-            }
-            k.lines = n;
+            k.lines = ord;  // a chunk that stopped early failed: its count is not used
         }
     });
     // the first error in file order ends the read; else the cards apply in order
