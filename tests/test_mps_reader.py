@@ -508,3 +508,58 @@ def test_chunked_bounds_report_the_first_error_with_its_line(pkg, orc):
     r = same_as_reference(pkg, orc, text, threads=8)
     assert r == ours(pkg, text, threads=1)
     assert isinstance(r, str) and "expected a number, got 'notanumber'" in r
+
+
+FUZZ_ALPHABET = list(" \t\r\n*'+-.eE0123456789ABCDEFGHIJKLMNOPQRSTUVWXYZabcxyz") + [
+    "INF", "MARKER", "'INTORG'", "RHS", "ROWS", "BOUNDS", "COLUMNS", "RANGES", "N", "UP", "FR"]
+
+
+def mutate(rng, s):
+    """One to four random edits: a character deleted, inserted or replaced
+    (from MPS's own vocabulary), a line duplicated or two lines swapped."""
+    for _ in range(rng.randint(1, 4)):
+        if not s:
+            s = "x"
+        i = rng.randrange(len(s))
+        op = rng.random()
+        if op < 0.3:
+            s = s[:i] + s[i + 1:]
+        elif op < 0.6:
+            s = s[:i] + rng.choice(FUZZ_ALPHABET) + s[i:]
+        elif op < 0.8:
+            s = s[:i] + rng.choice(FUZZ_ALPHABET) + s[i + 1:]
+        else:
+            lines = s.split("\n")
+            a, b = rng.randrange(len(lines)), rng.randrange(len(lines))
+            if rng.random() < 0.5:
+                lines.insert(b, lines[a])
+            else:
+                lines[a], lines[b] = lines[b], lines[a]
+            s = "\n".join(lines)
+    return s
+
+
+def test_mutated_models_read_like_the_reference(pkg, orc):
+    # seeded byte-level mutations of valid free and fixed-layout models: the
+    # two readers must agree on every one (the same error text or the same
+    # model, warnings included)
+    import random
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+    fixed = "\n".join([
+        "NAME          FIXED", "ROWS", fixed_card("N", "COST"), fixed_card("L", "LIM 1"),
+        fixed_card("G", "LIM 2"), "COLUMNS", fixed_card("", "X ONE", "COST", "1.0", "LIM 1", "1.0"),
+        fixed_card("", "X ONE", "LIM 2", "2.0"), fixed_card("", "X TWO", "COST", "-1.0", "LIM 2", "1.0"),
+        "RHS", fixed_card("", "RHS", "LIM 1", "4.0", "LIM 2", "1.0"),
+        "RANGES", fixed_card("", "RNG", "LIM 1", "2.5"),
+        "BOUNDS", fixed_card("UP", "BND", "X TWO", "3.5"), fixed_card("MI", "BND", "X ONE"),
+        "ENDATA"]) + "\n"
+    bases = [BASIC, fixed, fixed.replace("\n", "\r\n")] + [write_random_mps(s, m=6, n=10) for s in range(8)]
+    rng = random.Random(2024)
+    models = 0
+    for _ in range(600):
+        text = mutate(rng, rng.choice(bases))
+        for lit in (False, True):
+            r = same_as_reference(pkg, orc, text, keep_lower_at_zero=lit)
+            models += not isinstance(r, str)
+    assert models > 100  # the mutations leave many models readable
