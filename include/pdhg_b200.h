@@ -104,14 +104,24 @@ typedef struct pdhg_options {
     /* extensions (off = reference behaviour) */
     int precision;           /* pdhg_precision; default PDHG_PREC_FP64_EXACT */
     int termination_rule;    /* 0 = reference absolute residual (pdhg.cpp:383);
-                                1 = relative KKT: max(primal/(1+|b|inf), dual/(1+|c|inf), gap) */
+                                1 = relative KKT on the reference's residual terms:
+                                    max(primal/(1+|b|inf), dual/(1+|c|inf), gap), primal and
+                                    dual the max-norm terms of pdhg.cpp:166-197;
+                                2 = PDLP's relative KKT error (MIXED / FP64):
+                                    max(|row violation|_2/(1+|b|_2),
+                                        |sign violations of y and c - A^T y|_2/(1+|c|_2), gap),
+                                    b_i the larger finite |row bound|; the gap of rules 1 and 2
+                                    is |p - d|/(1 + |p| + |d|) on the bounded dual objective */
     long long polish_iterations; /* MIXED only: FP64 iterations allowed after the FP32
                                     phase stalls (no 2% gain in 25 checks); -1 = the rest
                                     of max_iterations, 0 = never leave FP32 */
     int restart_rule;        /* 0 = reference (pdhg.cpp:391-408); 1 = adaptive: restart to
                                 the better of average/current on sufficient (0.2x) or
                                 necessary (0.8x, no progress) decay or when the average
-                                spans 36% of all iterations. 1 needs MIXED or FP64. */
+                                spans 36% of all iterations, residuals measured by the
+                                scaled max-norm KKT residual (pdhg.cpp:87-136); 2 = the same
+                                rule measured by the l2 norm of termination rule 2's three
+                                parts (needs termination_rule 2). 1, 2 need MIXED or FP64. */
     int primal_weight_update; /* 0 = reference tau = sigma (pdhg.cpp:263-265); 1 = primal
                                 weight omega (tau = eta/omega, sigma = eta*omega) starts at
                                 |c|/|b| and moves to sqrt(omega |dy|/|dx|) at each restart */
@@ -271,18 +281,26 @@ int pdhg_project_box(int device, int32_t n, const double* lo, const double* hi, 
  * that own every device byte through their own pool (an allocation behind the
  * pool's back can fail or fragment it), latency-critical loops that must stay
  * away from the driver's allocator (an allocation can synchronise the device).
- * Every pointer is a DEVICE pointer the caller owns; the
- * work is queued on `stream` (a cudaStream_t, NULL = default stream) on the
- * current device and the call returns without waiting. Results are
- * bit-identical to pdhg_csr_spmv's.
+ * Every pointer is a DEVICE pointer the caller owns (d_x and d_y may be NULL
+ * when their length is 0); the work is queued on `stream` (a cudaStream_t,
+ * NULL = default stream) on the current device and the call returns without
+ * waiting. Results are bit-identical to pdhg_csr_spmv's, duplicate
+ * (row, column) entries included.
+ * The CSR must be well formed: d_row_ptr[0] = 0, d_row_ptr[m] = nnz, no row
+ * pointer decreasing, every column index in [0, n). The call cannot check this
+ * on the host (the arrays live on the device); its kernels check it first, and
+ * a CSR that breaks it fills every entry of y with NaN and touches nothing
+ * outside the caller's buffers (pdhg_csr_spmv returns
+ * PDHG_ERR_INVALID_ARGUMENT for the same input).
  * The transposed product needs A^T: it is built in a fixed scratch array that
- * every GPU loading this library reserves until exit (about 5 MB). Limits for
- * transpose != 0: n <= 262,144 columns and nnz <= 262,144 nonzeros; larger
- * sizes return PDHG_ERR_INVALID_ARGUMENT before any work is queued
- * (transpose == 0 uses no scratch and has no limit). The first transposed call
- * on a device looks up the scratch address for that device: make it before any
- * stream capture. All calls share the one array, so calls that overlap on the
- * GPU (different streams, no ordering between them) race; serialise them. */
+ * every GPU loading this library reserves until exit (about 6 MB; the check
+ * above keeps its flag there too). Limits for transpose != 0: n <= 262,144
+ * columns and nnz <= 262,144 nonzeros; larger sizes return
+ * PDHG_ERR_INVALID_ARGUMENT before any work is queued (transpose == 0 has no
+ * limit). The first call on a device looks up the scratch address for that
+ * device: make it before any stream capture. All calls share the one array,
+ * so calls that overlap on the GPU (different streams, no ordering between
+ * them) race; serialise them. */
 int pdhg_csr_spmv_noalloc(int transpose, int32_t m, int32_t n, int64_t nnz,
                           const int32_t* d_row_ptr, const int32_t* d_col_idx,
                           const double* d_values, double alpha, const double* d_x, double beta,
@@ -316,6 +334,12 @@ int pdhg_mlp_gradients(pdhg_mlp* mlp, int batch, const float* x, const float* t,
  * epoch's mean loss. */
 int pdhg_mlp_train(pdhg_mlp* mlp, int64_t samples, const float* x, const float* t, int epochs,
                    int batch, float lr, uint64_t seed, float* epoch_loss);
+/* One Adam step (the hyper-parameters and step counter of pdhg_mlp_train)
+ * with caller-supplied gradients in parameter order: the update of
+ * data-parallel training, where each replica applies the gradients of
+ * pdhg_mlp_gradients averaged over all ranks (one allreduce), so every
+ * replica keeps the same parameters. */
+int pdhg_mlp_adam_step(pdhg_mlp* mlp, const float* grads, float lr);
 /* The network's tensor-core GEMM alone (engine extension, for tests):
  * c (m x n) = a (m x k) b (n x k)^T (+ bias (n), ReLU), operands rounded to
  * BF16, FP32 accumulation; k a multiple of 8; host FP32 buffers. */

@@ -56,7 +56,7 @@ class OrcInfo(C.Structure):
                 ("duality_gap", C.c_double), ("iterations", C.c_longlong),
                 ("restarts", C.c_longlong), ("seconds", C.c_double),
                 ("operator_norm_estimate", C.c_double), ("has_point", C.c_int),
-                ("message", C.c_char * 256)]
+                ("message", C.c_char * 256), ("relative_kkt", C.c_double)]
 
 
 @dataclass
@@ -79,6 +79,7 @@ class Result:
     checkpoints: list = field(default_factory=list)
     loop_seconds: float = 0.0
     loop_iterations: int = 0
+    relative_kkt: float = 0.0
 
 
 _libs: dict = {}
@@ -216,7 +217,8 @@ def _solve(which: str, p, trace_iters: int = 0, checkpoints: bool = False,
         iterations=info.iterations, restarts=info.restarts, seconds=info.seconds,
         operator_norm_estimate=info.operator_norm_estimate, message=info.message.decode(),
         trace_x=None if tx is None else tx[:, : p.n], trace_y=None if ty is None else ty[:, : p.m],
-        checkpoints=cps, loop_seconds=float(loop[0]), loop_iterations=int(loop[1]))
+        checkpoints=cps, loop_seconds=float(loop[0]), loop_iterations=int(loop[1]),
+        relative_kkt=float(info.relative_kkt))
 
 
 def oracle_solve(p, **kw) -> Result:

@@ -482,6 +482,76 @@ static double original_residual(const orc_problem* p, double obj_sign, const dou
     return smax(primal_res, dual_res);
 }
 
+/* The part of v outside the sign its bounds allow a multiplier or reduced
+ * cost (internal minimize sense): >= 0 with only a finite lower end, <= 0
+ * with only a finite upper end, any sign with both, 0 with neither. */
+static double sign_violation(double v, double lo, double hi) {
+    const int fl = finite_bound(lo), fh = finite_bound(hi);
+    if (fl && fh) return 0.0;
+    if (fl) return v < 0.0 ? -v : 0.0;
+    if (fh) return v > 0.0 ? v : 0.0;
+    return fabs(v);
+}
+
+/* Termination rule 2 (engine extension, PDLP's relative KKT error; the
+ * reference defines no relative measure): the scaled point (xs, ys) in
+ * original units (xo, yo as in original_residual) gives
+ *   part[0] = ||row bound violation of A xo||_2 / (1 + ||b||_2)
+ *   part[1] = ||(sign violations of y, of c - A^T y)||_2 / (1 + ||c||_2)
+ *   part[2] = |p - d| / (1 + |p| + |d|)
+ * in the internal minimize sense, b_i = the largest finite |row bound|, d the
+ * dual objective on the bounded parts (clipped_inf_over_box), the objective
+ * constant added to both p and d. Returns max(part). */
+static double pdlp_kkt(const orc_problem* p, double obj_sign, const double* rs, const double* cs,
+                       const double* xs, const double* ys, double* xo, double* yo, double* act,
+                       double* aty, double part[3]) {
+    for (int32_t j = 0; j < p->n; ++j) xo[j] = xs[j] * cs[j];
+    for (int32_t i = 0; i < p->m; ++i) {
+        yo[i] = ys[i] * obj_sign;
+        yo[i] *= rs[i];
+    }
+    csr_multiply(p->m, p->row_ptr, p->col_idx, p->val, xo, act);
+    csr_multiply_transpose(p->m, p->n, p->row_ptr, p->col_idx, p->val, yo, aty);
+    double pp = 0.0, dd = 0.0, bn = 0.0, cn = 0.0;
+    double pobj = obj_sign * p->obj_const, dobj = obj_sign * p->obj_const;
+    for (int32_t i = 0; i < p->m; ++i) {
+        const double lo = p->row_lo[i], hi = p->row_hi[i];
+        double v = 0.0, b = 0.0;
+        if (finite_bound(lo)) {
+            v += smax(lo - act[i], 0.0);
+            b = fabs(lo);
+        }
+        if (finite_bound(hi)) {
+            v += smax(act[i] - hi, 0.0);
+            b = smax(b, fabs(hi));
+        }
+        pp += v * v;
+        bn += b * b;
+        const double y_int = obj_sign * yo[i];
+        const double dv = sign_violation(y_int, lo, hi);
+        dd += dv * dv;
+        dobj += clipped_inf_over_box(y_int, lo, hi);
+    }
+    for (int32_t j = 0; j < p->n; ++j) {
+        const double r_int = obj_sign * (p->c[j] - aty[j]);
+        const double dv = sign_violation(r_int, p->col_lo[j], p->col_hi[j]);
+        dd += dv * dv;
+        cn += p->c[j] * p->c[j];
+        pobj += obj_sign * p->c[j] * xo[j];
+        dobj += clipped_inf_over_box(r_int, p->col_lo[j], p->col_hi[j]);
+    }
+    part[0] = sqrt(pp) / (1.0 + sqrt(bn));
+    part[1] = sqrt(dd) / (1.0 + sqrt(cn));
+    part[2] = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    return smax(smax(part[0], part[1]), part[2]);
+}
+
+/* The restart measure of restart_rule 2: the l2 norm of the three relative
+ * parts of pdlp_kkt. */
+static double l2_of_parts(const double part[3]) {
+    return sqrt(part[0] * part[0] + part[1] * part[1] + part[2] * part[2]);
+}
+
 /* ---------------------------------------------------------------------------
  * Pdhg::solve, src/l1/pdhg.cpp:218-502
  * ------------------------------------------------------------------------- */
@@ -618,11 +688,21 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         if ((it + 1) % opt->restart_check_period != 0) continue; /* pdhg.cpp:333-334 */
 
         /* pdhg.cpp:336-345 */
-        const double cur = kkt_residual(&s, c, x, y, opt->tolerance, act, aty);
         const double inv = 1.0 / (double)since_restart;
         for (int32_t j = 0; j < n; ++j) x_avg[j] = x_sum[j] * inv;
         for (int32_t i = 0; i < m; ++i) y_avg[i] = y_sum[i] * inv;
-        const double avg = kkt_residual(&s, c, x_avg, y_avg, opt->tolerance, act, aty);
+        /* restart_rule 2: current and average measured by rule 2's parts */
+        double part_cur[3] = {0, 0, 0}, part_avg[3] = {0, 0, 0};
+        double cur, avg;
+        if (opt->restart_rule == 2) {
+            pdlp_kkt(p, obj_sign, rs, cs, x, y, xo, yo, act, aty, part_cur);
+            pdlp_kkt(p, obj_sign, rs, cs, x_avg, y_avg, xo, yo, act, aty, part_avg);
+            cur = l2_of_parts(part_cur);
+            avg = l2_of_parts(part_avg);
+        } else {
+            cur = kkt_residual(&s, c, x, y, opt->tolerance, act, aty);
+            avg = kkt_residual(&s, c, x_avg, y_avg, opt->tolerance, act, aty);
+        }
         if (!isfinite(cur) || !isfinite(avg)) { /* pdhg.cpp:347-352 */
             info->status = ORC_NUMERICAL_FAILURE;
             snprintf(info->message, sizeof info->message,
@@ -635,6 +715,13 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         const double* cy = avg_better ? y_avg : y;
         const double bound_tol = opt->tolerance > 1e-6 ? opt->tolerance : 1e-6;
         double rel = 0.0;
+        double part[3];
+        if (opt->termination_rule == 2)
+            rel = (opt->restart_rule == 2)
+                      ? smax(smax((avg_better ? part_avg : part_cur)[0],
+                                  (avg_better ? part_avg : part_cur)[1]),
+                             (avg_better ? part_avg : part_cur)[2])
+                      : pdlp_kkt(p, obj_sign, rs, cs, cx, cy, xo, yo, act, aty, part);
         const double orig = original_residual(p, obj_sign, rs, cs, cx, cy, bound_tol, xo, yo,
                                               act, aty,
                                               opt->termination_rule == 1 ? &rel : NULL);
@@ -648,7 +735,8 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         if (opt->checkpoint != NULL) /* pdhg.cpp:378-381 (xo, yo are unscale_to_original) */
             opt->checkpoint(opt->checkpoint_user, it, xo, yo, orig);
 
-        const int done = (opt->termination_rule == 1) ? (rel < opt->tolerance)
+        info->relative_kkt = rel;
+        const int done = (opt->termination_rule != 0) ? (rel < opt->tolerance)
                                                         : (orig < opt->tolerance);
         if (done) { /* pdhg.cpp:383-389 */
             best_x = cx;
@@ -662,7 +750,7 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         if (opt->restart_rule == 0) {
             restart = avg <= opt->restart_sufficient_decrease * res_last; /* pdhg.cpp:393 */
             if (restart) res_last = avg;
-        } else { /* extension: adaptive rule */
+        } else { /* extension: adaptive rule (restart_rule 1 and 2) */
             const double cand = avg_better ? avg : cur;
             const int sufficient = cand <= 0.2 * res_last;
             const int necessary = cand <= 0.8 * res_last && cand > res_prev_cand;

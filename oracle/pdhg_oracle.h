@@ -63,7 +63,11 @@ typedef void (*orc_checkpoint_fn)(void* user, long long iteration, const double*
  * (include/sovereign/scaling.hpp:296-310), plus extensions that are OFF by
  * default (the reference has none of them):
  *   termination_rule  0 = reference absolute original-space residual < tol,
- *                     1 = relative KKT (see orc_relative_kkt below);
+ *                     1 = relative KKT on the reference's max-norm residual
+ *                         terms (original_residual in pdhg_oracle.c),
+ *                     2 = PDLP's relative KKT with l2 norms (pdlp_kkt in
+ *                         pdhg_oracle.c): max(||row violation||/(1+||b||),
+ *                         ||dual sign violation||/(1+||c||), gap) < tol;
  *   trace_iters       record x, y after each of the first trace_iters iterations. */
 typedef struct {
     double tolerance;
@@ -117,6 +121,9 @@ typedef struct {
     double operator_norm_estimate;
     int has_point; /* 0 when the reference returns empty primal/dual vectors */
     char message[256];
+    /* extension: the relative-KKT value (termination_rule 1 or 2) of the last
+     * check's candidate; 0 under rule 0 and in the reference */
+    double relative_kkt;
 } orc_info;
 
 void orc_default_options(orc_options* opt);

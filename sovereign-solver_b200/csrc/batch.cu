@@ -358,7 +358,7 @@ int batch_load(BatchCtx& c, int32_t count, const int32_t* row_off, const int32_t
         }
         c.n_chk = static_cast<int32_t>(items.size());
         BCK(upload(c.chk_item, items, s));
-        BCK(c.chk_part.alloc(12 * items.size()));
+        BCK(c.chk_part.alloc(kBatchCheckVals * items.size()));
         BCK(c.chk_ticket.alloc(static_cast<size_t>(count)));
         BCK(cudaMemsetAsync(c.chk_ticket.p, 0, sizeof(unsigned int) * count, s));
         BCK(cudaStreamSynchronize(s));  // the host vector is read by the copy above
@@ -576,10 +576,11 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
     }
     if (o.checkpoint != nullptr || o.trace_iters > 0 || o.infeasibility_detection != 0 ||
         o.restart_check_period < 1 ||
-        o.termination_rule < 0 || o.termination_rule > 1 || o.restart_rule < 0 ||
-        o.restart_rule > 1 || o.power_iterations < 0) {
+        o.termination_rule < 0 || o.termination_rule > 2 || o.restart_rule < 0 ||
+        o.restart_rule > 2 || o.power_iterations < 0 ||
+        (o.restart_rule == 2 && o.termination_rule != 2)) {
         c.err = "pdhg_solve_batch: invalid options (no checkpoint / trace / infeasibility "
-                "detection in batches)";
+                "detection in batches; restart rule 2 needs termination rule 2)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     BCK(cudaSetDevice(c.device));

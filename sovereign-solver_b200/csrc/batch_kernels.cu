@@ -134,9 +134,18 @@ __device__ __forceinline__ void inst_row_terms(const BatchView& b, const Iterate
     t.oap = smax(t.oap, primal_term(aoa, lo_o, hi_o));
     t.ocd = smax(t.ocd, cs_term(yc * rs, aoc, lo_o, hi_o, p.bound_tol));
     t.oad = smax(t.oad, cs_term(ya * rs, aoa, lo_o, hi_o, p.bound_tol));
-    if (p.termination_rule == 1) {
+    if (p.termination_rule != 0) {
         t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
+    }
+    if (p.termination_rule == 2) {  // squares of the row violation and of y's sign violation
+        const double pc = primal_term(aoc, lo_o, hi_o), pa = primal_term(aoa, lo_o, hi_o);
+        const double dc = sign_violation(yc * rs, lo_o, hi_o);
+        const double da = sign_violation(ya * rs, lo_o, hi_o);
+        t.ppc += pc * pc;
+        t.ppa += pa * pa;
+        t.ddc += dc * dc;
+        t.dda += da * da;
     }
 }
 
@@ -157,7 +166,13 @@ __device__ __forceinline__ void inst_col_terms(const BatchView& b, const Iterate
     const double lo_o = P.lo_o[j], hi_o = P.hi_o[j];
     t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, p.bound_tol));
     t.oad = smax(t.oad, cs_term(ra / cs, xa * cs, lo_o, hi_o, p.bound_tol));
-    if (p.termination_rule == 1) {
+    if (p.termination_rule == 2) {  // squares of the reduced cost's sign violation
+        const double dc = sign_violation(rc / cs, lo_o, hi_o);
+        const double da = sign_violation(ra / cs, lo_o, hi_o);
+        t.ddc += dc * dc;
+        t.dda += da * da;
+    }
+    if (p.termination_rule != 0) {
         t.pobj_c += sign * P.c_o[j] * (xc * cs);
         t.pobj_a += sign * P.c_o[j] * (xa * cs);
         t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
@@ -224,31 +239,38 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
     Terms t;
     inst_pass<T, false>(b, it, p, k, part, parts, inv, s.obj_sign, t);
     inst_pass<T, true>(b, it, p, k, part, parts, inv, s.obj_sign, t);
-    double v[12];
+    constexpr int K = kBatchCheckVals;
+    double v[K];
     v[0] = bmax(t.cp); v[1] = bmax(t.cd); v[2] = bmax(t.ap); v[3] = bmax(t.ad);
     v[4] = bmax(t.ocp); v[5] = bmax(t.ocd); v[6] = bmax(t.oap); v[7] = bmax(t.oad);
-    v[8] = v[9] = v[10] = v[11] = 0.0;
-    if (p.termination_rule == 1) {
+    for (int q = 8; q < K; ++q) v[q] = 0.0;
+    if (p.termination_rule != 0) {
         v[8] = block_sum_det(t.pobj_c);
         v[9] = block_sum_det(t.dobj_c);
         v[10] = block_sum_det(t.pobj_a);
         v[11] = block_sum_det(t.dobj_a);
     }
+    if (p.termination_rule == 2) {
+        v[12] = block_sum_det(t.ppc);
+        v[13] = block_sum_det(t.ddc);
+        v[14] = block_sum_det(t.ppa);
+        v[15] = block_sum_det(t.dda);
+    }
     if (threadIdx.x != 0) return;
     if (parts > 1) {
         // store this part, take the instance's ticket; the last part merges
         // (maxima order-free, sums in part order) and goes on to the decision
-        double* mine = b.chk_part + 12 * static_cast<int64_t>(blockIdx.x);
-        for (int q = 0; q < 12; ++q) mine[q] = v[q];
+        double* mine = b.chk_part + K * static_cast<int64_t>(blockIdx.x);
+        for (int q = 0; q < K; ++q) mine[q] = v[q];
         __threadfence();
         if (atomicAdd(b.chk_ticket + k, 1u) != static_cast<unsigned>(parts - 1)) return;
         __threadfence();
-        const double* first = b.chk_part + 12 * (static_cast<int64_t>(blockIdx.x) - part);
-        for (int q = 0; q < 12; ++q) v[q] = q < 8 ? 0.0 : __ldcg(first + q);
+        const double* first = b.chk_part + K * (static_cast<int64_t>(blockIdx.x) - part);
+        for (int q = 0; q < K; ++q) v[q] = q < 8 ? 0.0 : __ldcg(first + q);
         for (int j = 0; j < parts; ++j) {
-            for (int q = 0; q < 8; ++q) v[q] = smax(v[q], __ldcg(first + 12 * j + q));
+            for (int q = 0; q < 8; ++q) v[q] = smax(v[q], __ldcg(first + K * j + q));
             if (j > 0)
-                for (int q = 8; q < 12; ++q) v[q] += __ldcg(first + 12 * j + q);
+                for (int q = 8; q < K; ++q) v[q] += __ldcg(first + K * j + q);
         }
         b.chk_ticket[k] = 0u;
     }
@@ -256,7 +278,27 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
     const double ocp = v[4], ocd = v[5], oap = v[6], oad = v[7];
     const double s0 = v[8], s1 = v[9], s2 = v[10], s3 = v[11];
     // ---- the instance's decision (as the single engine's check) ----
-    const double cur = smax(cp, cd), avg = smax(ap, ad);
+    double cur = smax(cp, cd), avg = smax(ap, ad);
+    // termination rule 2: relative parts of the current point and the average
+    // (original units, l2 norms); their l2 norm is restart rule 2's measure
+    double part_c[3] = {0, 0, 0}, part_a[3] = {0, 0, 0};
+    if (p.termination_rule == 2) {
+        const double k0 = s.obj_sign * s.obj_const;
+        const double pp[2] = {v[12], v[14]}, dd[2] = {v[13], v[15]};
+        const double ps[2] = {s0 + k0, s2 + k0}, ds[2] = {s1 + k0, s3 + k0};
+        for (int w = 0; w < 2; ++w) {
+            double* pt = w ? part_a : part_c;
+            pt[0] = sqrt(pp[w]) / (1.0 + s.bnorm2);
+            pt[1] = sqrt(dd[w]) / (1.0 + s.cnorm2);
+            pt[2] = fabs(ps[w] - ds[w]) / (1.0 + fabs(ps[w]) + fabs(ds[w]));
+        }
+        if (p.restart_rule == 2) {
+            const double mc = sqrt(part_c[0] * part_c[0] + part_c[1] * part_c[1] + part_c[2] * part_c[2]);
+            const double ma = sqrt(part_a[0] * part_a[0] + part_a[1] * part_a[1] + part_a[2] * part_a[2]);
+            cur = isfinite(cur) ? mc : cur;
+            avg = isfinite(avg) ? ma : avg;
+        }
+    }
     s.cur_res = cur;
     s.avg_res = avg;
     s.inv = inv;
@@ -285,7 +327,10 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
         return;
     }
     double rel = 0.0;
-    if (p.termination_rule == 1) {
+    if (p.termination_rule == 2) {
+        const double* pt = ab ? part_a : part_c;
+        rel = smax(smax(pt[0], pt[1]), pt[2]);
+    } else if (p.termination_rule == 1) {
         // the objective constant shifts both objectives
         const double ps = (ab ? s2 : s0) + s.obj_sign * s.obj_const;
         const double ds = (ab ? s3 : s1) + s.obj_sign * s.obj_const;
@@ -293,7 +338,7 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
         rel = smax(smax(op / (1.0 + s.bnorm), od / (1.0 + s.cnorm)), gap);
     }
     s.rel_kkt = rel;
-    const bool conv = (p.termination_rule == 1) ? (rel < p.tol) : (orig < p.tol);
+    const bool conv = (p.termination_rule != 0) ? (rel < p.tol) : (orig < p.tol);
     if (conv) {
         s.done = 1;
         s.converged = 1;
@@ -335,8 +380,13 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
     s.fresh = s.restart;
     s.fold = std::is_same<T, float>::value ? 1 : 0;
     if (p.allow_switch) {  // no 2% gain in 25 checks: the FP32 phase of this instance ends
-        const double r = p.termination_rule == 1 ? rel : orig;
-        if (r < 0.98 * s.best_res) {
+        // under the relative rules only at FP32's precision floor (as the
+        // single engine: plateaus above kFp32Zone are the method's own)
+        const double r = p.termination_rule != 0 ? rel : orig;
+        if (p.termination_rule != 0 && r > kFp32Zone) {
+            s.since_improve = 0;
+            if (r < s.best_res) s.best_res = r;
+        } else if (r < 0.98 * s.best_res) {
             s.best_res = r;
             s.since_improve = 0;
         } else if (++s.since_improve >= 25) {
@@ -671,10 +721,11 @@ __global__ void __launch_bounds__(kBlock) batch_norms(BatchView b) {
     const int k = blockIdx.x;
     InstState& s = b.is[k];
     const DevProblem& P = b.P;
-    double c2 = 0.0, b2 = 0.0, cm = 0.0, bm = 0.0;
+    double c2 = 0.0, b2 = 0.0, cm = 0.0, bm = 0.0, c2o = 0.0, b2o = 0.0;
     for (int j = b.col_off[k] + threadIdx.x; j < b.col_off[k + 1]; j += kBlock) {
         c2 += P.c[j] * P.c[j];
         cm = fmax(cm, fabs(P.c_o[j]));
+        c2o += P.c_o[j] * P.c_o[j];
     }
     for (int i = b.row_off[k] + threadIdx.x; i < b.row_off[k + 1]; i += kBlock) {
         double bb = 0.0;
@@ -685,14 +736,18 @@ __global__ void __launch_bounds__(kBlock) batch_norms(BatchView b) {
         if (fb(P.rlo_o[i])) bo = fabs(P.rlo_o[i]);
         if (fb(P.rhi_o[i])) bo = smax(bo, fabs(P.rhi_o[i]));
         bm = fmax(bm, bo);
+        b2o += bo * bo;
     }
     const double c2t = block_sum_det(c2), b2t = block_sum_det(b2);
+    const double c2ot = block_sum_det(c2o), b2ot = block_sum_det(b2o);
     const double cmt = bmax(cm), bmt = bmax(bm);
     if (threadIdx.x == 0) {
         s.cnorm2_s = sqrt(c2t);
         s.bnorm2_s = sqrt(b2t);
         s.cnorm = cmt;
         s.bnorm = bmt;
+        s.cnorm2 = sqrt(c2ot);
+        s.bnorm2 = sqrt(b2ot);
     }
 }
 

@@ -35,9 +35,14 @@ struct InstState {
     double res_last, res_prev_cand, cur_res, avg_res, orig_res, rel_kkt, inv;
     double tau, sigma, omega, eta;
     double obj_sign, obj_const, bnorm, cnorm, cnorm2_s, bnorm2_s;
+    double bnorm2, cnorm2;  // termination rule 2 norms (original, l2)
     double opnorm;
     double objective, dual_objective, gap, pinf, dinf;
 };
+
+// Values per check item: 8 maxima, 4 objective sums, 4 sums of squares of
+// termination rule 2.
+constexpr int kBatchCheckVals = 16;
 
 struct BatchGlobal {
     int done;          // every instance finished (or the budget ended)
@@ -61,7 +66,7 @@ struct BatchView {
     // The check's CTA items: instance k's rows and columns in C parts, part j
     // of C = {k, j, C, -} (C by the instance's size, so that no single CTA
     // sums a large instance while the rest of the GPU waits). A CTA stores its
-    // partial maxima and sums (12 per item) and takes the instance's ticket;
+    // partial maxima and sums (kBatchCheckVals per item) and takes the instance's ticket;
     // the last CTA of the instance merges them in item order and decides.
     const int4* chk_item = nullptr;
     int32_t n_chk = 0;

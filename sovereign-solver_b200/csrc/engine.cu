@@ -71,6 +71,7 @@ struct Ctx {
     ScalingParams sp;
     bool scaled = false;
     double bnorm = 0, cnorm = 0;       // relative-KKT norms, original space (inf-norms)
+    double bnorm2 = 0, cnorm2 = 0;     // termination rule 2 norms, original space (l2)
     double cnorm2_s = 0, bnorm2_s = 0;  // initial primal weight |c|_2 / |b|_2, scaled space
 
     MatDev Ao, ATo, As, ATs;
@@ -152,6 +153,8 @@ struct Ctx {
         P.rhi32 = rhi32.p;
         P.bnorm = bnorm;
         P.cnorm = cnorm;
+        P.bnorm2 = bnorm2;
+        P.cnorm2 = cnorm2;
         return P;
     }
 };
@@ -284,6 +287,8 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     c.bnorm2_s = std::sqrt(h.norms[1]);
     c.cnorm = h.norms[2];
     c.bnorm = h.norms[3];
+    c.cnorm2 = std::sqrt(h.norms[4]);
+    c.bnorm2 = std::sqrt(h.norms[5]);
     c.scaled = true;
     c.have_opnorm = false;
     c.gen += 1;
@@ -638,8 +643,16 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
             }
         }
         if (allow_switch && !done) {
-            const double r = o.termination_rule == 1 ? rel_kkt : orig_res;
-            if (r < 0.98 * best) {
+            // The FP32 phase hands over to FP64 when it stops improving (no 2%
+            // gain in 25 checks) at its precision floor. Under the relative
+            // rules a plateau counts only within kFp32Zone of FP32's unit
+            // roundoff: higher plateaus are the method's, and FP64 iterations
+            // would not end them sooner.
+            const double r = o.termination_rule != 0 ? rel_kkt : orig_res;
+            if (o.termination_rule != 0 && r > kFp32Zone) {
+                since_improve = 0;
+                if (r < best) best = r;
+            } else if (r < 0.98 * best) {
                 best = r;
                 since_improve = 0;
             } else if (++since_improve >= 25 && !stop_sent) {
@@ -1014,10 +1027,16 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
         return PDHG_OK;
     }
     if (o.restart_check_period < 1 || o.power_iterations < 0 || o.precision < 0 ||
-        o.precision > 2 || o.termination_rule < 0 || o.termination_rule > 1 ||
-        o.restart_rule < 0 || o.restart_rule > 1 || o.primal_weight_update < 0 ||
+        o.precision > 2 || o.termination_rule < 0 || o.termination_rule > 2 ||
+        o.restart_rule < 0 || o.restart_rule > 2 || o.primal_weight_update < 0 ||
         o.primal_weight_update > 1) {
         c.err = "pdhg_solve: invalid options";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
+    if ((o.termination_rule == 2 && o.precision == PDHG_PREC_FP64_EXACT) ||
+        (o.restart_rule == 2 && o.termination_rule != 2)) {
+        c.err = "pdhg_solve: termination rule 2 needs precision mixed or fp64, and restart rule 2 "
+                "needs termination rule 2 (it restarts on rule 2's measure)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     if (o.precision == PDHG_PREC_FP64_EXACT && (o.restart_rule != 0 || o.primal_weight_update)) {

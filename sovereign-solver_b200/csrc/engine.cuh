@@ -153,7 +153,12 @@ enum Ticket { TK_CHECK1 = 0, TK_CHECK2, TK_FAST, TK_RESTART, TK_COUNT = 4 };
 
 // Per-CTA partial sums of the fast check kernel: the objectives (4), the
 // Farkas ranges (4), c^T dx of the ray test (1).
-constexpr int kCheckSums = 9;
+constexpr int kCheckSums = 13;
+
+// Mixed precision: a relative-KKT plateau above this value (1024 units of
+// FP32 roundoff) is the method's own, not FP32's precision floor, so the FP32
+// phase keeps running there.
+constexpr double kFp32Zone = 1024.0 * 1.1920928955078125e-7;
 
 struct DevState {
     int done;         // 1 = every later kernel returns at once
@@ -215,7 +220,8 @@ struct DevProblem {
     const double *rs = nullptr, *cs = nullptr;                  // row / column scale
     const float *c32 = nullptr, *lo32 = nullptr, *hi32 = nullptr;
     const float *rlo32 = nullptr, *rhi32 = nullptr;
-    double bnorm = 0.0, cnorm = 0.0;  // relative-KKT norms (original space)
+    double bnorm = 0.0, cnorm = 0.0;    // relative-KKT norms (original space, inf-norms)
+    double bnorm2 = 0.0, cnorm2 = 0.0;  // termination rule 2 norms (original space, l2)
 };
 
 // Iterates. T = double for the FP64 modes, float for the mixed mode; the
@@ -404,11 +410,14 @@ int build_transpose(int32_t m, int32_t n, int64_t nnz, const int32_t* rp, const 
 void launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
 
 // ---- intake (intake.cu) --------------------------------------------------------
+constexpr int kNorms = 6;
 struct IntakeState {
     unsigned long long worst;  // Ruiz: max |row/col max - 1| of the sweep (bit pattern)
     unsigned int ticket;
     int ruiz_done;             // set when a sweep's worst < tolerance (scaling.cpp:72)
-    double norms[4];           // |c_s|^2, |b_s|^2, max|c_o|, max finite |row bound|
+    // |c_s|_2^2, |b_s|_2^2, |c_o|_inf, |b_o|_inf, |c_o|_2^2, |b_o|_2^2, with b_i
+    // the larger finite |row bound| of row i (0 if none)
+    double norms[kNorms];
 };
 // Device problem checks, OR-ed into *flags: 1 a column, 2 a row, 4 an entry's
 // column out of range, 8 an entry out of order or non-finite. c == NULL skips

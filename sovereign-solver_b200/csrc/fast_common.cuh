@@ -417,10 +417,30 @@ __device__ __forceinline__ double clipped_inf(double coeff, double lo, double hi
     return 0.0;
 }
 
+// Instances of the check kernel: with the infeasibility tests, with the sums
+// of squares of termination rule 2.
+constexpr int kCheckInf = 1;
+constexpr int kCheckL2 = 2;
+
+// The part of a multiplier or reduced cost v (internal minimize sense)
+// outside the sign the bounds of its row or column allow: >= 0 with only a
+// finite lower end, <= 0 with only a finite upper end, any sign with both,
+// 0 with neither.
+__device__ __forceinline__ double sign_violation(double v, double lo, double hi) {
+    const bool fl = fb(lo), fh = fb(hi);
+    if (fl && fh) return 0.0;
+    if (fl) return v < 0.0 ? -v : 0.0;
+    if (fh) return v > 0.0 ? v : 0.0;
+    return fabs(v);
+}
+
 struct Terms {
     double cp = 0, cd = 0, ap = 0, ad = 0;         // scaled: cur / avg, primal / dual
     double ocp = 0, ocd = 0, oap = 0, oad = 0;     // original space
     double pobj_c = 0, dobj_c = 0, pobj_a = 0, dobj_a = 0;
+    // termination rule 2: sums of squares of the primal and dual violations
+    // (original units), current and average
+    double ppc = 0, ddc = 0, ppa = 0, dda = 0;
     // infeasibility test: row-side and column-side ranges of the change of y
     // (FarkasCertificate::row_side_range / column_side_range), max |dy|
     double rlo = 0, rhi = 0, clo = 0, chi = 0, raymax = 0;

@@ -415,13 +415,16 @@ __global__ void __launch_bounds__(kBlock) k_norms(int32_t m, int32_t n, const do
                                                   const double* c_o, const double* rlo_o,
                                                   const double* rhi_o, double* part,
                                                   IntakeState* is) {
-    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    // sums of squares (q[0], q[1], q[4], q[5]) and maxima (q[2], q[3])
+    constexpr int K = kNorms;
+    double q[K] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     const int32_t nmax = m > n ? m : n;
     for (int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; t < nmax;
          t += static_cast<int64_t>(gridDim.x) * kBlock) {
         if (t < n) {
             q[0] += c_s[t] * c_s[t];
             q[2] = fmax(q[2], fabs(c_o[t]));
+            q[4] += c_o[t] * c_o[t];
         }
         if (t < m) {
             double b = 0.0;
@@ -432,45 +435,37 @@ __global__ void __launch_bounds__(kBlock) k_norms(int32_t m, int32_t n, const do
             if (fb(rlo_o[t])) bo = fabs(rlo_o[t]);
             if (fb(rhi_o[t])) bo = smax(bo, fabs(rhi_o[t]));
             q[3] = fmax(q[3], bo);
+            q[5] += bo * bo;
         }
     }
-    __shared__ double sh[4][kBlock];
-    for (int i = 0; i < 4; ++i) sh[i][threadIdx.x] = q[i];
-    __syncthreads();
-    for (int s = kBlock / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
-            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
-            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + s]);
-        }
+    __shared__ double sh[K][kBlock];
+    auto fold = [&]() {
         __syncthreads();
-    }
+        for (int s = kBlock / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
+                for (int i = 0; i < K; ++i)
+                    sh[i][threadIdx.x] = (i == 2 || i == 3)
+                                             ? fmax(sh[i][threadIdx.x], sh[i][threadIdx.x + s])
+                                             : sh[i][threadIdx.x] + sh[i][threadIdx.x + s];
+            }
+            __syncthreads();
+        }
+    };
+    for (int i = 0; i < K; ++i) sh[i][threadIdx.x] = q[i];
+    fold();
     if (threadIdx.x == 0)
-        for (int i = 0; i < 4; ++i) part[4 * blockIdx.x + i] = sh[i][0];
+        for (int i = 0; i < K; ++i) part[K * blockIdx.x + i] = sh[i][0];
     if (!last_cta(&is->ticket)) return;
     // last CTA: each thread folds a strided subset of the partials in block order
-    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    double r[K] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     const volatile double* p = part;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock) {
-        r[0] += p[4 * b];
-        r[1] += p[4 * b + 1];
-        r[2] = fmax(r[2], p[4 * b + 2]);
-        r[3] = fmax(r[3], p[4 * b + 3]);
-    }
-    for (int i = 0; i < 4; ++i) sh[i][threadIdx.x] = r[i];
-    __syncthreads();
-    for (int s = kBlock / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
-            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
-            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + s]);
-        }
-        __syncthreads();
-    }
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock)
+        for (int i = 0; i < K; ++i)
+            r[i] = (i == 2 || i == 3) ? fmax(r[i], p[K * b + i]) : r[i] + p[K * b + i];
+    for (int i = 0; i < K; ++i) sh[i][threadIdx.x] = r[i];
+    fold();
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 4; ++i) is->norms[i] = sh[i][0];
+        for (int i = 0; i < K; ++i) is->norms[i] = sh[i][0];
         is->ticket = 0u;
     }
 }
@@ -578,7 +573,7 @@ void launch_validate(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
     k_validate<<<g, kBlock, 0, s>>>(m, n, rp, ci, v, c, clo, chi, rlo, rhi, lanes, flags);
 }
 
-int norms_part_size(int32_t m, int32_t n) { return 4 * (kGridCap + 1); }
+int norms_part_size(int32_t m, int32_t n) { return kNorms * (kGridCap + 1); }
 
 void launch_norms(int32_t m, int32_t n, const double* c_s, const double* rlo_s,
                   const double* rhi_s, const double* c_o, const double* rlo_o,

@@ -503,9 +503,11 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
 // Per-row terms, merged into the thread's running maxima / sums. INF: with
 // the infeasibility tests (option infeasibility_detection), a separate
 // instance so that the plain check keeps its registers.
-template <class T, bool INF>
+template <class T, int F>
 __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double act_c,
                                           double act_a, double inv, Terms& t) {
+    constexpr bool INF = (F & kCheckInf) != 0;
+    constexpr bool L2 = (F & kCheckL2) != 0;
     const DevProblem& P = a.P;
     a.cs.act_avg[i] = act_a;
     const double lo = P.rlo[i], hi = P.rhi[i];
@@ -522,9 +524,18 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
     t.oap = smax(t.oap, primal_term(aoa, lo_o, hi_o));
     t.ocd = smax(t.ocd, cs_term(yc * rs, aoc, lo_o, hi_o, a.bound_tol));
     t.oad = smax(t.oad, cs_term(ya * rs, aoa, lo_o, hi_o, a.bound_tol));
-    if (a.termination_rule == 1) {  // internal (minimize) sense: y_int = y_s * rs
+    if (a.termination_rule != 0) {  // internal (minimize) sense: y_int = y_s * rs
         t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
+    }
+    if (L2) {  // termination rule 2: squares of the row violation and of y's sign violation
+        const double pc = primal_term(aoc, lo_o, hi_o), pa = primal_term(aoa, lo_o, hi_o);
+        const double dc = sign_violation(yc * rs, lo_o, hi_o);
+        const double da = sign_violation(ya * rs, lo_o, hi_o);
+        t.ppc += pc * pc;
+        t.ppa += pa * pa;
+        t.ddc += dc * dc;
+        t.dda += da * da;
     }
     if (INF) {  // the change of y since the previous check, original units
         const double dy = P.obj_sign * rs * (yc - a.ray_y_prev[i]);
@@ -535,9 +546,11 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
     }
 }
 
-template <class T, bool INF>
+template <class T, int F>
 __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double aty_c,
                                           double aty_a, double inv, Terms& t) {
+    constexpr bool INF = (F & kCheckInf) != 0;
+    constexpr bool L2 = (F & kCheckL2) != 0;
     const DevProblem& P = a.P;
     const double cj = P.c[j];
     const double lo = P.lo[j], hi = P.hi[j];
@@ -550,7 +563,13 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
     const double lo_o = P.lo_o[j], hi_o = P.hi_o[j];
     t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol));
     t.oad = smax(t.oad, cs_term(ra / cs, xa * cs, lo_o, hi_o, a.bound_tol));
-    if (a.termination_rule == 1) {  // internal sense: c_int x = sign c_o x, r_int = r_s / cs
+    if (L2) {  // termination rule 2: squares of the reduced cost's sign violation
+        const double dc = sign_violation(rc / cs, lo_o, hi_o);
+        const double da = sign_violation(ra / cs, lo_o, hi_o);
+        t.ddc += dc * dc;
+        t.dda += da * da;
+    }
+    if (a.termination_rule != 0) {  // internal sense: c_int x = sign c_o x, r_int = r_s / cs
         t.pobj_c += P.obj_sign * P.c_o[j] * (xc * cs);
         t.pobj_a += P.obj_sign * P.c_o[j] * (xa * cs);
         t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
@@ -621,17 +640,17 @@ __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr
     }
 }
 
-template <class T, bool ROWS, bool INF>
+template <class T, bool ROWS, int F>
 __device__ __forceinline__ void row_or_col_terms(const FastCheck<T>& a, int r, double ac, double aa,
                                                  double inv, Terms& t) {
-    if (ROWS) row_terms<T, INF>(a, r, ac, aa, inv, t);
-    else col_terms<T, INF>(a, r, ac, aa, inv, t);
+    if (ROWS) row_terms<T, F>(a, r, ac, aa, inv, t);
+    else col_terms<T, F>(a, r, ac, aa, inv, t);
 }
 
 // Virtual block vb of one matrix's part [short | warp rows | CTA items]:
 // short rows on groups of M.vw lanes, rows up to kLongRow one warp each
 // (warp_rows0), longer ones as CTA items (items_long). Block-uniform.
-template <class T, bool ROWS, bool INF>
+template <class T, bool ROWS, int F>
 __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int sb, int wb,
                            double inv, Terms& t) {
     double ac = 0.0, aa = 0.0;
@@ -645,7 +664,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         row_products<T, ROWS>(a, M, b + lane, e, vw, inv, ac, aa);
         ac = group_sum(ac, vw);
         aa = group_sum(aa, vw);
-        if (lane == 0) row_or_col_terms<T, ROWS, INF>(a, r, ac, aa, inv, t);
+        if (lane == 0) row_or_col_terms<T, ROWS, F>(a, r, ac, aa, inv, t);
     } else if (vb < sb + wb) {
         const int w = (vb - sb) * (kBlock / 32) + (threadIdx.x >> 5);
         if (w >= M.n_warp0) return;
@@ -656,7 +675,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
             ac += __shfl_xor_sync(0xffffffffu, ac, o);
             aa += __shfl_xor_sync(0xffffffffu, aa, o);
         }
-        if (lane == 0) row_or_col_terms<T, ROWS, INF>(a, r, ac, aa, inv, t);
+        if (lane == 0) row_or_col_terms<T, ROWS, F>(a, r, ac, aa, inv, t);
     } else {
         const int idx = vb - sb - wb;
         const int4 w = M.items_long.item[idx];
@@ -664,7 +683,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         ac = block_total(ac);
         aa = block_total(aa);
         if (w.w >= 0 && !segment_finish(M.items_long, idx, w.w, ac, aa, &ac, &aa)) return;
-        if (threadIdx.x == 0) row_or_col_terms<T, ROWS, INF>(a, w.x, ac, aa, inv, t);
+        if (threadIdx.x == 0) row_or_col_terms<T, ROWS, F>(a, w.x, ac, aa, inv, t);
     }
 }
 
@@ -674,7 +693,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
 // demand rows of a transportation LP). Each lane sums in k order; a slice cut
 // into several items combines each lane's two sums in item order through the
 // check's own ticket and partials.
-template <class T, bool ROWS, bool INF>
+template <class T, bool ROWS, int F>
 __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, double inv, Terms& t) {
     const RowSlices& S = M.slices;
     const int idx = vb * (kBlock / 32) + (threadIdx.x >> 5);
@@ -738,7 +757,7 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
         ac = sc;
         aa = sa;
     }
-    if (row >= 0) row_or_col_terms<T, ROWS, INF>(a, row, ac, aa, inv, t);
+    if (row >= 0) row_or_col_terms<T, ROWS, F>(a, row, ac, aa, inv, t);
 }
 
 // Virtual blocks of the check over one matrix: short-row blocks (M.vw lanes
@@ -781,9 +800,11 @@ inline DevCsr check_view(const DevCsr& M) {
 // CTAs without spills (and 484 before the slice walk). Unbounded it took
 // 109-118 registers and two CTAs per SM. The instance with the infeasibility
 // tests (INF) carries 11 more running terms: two CTAs per SM.
-template <class T, bool INF>
-__global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
+template <class T, int F>
+__global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 ? 4 : 3))
     fast_check(FastCheck<T> a) {
+    constexpr bool INF = (F & kCheckInf) != 0;
+    constexpr bool L2 = (F & kCheckL2) != 0;
     DevState* st = a.st;
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
@@ -795,18 +816,19 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
     const int nA = pA + check_slice_blocks(a.A);
     const int nT = pT + check_slice_blocks(a.AT);
     for (int bid = blockIdx.x; bid < nA + nT; bid += gridDim.x) {
-        if (bid < pA) check_part<T, true, INF>(a, a.A, bid, sbA, wbA, inv, t);
-        else if (bid < nA) check_slices<T, true, INF>(a, a.A, bid - pA, inv, t);
-        else if (bid < nA + pT) check_part<T, false, INF>(a, a.AT, bid - nA, sbT, wbT, inv, t);
-        else check_slices<T, false, INF>(a, a.AT, bid - nA - pT, inv, t);
+        if (bid < pA) check_part<T, true, F>(a, a.A, bid, sbA, wbA, inv, t);
+        else if (bid < nA) check_slices<T, true, F>(a, a.A, bid - pA, inv, t);
+        else if (bid < nA + pT) check_part<T, false, F>(a, a.AT, bid - nA, sbT, wbT, inv, t);
+        else check_slices<T, false, F>(a, a.AT, bid - nA - pT, inv, t);
     }
     block_max_terms<INF>(t, st->acc);
     // per-CTA partial sums, kCheckSums per CTA: the objectives [0..3]
-    // (relative-KKT rule), the infeasibility test's ranges [4..7], the ray
-    // test's c^T dx [8]
-    const bool sum_obj = a.termination_rule == 1, sum_ray = INF;
-    if (sum_obj || sum_ray) {
-        double v[kCheckSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // (relative-KKT rules), the infeasibility test's ranges [4..7], the ray
+    // test's c^T dx [8], rule 2's sums of squares [9..12]
+    const bool sum_obj = a.termination_rule != 0, sum_ray = INF;
+    auto summed = [&](int q) { return q < 4 ? sum_obj : q < 9 ? sum_ray : L2; };
+    if (sum_obj || sum_ray || L2) {
+        double v[kCheckSums] = {};
         if (sum_obj) {
             v[0] = block_sum_det(t.pobj_c);
             v[1] = block_sum_det(t.dobj_c);
@@ -820,18 +842,24 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
             v[7] = block_sum_det(t.chi);
             v[8] = block_sum_det(t.xobj);
         }
+        if (L2) {
+            v[9] = block_sum_det(t.ppc);
+            v[10] = block_sum_det(t.ddc);
+            v[11] = block_sum_det(t.ppa);
+            v[12] = block_sum_det(t.dda);
+        }
         if (threadIdx.x == 0)
             for (int q = 0; q < kCheckSums; ++q) a.cs.part[kCheckSums * blockIdx.x + q] = v[q];
     }
     if (!last_block(&st->ticket[TK_FAST])) return;
     // the per-CTA partial sums, added by the whole last CTA in a fixed order
     // (strided, then a tree)
-    double obj[kCheckSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (sum_obj || sum_ray) {
+    double obj[kCheckSums] = {};
+    if (sum_obj || sum_ray || L2) {
         for (unsigned b = threadIdx.x; b < gridDim.x; b += kBlock)
             for (int q = 0; q < kCheckSums; ++q) obj[q] += __ldcg(a.cs.part + kCheckSums * b + q);
         for (int q = 0; q < kCheckSums; ++q)
-            if (q < 4 ? sum_obj : sum_ray) obj[q] = block_sum_det(obj[q]);
+            if (summed(q)) obj[q] = block_sum_det(obj[q]);
     }
     if (threadIdx.x != 0) return;
 
@@ -845,7 +873,30 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
     for (int q = ACC_CUR_P; q <= ACC_OA_D; ++q) st->acc[q] = 0ull;
     st->acc[ACC_RAY] = st->acc[ACC_XRAY_V] = st->acc[ACC_XRAY_MAX] = 0ull;
     st->ticket[TK_FAST] = 0u;
-    const double cur = smax(cp, cd), avg = smax(ap, ad);
+    double cur = smax(cp, cd), avg = smax(ap, ad);
+    // termination rule 2: the three relative parts of the current point and
+    // of the average (original units, l2 norms), and their l2 norm, which is
+    // restart rule 2's measure
+    double part_c[3] = {0, 0, 0}, part_a[3] = {0, 0, 0};
+    if (L2) {
+        const double k0 = a.P.obj_sign * a.P.obj_const;  // the constant shifts both objectives
+        const double sides[2][3] = {{obj[9], obj[10], obj[0]}, {obj[11], obj[12], obj[2]}};
+        const double dsum[2] = {obj[1], obj[3]};
+        for (int w = 0; w < 2; ++w) {
+            double* part = w ? part_a : part_c;
+            const double ps = sides[w][2] + k0, ds = dsum[w] + k0;
+            part[0] = sqrt(sides[w][0]) / (1.0 + a.P.bnorm2);
+            part[1] = sqrt(sides[w][1]) / (1.0 + a.P.cnorm2);
+            part[2] = fabs(ps - ds) / (1.0 + fabs(ps) + fabs(ds));
+        }
+        if (a.restart_rule == 2) {
+            const double mc = sqrt(part_c[0] * part_c[0] + part_c[1] * part_c[1] + part_c[2] * part_c[2]);
+            const double ma = sqrt(part_a[0] * part_a[0] + part_a[1] * part_a[1] + part_a[2] * part_a[2]);
+            // a non-finite scaled residual still stops the solve below
+            cur = isfinite(cur) ? mc : cur;
+            avg = isfinite(avg) ? ma : avg;
+        }
+    }
     st->cur_res = cur;
     st->avg_res = avg;
     st->inv = inv;
@@ -871,7 +922,10 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
             st->stop_iter = it_idx;
         } else {
             double rel = 0.0;
-            if (a.termination_rule == 1) {
+            if (L2) {
+                const double* part = ab ? part_a : part_c;
+                rel = smax(smax(part[0], part[1]), part[2]);
+            } else if (a.termination_rule == 1) {
                 double ps = ab ? obj[2] : obj[0], ds = ab ? obj[3] : obj[1];
                 ps += a.P.obj_sign * a.P.obj_const;  // the constant shifts both objectives
                 ds += a.P.obj_sign * a.P.obj_const;
@@ -879,7 +933,7 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
                 rel = smax(smax(op / (1.0 + a.P.bnorm), od / (1.0 + a.P.cnorm)), gap);
             }
             st->rel_kkt = rel;
-            const bool conv = (a.termination_rule == 1) ? (rel < a.tol) : (orig < a.tol);
+            const bool conv = (a.termination_rule != 0) ? (rel < a.tol) : (orig < a.tol);
             // Infeasibility test (engine extension): the change of y since the
             // previous check as a FarkasCertificate (duals.cpp:36-79), scaled
             // to max |dy| = 1; certified when the row-side and column-side
@@ -943,7 +997,8 @@ __global__ void __launch_bounds__(kBlock, INF ? 2 : (sizeof(T) == 4 ? 4 : 3))
                     st->since_restart += a.period_iters;
                 }
             } else {
-                // adaptive: candidate = the better of average and current
+                // adaptive (restart rules 1 and 2): candidate = the better of
+                // average and current
                 const double cand = ab ? avg : cur;
                 if (!isfinite(st->res_last)) st->res_last = cur;
                 const long long span = st->since_restart + a.period_iters;
@@ -1149,13 +1204,17 @@ void launch_fast_check(const FastCheck<T>& a0, cudaStream_t s) {
     int grid = check_blocks(a.A) + check_blocks(a.AT);
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid == 0) grid = 1;
+    const bool l2 = a.termination_rule == 2;
     if (a.infeas) {
-        fast_check<T, true><<<grid, kBlock, 0, s>>>(a);
+        if (l2) fast_check<T, kCheckInf | kCheckL2><<<grid, kBlock, 0, s>>>(a);
+        else fast_check<T, kCheckInf><<<grid, kBlock, 0, s>>>(a);
         const int rows_grid = (a.A.rows + kBlock / 32 - 1) / (kBlock / 32);
         const int xg = rows_grid < a.grid_cap || a.grid_cap <= 0 ? rows_grid : a.grid_cap;
         fast_xray_rows<T><<<xg > 0 ? xg : 1, kBlock, 0, s>>>(a);
+    } else if (l2) {
+        fast_check<T, kCheckL2><<<grid, kBlock, 0, s>>>(a);
     } else {
-        fast_check<T, false><<<grid, kBlock, 0, s>>>(a);
+        fast_check<T, 0><<<grid, kBlock, 0, s>>>(a);
     }
     if (a.want_candidate) {
         const int32_t nmax = a.P.n > a.P.m ? a.P.n : a.P.m;

@@ -617,6 +617,33 @@ int pdhg_mlp_gradients(pdhg_mlp* p, int batch, const float* x, const float* t, f
     return rc;
 }
 
+// One Adam step with gradients from outside (parameter order, host FP32):
+// the update of data-parallel training, where every replica applies the
+// gradients all ranks have averaged. The step counter is the one
+// pdhg_mlp_train advances, and the hyper-parameters are its own.
+int pdhg_mlp_adam_step(pdhg_mlp* p, const float* grads, float lr) {
+    using namespace pdhg;
+    if (p == nullptr || grads == nullptr || !(lr > 0.f)) return PDHG_ERR_INVALID_ARGUMENT;
+    Mlp& h = p->h;
+    MCK(cudaSetDevice(h.device));
+    int64_t src = 0;
+    for (int i = 0; i < 6; ++i) {
+        MCK(cudaMemcpyAsync(h.g.p + h.off[i], grads + src, sizeof(float) * h.cnt[i],
+                            cudaMemcpyHostToDevice, h.stream));
+        src += h.cnt[i];
+    }
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    h.adam_t += 1;
+    const float c1 = 1.f - std::pow(b1, static_cast<float>(h.adam_t));
+    const float c2 = 1.f - std::pow(b2, static_cast<float>(h.adam_t));
+    k_adam<<<blocks(h.total, 256), 256, 0, h.stream>>>(h.w.p, h.g.p, h.m.p, h.v.p, h.w16.p,
+                                                      h.total, lr, b1, b2, eps, c1, c2);
+    transpose(h.W16(1), h.hidden, h.w2t.p, h.hidden, h.hidden, h.hidden, h.stream);
+    transpose(h.W16(2), h.hidden, h.w3t.p, h.n_out, h.n_out, h.hidden, h.stream);
+    MCK(cudaStreamSynchronize(h.stream));
+    return check_err(h);
+}
+
 // Adam over `epochs` passes of shuffled mini-batches of the samples x (S x
 // n_in) with targets t (S x n_out); the last incomplete batch of an epoch is
 // dropped. epoch_loss (epochs entries, may be NULL) gets each epoch's mean

@@ -34,6 +34,7 @@ def _lib() -> C.CDLL:
         L.pdhg_mlp_gradients.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp]
         L.pdhg_mlp_train.argtypes = [C.c_void_p, C.c_int64, _fp, _fp, C.c_int, C.c_int,
                                      C.c_float, C.c_uint64, _fp]
+        L.pdhg_mlp_adam_step.argtypes = [C.c_void_p, _fp, C.c_float]
         L.pdhg_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, C.c_int,
                                      _fp]
         _declared = True
@@ -120,6 +121,13 @@ class Mlp:
         self._check(_lib().pdhg_mlp_gradients(self._h, x.shape[0], _f(x), _f(t), _f(g),
                                               C.byref(loss)), "pdhg_mlp_gradients")
         return g, float(loss.value)
+
+    def adam_step(self, grads: np.ndarray, lr: float = 1e-3) -> None:
+        """One Adam step with the given gradients (parameter order): the update
+        of data-parallel training, after the ranks averaged their gradients."""
+        g = _f32(grads)
+        assert g.size == self.param_count
+        self._check(_lib().pdhg_mlp_adam_step(self._h, _f(g), lr), "pdhg_mlp_adam_step")
 
     def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int = 256,
               lr: float = 1e-3, seed: int = 0) -> np.ndarray:

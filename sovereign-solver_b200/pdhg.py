@@ -129,6 +129,10 @@ def _check(code: int, what: str, ctx=None) -> None:
         raise PdhgError(code, f"{what} ({detail})" if detail else what)
 
 
+TERMINATION_RULES = {"absolute": 0, "relative_kkt": 1, "relative_kkt_l2": 2}
+RESTART_RULES = {"reference": 0, "adaptive": 1, "adaptive_l2": 2}
+
+
 @dataclass
 class PdhgOptions:
     """``sov::PdhgOptions`` (pdhg.hpp:85-134) + ``ScalingOptions`` + engine extensions."""
@@ -147,9 +151,15 @@ class PdhgOptions:
     apply_pock_chambolle: bool = True
     # extensions (defaults = reference behaviour)
     precision: str = "fp64_exact"
-    termination_rule: str = "absolute"  # or "relative_kkt"
+    # "absolute" (the reference's rule), "relative_kkt" (max-norm relative KKT on
+    # the reference's residual terms) or "relative_kkt_l2" (PDLP's relative KKT
+    # error: l2 norms, sign violations of the duals, relative gap)
+    termination_rule: str = "absolute"
     polish_iterations: int = -1
-    restart_rule: str = "reference"  # or "adaptive"
+    # "reference", "adaptive" (adaptive restarts on the scaled max-norm KKT
+    # residual) or "adaptive_l2" (the same rule on the relative_kkt_l2 measure;
+    # needs termination_rule "relative_kkt_l2")
+    restart_rule: str = "reference"
     primal_weight_update: bool = False
     checkpoint: Optional[Callable[[int, np.ndarray, np.ndarray, float], None]] = None
     trace_iters: int = 0
@@ -222,9 +232,9 @@ def _c_options(opt: PdhgOptions) -> _Options:
         if name == "precision":
             o.precision = PREC[val]
         elif name == "termination_rule":
-            o.termination_rule = 1 if val in ("relative_kkt", 1) else 0
+            o.termination_rule = TERMINATION_RULES[val] if isinstance(val, str) else int(val)
         elif name == "restart_rule":
-            o.restart_rule = 1 if val in ("adaptive", 1) else 0
+            o.restart_rule = RESTART_RULES[val] if isinstance(val, str) else int(val)
         elif name in ("checkpoint", "trace_iters"):
             continue
         else:

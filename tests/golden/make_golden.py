@@ -1,9 +1,11 @@
 """Regenerates the golden fixtures in this directory from the REFERENCE itself.
 
-Run in a container that has the reference sources (default /root/reference,
-override with REF_SRC) after ``make -C oracle ref``:
+Run in a container that has the reference sources, after
+``make -C oracle ref REF_SRC=<reference source tree>``:
 
-    python tests/golden/make_golden.py
+    REF_SRC=<reference source tree> python tests/golden/make_golden.py [c0]
+
+(`c0` regenerates only the two 2,000 x 5,000 fixtures.)
 
 Every expected value stored here comes from the reference's own code: its LP
 and MPS readers parse the models, its ``sov::Pdhg::solve`` on the Host backend
@@ -16,6 +18,7 @@ The GPU box has no reference sources; the tests there read only these files.
 """
 from __future__ import annotations
 
+import hashlib
 import importlib
 import json
 import os
@@ -32,7 +35,9 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import orc  # noqa: E402
 
 pkg = importlib.import_module("sovereign-solver_b200")
-REF_SRC = os.environ.get("REF_SRC", "/root/reference")
+REF_SRC = os.environ.get("REF_SRC", "")
+if not os.path.isfile(os.path.join(REF_SRC, "src", "l1", "pdhg.cpp")):
+    sys.exit("make_golden.py: set REF_SRC to the reference's source tree")
 
 PROBLEM_KEYS = ("m", "n", "row_ptr", "col_idx", "val", "c", "col_lo", "col_hi", "row_lo",
                 "row_hi", "obj_const", "maximize")
@@ -140,9 +145,34 @@ def save(name: str, problem, options: dict, result: "orc.Result", extra: dict | 
           f"restarts={result.restarts} obj={result.objective:.10g}")
 
 
+def trace_digests(trace: np.ndarray) -> np.ndarray:
+    """SHA-256 of each traced iterate's FP64 bytes: (iterations, 32) uint8."""
+    return np.stack([np.frombuffer(hashlib.sha256(np.ascontiguousarray(row).tobytes()).digest(),
+                                   dtype=np.uint8) for row in trace])
+
+
+def c0_fixtures() -> None:
+    """The 2,000 x 5,000 random equality LP: at tol 1e-4 (converges) and at
+    the stated tol 1e-6 under the reference's default 1,000,000-iteration cap
+    (ends iteration_limit: it needs about 10.6M iterations). Every one of the
+    first 100 iterates is pinned by its digest; three are kept in full."""
+    p0 = pkg.lpgen.random_equality_lp(2000, 5000, 5, seed=0)
+    keep = [0, 9, 99]
+    for name, opts in (("c0_2000x5000_tol1e-4", {"tolerance": 1e-4}),
+                       ("c0_2000x5000_tol1e-6", {"tolerance": 1e-6})):
+        r = orc.reference_solve(p0, trace_iters=100, **opts)
+        save(name, p0, opts, r,
+             {"trace_iters_kept": np.asarray(keep), "trace_x": r.trace_x[keep],
+              "trace_y": r.trace_y[keep], "trace_digest_x": trace_digests(r.trace_x),
+              "trace_digest_y": trace_digests(r.trace_y)})
+
+
 def main() -> None:
     if not orc.ref_available():
         raise SystemExit("oracle/_ref/libsovref.so missing: run make -C oracle ref")
+    if sys.argv[1:] == ["c0"]:  # only the 2,000 x 5,000 fixtures
+        c0_fixtures()
+        return
     # 1. the reference's PDHG unit tests (tests/test_pdhg.cpp)
     for case in pdhg_test_cases():
         d = orc.reference_read_model(case["text"])
@@ -170,14 +200,7 @@ def main() -> None:
     for name, p, opts in synth:
         r = orc.reference_solve(p, trace_iters=100, **opts)
         save(name, p, opts, r, {"trace_x": r.trace_x, "trace_y": r.trace_y})
-    # 4. the 2,000 x 5,000 random equality LP at tol 1e-4 (converges)
-    p0 = pkg.lpgen.random_equality_lp(2000, 5000, 5, seed=0)
-    opts = {"tolerance": 1e-4}
-    r = orc.reference_solve(p0, trace_iters=100, **opts)
-    keep = [0, 9, 99]
-    save("c0_2000x5000_tol1e-4", p0, opts, r,
-         {"trace_iters_kept": np.asarray(keep), "trace_x": r.trace_x[keep],
-          "trace_y": r.trace_y[keep]})
+    c0_fixtures()
     # 5. backend known answers (tests/test_l0_backend.cpp) through the reference Host backend
     A = backend_matrix()
     ba = {}

@@ -9,6 +9,8 @@ reference's outputs (golden fixtures) and the oracle on the same inputs.
 * Mixed mode (FP32 iterates, FP64 checks): same status, objective within the
   tolerance the relative-KKT rule promises.
 """
+import hashlib
+
 import numpy as np
 import pytest
 
@@ -59,11 +61,48 @@ def test_exact_mode_is_bit_identical_to_the_reference(pkg, engine, name):
         tx = r.trace_x if keep is None else r.trace_x[keep]
         ty = r.trace_y if keep is None else r.trace_y[keep]
         assert np.array_equal(tx, g["trace_x"]) and np.array_equal(ty, g["trace_y"])
+        if "trace_digest_x" in g:  # every one of the first 100 iterates, bit for bit
+            assert np.array_equal(trace_digests(r.trace_x), g["trace_digest_x"])
+            assert np.array_equal(trace_digests(r.trace_y), g["trace_digest_y"])
+
+
+def trace_digests(trace):
+    """SHA-256 of each traced iterate's FP64 bytes (as make_golden.py stores them)."""
+    return np.stack([np.frombuffer(hashlib.sha256(np.ascontiguousarray(row).tobytes()).digest(),
+                                   dtype=np.uint8) for row in trace])
 
 
 def rel_err(a, b):
     a, b = np.asarray(a, float), np.asarray(b, float)
     return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+
+@pytest.mark.parametrize("name", ["c0_2000x5000_tol1e-4", "c0_2000x5000_tol1e-6"])
+def test_fp64_mode_tracks_all_first_100_iterates_of_the_2000x5000_lp(pkg, orc, engine, name):
+    # the oracle's first 100 iterates are the reference's (their digests are
+    # in the fixture); FP64 mode stays within 1e-10 of every one of them
+    g = load_golden(name)
+    p = golden_problem(pkg, g)
+    o = orc.oracle_solve(p, trace_iters=100, max_iterations=100, **g["options"])
+    assert np.array_equal(trace_digests(o.trace_x), g["trace_digest_x"])
+    assert np.array_equal(trace_digests(o.trace_y), g["trace_digest_y"])
+    r = solve(pkg, engine, p, precision="fp64", trace_iters=100, max_iterations=100,
+              **g["options"])
+    for k in range(100):
+        assert rel_err(r.trace_x[k], o.trace_x[k]) <= 1e-10, k
+        assert rel_err(r.trace_y[k], o.trace_y[k]) <= 1e-10, k
+
+
+def test_fp64_mode_at_the_stated_tolerance_of_the_2000x5000_lp(pkg, engine):
+    # tol 1e-6 under the reference's 1,000,000-iteration cap: the reference
+    # ends iteration_limit there; FP64 mode must end the same way, at the same
+    # iteration, with the objective within 1e-8
+    g = load_golden("c0_2000x5000_tol1e-6")
+    p = golden_problem(pkg, g)
+    r = solve(pkg, engine, p, precision="fp64", **g["options"])
+    assert r.status == g["ref_status"] == "iteration_limit"
+    assert r.iterations == g["ref_iterations"] == 1_000_000
+    assert abs(r.objective - g["ref_objective"]) <= 1e-8 * max(1.0, abs(g["ref_objective"]))
 
 
 @pytest.mark.parametrize("name", ["rand_eq_60x150", "rand_eq_max_40x100", "mixed_bounds_50x90",
@@ -299,6 +338,57 @@ def test_fp64_adaptive_and_primal_weight_follow_the_oracle(pkg, orc, engine, see
         assert r.status == o.status == "optimal"
         assert r.restarts == o.restarts and r.iterations == o.iterations, (r.iterations, o.iterations)
         assert abs(r.objective - o.objective) <= 1e-8 * abs(o.objective)
+
+
+RULE2_CASES = {"equality_200x500": ("random_equality_lp", (200, 500, 5), dict(seed=3)),
+               "badly_scaled_300x800": ("badly_scaled_lp", (300, 800, 5), dict(seed=2001)),
+               "transportation_40x100": ("transportation_lp", (40, 100), dict(seed=1000)),
+               "maximize_80x200": ("random_equality_lp", (80, 200, 4), dict(seed=8, maximize=True))}
+
+
+@pytest.mark.parametrize("name", sorted(RULE2_CASES))
+def test_fp64_rule2_follows_the_oracle(pkg, orc, engine, name):
+    # termination rule 2 (PDLP's relative KKT) with restart rule 2 on its
+    # measure: FP64 mode takes the oracle's restarts and stops where it stops
+    fn, args, kw = RULE2_CASES[name]
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    for pw in (0, 1):
+        o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=pw,
+                             max_iterations=200_000)
+        r = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt_l2",
+                  restart_rule="adaptive_l2", primal_weight_update=bool(pw),
+                  max_iterations=200_000)
+        assert r.status == o.status == "optimal", (pw, r.status, o.status)
+        assert abs(r.iterations - o.iterations) <= 40 and abs(r.restarts - o.restarts) <= 1, \
+            (pw, r.iterations, o.iterations, r.restarts, o.restarts)
+        if r.iterations == o.iterations:
+            assert abs(r.objective - o.objective) <= 1e-8 * max(1.0, abs(o.objective))
+            assert r.relative_kkt == pytest.approx(o.relative_kkt, rel=1e-8, abs=1e-14)
+        assert r.relative_kkt < 1e-4
+
+
+@pytest.mark.parametrize("name", sorted(RULE2_CASES))
+def test_mixed_rule2_reaches_the_fp64_optimum(pkg, orc, engine, name):
+    fn, args, kw = RULE2_CASES[name]
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=1,
+                         max_iterations=200_000)
+    r = solve(pkg, engine, p, precision="mixed", termination_rule="relative_kkt_l2",
+              restart_rule="adaptive_l2", primal_weight_update=True, max_iterations=200_000)
+    assert r.status == "optimal", (r.status, r.relative_kkt, r.iterations)
+    assert r.relative_kkt < 1e-4
+    # both points meet 1e-4 relative KKT: their objectives agree to the gap
+    # the measure allows
+    assert abs(r.objective - o.objective) <= 1e-3 * (1 + abs(o.objective))
+
+
+def test_rule2_option_combinations_are_checked(pkg, engine):
+    p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=1)
+    with pytest.raises(pkg.PdhgError):  # rule 2 needs mixed or fp64
+        solve(pkg, engine, p, termination_rule="relative_kkt_l2")
+    with pytest.raises(pkg.PdhgError):  # restart rule 2 restarts on rule 2's measure
+        solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt",
+              restart_rule="adaptive_l2")
 
 
 def test_exact_mode_rejects_the_extensions(pkg, engine):

@@ -4,6 +4,8 @@ tests/golden/), and the hand-derived answers of the reference's own tests.
 Runs everywhere (no reference sources needed): this is what pins the oracle
 on the GPU box, where the oracle then checks the CUDA engine.
 """
+import hashlib
+
 import numpy as np
 import pytest
 
@@ -37,11 +39,35 @@ def test_oracle_reproduces_reference_fixture(pkg, orc, name):
         assert np.array_equal(r.trace_y, g["trace_y"])
 
 
+def trace_digests(trace):
+    """SHA-256 of each traced iterate's FP64 bytes (as make_golden.py stores them)."""
+    return np.stack([np.frombuffer(hashlib.sha256(np.ascontiguousarray(row).tobytes()).digest(),
+                                   dtype=np.uint8) for row in trace])
+
+
 def test_oracle_reproduces_the_2000x5000_fixture(pkg, orc):
     g = load_golden("c0_2000x5000_tol1e-4")
     p = golden_problem(pkg, g)
     r = orc.oracle_solve(p, trace_iters=100, **g["options"])
     check_against_golden(r, g)
+    keep = g["trace_iters_kept"]
+    assert np.array_equal(r.trace_x[keep], g["trace_x"])
+    assert np.array_equal(r.trace_y[keep], g["trace_y"])
+    assert np.array_equal(trace_digests(r.trace_x), g["trace_digest_x"])
+    assert np.array_equal(trace_digests(r.trace_y), g["trace_digest_y"])
+
+
+def test_oracle_reproduces_the_first_100_iterates_at_tol_1e6(pkg, orc):
+    # the stated tolerance of the 2,000 x 5,000 LP: the reference ends
+    # iteration_limit at its 1,000,000-iteration cap (about 2 minutes of CPU
+    # here, so only the first 100 iterates are checked on the CPU; the GPU
+    # tests compare the engine's whole run with the fixture)
+    g = load_golden("c0_2000x5000_tol1e-6")
+    assert g["ref_status"] == "iteration_limit" and g["ref_iterations"] == 1_000_000
+    p = golden_problem(pkg, g)
+    r = orc.oracle_solve(p, trace_iters=100, max_iterations=100, **g["options"])
+    assert np.array_equal(trace_digests(r.trace_x), g["trace_digest_x"])
+    assert np.array_equal(trace_digests(r.trace_y), g["trace_digest_y"])
     keep = g["trace_iters_kept"]
     assert np.array_equal(r.trace_x[keep], g["trace_x"])
     assert np.array_equal(r.trace_y[keep], g["trace_y"])
