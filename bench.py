@@ -2,7 +2,11 @@
 
 Workload: 2,000 supplies x 5,000 demands = 10,000,000 columns, 7,000 rows,
 20,000,000 nonzeros (all 1.0), costs U[1,100], x >= 0; mixed precision (FP32
-iterates and SpMVs, FP64 residual / restart checks); relative-KKT rule.
+iterates and SpMVs, FP64 residual / restart checks); PDLP's relative KKT
+(termination rule 2) with adaptive restarts on its measure. Beside it: the
+same steps in all-FP64 arithmetic (`fp64`), one full solve of the LP to 1e-4
+(`full_solve`), the batched engine on 4,096 LPs (`batch`), the precision study
+on the badly scaled LP (`precision`) and the learned warm start (`warmstart`).
 
 A step is one call of the engine's solve on that LP running
 `--iters-per-step` PDHG iterations (default 2,000 = 50 check periods) from the
@@ -48,11 +52,24 @@ SUPPLIES, DEMANDS = 2000, 5000
 
 
 def workload_name(supplies: int, demands: int) -> str:
+    """The LP both arms solve (the arithmetic is each arm's `dtype`)."""
     return (f"transportation LP {supplies:,} x {demands:,} ({supplies * demands:,} columns, "
-            f"{supplies + demands:,} rows, {2 * supplies * demands:,} nnz), FP32-bulk/FP64-check PDHG")
+            f"{supplies + demands:,} rows, {2 * supplies * demands:,} nnz), PDHG iterations")
 
 
-WORKLOAD = workload_name(SUPPLIES, DEMANDS)
+def bench_config(args, world: int) -> dict:
+    """The `config` object, identical in both arms' lines."""
+    return {"workload": workload_name(args.supplies, args.demands),
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (resident set ~1.3 GB > 126 MB)"}
+
+
+# Options of the headline solves: FP32 iterates with FP64 checks, PDLP's
+# relative KKT (termination rule 2) and adaptive restarts on its measure. The
+# primal weight stays 1 on the transportation LP: its update drives omega from
+# |c|/|b| ~ 135 towards 0.1 there and costs 2-3x the iterations (oracle, 100 x
+# 250 and 200 x 500 instances of the family).
+HEADLINE = dict(termination_rule="relative_kkt_l2", restart_rule="adaptive_l2")
 
 
 def replica_problem(pkg, rank: int, supplies: int = SUPPLIES, demands: int = DEMANDS):
@@ -215,9 +232,9 @@ def run_reference(args) -> None:
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded transportation LP)",
-        "config": {"workload": workload_name(args.supplies, args.demands),
-                   "iterations_per_step": per_step,
-                   "implementation": "reference sov::Pdhg::solve, Host backend (single-threaded)"},
+        "config": bench_config(args, world),
+        "iterations_per_step": per_step,
+        "implementation": "reference sov::Pdhg::solve, Host backend (single-threaded), FP64",
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": f"{args.steps} steps x {per_step} iterations of one stock "
@@ -235,32 +252,44 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
     KKT in one batched solve (pdhg_solve_batch: one CUDA-graph launch), beside
     the plain single-LP engine on the first instances of the same family."""
     ps = pkg.lpgen.batch_family(args.batch_instances, seed_base=3000 + 100_000 * rank)
-    opt = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
-                          restart_rule="adaptive", tolerance=1e-4, max_iterations=200_000)
+    opt = pkg.PdhgOptions(precision="mixed", tolerance=1e-4, max_iterations=200_000,
+                          primal_weight_update=True, **HEADLINE)
+    # the plain engine solves an evenly spaced sample of the same instances
+    step = max(1, len(ps) // max(1, args.plain_instances))
+    sample = list(range(0, len(ps), step))[: args.plain_instances]
     with pkg.Engine(eng.device) as e:
-        e.load_batch(ps)
-        e.solve_batch(opt, want_point=False)  # warm-up
+        warm = ps[: min(len(ps), 64)]
+        e.load_batch(warm)
+        e.solve_batch(opt, want_point=False)  # warm-up (graph build, clocks)
         t0 = time.perf_counter()
         e.load_batch(ps)
         rs = e.solve_batch(opt, want_point=False)
         t_batch = time.perf_counter() - t0
         t0 = time.perf_counter()
         plain = []
-        for p in ps[: args.plain_instances]:
-            e.load(p)
+        for k in sample:
+            e.load(ps[k])
             plain.append(e.solve(opt, want_point=False))
         t_plain = time.perf_counter() - t0
     solved = sum(r.status == "optimal" for r in rs)
     plain_solved = sum(r.status == "optimal" for r in plain)
     its = sorted(r.iterations for r in rs)
+    fp64_its = sum(r.fp64_iterations for r in rs)
     return {"workload": f"{len(ps)} seeded LPs, m log-uniform [50, 5000], n = 2-3 m, "
-                        f"4-10 nnz/column ({sum(p.nnz for p in ps):,} nnz), rel KKT 1e-4, mixed",
-            "solved": solved, "seconds": t_batch, "solves_per_s": solved / t_batch,
+                        f"4-10 nnz/column ({sum(p.nnz for p in ps):,} nnz), PDLP relative KKT "
+                        f"1e-4, mixed, adaptive restarts, primal weight",
+            "instances": len(ps), "solved": solved, "seconds": t_batch,
+            "solves_per_s": solved / t_batch,
             "iterations_median": its[len(its) // 2], "iterations_max": its[-1],
             "polished": sum(r.fp64_iterations > 0 for r in rs),
+            "fp64_iteration_fraction": fp64_its / max(1, sum(its)),
             "gpu_launches": rs[0].kernel_launches if rs else 0,
-            "plain_gpu": {"instances": len(plain), "solved": plain_solved, "seconds": t_plain,
-                          "solves_per_s": plain_solved / t_plain},
+            "plain_gpu": {"instances": len(plain), "sample": f"every {step}th instance of the "
+                          f"same family ({len(plain)} of {len(ps)})", "solved": plain_solved,
+                          "seconds": t_plain, "solves_per_s": plain_solved / t_plain,
+                          "batched_solves_per_s_same_rate": solved / t_batch},
+            "speedup_vs_plain_gpu": (solved / t_batch) / (plain_solved / t_plain)
+            if plain_solved else None,
             "timing": "host wall clock around load + solve on both sides (pdhg_load_batch + "
                       "pdhg_solve_batch; per instance pdhg_load_problem + pdhg_solve)"}
 
@@ -275,20 +304,21 @@ def precision_line(pkg, eng, args, rank: int) -> dict:
     objective error is taken against the FP64 run."""
     p = pkg.lpgen.badly_scaled_lp(200_000, 500_000, 8, seed=2000 + rank)
     out = {"workload": f"badly scaled LP {p.m:,} x {p.n:,}, {p.nnz:,} nnz (power-law rows, "
-                       f"|a| log-uniform [1e-3, 1e3], 30% <= rows)",
+                       f"|a| log-uniform [1e-3, 1e3], 30% <= rows), PDLP relative KKT 1e-4, "
+                       f"adaptive restarts, primal weight",
            "iteration_budget": args.precision_iters}
     arms = {"fp64": dict(precision="fp64"), "mixed": dict(precision="mixed"),
             "fp32_only": dict(precision="mixed", polish_iterations=0)}
     with pkg.Engine(eng.device) as e:
         e.load(p)
         for name, kw in arms.items():
-            o = pkg.PdhgOptions(termination_rule="relative_kkt", restart_rule="adaptive",
-                                primal_weight_update=True, tolerance=1e-4,
-                                max_iterations=args.precision_iters, **kw)
+            o = pkg.PdhgOptions(primal_weight_update=True, tolerance=1e-4,
+                                max_iterations=args.precision_iters, **HEADLINE, **kw)
             r = e.solve(o, want_point=False)
             out[name] = {"status": r.status, "iterations": r.iterations,
                          "relative_kkt": r.relative_kkt, "objective": r.objective,
                          "fp64_iterations": r.fp64_iterations,
+                         "fp64_iteration_fraction": r.fp64_iterations / max(1, r.iterations),
                          "device_seconds": r.device_seconds,
                          "iterations_per_s": r.iterations / r.device_seconds
                          if r.device_seconds > 0 else None,
@@ -296,6 +326,9 @@ def precision_line(pkg, eng, args, rank: int) -> dict:
                          / r.device_seconds / 1e9 if r.device_seconds > 0 else None}
         out["tuning"] = {"fp64": e.tuning("fp64"), "mixed": e.tuning("mixed")}
     ref = out["fp64"]["objective"]
+    out["fp64_reference"] = ("the all-FP64 arm's objective" if out["fp64"]["status"] == "optimal"
+                             else "the all-FP64 arm did not converge: errors compare "
+                                  "unconverged points")
     for name in ("mixed", "fp32_only"):
         out[name]["objective_error_vs_fp64"] = (abs(out[name]["objective"] - ref)
                                                 / max(1.0, abs(ref)))
@@ -311,9 +344,8 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
     warm start. Solves/s include, for the warm line, prediction and gating."""
     W = pkg.warmstart
     fam = pkg.lpgen.parametric_family(500, 1200, 5, seed=4001)
-    opt = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
-                          restart_rule="adaptive", primal_weight_update=True, tolerance=1e-4,
-                          max_iterations=300_000)
+    opt = pkg.PdhgOptions(precision="mixed", primal_weight_update=True, tolerance=1e-4,
+                          max_iterations=300_000, **HEADLINE)
     tr_th = fam.thetas(args.ws_train, seed=1 + 1000 * rank)
     te_th = fam.thetas(args.ws_test, seed=2 + 1000 * rank)
     tr = [fam.instance(t) for t in tr_th]
@@ -383,10 +415,10 @@ def profile_case(args) -> None:
         name = f"transportation {args.supplies}x{args.demands}"
     with pkg.Engine(0) as eng:
         eng.load(prob)
-        r = eng.solve(pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
-                                      restart_rule="adaptive", primal_weight_update=True,
+        r = eng.solve(pkg.PdhgOptions(precision="mixed", primal_weight_update=True,
                                       tolerance=1e-12, polish_iterations=0,
-                                      max_iterations=args.iters_per_step), want_point=False)
+                                      max_iterations=args.iters_per_step, **HEADLINE),
+                      want_point=False)
         tuning = eng.tuning("mixed")
     print(json.dumps({"profile_case": name, "iterations": r.iterations, "status": r.status,
                       "tuning": tuning}))
@@ -459,11 +491,13 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--full-solve-cap", type=int, default=60_000)
-    ap.add_argument("--batch-instances", type=int, default=256,
+    ap.add_argument("--full-solve-cap", type=int, default=100_000)
+    ap.add_argument("--fp64-steps", type=int, default=3,
+                    help="steps of the same LP in all-FP64 arithmetic (0 = skip)")
+    ap.add_argument("--batch-instances", type=int, default=4096,
                     help="config-3 family size for the batched line (0 = skip)")
-    ap.add_argument("--plain-instances", type=int, default=16,
-                    help="instances of that family solved one at a time for comparison")
+    ap.add_argument("--plain-instances", type=int, default=32,
+                    help="an evenly spaced sample of that family solved one at a time")
     ap.add_argument("--ws-train", type=int, default=1024,
                     help="config-4 training solves for the learned warm start (0 = skip)")
     ap.add_argument("--ws-test", type=int, default=128, help="config-4 held-out instances")
@@ -507,8 +541,8 @@ def main() -> None:
     b_spmv = spmv_bytes(m, n, nnz)
     eng = pkg.Engine(local)
     eng.load(prob)
-    opts = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt", tolerance=1e-12,
-                           restart_rule="adaptive", max_iterations=args.iters_per_step)
+    opts = pkg.PdhgOptions(precision="mixed", tolerance=1e-12, max_iterations=args.iters_per_step,
+                           **HEADLINE)
     stream = torch.cuda.ExternalStream(eng.stream_handle())
 
     # ---- device-resident throughput (value) ----
@@ -564,7 +598,9 @@ def main() -> None:
     eng2 = pkg.Engine(local)
     o = pkg.pdhg._Options()
     lib.pdhg_default_options(C.byref(o))
-    o.precision, o.termination_rule, o.tolerance, o.restart_rule = 1, 1, 1e-12, 1
+    o.precision, o.tolerance = 1, 1e-12
+    o.termination_rule = pkg.pdhg.TERMINATION_RULES[HEADLINE["termination_rule"]]
+    o.restart_rule = pkg.pdhg.RESTART_RULES[HEADLINE["restart_rule"]]
     o.max_iterations = args.iters_per_step
     info = pkg.pdhg._Info()
 
@@ -591,10 +627,28 @@ def main() -> None:
     d2h = int((2 * n + m) * 8)
     eng2.close()
 
+    # ---- the same steps in all-FP64 arithmetic (same-precision comparison
+    # with the FP64 reference arm) ----
+    fp64 = None
+    if args.fp64_steps > 0:
+        o64 = pkg.PdhgOptions(precision="fp64", tolerance=1e-12,
+                              max_iterations=args.iters_per_step, **HEADLINE)
+        eng.solve(o64, want_point=False)  # warm-up (and the FP64 shapes' tuning)
+        f_its, f_t = 0, 0.0
+        for _ in range(args.fp64_steps):
+            r = eng.solve(o64, want_point=False)
+            f_its += r.iterations
+            f_t += r.device_seconds
+        f_t = max_over_ranks(f_t, world)
+        fp64 = {"value": sum_over_ranks(b_spmv * f_its, world) / f_t / 1e9, "unit": UNIT,
+                "iterations_per_s": sum_over_ranks(f_its, world) / f_t, "steps": args.fp64_steps,
+                "dtype": "f64", "tuning": eng.tuning("fp64"),
+                "timing": "CUDA events around each solve's iteration loop (device_seconds), "
+                          "problem resident in HBM"}
+
     # ---- one full solve to 1e-4 relative KKT (LPs solved/s, reported beside) ----
-    solve_opts = pkg.PdhgOptions(precision="mixed", termination_rule="relative_kkt",
-                                 restart_rule="adaptive", tolerance=1e-4,
-                                 max_iterations=args.full_solve_cap)
+    solve_opts = pkg.PdhgOptions(precision="mixed", tolerance=1e-4,
+                                 max_iterations=args.full_solve_cap, **HEADLINE)
     t0 = time.perf_counter()
     full = eng.solve(solve_opts, want_point=False)
     full_s = time.perf_counter() - t0
@@ -608,10 +662,12 @@ def main() -> None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded transportation LP, one per rank)",
-        "config": {"workload": WORKLOAD, "iterations_per_step": args.iters_per_step,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (resident set ~1.3 GB > 126 MB)",
-                   "b_spmv_bytes_per_iteration": b_spmv},
+        "config": bench_config(args, world),
+        "iterations_per_step": args.iters_per_step,
+        "b_spmv_bytes_per_iteration": b_spmv,
+        "options": "FP32 iterates, FP64 checks; PDLP relative KKT (rule 2), adaptive restarts "
+                   "on its measure, primal weight 1; tolerance 1e-12 in the timed steps (fixed "
+                   "work per step)",
         "iterations_per_s": sum_over_ranks(its, world) / t_max,
         "clocks": clocks,
         "gpu_launches": launches,
@@ -621,9 +677,15 @@ def main() -> None:
         "roofline": roofline,
         "full_solve": {"status": full.status, "iterations": full.iterations,
                        "relative_kkt": full.relative_kkt, "seconds": full_s,
+                       "device_seconds": full.device_seconds,
                        "lps_solved_per_s": (1.0 / full_s) if full.status == "optimal" else 0.0,
-                       "restarts": full.restarts, "objective": full.objective},
+                       "restarts": full.restarts, "objective": full.objective,
+                       "fp64_iterations": full.fp64_iterations,
+                       "measure": "PDLP relative KKT (termination rule 2) < 1e-4, mixed, "
+                                  "problem resident; host wall clock around pdhg_solve"},
     }
+    if fp64 is not None:
+        line["fp64"] = fp64
     if batch is not None:
         line["batch"] = batch
     if warm is not None:
