@@ -253,6 +253,15 @@ int pdhg_batch_start_kkt(pdhg_ctx* ctx, const double* x, const double* y, double
  * variable PDHG_B200_TUNE_CACHE when it is set. */
 int pdhg_get_tuning(const pdhg_ctx* ctx, int precision, int* out);
 
+/* Lanes per row of the batched engine's iteration kernels for the loaded
+ * batch in `precision` (PDHG_PREC_MIXED or PDHG_PREC_FP64): out[0] the primal
+ * pass (rows of A^T), out[1] the dual pass (rows of A), out[2] = 1 when chosen
+ * by timing. Engine extension: on the first pdhg_solve_batch of a loaded batch
+ * with >= 2^20 nonzeros (option autotune on) each pass's width is timed at the
+ * binning's choice, half and twice it, and the fastest kept until the next
+ * load; smaller batches and autotune = 0 keep the binning's choice. */
+int pdhg_get_batch_tuning(const pdhg_ctx* ctx, int precision, int* out);
+
 /* Per-kernel timing of the iteration kernels on the loaded problem (CUDA events
  * on the engine's stream around each launch, after `warmup` untimed iterations).
  * Runs `iterations` iterations from the state the last pdhg_solve left. */

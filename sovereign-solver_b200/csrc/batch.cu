@@ -6,6 +6,7 @@
 // (Pdhg::solve, src/l1/pdhg.cpp:218-502) in its fast precisions. A batch
 // lives inside a pdhg_ctx (pdhg_load_batch / pdhg_solve_batch) and shares its
 // stream and error text.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -65,7 +66,14 @@ struct BatchCtx {
 
     // solve graphs, [0] FP32 and [1] FP64, with what they bake in
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    long long graph_key[2][9] = {};
+    long long graph_key[2][11] = {};
+
+    // lanes per row of the lane-group path: the binning's choice for A's rows
+    // [0] and A^T's rows [1], and the autotuner's per precision ([0] FP32, [1]
+    // FP64; 0 = not tuned since the load)
+    int bin_vw[2] = {1, 1};
+    int tuned_vw[2][2] = {{0, 0}, {0, 0}};
+    bool tune_timed[2] = {false, false};
 
     BatchCtx(int dev, cudaStream_t s, std::string& e) : device(dev), stream(s), err(e) {}
     ~BatchCtx() {
@@ -263,10 +271,16 @@ int batch_intake(BatchCtx& c, const pdhg_options& o) {
     if (rc != PDHG_OK) return rc;
     rc = bin_matrix(c.ATs, s, &c.err);
     if (rc != PDHG_OK) return rc;
+    c.bin_vw[0] = c.As.vw;
+    c.bin_vw[1] = c.ATs.vw;
+    c.tuned_vw[0][0] = c.tuned_vw[0][1] = c.tuned_vw[1][0] = c.tuned_vw[1][1] = 0;
+    c.tune_timed[0] = c.tune_timed[1] = false;
     {
-        // active block lists of the iteration kernels (one entry per lane-group block)
-        const size_t nba = static_cast<size_t>((static_cast<int64_t>(c.As.rows) * c.As.vw + kBlock - 1) / kBlock) + 1;
-        const size_t nbt = static_cast<size_t>((static_cast<int64_t>(c.ATs.rows) * c.ATs.vw + kBlock - 1) / kBlock) + 1;
+        // active block lists of the iteration kernels (one entry per lane-group
+        // block), sized for the widest lane group the autotuner may pick
+        const int64_t wa = std::min(32, 2 * c.As.vw), wt = std::min(32, 2 * c.ATs.vw);
+        const size_t nba = static_cast<size_t>((static_cast<int64_t>(c.As.rows) * wa + kBlock - 1) / kBlock) + 1;
+        const size_t nbt = static_cast<size_t>((static_cast<int64_t>(c.ATs.rows) * wt + kBlock - 1) / kBlock) + 1;
         BCK(c.blk_list_a.alloc(nba));
         BCK(c.blk_flag_a.alloc(nba));
         BCK(c.blk_list_t.alloc(nbt));
@@ -486,6 +500,87 @@ int build_batch_graph(BatchCtx& c, const BatchParams& p, long long budget) {
     return PDHG_OK;
 }
 
+// ---- autotuner of the lane-group width (lanes per row) of each pass --------
+
+constexpr int64_t kBatchTuneMinNnz = int64_t{1} << 20;
+
+// Rebuilds the active block lists for the current lane widths.
+int batch_relist(BatchCtx& c, cudaStream_t s) {
+    const int one = 1;
+    BCK(cudaMemcpyAsync(&c.g.p->dirty, &one, sizeof one, cudaMemcpyHostToDevice, s));
+    launch_batch_compact(c.view(), s);
+    BCK(cudaGetLastError());
+    return PDHG_OK;
+}
+
+// Device time of 5 launches of one pass after 2 untimed ones.
+template <class T>
+float batch_time_pass(BatchCtx& c, bool primal, cudaEvent_t e0, cudaEvent_t e1) {
+    const BatchView b = c.view();
+    const Iterates<T> it = batch_iterates<T>(c);
+    launch_batch_iter<T>(b, it, primal, 0, c.stream);
+    launch_batch_iter<T>(b, it, primal, 0, c.stream);
+    cudaEventRecord(e0, c.stream);
+    for (int r = 0; r < 5; ++r) launch_batch_iter<T>(b, it, primal, 0, c.stream);
+    cudaEventRecord(e1, c.stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+}
+
+// Lanes per row for each pass of this precision: the binning's width (about
+// half the mean row length), half of it and twice it, each timed in two
+// rounds (so none is timed only on a cold GPU), a candidate replacing the
+// current pick only when 5% faster. Runs on the solve's own iterates before
+// the initial point is written (the initial point resets them). Batches
+// under 2^20 nonzeros keep the binning's width (their passes are
+// launch-bound). The choice holds until the next load.
+template <class T>
+int batch_tune(BatchCtx& c, bool autotune) {
+    const int pi = std::is_same<T, float>::value ? 0 : 1;
+    if (!autotune || c.nnz < kBatchTuneMinNnz) {
+        c.As.vw = c.bin_vw[0];
+        c.ATs.vw = c.bin_vw[1];
+        return PDHG_OK;
+    }
+    if (c.tuned_vw[pi][0] != 0) {
+        c.As.vw = c.tuned_vw[pi][0];
+        c.ATs.vw = c.tuned_vw[pi][1];
+        return PDHG_OK;
+    }
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    for (int pass = 0; pass < 2; ++pass) {  // 0: rows of A (dual), 1: rows of A^T (primal)
+        MatDev& M = pass ? c.ATs : c.As;
+        const int base = c.bin_vw[pass];
+        std::vector<int> cand{base};
+        if (M.n_short > 0) {
+            if (base > 1) cand.push_back(base / 2);
+            if (base < 32) cand.push_back(base * 2);
+        }
+        std::vector<float> t(cand.size(), 3.0e38f);
+        for (int round = 0; round < 2; ++round)
+            for (size_t i = 0; i < cand.size(); ++i) {
+                M.vw = cand[i];
+                int rc = batch_relist(c, c.stream);
+                if (rc != PDHG_OK) return rc;
+                t[i] = std::min(t[i], batch_time_pass<T>(c, pass == 1, e0, e1));
+            }
+        size_t pick = 0;
+        for (size_t i = 1; i < cand.size(); ++i)
+            if (t[i] < 0.95f * t[pick]) pick = i;
+        M.vw = cand[pick];
+        c.tuned_vw[pi][pass] = cand[pick];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BCK(cudaGetLastError());
+    c.tune_timed[pi] = true;
+    return PDHG_OK;
+}
+
 // Runs check periods from iteration iter0 (the global count) until every
 // instance is done or iteration `last` (absolute) is reached; returns the
 // negated stop code when the host asked the device to stop.
@@ -526,7 +621,7 @@ int batch_run(BatchCtx& c, const pdhg_options& o, std::chrono::steady_clock::tim
     };
     if (n_periods > 0) {
         const int gi = std::is_same<T, float>::value ? 0 : 1;
-        long long key[9];
+        long long key[11];
         key[0] = 1;
         key[1] = p.period;
         key[2] = budget;
@@ -536,6 +631,8 @@ int batch_run(BatchCtx& c, const pdhg_options& o, std::chrono::steady_clock::tim
         key[6] = p.allow_switch;
         std::memcpy(&key[7], &p.tol, sizeof(double));
         std::memcpy(&key[8], &p.restart_decrease, sizeof(double));
+        key[9] = c.As.vw;  // the lane groups baked into the iteration launches
+        key[10] = c.ATs.vw;
         if (c.graph[gi] == nullptr || std::memcmp(key, c.graph_key[gi], sizeof key) != 0) {
             int rc = build_batch_graph<T>(c, p, budget);
             if (rc != PDHG_OK) return rc;
@@ -658,6 +755,13 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
     }
     BatchView b = c.view();
     launch_batch_steps(b, o.step_size_safety, o.primal_weight_update, s);
+    {
+        const int rc = f32 ? batch_tune<float>(c, o.autotune != 0)
+                           : batch_tune<double>(c, o.autotune != 0);
+        if (rc != PDHG_OK) return rc;
+        BCK(cudaMemcpyAsync(c.g.p, &gh, sizeof gh, cudaMemcpyHostToDevice, s));  // lists rebuilt
+        b = c.view();
+    }
     // initial point (pdhg.cpp:268-270) or the warm start
     const double* x0d = nullptr;
     const double* y0d = nullptr;
@@ -869,6 +973,15 @@ int batch_solve_abi(BatchCtx& c, const pdhg_options* options, pdhg_info* infos, 
 }
 
 int32_t batch_count(const BatchCtx& c) { return c.loaded ? c.count : 0; }
+
+int batch_tuning_abi(const BatchCtx& c, int precision, int* out) {
+    const int pi = precision == PDHG_PREC_MIXED ? 0 : 1;
+    const bool have = c.tuned_vw[pi][0] != 0;
+    out[0] = have ? c.tuned_vw[pi][1] : c.bin_vw[1];
+    out[1] = have ? c.tuned_vw[pi][0] : c.bin_vw[0];
+    out[2] = c.tune_timed[pi] ? 1 : 0;
+    return PDHG_OK;
+}
 
 int batch_point_kkt_abi(BatchCtx& c, const double* x, const double* y, double* kkt) {
     if (!c.loaded || kkt == nullptr) {

@@ -1653,6 +1653,15 @@ int pdhg_get_tuning(const pdhg_ctx* ctx, int precision, int* out) {
     return PDHG_OK;
 }
 
+int pdhg_get_batch_tuning(const pdhg_ctx* ctx, int precision, int* out) {
+    if (ctx == nullptr || out == nullptr ||
+        (precision != PDHG_PREC_MIXED && precision != PDHG_PREC_FP64))
+        return PDHG_ERR_INVALID_ARGUMENT;
+    const pdhg::Ctx& cx = ctx->c;
+    if (cx.batch == nullptr || pdhg::batch_count(*cx.batch) == 0) return PDHG_ERR_INVALID_ARGUMENT;
+    return pdhg::batch_tuning_abi(*cx.batch, precision, out);
+}
+
 int pdhg_load_batch(pdhg_ctx* ctx, int32_t count, const int32_t* row_off, const int32_t* col_off,
                     int64_t nnz, const int32_t* row_ptr, const int32_t* col_idx,
                     const double* values, const double* c, const double* obj_const,

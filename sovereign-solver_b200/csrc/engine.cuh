@@ -477,5 +477,6 @@ int batch_solve_abi(BatchCtx& c, const pdhg_options* options, pdhg_info* infos, 
                     double* y, double* rc);
 int32_t batch_count(const BatchCtx& c);
 int batch_point_kkt_abi(BatchCtx& c, const double* x, const double* y, double* kkt);
+int batch_tuning_abi(const BatchCtx& c, int precision, int* out);
 
 }  // namespace pdhg

@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
                                    C.POINTER(_Options), _dp, _dp]
         L.pdhg_get_scaling.argtypes = [C.c_void_p, _dp, _dp]
         L.pdhg_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.pdhg_get_batch_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.pdhg_load_batch.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, C.c_int64, _ip, _ip, _dp,
                                       _dp, _dp, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.pdhg_solve_batch.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Info), _dp,
@@ -465,6 +466,13 @@ class Engine:
         _check(lib().pdhg_get_tuning(self._h, PREC[precision], out), "pdhg_get_tuning", self._h)
         return {"primal_lanes": out[0], "primal_long_mode": out[1], "dual_lanes": out[2],
                 "dual_long_mode": out[3], "timed": bool(out[4])}
+
+    def batch_tuning(self, precision: str = "mixed") -> dict:
+        """Lanes per row of the batched passes for the loaded batch (pdhg_get_batch_tuning)."""
+        out = (C.c_int * 3)()
+        _check(lib().pdhg_get_batch_tuning(self._h, PREC[precision], out),
+               "pdhg_get_batch_tuning", self._h)
+        return {"primal_lanes": out[0], "dual_lanes": out[1], "timed": bool(out[2])}
 
     def profile_kernels(self, precision: str = "mixed", warmup: int = 3,
                         iterations: int = 20) -> list[dict]:

@@ -73,6 +73,32 @@ def test_batch_rule2_follows_the_oracle_per_instance(pkg, orc, engine):
                 (prec, k, r.objective, o.objective)
 
 
+def test_batch_autotuner_keeps_the_answers(pkg, engine):
+    # a batch above the tuner's 2^20-nonzero threshold: the tuned lane widths
+    # must give the untuned solve's answers (mixed precision, to the rule's
+    # tolerance; the width changes only the order of FP32 sums)
+    ps = pkg.lpgen.batch_family(96, seed_base=3000, m_lo=2000, m_hi=5000)
+    assert sum(p.nnz for p in ps) >= 1 << 20
+    opt = dict(precision="mixed", max_iterations=200_000, termination_rule="relative_kkt_l2",
+               restart_rule="adaptive_l2", primal_weight_update=True)
+    engine.load_batch(ps)
+    fixed = engine.solve_batch(pkg.PdhgOptions(autotune=False, **opt), want_point=False)
+    t0 = engine.batch_tuning("mixed")
+    assert not t0["timed"]
+    tuned = engine.solve_batch(pkg.PdhgOptions(**opt), want_point=False)
+    t1 = engine.batch_tuning("mixed")
+    assert t1["timed"]
+    for lanes in (t1["primal_lanes"], t1["dual_lanes"]):
+        assert lanes in (1, 2, 4, 8, 16, 32)
+    for k, (a, b) in enumerate(zip(fixed, tuned)):
+        assert a.status == b.status == "optimal", (k, a.status, b.status)
+        assert b.relative_kkt < 1e-4
+        assert abs(a.objective - b.objective) <= 1e-3 * (1 + abs(a.objective)), k
+    again = engine.solve_batch(pkg.PdhgOptions(**opt), want_point=False)
+    assert engine.batch_tuning("mixed") == t1  # kept until the next load
+    assert [r.iterations for r in again] == [r.iterations for r in tuned]
+
+
 def test_batch_mixed_solves_every_instance(pkg, orc, engine):
     ps = family(pkg)
     engine.load_batch(ps)
