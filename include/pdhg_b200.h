@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define PDHG_B200_ABI_VERSION 3
+#define PDHG_B200_ABI_VERSION 4
 
 /* Return codes: the order and meaning of sov::Status (status.hpp:25-34). */
 typedef enum {
@@ -113,8 +113,9 @@ typedef struct pdhg_options {
                                     b_i the larger finite |row bound|; the gap of rules 1 and 2
                                     is |p - d|/(1 + |p| + |d|) on the bounded dual objective */
     long long polish_iterations; /* MIXED only: FP64 iterations allowed after the FP32
-                                    phase stalls (no 2% gain in 25 checks); -1 = the rest
-                                    of max_iterations, 0 = never leave FP32 */
+                                    phase stalls (no 2% gain in 25 checks; under
+                                    termination_rule 2 only below 1024 FP32 ulps, 1.2e-4);
+                                    -1 = the rest of max_iterations, 0 = never leave FP32 */
     int restart_rule;        /* 0 = reference (pdhg.cpp:391-408); 1 = adaptive: restart to
                                 the better of average/current on sufficient (0.2x) or
                                 necessary (0.8x, no progress) decay or when the average
@@ -149,6 +150,13 @@ typedef struct pdhg_options {
                                 finite lower end allows no decrease of x_j or (Ad)_i, a finite
                                 upper end no increase) by at most 1e-6 and 1e-6 |c^T d|, the
                                 solve stops with PDHG_STATUS_DUAL_INFEASIBLE and x receives d */
+    int halpern;             /* 0 (default) = the averaged PDHG of the reference. 1 (MIXED / FP64,
+                                with termination_rule 2 and restart_rule 2; not with
+                                infeasibility_detection): the reflected restarted Halpern
+                                iteration (Lu and Yang, 2024) -- with T the PDHG step and k the
+                                iterations since the last restart, z <- (k+1)/(k+2) (2 T(z) - z)
+                                + 1/(k+2) z_a for z = (x, s, y) and the anchor z_a = the last
+                                restart point; candidates and the reported point are T(z) */
 } pdhg_options;
 
 /* sov::PdhgResult (pdhg.hpp:136-153) minus the vectors, which pdhg_solve

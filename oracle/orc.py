@@ -47,7 +47,7 @@ class OrcOptions(C.Structure):
                 ("checkpoint", CHECKPOINT_FN), ("checkpoint_user", C.c_void_p),
                 ("cancel_flag", C.POINTER(C.c_int)), ("iter_times", _dp),
                 ("iter_times_cap", C.c_longlong), ("restart_rule", C.c_int),
-                ("primal_weight_update", C.c_int)]
+                ("primal_weight_update", C.c_int), ("halpern", C.c_int)]
 
 
 class OrcInfo(C.Structure):

@@ -632,6 +632,15 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
     double* y_last = NEWV(double, m);
     memcpy(x_last, x, sizeof(double) * (size_t)n);
     memcpy(y_last, y, sizeof(double) * (size_t)m);
+    /* extension (halpern): the anchor z_a = (xa, sa, ya) and y before the dual step */
+    const int halpern = opt->halpern;
+    double* xa = NEWV(double, n);
+    double* sa = NEWV(double, m);
+    double* ya = NEWV(double, m);
+    double* y_old = NEWV(double, m);
+    memcpy(xa, x, sizeof(double) * (size_t)n);
+    memcpy(sa, sl, sizeof(double) * (size_t)m);
+    memcpy(ya, y, sizeof(double) * (size_t)m);
     const double* best_x = NULL;
     const double* best_y = NULL;
     int converged = 0, failed = 0;
@@ -665,21 +674,38 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         scale(m, 2.0, s_bar);
         axpy(m, -1.0, sl, s_bar);
         /* pdhg.cpp:315-318 */
+        if (halpern) memcpy(y_old, y, sizeof(double) * (size_t)m);
         orc_spmv(m, s.rp, s.ci, s.v, -1.0, x_bar, 0.0, kb);
         axpy(m, 1.0, s_bar, kb);
         axpy(m, sigma, kb, y);
-        /* pdhg.cpp:320-321 */
-        memcpy(x, x_new, sizeof(double) * (size_t)n);
-        memcpy(sl, s_new, sizeof(double) * (size_t)m);
-        /* pdhg.cpp:323-331 */
-        if (since_restart == 0) {
-            memcpy(x_sum, x, sizeof(double) * (size_t)n);
+        if (halpern) {
+            /* T(z) = (x_new, s_new, y) is the candidate (kept in the sums'
+             * place, averaged over one term); z moves to the reflected
+             * Halpern point w (2 T(z) - z) + (1 - w) z_a, w = (k+1)/(k+2) */
+            const double w = (double)(since_restart + 1) / (double)(since_restart + 2);
+            const double wa = 1.0 - w;
+            memcpy(x_sum, x_new, sizeof(double) * (size_t)n);
             memcpy(y_sum, y, sizeof(double) * (size_t)m);
+            for (int32_t j = 0; j < n; ++j) x[j] = w * x_bar[j] + wa * xa[j];
+            for (int32_t i = 0; i < m; ++i) {
+                sl[i] = w * s_bar[i] + wa * sa[i];
+                y[i] = w * (2.0 * y[i] - y_old[i]) + wa * ya[i];
+            }
+            ++since_restart;
         } else {
-            axpy(n, 1.0, x, x_sum);
-            axpy(m, 1.0, y, y_sum);
+            /* pdhg.cpp:320-321 */
+            memcpy(x, x_new, sizeof(double) * (size_t)n);
+            memcpy(sl, s_new, sizeof(double) * (size_t)m);
+            /* pdhg.cpp:323-331 */
+            if (since_restart == 0) {
+                memcpy(x_sum, x, sizeof(double) * (size_t)n);
+                memcpy(y_sum, y, sizeof(double) * (size_t)m);
+            } else {
+                axpy(n, 1.0, x, x_sum);
+                axpy(m, 1.0, y, y_sum);
+            }
+            ++since_restart;
         }
-        ++since_restart;
         if (opt->trace_iters > 0 && it < opt->trace_iters) {
             if (opt->trace_x) memcpy(opt->trace_x + (size_t)it * n, x, sizeof(double) * (size_t)n);
             if (opt->trace_y) memcpy(opt->trace_y + (size_t)it * m, y, sizeof(double) * (size_t)m);
@@ -688,7 +714,7 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         if ((it + 1) % opt->restart_check_period != 0) continue; /* pdhg.cpp:333-334 */
 
         /* pdhg.cpp:336-345 */
-        const double inv = 1.0 / (double)since_restart;
+        const double inv = halpern ? 1.0 : 1.0 / (double)since_restart;
         for (int32_t j = 0; j < n; ++j) x_avg[j] = x_sum[j] * inv;
         for (int32_t i = 0; i < m; ++i) y_avg[i] = y_sum[i] * inv;
         /* restart_rule 2: current and average measured by rule 2's parts */
@@ -710,7 +736,8 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
             failed = 1;
             break;
         }
-        const int avg_better = avg <= cur; /* pdhg.cpp:354-364 */
+        /* pdhg.cpp:354-364; Halpern: the candidate is T(z) */
+        const int avg_better = halpern ? 1 : avg <= cur;
         const double* cx = avg_better ? x_avg : x;
         const double* cy = avg_better ? y_avg : y;
         const double bound_tol = opt->tolerance > 1e-6 ? opt->tolerance : 1e-6;
@@ -768,6 +795,11 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
                 csr_multiply(m, s.rp, s.ci, s.v, x_avg, sl);
                 orc_project_box(m, s.row_lo, s.row_hi, sl);
             }
+            if (halpern) { /* the restart point is the new anchor */
+                memcpy(xa, x, sizeof(double) * (size_t)n);
+                memcpy(sa, sl, sizeof(double) * (size_t)m);
+                memcpy(ya, y, sizeof(double) * (size_t)m);
+            }
             if (opt->primal_weight_update) {
                 double dx = 0.0, dy = 0.0;
                 for (int32_t j = 0; j < n; ++j) {
@@ -797,6 +829,10 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
     }
     free(x_last);
     free(y_last);
+    free(xa);
+    free(sa);
+    free(ya);
+    free(y_old);
     info->iterations = it;
 
     if (!failed) {

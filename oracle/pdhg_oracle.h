@@ -107,6 +107,14 @@ typedef struct {
      * |row bound|). */
     int restart_rule;
     int primal_weight_update;
+    /* halpern 1 (needs termination_rule 2 and restart_rule 2): the reflected
+     * Halpern iteration (Lu and Yang, "Restarted Halpern PDHG for linear
+     * programming", 2024): with T the PDHG step above and k the iterations
+     * since the last restart, z <- (k+1)/(k+2) (2 T(z) - z) + 1/(k+2) z_a for
+     * z = (x, s, y) and the anchor z_a = the last restart point. Candidates
+     * are T(z) (inside the column bounds; z itself need not be); a restart
+     * moves z and the anchor to T(z) (s to the row bounds' projection of A x). */
+    int halpern;
 } orc_options;
 
 typedef struct {

@@ -63,6 +63,9 @@ struct BatchCtx {
     DBuf<double> x64, xbar64, s64, y64, xsum, ysum, act_avg, xo, yo, rc, x_last, y_last;
     DBuf<double> pw_u, pw_v, pw_w, x0s, y0s;
     DBuf<float> x32, xbar32, s32, y32, psx, psy;
+    bool halpern = false;  // the current solve runs the Halpern iteration (its anchors below)
+    DBuf<double> xa64, sa64, ya64;
+    DBuf<float> xa32, sa32, ya32;
 
     // solve graphs, [0] FP32 and [1] FP64, with what they bake in
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -433,6 +436,12 @@ Iterates<double> batch_iterates<double>(BatchCtx& c) {
     it.y = c.y64.p;
     it.xsum = c.xsum.p;
     it.ysum = c.ysum.p;
+    if (c.halpern) {
+        it.xa = c.xa64.p;
+        it.sa = c.sa64.p;
+        it.ya = c.ya64.p;
+        it.halpern = 1;
+    }
     return it;
 }
 template <>
@@ -446,6 +455,12 @@ Iterates<float> batch_iterates<float>(BatchCtx& c) {
     it.psy = c.psy.p;
     it.xsum = c.xsum.p;
     it.ysum = c.ysum.p;
+    if (c.halpern) {
+        it.xa = c.xa32.p;
+        it.sa = c.sa32.p;
+        it.ya = c.ya32.p;
+        it.halpern = 1;
+    }
     return it;
 }
 
@@ -455,8 +470,8 @@ void batch_period(BatchCtx& c, const BatchParams& p, long long iters, bool with_
     const BatchView b = c.view();
     const Iterates<T> it = batch_iterates<T>(c);
     for (long long t = 0; t < iters; ++t) {
-        launch_batch_iter<T>(b, it, true, t == 0 ? 1 : 0, s);
-        launch_batch_iter<T>(b, it, false, t == 0 ? 1 : 0, s);
+        launch_batch_iter<T>(b, it, true, t == 0 ? 1 : 0, static_cast<int>(t), s);
+        launch_batch_iter<T>(b, it, false, t == 0 ? 1 : 0, static_cast<int>(t), s);
     }
     if (with_check) {
         launch_batch_check<T>(b, it, p, s);
@@ -518,10 +533,10 @@ template <class T>
 float batch_time_pass(BatchCtx& c, bool primal, cudaEvent_t e0, cudaEvent_t e1) {
     const BatchView b = c.view();
     const Iterates<T> it = batch_iterates<T>(c);
-    launch_batch_iter<T>(b, it, primal, 0, c.stream);
-    launch_batch_iter<T>(b, it, primal, 0, c.stream);
+    launch_batch_iter<T>(b, it, primal, 0, 0, c.stream);
+    launch_batch_iter<T>(b, it, primal, 0, 0, c.stream);
     cudaEventRecord(e0, c.stream);
-    for (int r = 0; r < 5; ++r) launch_batch_iter<T>(b, it, primal, 0, c.stream);
+    for (int r = 0; r < 5; ++r) launch_batch_iter<T>(b, it, primal, 0, 0, c.stream);
     cudaEventRecord(e1, c.stream);
     cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -675,9 +690,11 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
         o.restart_check_period < 1 ||
         o.termination_rule < 0 || o.termination_rule > 2 || o.restart_rule < 0 ||
         o.restart_rule > 2 || o.power_iterations < 0 ||
-        (o.restart_rule == 2 && o.termination_rule != 2)) {
+        (o.restart_rule == 2 && o.termination_rule != 2) || o.halpern < 0 || o.halpern > 1 ||
+        (o.halpern && (o.termination_rule != 2 || o.restart_rule != 2))) {
         c.err = "pdhg_solve_batch: invalid options (no checkpoint / trace / infeasibility "
-                "detection in batches; restart rule 2 needs termination rule 2)";
+                "detection in batches; restart rule 2 needs termination rule 2; halpern needs "
+                "both rules 2)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     BCK(cudaSetDevice(c.device));
@@ -716,6 +733,17 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
     if (o.primal_weight_update) {
         BCK(c.x_last.alloc(n1));
         BCK(c.y_last.alloc(m1));
+    }
+    c.halpern = o.halpern != 0;
+    if (c.halpern) {  // anchors: FP64 always (the FP64 phase), FP32 with f32
+        BCK(c.xa64.alloc(n1));
+        BCK(c.sa64.alloc(m1));
+        BCK(c.ya64.alloc(m1));
+        if (f32) {
+            BCK(c.xa32.alloc(n1));
+            BCK(c.sa32.alloc(m1));
+            BCK(c.ya32.alloc(m1));
+        }
     }
     // reset the solver part of every instance's state
     std::vector<InstState> h(static_cast<size_t>(c.count));
@@ -779,6 +807,10 @@ int batch_solve(BatchCtx& c, const pdhg_options& o, pdhg_info* infos, double* x,
         launch_init_point<float>(b.P, b.A, x0d, y0d, batch_iterates<float>(c), s);
     else
         launch_init_point<double>(b.P, b.A, x0d, y0d, batch_iterates<double>(c), s);
+    if (c.halpern) {  // the first anchor is the initial point
+        if (f32) launch_set_anchor<float>(batch_iterates<float>(c), c.n, c.m, s);
+        else launch_set_anchor<double>(batch_iterates<double>(c), c.n, c.m, s);
+    }
     if (o.primal_weight_update) {
         // restart points start at the initial point
         BCK(cudaStreamSynchronize(s));

@@ -42,7 +42,7 @@ __device__ double bmax(double v) {
 // rows of instances still iterating, rows above kLongRow left to the CTA path.
 template <class T, int VW, bool PRIMAL>
 __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T>& it, int first,
-                                            int blk) {
+                                            int hk, int blk) {
     const DevCsr& M = PRIMAL ? b.AT : b.A;
     const int32_t* inst_of = PRIMAL ? b.col_inst : b.row_inst;
     const T* __restrict__ vals = mvals<T>(M);
@@ -55,6 +55,7 @@ __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T
     if (s.done) return;  // uniform within the row's lane group
     const bool fresh = first && s.fresh;
     const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
+    const T hw = halpern_weight<T>(it, s.since_restart, hk);
     EpiIn<T> in{};
     if (lane == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
     const int rb = __ldcs(M.rp + r), re = __ldcs(M.rp + r + 1);
@@ -76,7 +77,7 @@ __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T
             if (k0 + u * VW < re) acc += v[u] * __ldg(xg + c[u]);
     }
     if (VW > 1) acc = group_sum(acc, VW);
-    if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
+    if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma, hw);
 }
 
 // The first short_grid CTAs take one block each of the active block list (the
@@ -86,12 +87,12 @@ __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T
 // lane-group path.
 template <class T, int VW, bool PRIMAL, bool LONG>
 __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it, int first,
-                                                     int short_grid) {
+                                                     int hk, int short_grid) {
     if (b.g->done) return;
     if (!LONG || static_cast<int>(blockIdx.x) < short_grid) {
         const int pi = PRIMAL ? 1 : 0;
         if (static_cast<int>(blockIdx.x) >= b.g->nblk[pi]) return;
-        batch_block<T, VW, PRIMAL>(b, it, first, b.blk_list[pi][blockIdx.x]);
+        batch_block<T, VW, PRIMAL>(b, it, first, hk, b.blk_list[pi][blockIdx.x]);
     } else {
         const DevCsr& M = PRIMAL ? b.AT : b.A;
         const int32_t* inst_of = PRIMAL ? b.col_inst : b.row_inst;
@@ -101,10 +102,11 @@ __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it
         const PV<T> pv = pvec<T>(b.P);
         const bool fresh = first && s.fresh;
         const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
+        const T hw = halpern_weight<T>(it, s.since_restart, hk);
         EpiIn<T> in{};
         if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
         const T acc = long_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? it.y : it.xbar, M.rp[r], M.rp[r + 1]);
-        if (threadIdx.x == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma);
+        if (threadIdx.x == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma, hw);
     }
 }
 
@@ -235,7 +237,8 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
     // early exit here; when it is set every instance is done anyway.)
     if (s.done) return;
     const long long k_avg = s.since_restart + p.period;
-    const double inv = 1.0 / static_cast<double>(k_avg);
+    // Halpern: the sums' slots hold T(z) itself
+    const double inv = it.halpern ? 1.0 : 1.0 / static_cast<double>(k_avg);
     Terms t;
     inst_pass<T, false>(b, it, p, k, part, parts, inv, s.obj_sign, t);
     inst_pass<T, true>(b, it, p, k, part, parts, inv, s.obj_sign, t);
@@ -313,7 +316,7 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
         finish_instance(b, s);
         return;
     }
-    const bool ab = avg <= cur;
+    const bool ab = it.halpern ? true : avg <= cur;  // Halpern: the candidate is T(z)
     s.avg_better = ab ? 1 : 0;
     const double op = ab ? oap : ocp, od = ab ? oad : ocd;
     const double orig = smax(op, od);
@@ -378,12 +381,12 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
         }
     }
     s.fresh = s.restart;
-    s.fold = std::is_same<T, float>::value ? 1 : 0;
+    s.fold = std::is_same<T, float>::value && !it.halpern ? 1 : 0;
     if (p.allow_switch) {  // no 2% gain in 25 checks: the FP32 phase of this instance ends
-        // under the relative rules only at FP32's precision floor (as the
-        // single engine: plateaus above kFp32Zone are the method's own)
+        // under rule 2 only at FP32's precision floor (as the single engine:
+        // plateaus above kFp32Zone are the method's own)
         const double r = p.termination_rule != 0 ? rel : orig;
-        if (p.termination_rule != 0 && r > kFp32Zone) {
+        if (p.termination_rule == 2 && r > kFp32Zone) {
             s.since_improve = 0;
             if (r < s.best_res) s.best_res = r;
         } else if (r < 0.98 * s.best_res) {
@@ -421,6 +424,7 @@ __global__ void __launch_bounds__(kBlock) batch_restart(BatchView b, Iterates<T>
     double dx2 = 0.0, dy2 = 0.0;
     for (int j = b.col_off[k] + threadIdx.x; j < b.col_off[k + 1]; j += kBlock) {
         if (restart && to_avg) it.x[j] = clampT<T>(static_cast<T>(avg_x(it, j, inv)), pv.lo[j], pv.hi[j]);
+        if (restart && it.halpern) it.xa[j] = it.x[j];  // the new anchor
         if (restart && p.primal_weight_update) {
             const double xn = static_cast<double>(it.x[j]);
             const double d = xn - p.x_last[j];
@@ -434,6 +438,10 @@ __global__ void __launch_bounds__(kBlock) batch_restart(BatchView b, Iterates<T>
         if (restart && to_avg) {
             it.y[i] = static_cast<T>(avg_y(it, i, inv));
             it.s[i] = clampT<T>(static_cast<T>(p.act_avg[i]), pv.rlo[i], pv.rhi[i]);
+        }
+        if (restart && it.halpern) {
+            it.ya[i] = it.y[i];
+            it.sa[i] = it.s[i];
         }
         if (restart && p.primal_weight_update) {
             const double yn = static_cast<double>(it.y[i]);
@@ -763,13 +771,19 @@ __device__ __forceinline__ double inf_box(double coeff, double lo, double hi) {
 
 __global__ void batch_widen(BatchView b, Iterates<float> f, Iterates<double> d) {
     const int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    // Halpern: the FP64 phase starts at T(z) as a restart point and anchor
     if (t < b.n) {
-        d.x[t] = f.x[t];
-        d.xbar[t] = f.xbar[t];
+        d.x[t] = d.halpern ? f.psx[t] : f.x[t];
+        d.xbar[t] = d.halpern ? f.psx[t] : f.xbar[t];
+        if (d.halpern) d.xa[t] = d.x[t];
     }
     if (t < b.m) {
-        d.y[t] = f.y[t];
+        d.y[t] = d.halpern ? f.psy[t] : f.y[t];
         d.s[t] = f.s[t];
+        if (d.halpern) {
+            d.ya[t] = d.y[t];
+            d.sa[t] = d.s[t];
+        }
     }
 }
 
@@ -781,8 +795,9 @@ __global__ void __launch_bounds__(kBlock) batch_final(BatchView b, Iterates<T> i
     InstState& s = b.is[k];
     if (which >= 0 && s.polished != which) return;  // uniform per CTA
     const DevProblem& P = b.P;
-    const bool cand_avg = s.converged && s.avg_better;
-    const double inv = s.inv, sign = s.obj_sign;
+    // Halpern: after a check the sums' slots hold T(z), the reported point
+    const bool cand_avg = it.halpern ? b.g->checks > 0 : (s.converged && s.avg_better);
+    const double inv = it.halpern ? 1.0 : s.inv, sign = s.obj_sign;
     // best point in original units (unscale_to_original, pdhg.cpp:205-214)
     for (int j = b.col_off[k] + threadIdx.x; j < b.col_off[k + 1]; j += kBlock) {
         const double xs = cand_avg ? avg_x(it, j, inv) : static_cast<double>(it.x[j]);
@@ -913,7 +928,7 @@ void launch_batch_point_kkt(const BatchView& b, const double* x, const double* y
 
 template <class T>
 void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, int first,
-                       cudaStream_t s) {
+                       int hk, cudaStream_t s) {
     const DevCsr& M = primal ? b.AT : b.A;
     if (M.rows == 0) return;
     const int sb = short_blocks(M);
@@ -921,11 +936,11 @@ void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, i
 #define PDHG_BATCH_ITER(VW)                                                                      \
     do {                                                                                         \
         if (M.n_long > 0) {                                                                      \
-            if (primal) batch_iter<T, VW, true, true><<<grid, kBlock, 0, s>>>(b, it, first, sb); \
-            else batch_iter<T, VW, false, true><<<grid, kBlock, 0, s>>>(b, it, first, sb);      \
+            if (primal) batch_iter<T, VW, true, true><<<grid, kBlock, 0, s>>>(b, it, first, hk, sb); \
+            else batch_iter<T, VW, false, true><<<grid, kBlock, 0, s>>>(b, it, first, hk, sb);      \
         } else {                                                                                 \
-            if (primal) batch_iter<T, VW, true, false><<<grid, kBlock, 0, s>>>(b, it, first, sb);\
-            else batch_iter<T, VW, false, false><<<grid, kBlock, 0, s>>>(b, it, first, sb);     \
+            if (primal) batch_iter<T, VW, true, false><<<grid, kBlock, 0, s>>>(b, it, first, hk, sb);\
+            else batch_iter<T, VW, false, false><<<grid, kBlock, 0, s>>>(b, it, first, hk, sb);     \
         }                                                                                        \
     } while (0)
     switch (M.vw) {
@@ -1018,8 +1033,8 @@ void launch_batch_final(const BatchView& b, const Iterates<T>& it, double bound_
     if (b.count > 0) batch_final<T><<<b.count, kBlock, 0, s>>>(b, it, bound_tol, xo, yo, rc, which);
 }
 
-template void launch_batch_iter<float>(const BatchView&, const Iterates<float>&, bool, int, cudaStream_t);
-template void launch_batch_iter<double>(const BatchView&, const Iterates<double>&, bool, int, cudaStream_t);
+template void launch_batch_iter<float>(const BatchView&, const Iterates<float>&, bool, int, int, cudaStream_t);
+template void launch_batch_iter<double>(const BatchView&, const Iterates<double>&, bool, int, int, cudaStream_t);
 template void launch_batch_check<float>(const BatchView&, const Iterates<float>&, const BatchParams&, cudaStream_t);
 template void launch_batch_check<double>(const BatchView&, const Iterates<double>&, const BatchParams&, cudaStream_t);
 template void launch_batch_restart<float>(const BatchView&, const Iterates<float>&, const BatchParams&, cudaStream_t);

@@ -94,7 +94,7 @@ struct BatchParams {
 // launchers (batch_kernels.cu)
 template <class T>
 void launch_batch_iter(const BatchView& b, const Iterates<T>& it, bool primal, int first,
-                       cudaStream_t s);
+                       int hk, cudaStream_t s);
 template <class T>
 void launch_batch_check(const BatchView& b, const Iterates<T>& it, const BatchParams& p,
                         cudaStream_t s);

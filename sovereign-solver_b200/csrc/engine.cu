@@ -46,12 +46,12 @@ struct GraphSig {
     long long period = 0;
     int cand = 0;
     double tol = 0, bt = 0, dec = 0;
-    int rule = 0, restart_rule = 0, pw = 0, infeas = 0;
+    int rule = 0, restart_rule = 0, pw = 0, infeas = 0, halpern = 0;
     long long gen = -1;
     bool operator==(const GraphSig& o) const {
         return prec == o.prec && period == o.period && cand == o.cand && tol == o.tol &&
                bt == o.bt && dec == o.dec && rule == o.rule && restart_rule == o.restart_rule &&
-               pw == o.pw && infeas == o.infeas && gen == o.gen;
+               pw == o.pw && infeas == o.infeas && halpern == o.halpern && gen == o.gen;
     }
 };
 
@@ -84,6 +84,9 @@ struct Ctx {
 
     DBuf<double> x64, xbar64, s64, y64, xsum, ysum;
     DBuf<float> x32, xbar32, s32, y32, psx, psy;
+    bool halpern = false;  // the current solve runs the Halpern iteration (its anchors below)
+    DBuf<double> xa64, sa64, ya64;
+    DBuf<float> xa32, sa32, ya32;
     DBuf<double> act_avg, cand_xo, cand_yo, part, bx, by, xo, yo, rc, trow, tcol;
     DBuf<double> pw_u, pw_v, pw_w, pw_part, pw_out, x0s, y0s;
     DBuf<double> x_last, y_last;  // restart points (primal-weight update)
@@ -356,6 +359,12 @@ Iterates<double> iterates<double>(Ctx& c) {
     it.y = c.y64.p;
     it.xsum = c.xsum.p;
     it.ysum = c.ysum.p;
+    if (c.halpern) {
+        it.xa = c.xa64.p;
+        it.sa = c.sa64.p;
+        it.ya = c.ya64.p;
+        it.halpern = 1;
+    }
     return it;
 }
 template <>
@@ -369,6 +378,12 @@ Iterates<float> iterates<float>(Ctx& c) {
     it.psy = c.psy.p;
     it.xsum = c.xsum.p;
     it.ysum = c.ysum.p;
+    if (c.halpern) {
+        it.xa = c.xa32.p;
+        it.sa = c.sa32.p;
+        it.ya = c.ya32.p;
+        it.halpern = 1;
+    }
     return it;
 }
 
@@ -376,6 +391,16 @@ int alloc_iterates(Ctx& c, bool f32) {
     const size_t n = static_cast<size_t>(c.lp.n) + 1, m = static_cast<size_t>(c.lp.m) + 1;
     CK(c.xsum.alloc(n));
     CK(c.ysum.alloc(m));
+    if (c.halpern) {  // anchors: FP64 always (the mixed mode's FP64 phase), FP32 with f32
+        CK(c.xa64.alloc(n));
+        CK(c.sa64.alloc(m));
+        CK(c.ya64.alloc(m));
+        if (f32) {
+            CK(c.xa32.alloc(n));
+            CK(c.sa32.alloc(m));
+            CK(c.ya32.alloc(m));
+        }
+    }
     if (f32) {
         CK(c.x32.alloc(n));
         CK(c.xbar32.alloc(n));
@@ -415,7 +440,10 @@ struct Launcher {
     FastCheck<float> fc32;
     FastCheck<double> fc64;
 
-    void iteration(int first, cudaStream_t s) {
+    // iteration t of a check period (t = 0 first): the Halpern weight uses t
+    void iteration(long long t, cudaStream_t s) {
+        const int first = t == 0 ? 1 : 0;
+        fi32.hk = fi64.hk = static_cast<int>(t);
         if (prec == PDHG_PREC_FP64_EXACT) {
             launch_exact_primal(ei, first, s);
             launch_exact_dual(ei, first, s);
@@ -536,7 +564,7 @@ int build_graph(Ctx& c, Launcher& L, long long period, const GraphSig& sig) {
     cudaGraph_t g = nullptr;
     const long long before = c.launches;
     CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-    for (long long t = 0; t < period; ++t) L.iteration(t == 0 ? 1 : 0, c.stream);
+    for (long long t = 0; t < period; ++t) L.iteration(t, c.stream);
     L.check(period, c.stream);
     cudaError_t e = cudaStreamEndCapture(c.stream, &g);
     c.launches = before;
@@ -644,12 +672,14 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         }
         if (allow_switch && !done) {
             // The FP32 phase hands over to FP64 when it stops improving (no 2%
-            // gain in 25 checks) at its precision floor. Under the relative
-            // rules a plateau counts only within kFp32Zone of FP32's unit
-            // roundoff: higher plateaus are the method's, and FP64 iterations
-            // would not end them sooner.
+            // gain in 25 checks). Under rule 2 (l2 relative KKT) a plateau
+            // counts only within kFp32Zone of FP32's unit roundoff: higher
+            // plateaus are the method's, and FP64 iterations would not end
+            // them sooner. The max-norm rules (0, 1) react to single entries,
+            // whose FP32 rounding sets floors far above that, so any plateau
+            // counts there.
             const double r = o.termination_rule != 0 ? rel_kkt : orig_res;
-            if (o.termination_rule != 0 && r > kFp32Zone) {
+            if (o.termination_rule == 2 && r > kFp32Zone) {
                 since_improve = 0;
                 if (r < best) best = r;
             } else if (r < 0.98 * best) {
@@ -682,7 +712,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
     while (p < n_periods && p * period < traced && !c.mail->done) {
         poll_stop();
         for (long long t = 0; t < period; ++t) {
-            L.iteration(t == 0 ? 1 : 0, c.stream);
+            L.iteration(t, c.stream);
             const long long k = iter0 + p * period + t;
             if (k < o.trace_iters) {
                 int rc = trace_copy(c, L.prec, k, o);
@@ -707,6 +737,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         sig.restart_rule = o.restart_rule;
         sig.pw = o.primal_weight_update;
         sig.infeas = o.infeasibility_detection;
+        sig.halpern = o.halpern;
         sig.gen = c.gen;
         int rc = build_graph(c, L, period, sig);
         if (rc != PDHG_OK) return rc;
@@ -757,7 +788,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         poll_stop();
         if (!stop_sent) {
             for (long long t = 0; t < tail; ++t) {
-                L.iteration(t == 0 ? 1 : 0, c.stream);
+                L.iteration(t, c.stream);
                 const long long k = iter0 + n_periods * period + t;
                 if (k < o.trace_iters) {
                     int rc = trace_copy(c, L.prec, k, o);
@@ -789,15 +820,22 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
 // Cesaro average there (the FP64 polish phase of the mixed mode).
 __global__ void k_widen(Iterates<float> a, Iterates<double> b, int32_t n, int32_t m) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
+    // Halpern: the FP64 phase starts at T(z) (inside the bounds) as a restart
+    // point, which is also its first anchor
     if (t < n) {
-        b.x[t] = a.x[t];
-        b.xbar[t] = a.xbar[t];
+        b.x[t] = b.halpern ? a.psx[t] : a.x[t];
+        b.xbar[t] = b.halpern ? a.psx[t] : a.xbar[t];
         b.xsum[t] = 0.0;
+        if (b.halpern) b.xa[t] = b.x[t];
     }
     if (t < m) {
-        b.y[t] = a.y[t];
+        b.y[t] = b.halpern ? a.psy[t] : a.y[t];
         b.s[t] = a.s[t];
         b.ysum[t] = 0.0;
+        if (b.halpern) {
+            b.ya[t] = b.y[t];
+            b.sa[t] = b.s[t];
+        }
     }
 }
 
@@ -1044,6 +1082,13 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
                 "mixed or fp64 (fp64_exact reproduces the reference, which has neither)";
         return PDHG_ERR_INVALID_ARGUMENT;
     }
+    if (o.halpern < 0 || o.halpern > 1 ||
+        (o.halpern && (o.precision == PDHG_PREC_FP64_EXACT || o.termination_rule != 2 ||
+                       o.restart_rule != 2 || o.infeasibility_detection))) {
+        c.err = "pdhg_solve: halpern is 0 or 1 and needs precision mixed or fp64, termination "
+                "rule 2 and restart rule 2, and no infeasibility detection";
+        return PDHG_ERR_INVALID_ARGUMENT;
+    }
     if (o.infeasibility_detection < 0 || o.infeasibility_detection > 1 ||
         (o.precision == PDHG_PREC_FP64_EXACT && o.infeasibility_detection)) {
         c.err = "pdhg_solve: infeasibility_detection is 0 or 1 and needs precision mixed or "
@@ -1051,6 +1096,7 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     CK(cudaSetDevice(c.device));
+    c.halpern = o.halpern != 0;
     ScalingParams sp;
     sp.ruiz_iterations = o.ruiz_iterations;
     sp.ruiz_tolerance = o.ruiz_tolerance;
@@ -1130,6 +1176,11 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     else
         launch_init_point<double>(P, c.As.view(), x0d, y0d, iterates<double>(c), c.stream);
     c.launches += 1;
+    if (c.halpern) {  // the first anchor is the initial point
+        if (prec == PDHG_PREC_MIXED) launch_set_anchor<float>(iterates<float>(c), n, m, c.stream);
+        else launch_set_anchor<double>(iterates<double>(c), n, m, c.stream);
+        c.launches += 1;
+    }
     if (o.primal_weight_update) {
         CK(c.x_last.alloc(static_cast<size_t>(n) + 1));
         CK(c.y_last.alloc(static_cast<size_t>(m) + 1));
@@ -1388,6 +1439,7 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     CK(cudaSetDevice(c.device));
+    c.halpern = false;  // the kernels are timed in the averaged form
     int rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
     if (rc != PDHG_OK) return rc;
     CK(c.st.alloc(1));
@@ -1404,7 +1456,7 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
         launch_init_point<float>(P, c.As.view(), nullptr, nullptr, iterates<float>(c), c.stream);
     else
         launch_init_point<double>(P, c.As.view(), nullptr, nullptr, iterates<double>(c), c.stream);
-    for (int i = 0; i < warmup; ++i) L.iteration(i == 0, c.stream);
+    for (int i = 0; i < warmup; ++i) L.iteration(i, c.stream);
     std::vector<cudaEvent_t> ev(3 * static_cast<size_t>(iters) + 2);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int i = 0; i < iters; ++i) {
@@ -1481,6 +1533,7 @@ void pdhg_default_options(pdhg_options* o) {
     o->polish_iterations = -1;
     o->autotune = 1;
     o->infeasibility_detection = 0;
+    o->halpern = 0;
 }
 
 const char* pdhg_status_string(int s) {

@@ -155,9 +155,9 @@ enum Ticket { TK_CHECK1 = 0, TK_CHECK2, TK_FAST, TK_RESTART, TK_COUNT = 4 };
 // Farkas ranges (4), c^T dx of the ray test (1).
 constexpr int kCheckSums = 13;
 
-// Mixed precision: a relative-KKT plateau above this value (1024 units of
-// FP32 roundoff) is the method's own, not FP32's precision floor, so the FP32
-// phase keeps running there.
+// Mixed precision under termination rule 2: a relative-KKT plateau above this
+// value (1024 units of FP32 roundoff) is the method's own, not FP32's
+// precision floor, so the FP32 phase keeps running there.
 constexpr double kFp32Zone = 1024.0 * 1.1920928955078125e-7;
 
 struct DevState {
@@ -232,6 +232,11 @@ struct Iterates {
     T *x = nullptr, *xbar = nullptr, *s = nullptr, *y = nullptr;
     T *psx = nullptr, *psy = nullptr;
     double *xsum = nullptr, *ysum = nullptr;
+    // option halpern: the anchor (the last restart point) of the reflected
+    // Halpern iteration; the sums' slots (psx / psy, or xsum / ysum in FP64)
+    // then hold the last PDHG output T(z) instead of running sums
+    T *xa = nullptr, *sa = nullptr, *ya = nullptr;
+    int halpern = 0;
 };
 
 struct CheckScratch {
@@ -283,6 +288,7 @@ struct FastIter {
     DevProblem P;
     Iterates<T> it;
     DevState* st;
+    int hk = 0;  // the iteration's index in its check period (Halpern weight)
 };
 // A pass's short-row, long-row and row-slice kernels touch disjoint rows and
 // only read the gathered vector, so they may run side by side: with a
@@ -379,6 +385,9 @@ void launch_select_point(const Iterates<T>& it, const DevState* st, int32_t n, i
                          double* bx, double* by, cudaStream_t s);
 
 // Initial point (pdhg.cpp:268-270) or warm start; FP64 scaled inputs.
+// z_a <- z for the Halpern option's anchor (x, s, y); n, m entries.
+template <class T>
+void launch_set_anchor(const Iterates<T>& it, int32_t n, int32_t m, cudaStream_t s);
 template <class T>
 void launch_init_point(const DevProblem& P, const DevCsr& A, const double* x0s,
                        const double* y0s, Iterates<T> it, cudaStream_t s);

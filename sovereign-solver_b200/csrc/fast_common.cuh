@@ -349,48 +349,74 @@ struct EpiIn {
     T a, b, lo, hi, ps;  // primal: c, x, lo, hi, sum; dual: y, s, row lo, row hi, sum
 };
 
+// The reflected Halpern weight w = (k+1)/(k+2) of an iteration, k the
+// iterations since the last restart (0 without the option).
+template <class T>
+__device__ __forceinline__ T halpern_weight(const Iterates<T>& it, long long since_restart, int hk) {
+    if (!it.halpern) return T(0);
+    const double k = static_cast<double>(since_restart + hk);
+    return static_cast<T>((k + 1.0) / (k + 2.0));
+}
+
 template <class T, bool PRIMAL>
 __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>& pv, int r,
                                              int first, bool fresh) {
     EpiIn<T> in;
+    // (Halpern: the sums' slot is only written; its anchors are read at the store)
     if (PRIMAL) {
         in.a = __ldcs(pv.c + r);
         in.b = __ldcs(it.x + r);
         in.lo = __ldcs(pv.lo + r);
         in.hi = __ldcs(pv.hi + r);
-        if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psx + r);
-        else in.ps = fresh ? T(0) : __ldcs(it.xsum + r);
+        if constexpr (std::is_same<T, float>::value) in.ps = first || it.halpern ? T(0) : __ldcs(it.psx + r);
+        else in.ps = fresh || it.halpern ? T(0) : __ldcs(it.xsum + r);
     } else {
         in.a = it.y[r];
         in.b = __ldcs(it.s + r);
         in.lo = __ldcs(pv.rlo + r);
         in.hi = __ldcs(pv.rhi + r);
-        if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psy + r);
-        else in.ps = fresh ? T(0) : __ldcs(it.ysum + r);
+        if constexpr (std::is_same<T, float>::value) in.ps = first || it.halpern ? T(0) : __ldcs(it.psy + r);
+        else in.ps = fresh || it.halpern ? T(0) : __ldcs(it.ysum + r);
     }
     return in;
 }
 
 // primal: x+ = proj(x - tau (c - aty)), x_bar = 2x+ - x, sum += x+
 // dual:   s+ = proj(s - tau y), y+ = y + sigma (2s+ - s - ax), sum += y+
+// With the Halpern option (weight hw = w) the step's output T(z) = (x+, s+, y+)
+// goes to the sums' slot and z moves to w (2 T(z) - z) + (1 - w) z_a.
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, const EpiIn<T>& in,
-                                          T tau, T sigma) {
+                                          T tau, T sigma, T hw) {
+    T* ps = nullptr;
+    if constexpr (std::is_same<T, float>::value) ps = PRIMAL ? it.psx : it.psy;
+    else ps = PRIMAL ? it.xsum : it.ysum;
     if (PRIMAL) {
         const T xo = in.b;
         const T xn = clampT<T>(xo - tau * (in.a - dot), in.lo, in.hi);
-        it.xbar[r] = T(2) * xn - xo;
-        __stcs(it.x + r, xn);
-        if constexpr (std::is_same<T, float>::value) __stcs(it.psx + r, in.ps + xn);
-        else __stcs(it.xsum + r, in.ps + xn);
+        const T xb = T(2) * xn - xo;
+        it.xbar[r] = xb;
+        if (it.halpern) {
+            __stcs(it.x + r, hw * xb + (T(1) - hw) * __ldcs(it.xa + r));
+            __stcs(ps + r, xn);
+        } else {
+            __stcs(it.x + r, xn);
+            __stcs(ps + r, in.ps + xn);
+        }
     } else {
         const T yo = in.a, so = in.b;
         const T sn = clampT<T>(so - tau * yo, in.lo, in.hi);
-        const T yn = yo + sigma * ((T(2) * sn - so) - dot);
-        it.y[r] = yn;
-        __stcs(it.s + r, sn);
-        if constexpr (std::is_same<T, float>::value) __stcs(it.psy + r, in.ps + yn);
-        else __stcs(it.ysum + r, in.ps + yn);
+        const T sb = T(2) * sn - so;
+        const T yn = yo + sigma * (sb - dot);
+        if (it.halpern) {
+            it.y[r] = hw * (T(2) * yn - yo) + (T(1) - hw) * __ldcs(it.ya + r);
+            __stcs(it.s + r, hw * sb + (T(1) - hw) * __ldcs(it.sa + r));
+            __stcs(ps + r, yn);
+        } else {
+            it.y[r] = yn;
+            __stcs(it.s + r, sn);
+            __stcs(ps + r, in.ps + yn);
+        }
     }
 }
 

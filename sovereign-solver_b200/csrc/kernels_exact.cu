@@ -647,8 +647,9 @@ template <class T>
 __global__ void k_select_point(Iterates<T> it, const DevState* st, int32_t n, int32_t m,
                                double* bx, double* by) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
-    const bool cand_avg = st->converged && st->avg_better;
-    const double inv = st->inv;
+    // Halpern: after a check the sums' slots hold T(z), the reported point
+    const bool cand_avg = it.halpern ? st->checks > 0 : (st->converged && st->avg_better);
+    const double inv = it.halpern ? 1.0 : st->inv;
     if (t < n) {
         if (cand_avg) {
             const double s = it.psx ? it.xsum[t] + static_cast<double>(it.psx[t]) : it.xsum[t];
@@ -857,6 +858,25 @@ template void launch_select_point<double>(const Iterates<double>&, const DevStat
                                           int32_t, double*, double*, cudaStream_t);
 template void launch_select_point<float>(const Iterates<float>&, const DevState*, int32_t,
                                          int32_t, double*, double*, cudaStream_t);
+
+// The Halpern anchor z_a <- z (the initial point).
+template <class T>
+__global__ void k_set_anchor(Iterates<T> it, int32_t n, int32_t m) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t < n) it.xa[t] = it.x[t];
+    if (t < m) {
+        it.sa[t] = it.s[t];
+        it.ya[t] = it.y[t];
+    }
+}
+
+template <class T>
+void launch_set_anchor(const Iterates<T>& it, int32_t n, int32_t m, cudaStream_t s) {
+    const int32_t nmax = n > m ? n : m;
+    if (nmax > 0) k_set_anchor<T><<<blocks_for(nmax), kBlock, 0, s>>>(it, n, m);
+}
+template void launch_set_anchor<float>(const Iterates<float>&, int32_t, int32_t, cudaStream_t);
+template void launch_set_anchor<double>(const Iterates<double>&, int32_t, int32_t, cudaStream_t);
 
 template <class T>
 void launch_init_point(const DevProblem& P, const DevCsr& A, const double* x0s,

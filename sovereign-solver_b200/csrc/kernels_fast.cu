@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
     const int lane = threadIdx.x & (VW - 1);
     const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
     if (r >= M.rows) return;
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
             if (k0 + u * VW < e) acc += v[u] * __ldg(xg + c[u]);
     }
     if (VW > 1) acc = group_sum(acc, VW);
-    if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw);
 }
 
 // One CTA work item of L (block-uniform): the dot of its entries, then for a
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
 // update when this CTA completes the row).
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void cta_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
-                                         int idx, int first, bool fresh, T tau, T sigma) {
+                                         int idx, int first, bool fresh, T tau, T sigma, T hw) {
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     const PV<T> pv = pvec<T>(a.P);
@@ -141,7 +142,7 @@ __device__ __forceinline__ void cta_item(const FastIter<T>& a, const DevCsr& M, 
         acc = static_cast<T>(tot);
         if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
     }
-    if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+    if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw);
 }
 
 // WARPS = true: the first warp_blocks CTAs take the warp rows, one CTA per
@@ -158,12 +159,13 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
     const RowItems& L = MODE == 0 ? M.items_long : M.items_huge;
     if (!WARPS) {
         for (;;) {
             const int idx = cta_fetch(L.fetch);
             if (idx >= L.n_item) break;
-            cta_item<T, PRIMAL>(a, M, L, idx, first, fresh, tau, sigma);
+            cta_item<T, PRIMAL>(a, M, L, idx, first, fresh, tau, sigma, hw);
         }
         cta_exit(L.fetch);
         return;
@@ -180,12 +182,12 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
         const T acc = warp_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? a.it.y : a.it.xbar,
                                       __ldg(M.rp + r), __ldg(M.rp + r + 1));
-        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma);
+        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw);
     } else {
         // CTA work items: rows above kLongRow (mode 0) or kHugeRow (mode 1),
         // those above the segment length in segments
         cta_item<T, PRIMAL>(a, M, L, static_cast<int>(blockIdx.x) - warp_blocks, first, fresh,
-                            tau, sigma);
+                            tau, sigma, hw);
     }
 }
 
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
 // of a longer one whose last warp adds the segments in order.
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void warp_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
-                                          int idx, int first, bool fresh, T tau, T sigma) {
+                                          int idx, int first, bool fresh, T tau, T sigma, T hw) {
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     const PV<T> pv = pvec<T>(a.P);
@@ -208,7 +210,7 @@ __device__ __forceinline__ void warp_item(const FastIter<T>& a, const DevCsr& M,
         acc = static_cast<T>(tot);
         if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
     }
-    if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma);
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw);
 }
 
 // long_mode 2: every row above short_max as warp work items; no block barrier
@@ -224,7 +226,8 @@ __global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
     if (idx >= M.items_warp.n_item) return;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    warp_item<T, PRIMAL>(a, M, M.items_warp, idx, first, fresh, tau, sigma);
+    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
+    warp_item<T, PRIMAL>(a, M, M.items_warp, idx, first, fresh, tau, sigma, hw);
 }
 
 template <class T>
@@ -287,7 +290,7 @@ __device__ __forceinline__ T slice_dot(const RowSlices& S, int off, int k0s, int
 // interleaved sums, fixed) before the 32 rows' updates.
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices& S, int idx,
-                                           int first, bool fresh, T tau, T sigma) {
+                                           int first, bool fresh, T tau, T sigma, T hw) {
     const int lane = threadIdx.x & 31;
     const int4 w = __ldg(S.item + idx);
     const int4 d = __ldg(S.slice + w.x);
@@ -324,7 +327,7 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
     if (row < 0) return;
     const PV<T> pv = pvec<T>(a.P);
     const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, row, first, fresh);
-    epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma);
+    epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma, hw);
 }
 
 // The row-slice kernel: a persistent grid (the resident CTAs) whose warps
@@ -341,13 +344,14 @@ __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     const RowSlices& S = M.slices;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
     const int ns = S.n_item;
     const int nt = ns + (WITEMS ? M.items_warp.n_item : 0);
     for (;;) {
         const int idx = warp_fetch(S.fetch);
         if (idx >= nt) break;
-        if (!WITEMS || idx < ns) slice_item<T, PRIMAL>(a, S, idx, first, fresh, tau, sigma);
-        else warp_item<T, PRIMAL>(a, M, M.items_warp, idx - ns, first, fresh, tau, sigma);
+        if (!WITEMS || idx < ns) slice_item<T, PRIMAL>(a, S, idx, first, fresh, tau, sigma, hw);
+        else warp_item<T, PRIMAL>(a, M, M.items_warp, idx - ns, first, fresh, tau, sigma, hw);
     }
     warp_exit(S.fetch);
 }
@@ -808,7 +812,8 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
     DevState* st = a.st;
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
-    const double inv = 1.0 / static_cast<double>(k_avg);
+    // Halpern: the sums' slots hold T(z) itself
+    const double inv = a.it.halpern ? 1.0 : 1.0 / static_cast<double>(k_avg);
     Terms t;
     const int sbA = check_short_blocks(a.A), wbA = check_warp_blocks(a.A);
     const int sbT = check_short_blocks(a.AT), wbT = check_warp_blocks(a.AT);
@@ -910,7 +915,9 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
         st->fail_kind = 1;
         st->stop_iter = it_idx;
     } else {
-        const bool ab = avg <= cur;  // pdhg.cpp:354
+        // pdhg.cpp:354; Halpern: the candidate is T(z) (z itself may lie
+        // outside the column bounds)
+        const bool ab = a.it.halpern ? true : avg <= cur;
         st->avg_better = ab ? 1 : 0;
         const double op = ab ? oap : ocp, od = ab ? oad : ocd;
         const double orig = smax(op, od);
@@ -1017,7 +1024,7 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
                     st->since_restart = span;
                 }
                 st->fresh = st->restart;
-                st->fold = std::is_same<T, float>::value ? 1 : 0;
+                st->fold = std::is_same<T, float>::value && !a.it.halpern ? 1 : 0;
                 const int stop = a.mail != nullptr ? a.mail->stop_request : 0;
                 if (stop != 0) {
                     st->done = 1;
@@ -1081,6 +1088,7 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
     if (t < a.P.n) {
         if (restart && to_avg)
             a.it.x[t] = clampT<T>(static_cast<T>(avg_x(a.it, t, inv)), pv.lo[t], pv.hi[t]);
+        if (restart && a.it.halpern) a.it.xa[t] = a.it.x[t];  // the new anchor
         if (restart && a.primal_weight_update) {
             const double xn = static_cast<double>(a.it.x[t]);
             const double d = xn - a.x_last[t];
@@ -1095,6 +1103,10 @@ __global__ void __launch_bounds__(kBlock) fast_restart(FastCheck<T> a) {
         if (restart && to_avg) {
             a.it.y[t] = static_cast<T>(avg_y(a.it, t, inv));
             a.it.s[t] = clampT<T>(static_cast<T>(a.cs.act_avg[t]), pv.rlo[t], pv.rhi[t]);
+        }
+        if (restart && a.it.halpern) {
+            a.it.ya[t] = a.it.y[t];
+            a.it.sa[t] = a.it.s[t];
         }
         if (restart && a.primal_weight_update) {
             const double yn = static_cast<double>(a.it.y[t]);

@@ -45,7 +45,8 @@ class _Options(C.Structure):
                 ("x0", _dp), ("y0", _dp), ("checkpoint", CHECKPOINT_FN),
                 ("checkpoint_user", C.c_void_p), ("cancel_flag", C.POINTER(C.c_int)),
                 ("trace_iters", C.c_int), ("trace_x", _dp), ("trace_y", _dp),
-                ("autotune", C.c_int), ("infeasibility_detection", C.c_int)]
+                ("autotune", C.c_int), ("infeasibility_detection", C.c_int),
+                ("halpern", C.c_int)]
 
 
 class _Info(C.Structure):
@@ -171,6 +172,11 @@ class PdhgOptions:
     # ray (PdhgResult.ray) when the change of x between two checks is a
     # direction of unbounded descent
     infeasibility_detection: bool = False
+    # engine extension (MIXED / FP64, with termination_rule "relative_kkt_l2" and
+    # restart_rule "adaptive_l2"): the reflected restarted Halpern iteration
+    # instead of the averaged PDHG; candidates and the reported point are the
+    # PDHG step's output T(z)
+    halpern: bool = False
 
 
 @dataclass

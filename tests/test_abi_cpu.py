@@ -48,7 +48,8 @@ def test_defaults_are_the_reference_defaults(pkg):
     assert o.precision == 0 and o.termination_rule == 0
     assert o.autotune == 1  # an engine extension; it never applies to fp64_exact
     assert o.infeasibility_detection == 0  # extension, off: the reference never reports it
-    assert lib.pdhg_abi_version() == 3
+    assert o.halpern == 0  # extension, off: the reference's averaged PDHG
+    assert lib.pdhg_abi_version() == 4
     d = pkg.PdhgOptions()
     assert d.tolerance == o.tolerance and d.max_iterations == o.max_iterations
 

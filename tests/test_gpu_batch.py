@@ -73,6 +73,24 @@ def test_batch_rule2_follows_the_oracle_per_instance(pkg, orc, engine):
                 (prec, k, r.objective, o.objective)
 
 
+def test_batch_halpern_follows_the_oracle_per_instance(pkg, orc, engine):
+    ps = family(pkg)
+    engine.load_batch(ps)
+    for prec in ("fp64", "mixed"):
+        rs = engine.solve_batch(pkg.PdhgOptions(
+            precision=prec, max_iterations=200_000, termination_rule="relative_kkt_l2",
+            restart_rule="adaptive_l2", primal_weight_update=True, halpern=True))
+        for k, (p, r) in enumerate(zip(ps, rs)):
+            o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=1,
+                                 halpern=1, max_iterations=200_000)
+            assert r.status == o.status == "optimal", (prec, k, r.status, o.status, r.message)
+            assert r.relative_kkt < 1e-4
+            if prec == "fp64":
+                assert abs(r.iterations - o.iterations) <= 80, (k, r.iterations, o.iterations)
+            assert abs(r.objective - o.objective) <= 1e-3 * (1 + abs(o.objective)), \
+                (prec, k, r.objective, o.objective)
+
+
 def test_batch_autotuner_keeps_the_answers(pkg, engine):
     # a batch above the tuner's 2^20-nonzero threshold: the tuned lane widths
     # must give the untuned solve's answers (mixed precision, to the rule's

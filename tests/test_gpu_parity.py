@@ -382,6 +382,51 @@ def test_mixed_rule2_reaches_the_fp64_optimum(pkg, orc, engine, name):
     assert abs(r.objective - o.objective) <= 1e-3 * (1 + abs(o.objective))
 
 
+@pytest.mark.parametrize("name", sorted(RULE2_CASES))
+def test_fp64_halpern_follows_the_oracle(pkg, orc, engine, name):
+    # the reflected restarted Halpern iteration: FP64 mode takes the oracle's
+    # restarts and stops where it stops, reporting T(z)
+    fn, args, kw = RULE2_CASES[name]
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    for pw in (0, 1):
+        o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=pw,
+                             halpern=1, max_iterations=200_000)
+        r = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt_l2",
+                  restart_rule="adaptive_l2", primal_weight_update=bool(pw), halpern=True,
+                  max_iterations=200_000)
+        assert r.status == o.status == "optimal", (pw, r.status, o.status)
+        assert abs(r.iterations - o.iterations) <= 40 and abs(r.restarts - o.restarts) <= 1, \
+            (pw, r.iterations, o.iterations, r.restarts, o.restarts)
+        if r.iterations == o.iterations:
+            assert abs(r.objective - o.objective) <= 1e-8 * max(1.0, abs(o.objective))
+        assert r.relative_kkt < 1e-4
+        assert np.all(r.primal >= p.col_lo - 1e-9) and np.all(r.primal <= p.col_hi + 1e-9)
+
+
+@pytest.mark.parametrize("name", sorted(RULE2_CASES))
+def test_mixed_halpern_reaches_the_fp64_optimum(pkg, orc, engine, name):
+    fn, args, kw = RULE2_CASES[name]
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=1,
+                         max_iterations=200_000)
+    r = solve(pkg, engine, p, precision="mixed", termination_rule="relative_kkt_l2",
+              restart_rule="adaptive_l2", primal_weight_update=True, halpern=True,
+              max_iterations=200_000)
+    assert r.status == "optimal", (r.status, r.relative_kkt, r.iterations)
+    assert r.relative_kkt < 1e-4
+    assert abs(r.objective - o.objective) <= 1e-3 * (1 + abs(o.objective))
+
+
+def test_halpern_option_combinations_are_checked(pkg, engine):
+    p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=1)
+    with pytest.raises(pkg.PdhgError):  # needs rule 2 and restart rule 2
+        solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt",
+              restart_rule="adaptive", halpern=True)
+    with pytest.raises(pkg.PdhgError):  # not in the reference's exact mode
+        solve(pkg, engine, p, termination_rule="relative_kkt_l2", restart_rule="adaptive_l2",
+              halpern=True)
+
+
 def test_rule2_option_combinations_are_checked(pkg, engine):
     p = pkg.lpgen.random_equality_lp(20, 50, 3, seed=1)
     with pytest.raises(pkg.PdhgError):  # rule 2 needs mixed or fp64

@@ -114,3 +114,32 @@ def test_restart_rule_2_restarts_on_its_measure(pkg, orc):
     p = pkg.lpgen.random_equality_lp(30, 70, 3, seed=5)
     r = orc.oracle_solve(p, termination_rule=2, restart_rule=2, max_iterations=100_000)
     assert r.status == "optimal" and r.restarts >= 1
+
+
+@pytest.mark.parametrize("name", ["equality_60x150", "transportation_20x50",
+                                  "badly_scaled_120x300", "maximize_40x90"])
+@pytest.mark.parametrize("pw", [0, 1])
+def test_halpern_solutions_meet_the_measure_and_the_optimum(pkg, orc, name, pw):
+    # the reflected restarted Halpern iteration (option halpern) on rule 2
+    p = cases(pkg)[name]
+    r = orc.oracle_solve(p, tolerance=1e-4, termination_rule=2, restart_rule=2,
+                         primal_weight_update=pw, halpern=1, max_iterations=400_000)
+    assert r.status == "optimal", (r.status, r.iterations, r.relative_kkt)
+    assert r.relative_kkt < 1e-4
+    assert pdlp_relative_kkt(p, r.primal, r.dual) == pytest.approx(r.relative_kkt, rel=1e-9, abs=1e-14)
+    # the reported point is T(z): inside the column bounds
+    assert np.all(r.primal >= p.col_lo - 1e-12) and np.all(r.primal <= p.col_hi + 1e-12)
+    opt = highs_optimum(p)
+    assert abs(r.objective - opt) <= 5e-4 * (1 + abs(opt)), (r.objective, opt)
+
+
+def test_halpern_takes_fewer_iterations_than_the_average(pkg, orc):
+    L = pkg.lpgen
+    for p, pw in ((L.transportation_lp(100, 250, seed=1000), 0),
+                  (L.random_equality_lp(400, 1000, 5, seed=0), 1)):
+        kw = dict(tolerance=1e-4, termination_rule=2, restart_rule=2, primal_weight_update=pw,
+                  max_iterations=200_000)
+        avg = orc.oracle_solve(p, **kw)
+        hal = orc.oracle_solve(p, halpern=1, **kw)
+        assert avg.status == hal.status == "optimal"
+        assert hal.iterations < avg.iterations, (hal.iterations, avg.iterations)
