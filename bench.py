@@ -64,12 +64,14 @@ def bench_config(args, world: int) -> dict:
             "l2": "inputs larger than L2 (resident set ~1.3 GB > 126 MB)"}
 
 
-# Options of the headline solves: FP32 iterates with FP64 checks, PDLP's
-# relative KKT (termination rule 2) and adaptive restarts on its measure. The
-# primal weight stays 1 on the transportation LP: its update drives omega from
-# |c|/|b| ~ 135 towards 0.1 there and costs 2-3x the iterations (oracle, 100 x
-# 250 and 200 x 500 instances of the family).
-HEADLINE = dict(termination_rule="relative_kkt_l2", restart_rule="adaptive_l2")
+# Options of the solves: PDLP's relative KKT (termination rule 2), adaptive
+# restarts on its measure and the reflected restarted Halpern iteration (on
+# one B200: 13,200 instead of 29,160 iterations for the transportation LP,
+# 1.4x the batch's solves/s). The primal weight stays 1 on the transportation
+# LP: its update drives omega from |c|/|b| ~ 135 towards 0.1 there and costs
+# 2-3x the iterations (oracle, 100 x 250 and 200 x 500 instances of the
+# family); the other workloads turn it on.
+HEADLINE = dict(termination_rule="relative_kkt_l2", restart_rule="adaptive_l2", halpern=True)
 
 
 def replica_problem(pkg, rank: int, supplies: int = SUPPLIES, demands: int = DEMANDS):
@@ -277,7 +279,7 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
     fp64_its = sum(r.fp64_iterations for r in rs)
     return {"workload": f"{len(ps)} seeded LPs, m log-uniform [50, 5000], n = 2-3 m, "
                         f"4-10 nnz/column ({sum(p.nnz for p in ps):,} nnz), PDLP relative KKT "
-                        f"1e-4, mixed, adaptive restarts, primal weight",
+                        f"1e-4, mixed, adaptive restarts, Halpern iteration, primal weight",
             "instances": len(ps), "solved": solved, "seconds": t_batch,
             "solves_per_s": solved / t_batch,
             "iterations_median": its[len(its) // 2], "iterations_max": its[-1],
@@ -305,7 +307,7 @@ def precision_line(pkg, eng, args, rank: int) -> dict:
     p = pkg.lpgen.badly_scaled_lp(200_000, 500_000, 8, seed=2000 + rank)
     out = {"workload": f"badly scaled LP {p.m:,} x {p.n:,}, {p.nnz:,} nnz (power-law rows, "
                        f"|a| log-uniform [1e-3, 1e3], 30% <= rows), PDLP relative KKT 1e-4, "
-                       f"adaptive restarts, primal weight",
+                       f"adaptive restarts, Halpern iteration, primal weight",
            "iteration_budget": args.precision_iters}
     arms = {"fp64": dict(precision="fp64"), "mixed": dict(precision="mixed"),
             "fp32_only": dict(precision="mixed", polish_iterations=0)}
@@ -375,50 +377,91 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
     ok = lambda rs: sum(r.status == "optimal" for r in rs)  # noqa: E731
     plain_rate = ok(plain) / t_plain
     warm_rate = ok(warm) / t_warm
+    it_c = np.array([r.iterations for r in cold], dtype=float)
+    it_w = np.array([r.iterations for r in warm], dtype=float)
+    ratio = it_w / np.maximum(it_c, 1.0)  # per held-out instance, warm over cold
+    cap = opt.max_iterations
     return {"workload": f"parametric family over a config-2-structure base (500 x 1,200, 6,000 "
                         f"nnz, 64 parameters, b and c moved ~10%); {len(tr)} training solves, "
-                        f"{len(te)} held-out; mixed, rel KKT 1e-4, adaptive restarts, primal "
-                        f"weight",
+                        f"{len(te)} held-out; mixed, PDLP relative KKT 1e-4, adaptive restarts, "
+                        f"Halpern iteration, primal weight",
             "training": {"solves_s": t_train_solves, "solved": ok(res), "fit_s": t_fit,
                          "basis_rank": rep.rank, "explained_primal": rep.explained_primal,
                          "explained_dual": rep.explained_dual, "val_loss": ws.val_loss},
             "gate": {"warm_used": int(used.sum()), "start_kkt_warm_median": float(np.median(kw)),
                      "start_kkt_cold_median": float(np.median(kc))},
-            "plain_gpu": {"instances": len(plain), "solved": ok(plain), "seconds": t_plain,
-                          "solves_per_s": plain_rate,
-                          "iterations_mean": float(np.mean([r.iterations for r in plain]))},
+            "plain_gpu": {"instances": len(plain),
+                          "sample": f"the first {len(plain)} of the {len(te)} held-out instances "
+                                    f"(the batched arms solve all {len(te)})",
+                          "solved": ok(plain), "seconds": t_plain, "solves_per_s": plain_rate,
+                          "iterations_mean": float(np.mean([r.iterations for r in plain])),
+                          "batched_cold_iterations_mean_same_sample":
+                              float(np.mean(it_c[: len(plain)]))},
             "batched_cold": {"solved": ok(cold), "seconds": t_cold, "solves_per_s": ok(cold) / t_cold,
-                             "iterations_mean": float(np.mean([r.iterations for r in cold]))},
+                             "iterations_mean": float(it_c.mean()),
+                             "iterations_median": float(np.median(it_c)),
+                             "iterations_max": int(it_c.max()), "at_cap": int((it_c >= cap).sum())},
             "batched_learned_warm": {"solved": ok(warm), "seconds": t_warm,
                                      "solves_per_s": warm_rate,
-                                     "iterations_mean": float(np.mean([r.iterations for r in warm])),
+                                     "iterations_mean": float(it_w.mean()),
+                                     "iterations_median": float(np.median(it_w)),
+                                     "iterations_max": int(it_w.max()),
+                                     "at_cap": int((it_w >= cap).sum()),
                                      "max_relative_kkt": float(max(r.relative_kkt for r in warm
                                                                    if r.status == "optimal"))},
+            "warm_over_cold_iterations": {"median": float(np.median(ratio)),
+                                          "geometric_mean": float(np.exp(np.mean(np.log(
+                                              np.maximum(ratio, 1e-9))))),
+                                          "instances_faster": int((ratio < 1.0).sum()),
+                                          "instances": int(ratio.size)},
             "speedup_vs_plain_gpu": warm_rate / plain_rate if plain_rate > 0 else None,
             "timing": "host wall clock; batched lines include load, the warm line also "
                       "prediction and the start-KKT gate"}
 
 
 def profile_case(args) -> None:
-    """One mixed-precision solve of --iters-per-step iterations: the ncu target.
-    --profile-lp transportation: the transportation LP of --supplies x
-    --demands; badly_scaled: the 200,000 x 500,000 badly scaled LP (FP32 to the
-    end, no polish)."""
+    """The ncu target: one mixed-precision solve of --iters-per-step iterations
+    (FP32 to the end, no polish). --profile-lp transportation: the
+    transportation LP of --supplies x --demands; badly_scaled: the 200,000 x
+    500,000 badly scaled LP; batch: the first --batch-instances LPs of the
+    batched family in one batched solve (below one check period, 40
+    iterations, the iteration kernels launch one by one instead of inside the
+    solve graph); mlp: --iters-per-step Adam steps of the warm start's network
+    (64 -> 512 -> 512 -> 512, mini-batches of 256) on random data."""
     import torch
     torch.cuda.set_device(0)
     pkg = importlib.import_module("sovereign-solver_b200")
+    opt = dict(precision="mixed", tolerance=1e-12, polish_iterations=0,
+               max_iterations=args.iters_per_step, **HEADLINE)
+    if args.profile_lp == "mlp":
+        rng = np.random.default_rng(0)
+        x = rng.standard_normal((4096, 64)).astype(np.float32)
+        t = rng.standard_normal((4096, 512)).astype(np.float32)
+        with pkg.mlp.Mlp(64, 512, 512, max_batch=256) as net:
+            steps = max(1, args.iters_per_step)
+            net.train(x[: 256 * steps], t[: 256 * steps], epochs=1, batch=256)
+        print(json.dumps({"profile_case": "mlp 64-512-512-512", "adam_steps": steps}))
+        return
+    if args.profile_lp == "batch":
+        ps = pkg.lpgen.batch_family(args.batch_instances, seed_base=3000)
+        with pkg.Engine(0) as eng:
+            eng.load_batch(ps)
+            rs = eng.solve_batch(pkg.PdhgOptions(primal_weight_update=True, **opt),
+                                 want_point=False)
+            tuning = eng.batch_tuning("mixed")
+        print(json.dumps({"profile_case": f"batch of {len(ps)} LPs ({sum(p.nnz for p in ps)} nnz)",
+                          "iterations": max(r.iterations for r in rs), "tuning": tuning}))
+        return
     if args.profile_lp == "badly_scaled":
         prob = pkg.lpgen.badly_scaled_lp(200_000, 500_000, 8, seed=2000)
         name = "badly scaled 200000x500000"
+        opt["primal_weight_update"] = True
     else:
         prob = pkg.lpgen.transportation_lp(args.supplies, args.demands, seed=1000)
         name = f"transportation {args.supplies}x{args.demands}"
     with pkg.Engine(0) as eng:
         eng.load(prob)
-        r = eng.solve(pkg.PdhgOptions(precision="mixed", primal_weight_update=True,
-                                      tolerance=1e-12, polish_iterations=0,
-                                      max_iterations=args.iters_per_step, **HEADLINE),
-                      want_point=False)
+        r = eng.solve(pkg.PdhgOptions(**opt), want_point=False)
         tuning = eng.tuning("mixed")
     print(json.dumps({"profile_case": name, "iterations": r.iterations, "status": r.status,
                       "tuning": tuning}))
@@ -504,7 +547,7 @@ def main() -> None:
     ap.add_argument("--precision-iters", type=int, default=100_000,
                     help="iteration budget per mode of the config-2 precision study (0 = skip)")
     ap.add_argument("--profile-lp", default="transportation",
-                    choices=["transportation", "badly_scaled"],
+                    choices=["transportation", "badly_scaled", "batch", "mlp"],
                     help="the LP of --profile-case")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiler target: load the LP and run one solve of --iters-per-step "
@@ -666,8 +709,8 @@ def main() -> None:
         "iterations_per_step": args.iters_per_step,
         "b_spmv_bytes_per_iteration": b_spmv,
         "options": "FP32 iterates, FP64 checks; PDLP relative KKT (rule 2), adaptive restarts "
-                   "on its measure, primal weight 1; tolerance 1e-12 in the timed steps (fixed "
-                   "work per step)",
+                   "on its measure, reflected Halpern iteration, primal weight 1; tolerance "
+                   "1e-12 in the timed steps (fixed work per step)",
         "iterations_per_s": sum_over_ranks(its, world) / t_max,
         "clocks": clocks,
         "gpu_launches": launches,

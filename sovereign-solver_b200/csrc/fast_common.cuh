@@ -362,21 +362,24 @@ template <class T, bool PRIMAL>
 __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>& pv, int r,
                                              int first, bool fresh) {
     EpiIn<T> in;
-    // (Halpern: the sums' slot is only written; its anchors are read at the store)
+    // Halpern: the sums' slot is only written, so `ps` carries the anchor of x
+    // (primal) or y (dual) instead; the slack's anchor is read at the store
     if (PRIMAL) {
         in.a = __ldcs(pv.c + r);
         in.b = __ldcs(it.x + r);
         in.lo = __ldcs(pv.lo + r);
         in.hi = __ldcs(pv.hi + r);
-        if constexpr (std::is_same<T, float>::value) in.ps = first || it.halpern ? T(0) : __ldcs(it.psx + r);
-        else in.ps = fresh || it.halpern ? T(0) : __ldcs(it.xsum + r);
+        if (it.halpern) in.ps = __ldcs(it.xa + r);
+        else if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psx + r);
+        else in.ps = fresh ? T(0) : __ldcs(it.xsum + r);
     } else {
         in.a = it.y[r];
         in.b = __ldcs(it.s + r);
         in.lo = __ldcs(pv.rlo + r);
         in.hi = __ldcs(pv.rhi + r);
-        if constexpr (std::is_same<T, float>::value) in.ps = first || it.halpern ? T(0) : __ldcs(it.psy + r);
-        else in.ps = fresh || it.halpern ? T(0) : __ldcs(it.ysum + r);
+        if (it.halpern) in.ps = __ldcs(it.ya + r);
+        else if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psy + r);
+        else in.ps = fresh ? T(0) : __ldcs(it.ysum + r);
     }
     return in;
 }
@@ -384,7 +387,8 @@ __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>&
 // primal: x+ = proj(x - tau (c - aty)), x_bar = 2x+ - x, sum += x+
 // dual:   s+ = proj(s - tau y), y+ = y + sigma (2s+ - s - ax), sum += y+
 // With the Halpern option (weight hw = w) the step's output T(z) = (x+, s+, y+)
-// goes to the sums' slot and z moves to w (2 T(z) - z) + (1 - w) z_a.
+// goes to the sums' slot and z moves to w (2 T(z) - z) + (1 - w) z_a (the
+// anchor of x or y arrives in in.ps).
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, const EpiIn<T>& in,
                                           T tau, T sigma, T hw) {
@@ -397,7 +401,7 @@ __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, c
         const T xb = T(2) * xn - xo;
         it.xbar[r] = xb;
         if (it.halpern) {
-            __stcs(it.x + r, hw * xb + (T(1) - hw) * __ldcs(it.xa + r));
+            __stcs(it.x + r, hw * xb + (T(1) - hw) * in.ps);
             __stcs(ps + r, xn);
         } else {
             __stcs(it.x + r, xn);
@@ -409,7 +413,7 @@ __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, c
         const T sb = T(2) * sn - so;
         const T yn = yo + sigma * (sb - dot);
         if (it.halpern) {
-            it.y[r] = hw * (T(2) * yn - yo) + (T(1) - hw) * __ldcs(it.ya + r);
+            it.y[r] = hw * (T(2) * yn - yo) + (T(1) - hw) * in.ps;
             __stcs(it.s + r, hw * sb + (T(1) - hw) * __ldcs(it.sa + r));
             __stcs(ps + r, yn);
         } else {
