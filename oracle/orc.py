@@ -47,7 +47,8 @@ class OrcOptions(C.Structure):
                 ("checkpoint", CHECKPOINT_FN), ("checkpoint_user", C.c_void_p),
                 ("cancel_flag", C.POINTER(C.c_int)), ("iter_times", _dp),
                 ("iter_times_cap", C.c_longlong), ("restart_rule", C.c_int),
-                ("primal_weight_update", C.c_int), ("halpern", C.c_int)]
+                ("primal_weight_update", C.c_int), ("halpern", C.c_int),
+                ("x0", _dp), ("y0", _dp), ("primal_weight0", C.c_double)]
 
 
 class OrcInfo(C.Structure):
@@ -56,7 +57,8 @@ class OrcInfo(C.Structure):
                 ("duality_gap", C.c_double), ("iterations", C.c_longlong),
                 ("restarts", C.c_longlong), ("seconds", C.c_double),
                 ("operator_norm_estimate", C.c_double), ("has_point", C.c_int),
-                ("message", C.c_char * 256), ("relative_kkt", C.c_double)]
+                ("message", C.c_char * 256), ("relative_kkt", C.c_double),
+                ("primal_weight", C.c_double)]
 
 
 @dataclass
@@ -80,6 +82,7 @@ class Result:
     loop_seconds: float = 0.0
     loop_iterations: int = 0
     relative_kkt: float = 0.0
+    primal_weight: float = 1.0
 
 
 _libs: dict = {}
@@ -172,7 +175,13 @@ def _solve(which: str, p, trace_iters: int = 0, checkpoints: bool = False,
            cancel: bool = False, iter_times: np.ndarray | None = None, **kw) -> Result:
     keep: list = []
     prob = _problem(p, keep)
+    starts = {k: kw.pop(k) for k in ("x0", "y0") if k in kw}
     o = make_options(**kw)
+    for k, v in starts.items():  # warm start arrays (original units), kept alive
+        if v is not None:
+            a = np.ascontiguousarray(v, dtype=np.float64)
+            keep.append(a)
+            setattr(o, k, _d(a))
     if iter_times is not None:
         o.iter_times = _d(iter_times)
         o.iter_times_cap = int(iter_times.size)
@@ -218,7 +227,7 @@ def _solve(which: str, p, trace_iters: int = 0, checkpoints: bool = False,
         operator_norm_estimate=info.operator_norm_estimate, message=info.message.decode(),
         trace_x=None if tx is None else tx[:, : p.n], trace_y=None if ty is None else ty[:, : p.m],
         checkpoints=cps, loop_seconds=float(loop[0]), loop_iterations=int(loop[1]),
-        relative_kkt=float(info.relative_kkt))
+        relative_kkt=float(info.relative_kkt), primal_weight=float(info.primal_weight))
 
 
 def oracle_solve(p, **kw) -> Result:

@@ -602,6 +602,7 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
         cn = sqrt(cn);
         bn = sqrt(bn);
         if (cn > 1e-10 && bn > 1e-10) omega = cn / bn;
+        if (opt->primal_weight0 > 0.0) omega = opt->primal_weight0;
         tau = step / omega;
         sigma = step * omega;
     }
@@ -609,7 +610,12 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
     double* x = NEWV(double, n); /* pdhg.cpp:268-283 */
     double* sl = NEWV(double, m);
     double* y = NEWV(double, m);
+    if (opt->x0 != NULL) /* extension: warm start */
+        for (int32_t j = 0; j < n; ++j) x[j] = opt->x0[j] / cs[j];
+    if (opt->y0 != NULL)
+        for (int32_t i = 0; i < m; ++i) y[i] = (opt->y0[i] * obj_sign) / rs[i];
     orc_project_box(n, s.col_lo, s.col_hi, x);
+    if (opt->x0 != NULL) csr_multiply(m, s.rp, s.ci, s.v, x, sl);
     orc_project_box(m, s.row_lo, s.row_hi, sl);
     double* x_new = NEWV(double, n);
     double* s_new = NEWV(double, m);
@@ -834,6 +840,7 @@ int orc_pdhg_solve(const orc_problem* p, const orc_options* opt, orc_info* info,
     free(ya);
     free(y_old);
     info->iterations = it;
+    info->primal_weight = omega;
 
     if (!failed) {
         if (best_x == NULL) { /* pdhg.cpp:420-425 */

@@ -115,6 +115,14 @@ typedef struct {
      * are T(z) (inside the column bounds; z itself need not be); a restart
      * moves z and the anchor to T(z) (s to the row bounds' projection of A x). */
     int halpern;
+    /* warm start (the engine's x0 / y0 options), original units and sense:
+     * x = proj_X(x0 / col_scale), y = y0 obj_sign / row_scale,
+     * s = proj_S(A_scaled x); NULL = the reference's start (pdhg.cpp:268-283) */
+    const double* x0;
+    const double* y0;
+    /* primal_weight_update: the starting primal weight (scaled space);
+     * 0 = |c|_2 / |b|_2 */
+    double primal_weight0;
 } orc_options;
 
 typedef struct {
@@ -132,6 +140,8 @@ typedef struct {
     /* extension: the relative-KKT value (termination_rule 1 or 2) of the last
      * check's candidate; 0 under rule 0 and in the reference */
     double relative_kkt;
+    /* extension: the primal weight at the end (1 without primal_weight_update) */
+    double primal_weight;
 } orc_info;
 
 void orc_default_options(orc_options* opt);

@@ -203,10 +203,10 @@ __device__ __forceinline__ void inst_pass(const BatchView& b, const Iterates<T>&
             const int c = M.ci[q];
             const double v = M.v64[q];
             if (COLS) {
-                ac += v * static_cast<double>(it.y[c]);
+                ac += v * cur_y(it, c);
                 aa += v * avg_y(it, c, inv);
             } else {
-                ac += v * static_cast<double>(it.x[c]);
+                ac += v * cur_x(it, c);
                 aa += v * avg_x(it, c, inv);
             }
         }
@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(kBlock) batch_check(BatchView b, Iterates<T> i
             avg = isfinite(avg) ? ma : avg;
         }
     }
+    if (it.halpern) cur = avg;  // only T(z) is measured
     s.cur_res = cur;
     s.avg_res = avg;
     s.inv = inv;

@@ -504,15 +504,29 @@ __device__ __forceinline__ void ray_term(double mult, double lo, double hi, doub
 
 template <class T>
 __device__ __forceinline__ double avg_x(const Iterates<T>& it, int j, double inv) {
-    double s = it.xsum[j];
-    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psx[j]);
-    return s * inv;
+    if constexpr (std::is_same<T, float>::value) {
+        if (it.halpern) return static_cast<double>(it.psx[j]);  // T(z); the FP64 sums stay 0
+        return (it.xsum[j] + static_cast<double>(it.psx[j])) * inv;
+    }
+    return it.xsum[j] * inv;
 }
 template <class T>
 __device__ __forceinline__ double avg_y(const Iterates<T>& it, int i, double inv) {
-    double s = it.ysum[i];
-    if constexpr (std::is_same<T, float>::value) s += static_cast<double>(it.psy[i]);
-    return s * inv;
+    if constexpr (std::is_same<T, float>::value) {
+        if (it.halpern) return static_cast<double>(it.psy[i]);
+        return (it.ysum[i] + static_cast<double>(it.psy[i])) * inv;
+    }
+    return it.ysum[i] * inv;
+}
+// The current point's entry for the check's products; the Halpern form
+// measures T(z) alone (z itself is no candidate), so it skips the gather.
+template <class T>
+__device__ __forceinline__ double cur_x(const Iterates<T>& it, int j) {
+    return it.halpern ? 0.0 : static_cast<double>(it.x[j]);
+}
+template <class T>
+__device__ __forceinline__ double cur_y(const Iterates<T>& it, int i) {
+    return it.halpern ? 0.0 : static_cast<double>(it.y[i]);
 }
 
 }  // namespace

@@ -635,10 +635,10 @@ __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr
         const int j = M.ci[k];
         const double v = M.v64[k];
         if (ROWS) {
-            ac += v * static_cast<double>(a.it.x[j]);
+            ac += v * cur_x(a.it, j);
             aa += v * avg_x(a.it, j, inv);
         } else {
-            ac += v * static_cast<double>(a.it.y[j]);
+            ac += v * cur_y(a.it, j);
             aa += v * avg_y(a.it, j, inv);
         }
     }
@@ -722,10 +722,10 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
             if (ROWS) {
-                ac += v[u] * static_cast<double>(a.it.x[j[u]]);
+                ac += v[u] * cur_x(a.it, j[u]);
                 aa += v[u] * avg_x(a.it, j[u], inv);
             } else {
-                ac += v[u] * static_cast<double>(a.it.y[j[u]]);
+                ac += v[u] * cur_y(a.it, j[u]);
                 aa += v[u] * avg_y(a.it, j[u], inv);
             }
         }
@@ -734,10 +734,10 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
         const int j = __ldcs(col + 32 * static_cast<int64_t>(k));
         const double v = __ldcs(val + 32 * static_cast<int64_t>(k));
         if (ROWS) {
-            ac += v * static_cast<double>(a.it.x[j]);
+            ac += v * cur_x(a.it, j);
             aa += v * avg_x(a.it, j, inv);
         } else {
-            ac += v * static_cast<double>(a.it.y[j]);
+            ac += v * cur_y(a.it, j);
             aa += v * avg_y(a.it, j, inv);
         }
     }
@@ -902,6 +902,7 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
             avg = isfinite(avg) ? ma : avg;
         }
     }
+    if (a.it.halpern) cur = avg;  // only T(z) is measured
     st->cur_res = cur;
     st->avg_res = avg;
     st->inv = inv;

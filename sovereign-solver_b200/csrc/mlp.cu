@@ -56,12 +56,22 @@ struct GemmArgs {
     int* err;           // set when a bounded wait gives up
 };
 
+// 16-byte asynchronous global -> shared copy (cp.async, no register staging);
+// src_bytes = 0 writes zeros and reads nothing.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(tc::smem_u32(smem)),
+                 "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // C = A B^T on one 128 x kGemmBN tile: the K loop stages a 128 x 64 slice of
 // A and a kGemmBN x 64 slice of B in shared memory (core-matrix layout, see
-// tcgen05.cuh), one thread issues the four 16-deep MMAs into the TMEM
-// accumulator and commits them to an mbarrier that every thread waits on
-// before the slices are overwritten. The epilogue reads the accumulator with
-// tcgen05.ld, one TMEM lane (= output row) per thread.
+// tcgen05.cuh) with asynchronous 16-byte copies, all of a slice in flight at
+// once, one thread issues the four 16-deep MMAs into the TMEM accumulator and
+// commits them to an mbarrier that every thread waits on before the slices
+// are overwritten. The epilogue reads the accumulator with tcgen05.ld, one
+// TMEM lane (= output row) per thread.
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_tn(GemmArgs g) {
     __shared__ __align__(1024) bf16 sA[tc::kTileM * tc::kTileK];
     __shared__ __align__(1024) bf16 sB[kGemmBN * tc::kTileK];
@@ -86,22 +96,23 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tn(GemmArgs g) {
     int round = 0;
     bool aborted = false;
     for (int k0 = 0; k0 < g.K; k0 += tc::kTileK, ++round) {
+#pragma unroll
         for (int c = tid; c < tc::kTileM * (tc::kTileK / 8); c += kGemmThreads) {
             const int row = c >> 3, kc = (c & 7) * 8;
             const int gr = m0 + row, gk = k0 + kc;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (gr < g.M && gk < g.K)
-                v = *reinterpret_cast<const uint4*>(g.A + static_cast<size_t>(gr) * g.lda + gk);
-            *reinterpret_cast<uint4*>(sA + tc::tile_offset(row, kc)) = v;
+            const bool in = gr < g.M && gk < g.K;
+            cp_async16(sA + tc::tile_offset(row, kc),
+                       in ? g.A + static_cast<size_t>(gr) * g.lda + gk : g.A, in ? 16 : 0);
         }
+#pragma unroll
         for (int c = tid; c < kGemmBN * (tc::kTileK / 8); c += kGemmThreads) {
             const int row = c >> 3, kc = (c & 7) * 8;
             const int gr = n0 + row, gk = k0 + kc;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (gr < g.N && gk < g.K)
-                v = *reinterpret_cast<const uint4*>(g.B + static_cast<size_t>(gr) * g.ldb + gk);
-            *reinterpret_cast<uint4*>(sB + tc::tile_offset(row, kc)) = v;
+            const bool in = gr < g.N && gk < g.K;
+            cp_async16(sB + tc::tile_offset(row, kc),
+                       in ? g.B + static_cast<size_t>(gr) * g.ldb + gk : g.B, in ? 16 : 0);
         }
+        cp_async_wait_all();
         tc::fence_proxy_async_smem();
         __syncthreads();
         if (tid == 0) {

@@ -11,6 +11,8 @@ pin that restatement before the GPU tests compare the engine with it.
 import numpy as np
 import pytest
 
+from conftest import highs_optimum
+
 INF = np.inf
 
 
@@ -47,30 +49,6 @@ def pdlp_relative_kkt(p, x, y):
              np.linalg.norm(d) / (1 + np.linalg.norm(p.c)),
              abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj)))
     return max(parts)
-
-
-def highs_optimum(p):
-    from scipy.optimize import linprog
-    A = np.zeros((p.m, p.n))
-    for i in range(p.m):
-        for k in range(p.row_ptr[i], p.row_ptr[i + 1]):
-            A[i, p.col_idx[k]] += p.val[k]
-    eq = np.isfinite(p.row_lo) & np.isfinite(p.row_hi) & (p.row_lo == p.row_hi)
-    ub_rows, ub_rhs = [], []
-    for i in np.nonzero(~eq)[0]:
-        if np.isfinite(p.row_hi[i]):
-            ub_rows.append(A[i]); ub_rhs.append(p.row_hi[i])
-        if np.isfinite(p.row_lo[i]):
-            ub_rows.append(-A[i]); ub_rhs.append(-p.row_lo[i])
-    sgn = -1.0 if p.maximize else 1.0
-    res = linprog(sgn * p.c, A_ub=np.array(ub_rows) if ub_rows else None,
-                  b_ub=np.array(ub_rhs) if ub_rhs else None,
-                  A_eq=A[eq] if eq.any() else None, b_eq=p.row_lo[eq] if eq.any() else None,
-                  bounds=list(zip(np.where(np.isfinite(p.col_lo), p.col_lo, None),
-                                  np.where(np.isfinite(p.col_hi), p.col_hi, None))),
-                  method="highs")
-    assert res.status == 0, res.message
-    return sgn * res.fun + p.obj_const
 
 
 def cases(pkg):
