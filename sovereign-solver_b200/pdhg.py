@@ -283,23 +283,37 @@ def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray) -> PdhgRe
 
 def stack_batch(problems: list[Problem]) -> dict:
     """The block-diagonal stacking pdhg_load_batch takes: instance k's rows and
-    columns follow instance k-1's; column indices become global."""
+    columns follow instance k-1's; column indices become global. The output
+    arrays are allocated once and filled instance by instance."""
     ms = np.array([p.m for p in problems], dtype=np.int64)
     ns = np.array([p.n for p in problems], dtype=np.int64)
     nnzs = np.array([p.nnz for p in problems], dtype=np.int64)
-    row_off = np.concatenate([[0], np.cumsum(ms)]).astype(np.int32)
-    col_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int32)
+    row_off64 = np.concatenate([[0], np.cumsum(ms)])
+    col_off64 = np.concatenate([[0], np.cumsum(ns)])
     nz_off = np.concatenate([[0], np.cumsum(nnzs)])
-    rp = [np.asarray(p.row_ptr[:-1], dtype=np.int64) + nz_off[k] for k, p in enumerate(problems)]
-    row_ptr = np.concatenate(rp + [[nz_off[-1]]]).astype(np.int32)
-    col_idx = np.concatenate([np.asarray(p.col_idx, dtype=np.int64) + col_off[k]
-                              for k, p in enumerate(problems)] + [np.zeros(0, np.int64)])
-    cat = lambda name: np.ascontiguousarray(np.concatenate(  # noqa: E731
-        [np.asarray(getattr(p, name), dtype=np.float64) for p in problems] + [np.zeros(0)]))
-    return {"row_off": row_off, "col_off": col_off, "nnz": int(nz_off[-1]),
-            "row_ptr": row_ptr, "col_idx": col_idx.astype(np.int32),
-            "val": cat("val"), "c": cat("c"), "col_lo": cat("col_lo"), "col_hi": cat("col_hi"),
-            "row_lo": cat("row_lo"), "row_hi": cat("row_hi"),
+    if row_off64[-1] > np.iinfo(np.int32).max or col_off64[-1] > np.iinfo(np.int32).max or \
+            nz_off[-1] > np.iinfo(np.int32).max:
+        raise ValueError("the stacked batch does not fit int32 indices")
+    m, n, nnz = int(row_off64[-1]), int(col_off64[-1]), int(nz_off[-1])
+    row_ptr = np.empty(m + 1, dtype=np.int32)
+    col_idx = np.empty(nnz, dtype=np.int32)
+    vec = {name: np.empty(size, dtype=np.float64) for name, size in
+           (("val", nnz), ("c", n), ("col_lo", n), ("col_hi", n), ("row_lo", m), ("row_hi", m))}
+    for k, p in enumerate(problems):
+        r0, r1 = int(row_off64[k]), int(row_off64[k + 1])
+        c0, c1 = int(col_off64[k]), int(col_off64[k + 1])
+        z0, z1 = int(nz_off[k]), int(nz_off[k + 1])
+        np.add(p.row_ptr[:-1], z0, out=row_ptr[r0:r1], casting="unsafe")
+        np.add(p.col_idx, c0, out=col_idx[z0:z1], casting="unsafe")
+        vec["val"][z0:z1] = p.val
+        vec["c"][c0:c1] = p.c
+        vec["col_lo"][c0:c1] = p.col_lo
+        vec["col_hi"][c0:c1] = p.col_hi
+        vec["row_lo"][r0:r1] = p.row_lo
+        vec["row_hi"][r0:r1] = p.row_hi
+    row_ptr[m] = nnz
+    return {"row_off": row_off64.astype(np.int32), "col_off": col_off64.astype(np.int32),
+            "nnz": nnz, "row_ptr": row_ptr, "col_idx": col_idx, **vec,
             "obj_const": np.array([float(p.obj_const) for p in problems], dtype=np.float64),
             "maximize": np.array([int(bool(p.maximize)) for p in problems], dtype=np.intc)}
 
