@@ -54,6 +54,7 @@ struct GemmArgs {
     bf16* out16;        // M x N, or null
     int ld16;
     int* err;           // set when a bounded wait gives up
+    int vec;            // 1: every row of bias / mask / outputs starts 16-byte aligned
 };
 
 // 16-byte asynchronous global -> shared copy (cp.async, no register staging);
@@ -151,10 +152,61 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tn(GemmArgs g) {
             float v[32];
             tc::tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb, v);
             if (row >= g.M) continue;
+            const int c0 = n0 + cb;
+            if (g.vec && c0 + 32 <= g.N) {
+                // a thread's 32 columns are contiguous in its row: 16-byte
+                // loads of bias and mask, all issued before they are used,
+                // and 16-byte stores
+                if (g.bias != nullptr) {
+                    const float4* b4 = reinterpret_cast<const float4*>(g.bias + c0);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float4 b = __ldg(b4 + q);
+                        v[4 * q] += b.x;
+                        v[4 * q + 1] += b.y;
+                        v[4 * q + 2] += b.z;
+                        v[4 * q + 3] += b.w;
+                    }
+                }
+                if (g.relu)
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
+                if (g.mask != nullptr) {
+                    const uint4* m4 = reinterpret_cast<const uint4*>(g.mask + static_cast<size_t>(row) * g.ldm + c0);
+                    uint4 mk[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) mk[q] = __ldg(m4 + q);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const bf16* mb = reinterpret_cast<const bf16*>(&mk[q]);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            if (!(__bfloat162float(mb[j]) > 0.f)) v[8 * q + j] = 0.f;
+                    }
+                }
+                if (g.out32 != nullptr) {
+                    float4* o4 = reinterpret_cast<float4*>(g.out32 + static_cast<size_t>(row) * g.ld32 + c0);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        o4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                }
+                if (g.out16 != nullptr) {
+                    uint4* o4 = reinterpret_cast<uint4*>(g.out16 + static_cast<size_t>(row) * g.ld16 + c0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        uint4 w;
+                        bf16* wb = reinterpret_cast<bf16*>(&w);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) wb[j] = __float2bfloat16_rn(v[8 * q + j]);
+                        o4[q] = w;
+                    }
+                }
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                const int col = n0 + cb + j;
-                if (col >= g.N) break;
+                const int col = c0 + j;
+                if (col >= g.N) continue;
                 float x = v[j];
                 if (g.bias != nullptr) x += g.bias[col];
                 if (g.relu) x = fmaxf(x, 0.f);
@@ -264,7 +316,12 @@ int gemm(const GemmArgs& g, cudaStream_t s) {
         (reinterpret_cast<uintptr_t>(g.A) & 15u) || (reinterpret_cast<uintptr_t>(g.B) & 15u))
         return PDHG_ERR_INVALID_ARGUMENT;
     const dim3 grid((g.M + tc::kTileM - 1) / tc::kTileM, (g.N + kGemmBN - 1) / kGemmBN);
-    k_gemm_tn<<<grid, kGemmThreads, 0, s>>>(g);
+    GemmArgs a = g;
+    auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    a.vec = al16(g.bias) && (g.mask == nullptr || (al16(g.mask) && g.ldm % 8 == 0)) &&
+            (g.out32 == nullptr || (al16(g.out32) && g.ld32 % 4 == 0)) &&
+            (g.out16 == nullptr || (al16(g.out16) && g.ld16 % 8 == 0)) ? 1 : 0;
+    k_gemm_tn<<<grid, kGemmThreads, 0, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? PDHG_OK : PDHG_ERR_BACKEND;
 }
 
