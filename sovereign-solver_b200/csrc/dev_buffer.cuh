@@ -121,6 +121,7 @@ struct MatDev {
     int32_t n_long = 0, n_short = 0, n_wrows = 0, n_mid = 0, n_huge = 0;
     int32_t short_max = kLongRow, n_iter_short = 0, n_warp0 = 0, n_warp1 = 0;
     int vw = 1;
+    int32_t rp_stride = 0;  // every row this long (0: not uniform)
     DevCsr view() const {
         DevCsr d;
         d.rows = rows;
@@ -149,6 +150,7 @@ struct MatDev {
         d.items_warp = items_warp.view();
         d.slices = slices.view();
         d.no_slice_tiers = no_slice_tiers.view();
+        d.rp_stride = rp_stride;
         return d;
     }
 };
@@ -267,16 +269,21 @@ inline int bin_matrix(MatDev& M, cudaStream_t s, std::string* err) {
         (e = M.warp_rows1.alloc(static_cast<size_t>(M.rows) + 1)) != cudaSuccess)
         return cuda_fail(err, e, "bin_matrix");
     DBuf<unsigned long long> cnt;
-    if ((e = cnt.alloc(8)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
-    cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s);
+    if ((e = cnt.alloc(9)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
+    cudaMemsetAsync(cnt.p, 0, 9 * sizeof(unsigned long long), s);
     launch_bin(M.rp.p, M.rows, kLongRow, M.long_rows.p, cnt.p, s);
     launch_bin(M.rp.p, M.rows, kWarpRow, M.wrows.p, cnt.p + 3, s);
-    unsigned long long h[8];
+    // rows all of one length: the short-row kernel computes their extents
+    launch_uniform_rows(M.rp.p, M.rows, reinterpret_cast<unsigned*>(cnt.p + 8), s);
+    int32_t rp01[2] = {0, 0};
+    if (M.rows > 0) cudaMemcpyAsync(rp01, M.rp.p, sizeof rp01, cudaMemcpyDeviceToHost, s);
+    unsigned long long h[9];
     cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "bin_matrix");
     M.n_long = static_cast<int32_t>(h[0]);
     M.n_short = static_cast<int32_t>(h[1]);
     M.n_wrows = static_cast<int32_t>(h[3]);
+    M.rp_stride = (M.rows > 0 && h[8] == 0 && rp01[0] == 0) ? rp01[1] : 0;
     const double mean = h[1] > 0 ? static_cast<double>(h[2]) / static_cast<double>(h[1]) : 0.0;
     int w = 1;
     while (w < 32 && 2.0 * w <= mean / 2.0 + 1e-9) w *= 2;

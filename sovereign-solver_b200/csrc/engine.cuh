@@ -134,6 +134,10 @@ struct DevCsr {
     int iter_vw = 0;
     int long_mode = 0;
     int use_slices = 0;
+    // > 0 when every row has exactly this many entries (rp[r] = r * rp_stride):
+    // the short-row iteration kernel computes the row's extent instead of
+    // loading it
+    int32_t rp_stride = 0;
 };
 
 
@@ -222,6 +226,10 @@ struct DevProblem {
     const float *rlo32 = nullptr, *rhi32 = nullptr;
     double bnorm = 0.0, cnorm = 0.0;    // relative-KKT norms (original space, inf-norms)
     double bnorm2 = 0.0, cnorm2 = 0.0;  // termination rule 2 norms (original space, l2)
+    // every column has the same scaled bounds lo_u <= x <= hi_u (x >= 0 LPs):
+    // the iteration kernels use the two values instead of loading the vectors
+    int col_bounds_uniform = 0;
+    double lo_u = 0.0, hi_u = 0.0;
 };
 
 // Iterates. T = double for the FP64 modes, float for the mixed mode; the
@@ -437,6 +445,10 @@ void launch_validate(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
 // Rows with lo < length <= hi appended to `list`, their number added to *count.
 void launch_bin_range(const int32_t* rp, int32_t rows, int lo, int hi, int32_t* list,
                       unsigned long long* count, cudaStream_t s);
+// *flag |= 1 when the rows' lengths are not all equal / the entries of v not
+// all equal (flag zeroed by the caller).
+void launch_uniform_rows(const int32_t* rp, int32_t rows, unsigned* flag, cudaStream_t s);
+void launch_uniform_vec(const double* v, int32_t n, unsigned* flag, cudaStream_t s);
 void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                 unsigned long long* counters, cudaStream_t s);
 // out[k] = {rows[k], rp[rows[k]], rp[rows[k] + 1], 0} for k < n.

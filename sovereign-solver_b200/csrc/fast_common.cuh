@@ -34,16 +34,19 @@ __device__ __forceinline__ const double* mvals<double>(const DevCsr& A) { return
 template <class T>
 struct PV {
     const T *c, *lo, *hi, *rlo, *rhi;
+    int ub;       // every column has the bounds lo_u <= x <= hi_u
+    T lo_u, hi_u;
 };
 template <class T>
 __device__ __forceinline__ PV<T> pvec(const DevProblem& P);
 template <>
 __device__ __forceinline__ PV<float> pvec<float>(const DevProblem& P) {
-    return {P.c32, P.lo32, P.hi32, P.rlo32, P.rhi32};
+    return {P.c32, P.lo32, P.hi32, P.rlo32, P.rhi32, P.col_bounds_uniform,
+            static_cast<float>(P.lo_u), static_cast<float>(P.hi_u)};
 }
 template <>
 __device__ __forceinline__ PV<double> pvec<double>(const DevProblem& P) {
-    return {P.c, P.lo, P.hi, P.rlo, P.rhi};
+    return {P.c, P.lo, P.hi, P.rlo, P.rhi, P.col_bounds_uniform, P.lo_u, P.hi_u};
 }
 
 __device__ __forceinline__ unsigned group_mask(int vw) {
@@ -367,8 +370,8 @@ __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>&
     if (PRIMAL) {
         in.a = __ldcs(pv.c + r);
         in.b = __ldcs(it.x + r);
-        in.lo = __ldcs(pv.lo + r);
-        in.hi = __ldcs(pv.hi + r);
+        in.lo = pv.ub ? pv.lo_u : __ldcs(pv.lo + r);
+        in.hi = pv.ub ? pv.hi_u : __ldcs(pv.hi + r);
         if (it.halpern) in.ps = __ldcs(it.xa + r);
         else if constexpr (std::is_same<T, float>::value) in.ps = first ? T(0) : __ldcs(it.psx + r);
         else in.ps = fresh ? T(0) : __ldcs(it.xsum + r);

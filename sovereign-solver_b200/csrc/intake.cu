@@ -89,6 +89,27 @@ __global__ void __launch_bounds__(kBlock) k_validate(int32_t m, int32_t n, const
 
 // Row lengths -> long-row list, number and total length of short rows
 // (grid-stride, one atomic per CTA and counter).
+// *flag |= 1 when some row's length differs from row 0's (grid-stride).
+__global__ void k_uniform_rows(const int32_t* rp, int32_t rows, unsigned* flag) {
+    const int len0 = rp[1] - rp[0];
+    bool diff = false;
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; r < rows;
+         r += static_cast<int64_t>(gridDim.x) * kBlock)
+        diff = diff || (rp[r + 1] - rp[r] != len0);
+    if (diff) atomicOr(flag, 1u);
+}
+
+// *flag |= 1 when some entry differs from entry 0 (grid-stride; +-inf compare
+// equal to themselves).
+__global__ void k_uniform_vec(const double* v, int32_t n, unsigned* flag) {
+    const double v0 = v[0];
+    bool diff = false;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x; t < n;
+         t += static_cast<int64_t>(gridDim.x) * kBlock)
+        diff = diff || !(v[t] == v0);
+    if (diff) atomicOr(flag, 1u);
+}
+
 __global__ void k_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* long_rows,
                       unsigned long long* counters) {
     unsigned long long ns = 0, nz = 0;
@@ -478,6 +499,16 @@ void launch_bin(const int32_t* rp, int32_t rows, int long_threshold, int32_t* lo
                 unsigned long long* counters, cudaStream_t s) {
     const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
     if (rows > 0) k_bin<<<g, kBlock, 0, s>>>(rp, rows, long_threshold, long_rows, counters);
+}
+
+void launch_uniform_rows(const int32_t* rp, int32_t rows, unsigned* flag, cudaStream_t s) {
+    const int g = nblocks(rows) < kGridCap ? nblocks(rows) : kGridCap;
+    if (rows > 0) k_uniform_rows<<<g, kBlock, 0, s>>>(rp, rows, flag);
+}
+
+void launch_uniform_vec(const double* v, int32_t n, unsigned* flag, cudaStream_t s) {
+    const int g = nblocks(n) < kGridCap ? nblocks(n) : kGridCap;
+    if (n > 0) k_uniform_vec<<<g, kBlock, 0, s>>>(v, n, flag);
 }
 
 void launch_row_extents(const int32_t* rows, int32_t n, const int32_t* rp, int4* out,

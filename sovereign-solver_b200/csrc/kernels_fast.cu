@@ -101,7 +101,14 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     if (r >= M.rows) return;
     EpiIn<T> in{};
     if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
-    const int b = __ldcs(M.rp + r), e = __ldcs(M.rp + r + 1);
+    int b, e;
+    if (M.rp_stride > 0) {  // rows of one length: the extent is computed
+        b = r * M.rp_stride;
+        e = b + M.rp_stride;
+    } else {
+        b = __ldcs(M.rp + r);
+        e = __ldcs(M.rp + r + 1);
+    }
     if (e - b > M.short_max) return;  // fast_iter_long handles it
     // rounds of four entries per lane: the index and value loads of a round
     // are all in flight before its gathers, the gathers before the adds
