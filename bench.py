@@ -248,32 +248,46 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
-def batch_line(pkg, eng, args, rank: int) -> dict:
+def batch_line(pkg, eng, args, rank: int, world: int = 1) -> dict:
     """Config 3: a seeded family of config-0-structure LPs (m log-uniform in
     [50, 5000], n = 2-3 m, 4-10 nonzeros per column), solved to 1e-4 relative
-    KKT in one batched solve (pdhg_solve_batch: one CUDA-graph launch), beside
-    the plain single-LP engine on the first instances of the same family."""
-    ps = pkg.lpgen.batch_family(args.batch_instances, seed_base=3000 + 100_000 * rank)
+    KKT by the batched engine (pdhg_solve_batch: one CUDA-graph launch per
+    rank), beside the plain single-LP engine on an evenly spaced sample of the
+    same family. With N ranks the family has N x --batch-instances LPs and
+    shard.solve_sharded splits it by balanced nonzeros, one batched solve per
+    rank, results gathered to rank 0 in instance order (weak scaling; no
+    per-iteration collective)."""
+    ps = pkg.lpgen.batch_family(args.batch_instances * world, seed_base=3000)
     opt = pkg.PdhgOptions(precision="mixed", tolerance=1e-4, max_iterations=200_000,
                           primal_weight_update=True, **HEADLINE)
     # the plain engine solves an evenly spaced sample of the same instances
     step = max(1, len(ps) // max(1, args.plain_instances))
     sample = list(range(0, len(ps), step))[: args.plain_instances]
+    loads = []
     with pkg.Engine(eng.device) as e:
-        warm = ps[: min(len(ps), 64)]
-        e.load_batch(warm)
+        e.load_batch(ps[: min(len(ps), 64)])
         e.solve_batch(opt, want_point=False)  # warm-up (graph build, clocks)
+
+        def solve_part(part):
+            t = time.perf_counter()
+            e.load_batch(part)
+            loads.append(time.perf_counter() - t)
+            return e.solve_batch(opt, want_point=False)
+
+        barrier(world)
         t0 = time.perf_counter()
-        e.load_batch(ps)
-        t_load = time.perf_counter() - t0
-        rs = e.solve_batch(opt, want_point=False)
-        t_batch = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        plain = []
-        for k in sample:
-            e.load(ps[k])
-            plain.append(e.solve(opt, want_point=False))
-        t_plain = time.perf_counter() - t0
+        rs = pkg.shard.solve_sharded(ps, solve_part, rank, world)
+        t_batch = max_over_ranks(time.perf_counter() - t0, world)
+        t_load = max_over_ranks(loads[0] if loads else 0.0, world)
+        plain, t_plain = [], 1.0
+        if rank == 0:
+            t0 = time.perf_counter()
+            for k in sample:
+                e.load(ps[k])
+                plain.append(e.solve(opt, want_point=False))
+            t_plain = time.perf_counter() - t0
+    if rank != 0:
+        return {}
     solved = sum(r.status == "optimal" for r in rs)
     plain_solved = sum(r.status == "optimal" for r in plain)
     its = sorted(r.iterations for r in rs)
@@ -281,7 +295,7 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
     return {"workload": f"{len(ps)} seeded LPs, m log-uniform [50, 5000], n = 2-3 m, "
                         f"4-10 nnz/column ({sum(p.nnz for p in ps):,} nnz), PDLP relative KKT "
                         f"1e-4, mixed, adaptive restarts, Halpern iteration, primal weight",
-            "instances": len(ps), "solved": solved, "seconds": t_batch,
+            "instances": len(ps), "ranks": world, "solved": solved, "seconds": t_batch,
             "load_seconds": t_load, "solves_per_s": solved / t_batch,
             "solves_per_s_problem_resident": solved / max(t_batch - t_load, 1e-9),
             "iterations_median": its[len(its) // 2], "iterations_max": its[-1],
@@ -289,13 +303,14 @@ def batch_line(pkg, eng, args, rank: int) -> dict:
             "fp64_iteration_fraction": fp64_its / max(1, sum(its)),
             "gpu_launches": rs[0].kernel_launches if rs else 0,
             "plain_gpu": {"instances": len(plain), "sample": f"every {step}th instance of the "
-                          f"same family ({len(plain)} of {len(ps)})", "solved": plain_solved,
-                          "seconds": t_plain, "solves_per_s": plain_solved / t_plain,
-                          "batched_solves_per_s_same_rate": solved / t_batch},
+                          f"same family ({len(plain)} of {len(ps)}), on rank 0",
+                          "solved": plain_solved,
+                          "seconds": t_plain, "solves_per_s": plain_solved / t_plain},
             "speedup_vs_plain_gpu": (solved / t_batch) / (plain_solved / t_plain)
             if plain_solved else None,
-            "timing": "host wall clock around load + solve on both sides (pdhg_load_batch + "
-                      "pdhg_solve_batch; per instance pdhg_load_problem + pdhg_solve)"}
+            "timing": "host wall clock around load + solve (pdhg_load_batch + pdhg_solve_batch "
+                      "per rank, the gather to rank 0 included, max over ranks); the plain "
+                      "engine per instance pdhg_load_problem + pdhg_solve"}
 
 
 def precision_line(pkg, eng, args, rank: int) -> dict:
@@ -704,7 +719,7 @@ def main() -> None:
     full = eng.solve(solve_opts, want_point=False)
     full_s = time.perf_counter() - t0
 
-    batch = batch_line(pkg, eng, args, rank) if args.batch_instances > 0 else None
+    batch = batch_line(pkg, eng, args, rank, world) if args.batch_instances > 0 else None
     warm = warmstart_line(pkg, eng, args, rank) if args.ws_train > 0 else None
     prec = precision_line(pkg, eng, args, rank) if args.precision_iters > 0 else None
 
