@@ -272,7 +272,10 @@ int pdhg_get_batch_tuning(const pdhg_ctx* ctx, int precision, int* out);
 
 /* Per-kernel timing of the iteration kernels on the loaded problem (CUDA events
  * on the engine's stream around each launch, after `warmup` untimed iterations).
- * Runs `iterations` iterations from the state the last pdhg_solve left. */
+ * Runs `iterations` iterations from the cold start, in the form the last
+ * pdhg_solve ran: the averaged iteration, or (option halpern) the Halpern
+ * iteration without its once-a-period stores; then one check. bytes[] are the
+ * algorithmic bytes of that form. */
 typedef struct pdhg_kernel_stats {
     int count;                   /* kernels reported */
     char name[8][32];

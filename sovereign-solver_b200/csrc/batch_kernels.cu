@@ -55,9 +55,9 @@ __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T
     if (s.done) return;  // uniform within the row's lane group
     const bool fresh = first && s.fresh;
     const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
-    const T hw = halpern_weight<T>(it, s.since_restart, hk);
+    const Hw<T> hw = halpern_weight<T>(it, s.since_restart, hk);
     EpiIn<T> in{};
-    if (lane == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
+    if (lane == 0) in = epi_load<T, PRIMAL, false>(it, pv, r, first, fresh, hw);
     const int rb = __ldcs(M.rp + r), re = __ldcs(M.rp + r + 1);
     if (re - rb > kLongRow) return;
     // rounds of four entries per lane: the index and value loads of a round
@@ -77,7 +77,7 @@ __device__ __forceinline__ void batch_block(const BatchView& b, const Iterates<T
             if (k0 + u * VW < re) acc += v[u] * __ldg(xg + c[u]);
     }
     if (VW > 1) acc = group_sum(acc, VW);
-    if (lane == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma, hw);
+    if (lane == 0) epi_store<T, PRIMAL, false>(it, r, acc, in, tau, sigma, hw, 1);
 }
 
 // The first short_grid CTAs take one block each of the active block list (the
@@ -102,11 +102,11 @@ __global__ void __launch_bounds__(kBlock) batch_iter(BatchView b, Iterates<T> it
         const PV<T> pv = pvec<T>(b.P);
         const bool fresh = first && s.fresh;
         const T tau = static_cast<T>(s.tau), sigma = static_cast<T>(s.sigma);
-        const T hw = halpern_weight<T>(it, s.since_restart, hk);
+        const Hw<T> hw = halpern_weight<T>(it, s.since_restart, hk);
         EpiIn<T> in{};
-        if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(it, pv, r, first, fresh);
+        if (threadIdx.x == 0) in = epi_load<T, PRIMAL, false>(it, pv, r, first, fresh, hw);
         const T acc = long_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? it.y : it.xbar, M.rp[r], M.rp[r + 1]);
-        if (threadIdx.x == 0) epi_store<T, PRIMAL>(it, r, acc, in, tau, sigma, hw);
+        if (threadIdx.x == 0) epi_store<T, PRIMAL, false>(it, r, acc, in, tau, sigma, hw, 1);
     }
 }
 

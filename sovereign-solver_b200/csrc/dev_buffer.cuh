@@ -85,6 +85,7 @@ struct SlicesDev {
     DBuf<double> v64, part, cpart;
     DBuf<unsigned int> ticket, fetch, cticket;
     int32_t n_slice = 0, n_item = 0;
+    int64_t nnz_affine = 0;  // entries of the affine slices (columns computed)
     RowSlices view() const {
         RowSlices v;
         v.n_slice = n_slice;
@@ -110,7 +111,7 @@ struct SlicesDev {
 struct MatDev {
     int32_t rows = 0, cols = 0;
     int64_t nnz = 0;
-    DBuf<int32_t> rp, ci, long_rows, wrows, warp_rows0, warp_rows1;
+    DBuf<int32_t> rp, ci, long_rows, wrows, warp_rows0, warp_rows1, dense_off;
     ItemsDev items_long, items_huge, items_warp;
     std::vector<int4> ext;  // host: {row, begin, end, -} of every row above short_max, row order
     SlicesDev slices;
@@ -122,6 +123,7 @@ struct MatDev {
     int32_t short_max = kLongRow, n_iter_short = 0, n_warp0 = 0, n_warp1 = 0;
     int vw = 1;
     int32_t rp_stride = 0;  // every row this long (0: not uniform)
+    int64_t nnz_dense = 0;  // entries of the dense rows (columns computed)
     DevCsr view() const {
         DevCsr d;
         d.rows = rows;
@@ -151,6 +153,7 @@ struct MatDev {
         d.slices = slices.view();
         d.no_slice_tiers = no_slice_tiers.view();
         d.rp_stride = rp_stride;
+        d.dense_off = dense_off.p;
         return d;
     }
 };
@@ -375,6 +378,7 @@ constexpr int kSliceMinLen = 256;  // rows shorter than this are not worth a sli
 inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
     SlicesDev& S = M.slices;
     S.n_slice = 0;
+    S.nnz_affine = 0;
     S.n_item = 0;
     const std::vector<int4>& ext = M.ext;
     std::vector<size_t> cand;
@@ -495,10 +499,19 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
     }
     cudaMemsetAsync(S.fetch.p, 0, 2 * sizeof(unsigned int), s);
     launch_fill_slices(M.view(), S.view(), S.col.p, S.v32.p, S.v64.p, total, s);
-    if ((e = S.affine.alloc(static_cast<size_t>(S.n_slice))) != cudaSuccess)
-        return cuda_fail(err, e, "build_slices");
-    launch_affine_slices(S.view(), S.affine.p, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(err, e, "build_slices");
+    {
+        DBuf<unsigned long long> cnt;
+        unsigned long long h = 0;
+        if ((e = S.affine.alloc(static_cast<size_t>(S.n_slice))) != cudaSuccess ||
+            (e = cnt.alloc(1)) != cudaSuccess ||
+            (e = cudaMemsetAsync(cnt.p, 0, sizeof h, s)) != cudaSuccess)
+            return cuda_fail(err, e, "build_slices");
+        launch_affine_slices(S.view(), S.affine.p, cnt.p, s);
+        if ((e = cudaMemcpyAsync(&h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail(err, e, "build_slices");
+        S.nnz_affine = static_cast<int64_t>(h);
+    }
 
     // the long-row tiers without the rows of the slices kept
     std::vector<char> in_slice(ext.size(), 0);
@@ -511,7 +524,34 @@ inline int build_slices(MatDev& M, cudaStream_t s, std::string* err) {
     return build_tiers(rest, M.short_max, sms, M.no_slice_tiers, s, err);
 }
 
-// row_ptr structure on the host// row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,
+// Dense rows among the rows above short_max (k_dense_rows); none listed, no
+// array.
+inline int build_dense_rows(MatDev& M, cudaStream_t s, std::string* err) {
+    const char* knob = std::getenv("PDHG_B200_DENSE_ROWS");  // "0": load every column index
+    M.nnz_dense = 0;
+    if (M.ext.empty() || (knob != nullptr && knob[0] == '0')) {
+        M.dense_off.release();
+        return PDHG_OK;
+    }
+    DBuf<int4> d_ext;
+    DBuf<unsigned long long> cnt;
+    unsigned long long h = 0;
+    cudaError_t e;
+    if ((e = upload(d_ext, M.ext, s)) != cudaSuccess ||
+        (e = M.dense_off.alloc(static_cast<size_t>(M.rows))) != cudaSuccess ||
+        (e = cudaMemsetAsync(M.dense_off.p, 0x80, sizeof(int32_t) * static_cast<size_t>(M.rows), s)) !=
+            cudaSuccess ||
+        (e = cnt.alloc(1)) != cudaSuccess || (e = cudaMemsetAsync(cnt.p, 0, sizeof h, s)) != cudaSuccess)
+        return cuda_fail(err, e, "build_dense_rows");
+    launch_dense_rows(M.ci.p, d_ext.p, static_cast<int32_t>(M.ext.size()), M.dense_off.p, cnt.p, s);
+    if ((e = cudaMemcpyAsync(&h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(err, e, "build_dense_rows");
+    M.nnz_dense = static_cast<int64_t>(h);
+    return PDHG_OK;
+}
+
+// row_ptr structure on the host (rows + 1 reads): starts at 0, ends at nnz,
 // non-decreasing. Every device kernel that walks rows relies on it.
 inline bool row_ptr_ok(int32_t rows, int64_t nnz, const int32_t* rp) {
     if (rp[0] != 0 || rp[rows] != nnz) return false;

@@ -87,6 +87,7 @@ struct Ctx {
     DBuf<double> x64, xbar64, s64, y64, xsum, ysum;
     DBuf<float> x32, xbar32, s32, y32, psx, psy;
     bool halpern = false;  // the current solve runs the Halpern iteration (its anchors below)
+    bool lean = false;     // ... without storing z's x part (Iterates::lean); off when tracing
     DBuf<double> xa64, sa64, ya64;
     DBuf<float> xa32, sa32, ya32;
     DBuf<double> act_avg, cand_xo, cand_yo, part, bx, by, xo, yo, rc, trow, tcol;
@@ -271,6 +272,10 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     if (rc != PDHG_OK) return rc;
     rc = build_slices(c.ATs, s, &c.err);
     if (rc != PDHG_OK) return rc;
+    rc = build_dense_rows(c.As, s, &c.err);
+    if (rc != PDHG_OK) return rc;
+    rc = build_dense_rows(c.ATs, s, &c.err);
+    if (rc != PDHG_OK) return rc;
     const double sign = c.lp.maximize ? -1.0 : 1.0;
     CK(c.c_s.alloc(static_cast<size_t>(n) + 1));
     CK(c.lo_s.alloc(static_cast<size_t>(n) + 1));
@@ -386,6 +391,7 @@ Iterates<double> iterates<double>(Ctx& c) {
         it.sa = c.sa64.p;
         it.ya = c.ya64.p;
         it.halpern = 1;
+        it.lean = c.lean ? 1 : 0;
     }
     return it;
 }
@@ -405,6 +411,7 @@ Iterates<float> iterates<float>(Ctx& c) {
         it.sa = c.sa32.p;
         it.ya = c.ya32.p;
         it.halpern = 1;
+        it.lean = c.lean ? 1 : 0;
     }
     return it;
 }
@@ -462,10 +469,12 @@ struct Launcher {
     FastCheck<float> fc32;
     FastCheck<double> fc64;
 
-    // iteration t of a check period (t = 0 first): the Halpern weight uses t
-    void iteration(long long t, cudaStream_t s) {
+    // iteration t of a check period (t = 0 first): the Halpern weight uses t;
+    // tz: a check or the final selection reads this iteration's T(z)
+    void iteration(long long t, cudaStream_t s, bool tz) {
         const int first = t == 0 ? 1 : 0;
         fi32.hk = fi64.hk = static_cast<int>(t);
+        fi32.tz = fi64.tz = tz ? 1 : 0;
         if (prec == PDHG_PREC_FP64_EXACT) {
             launch_exact_primal(ei, first, s);
             launch_exact_dual(ei, first, s);
@@ -586,7 +595,7 @@ int build_graph(Ctx& c, Launcher& L, long long period, const GraphSig& sig) {
     cudaGraph_t g = nullptr;
     const long long before = c.launches;
     CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-    for (long long t = 0; t < period; ++t) L.iteration(t, c.stream);
+    for (long long t = 0; t < period; ++t) L.iteration(t, c.stream, t == period - 1);
     L.check(period, c.stream);
     cudaError_t e = cudaStreamEndCapture(c.stream, &g);
     c.launches = before;
@@ -734,7 +743,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
     while (p < n_periods && p * period < traced && !c.mail->done) {
         poll_stop();
         for (long long t = 0; t < period; ++t) {
-            L.iteration(t, c.stream);
+            L.iteration(t, c.stream, t == period - 1);
             const long long k = iter0 + p * period + t;
             if (k < o.trace_iters) {
                 int rc = trace_copy(c, L.prec, k, o);
@@ -759,7 +768,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         sig.restart_rule = o.restart_rule;
         sig.pw = o.primal_weight_update;
         sig.infeas = o.infeasibility_detection;
-        sig.halpern = o.halpern;
+        sig.halpern = o.halpern ? (c.lean ? 2 : 1) : 0;
         sig.gen = c.gen;
         int rc = build_graph(c, L, period, sig);
         if (rc != PDHG_OK) return rc;
@@ -810,7 +819,7 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
         poll_stop();
         if (!stop_sent) {
             for (long long t = 0; t < tail; ++t) {
-                L.iteration(t, c.stream);
+                L.iteration(t, c.stream, t == tail - 1);
                 const long long k = iter0 + n_periods * period + t;
                 if (k < o.trace_iters) {
                     int rc = trace_copy(c, L.prec, k, o);
@@ -843,17 +852,18 @@ int run_loop(Ctx& c, Launcher& L, const pdhg_options& o, long long budget, long 
 __global__ void k_widen(Iterates<float> a, Iterates<double> b, int32_t n, int32_t m) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
     // Halpern: the FP64 phase starts at T(z) (inside the bounds) as a restart
-    // point, which is also its first anchor
+    // point, which is also its first anchor and (in the T(z) slot) its
+    // reported point until its first iteration
     if (t < n) {
         b.x[t] = b.halpern ? a.psx[t] : a.x[t];
         b.xbar[t] = b.halpern ? a.psx[t] : a.xbar[t];
-        b.xsum[t] = 0.0;
+        b.xsum[t] = b.halpern ? static_cast<double>(a.psx[t]) : 0.0;
         if (b.halpern) b.xa[t] = b.x[t];
     }
     if (t < m) {
         b.y[t] = b.halpern ? a.psy[t] : a.y[t];
         b.s[t] = a.s[t];
-        b.ysum[t] = 0.0;
+        b.ysum[t] = b.halpern ? static_cast<double>(a.psy[t]) : 0.0;
         if (b.halpern) {
             b.ya[t] = b.y[t];
             b.sa[t] = b.s[t];
@@ -1119,6 +1129,7 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     }
     CK(cudaSetDevice(c.device));
     c.halpern = o.halpern != 0;
+    c.lean = c.halpern && o.trace_iters <= 0;
     ScalingParams sp;
     sp.ruiz_iterations = o.ruiz_iterations;
     sp.ruiz_tolerance = o.ruiz_tolerance;
@@ -1444,14 +1455,31 @@ int load(Ctx& c, int32_t m, int32_t n, int64_t nnz, const int32_t* row_ptr,
 
 // ---- profiling ----------------------------------------------------------------
 
-double iter_bytes(const Ctx& c, int prec, bool primal) {
+// Algorithmic bytes of one pass: the matrix stream (row pointer, index,
+// value), one read of each gathered vector entry, and the fused epilogue's
+// vector reads and writes per row. Averaged iteration: 5 reads (c, x, lo, hi,
+// sum; y, s, row bounds, sum) and 3 writes. Lean Halpern primal: 5 reads (c,
+// x_bar, anchor, lo, hi) and 1 write (x_bar), plus x and T(z) once a check
+// period; Halpern dual: 6 reads (y, s, row bounds, the two anchors), 2 writes,
+// plus T(z) once a period. What this LP's structure makes constant carries
+// no information and is not counted: the row pointer where every row has the
+// same length, the column bounds where all are equal, the column indices of
+// dense rows and (where the pass uses them) of affine row slices -- the
+// kernels compute those instead of loading them.
+double iter_bytes(const Ctx& c, int prec, bool primal, bool halpern, long long period,
+                  const DevCsr& D) {
     const double vb = prec == PDHG_PREC_MIXED ? 4.0 : 8.0;  // value / vector element bytes
-    const double nnz = static_cast<double>(c.As.nnz);
-    const double n = c.lp.n, m = c.lp.m;
-    // matrix stream (row pointer + index + value), one read of each gathered
-    // vector entry, the fused epilogue's vector reads and writes
-    if (primal) return 4.0 * (n + 1) + (4.0 + vb) * nnz + vb * m + vb * (5 * n) + vb * (3 * n);
-    return 4.0 * (m + 1) + (4.0 + vb) * nnz + vb * n + vb * (5 * m) + vb * (3 * m);
+    const MatDev& M = primal ? c.ATs : c.As;
+    const double nnz = static_cast<double>(M.nnz);
+    const double rows = M.rows, cols = M.cols;
+    const double per = period > 0 ? 1.0 / static_cast<double>(period) : 0.0;
+    const double touches = primal ? (halpern ? 6.0 + 2.0 * per : 8.0) : (halpern ? 8.0 + per : 8.0);
+    double b = 4.0 * (rows + 1) + (4.0 + vb) * nnz + vb * cols + vb * touches * rows;
+    if (prec == PDHG_PREC_FP64_EXACT) return b;  // the ordered kernels load everything
+    if (D.rp_stride > 0) b -= 4.0 * (rows + 1);
+    if (primal && c.col_uniform) b -= 2.0 * vb * rows;
+    b -= 4.0 * static_cast<double>(M.nnz_dense + (D.use_slices ? M.slices.nnz_affine : 0));
+    return b;
 }
 
 int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
@@ -1461,14 +1489,19 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
         return PDHG_ERR_INVALID_ARGUMENT;
     }
     CK(cudaSetDevice(c.device));
-    c.halpern = false;  // the kernels are timed in the averaged form
+    // the kernels are timed in the form the last solve ran: averaged, or the
+    // lean Halpern iteration (its T(z) and x stores, once a check period, left out)
+    const bool hal = c.halpern && prec != PDHG_PREC_FP64_EXACT;
+    c.halpern = hal;
+    c.lean = hal;
     int rc = alloc_iterates(c, prec == PDHG_PREC_MIXED);
     if (rc != PDHG_OK) return rc;
     CK(c.st.alloc(1));
     pdhg_options o;
     pdhg_default_options(&o);
     o.precision = prec;
-    o.termination_rule = 1;
+    o.termination_rule = hal ? 2 : 1;  // the check instance the solve's form runs
+    o.restart_rule = hal ? 2 : o.restart_rule;
     const double step = c.opnorm > 1e-9 ? 0.9 / c.opnorm : 0.9;
     Launcher L = make_launcher(c, prec, o, false);
     rc = reset_state(c, step, 1.0);
@@ -1478,7 +1511,12 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
         launch_init_point<float>(P, c.As.view(), nullptr, nullptr, iterates<float>(c), c.stream);
     else
         launch_init_point<double>(P, c.As.view(), nullptr, nullptr, iterates<double>(c), c.stream);
-    for (int i = 0; i < warmup; ++i) L.iteration(i, c.stream);
+    if (hal) {
+        if (prec == PDHG_PREC_MIXED) launch_set_anchor<float>(iterates<float>(c), c.lp.n, c.lp.m, c.stream);
+        else launch_set_anchor<double>(iterates<double>(c), c.lp.n, c.lp.m, c.stream);
+    }
+    for (int i = 0; i < warmup; ++i) L.iteration(i, c.stream, true);
+    L.fi32.tz = L.fi64.tz = 0;
     std::vector<cudaEvent_t> ev(3 * static_cast<size_t>(iters) + 2);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int i = 0; i < iters; ++i) {
@@ -1514,8 +1552,11 @@ int profile(Ctx& c, int prec, int warmup, int iters, pdhg_kernel_stats* out) {
     out->avg_ms[0] = iters ? tp / iters : 0;
     out->avg_ms[1] = iters ? td / iters : 0;
     out->avg_ms[2] = tc;
-    out->bytes[0] = iter_bytes(c, prec, true);
-    out->bytes[1] = iter_bytes(c, prec, false);
+    const FastIter<float>& F32 = L.fi32;
+    const FastIter<double>& F64 = L.fi64;
+    const bool f32 = prec == PDHG_PREC_MIXED;
+    out->bytes[0] = iter_bytes(c, prec, true, hal, o.restart_check_period, f32 ? F32.AT : F64.AT);
+    out->bytes[1] = iter_bytes(c, prec, false, hal, o.restart_check_period, f32 ? F32.A : F64.A);
     out->bytes[2] = 2.0 * (12.0 * c.As.nnz) + 8.0 * 10 * (c.lp.n + c.lp.m);
     out->launches[0] = iters;
     out->launches[1] = iters;

@@ -138,7 +138,13 @@ struct DevCsr {
     // the short-row iteration kernel computes the row's extent instead of
     // loading it
     int32_t rp_stride = 0;
+    // per row (null when the matrix has no row above short_max): off when
+    // entry k of the row sits in column k + off (every entry, consecutive
+    // columns), kNotDense otherwise; the long-row iteration paths then compute
+    // the columns and stream the gathered vector
+    const int32_t* dense_off = nullptr;
 };
+constexpr int32_t kNotDense = static_cast<int32_t>(0x80808080u);  // a byte-wise memset value
 
 
 // Accumulator slots (bit patterns of non-negative doubles, combined with
@@ -245,6 +251,12 @@ struct Iterates {
     // then hold the last PDHG output T(z) instead of running sums
     T *xa = nullptr, *sa = nullptr, *ya = nullptr;
     int halpern = 0;
+    // with halpern, lean = 1: z's x part and T(z) are stored only by the
+    // iterations whose point a check or the result reads (the last of a check
+    // period or of the solve). The primal pass rebuilds x as
+    // w' x_bar + (1 - w') x_a (w' the previous iteration's weight, x_bar its
+    // reflected point, which every iteration writes).
+    int lean = 0;
 };
 
 struct CheckScratch {
@@ -297,6 +309,7 @@ struct FastIter {
     Iterates<T> it;
     DevState* st;
     int hk = 0;  // the iteration's index in its check period (Halpern weight)
+    int tz = 1;  // Halpern: this iteration stores T(z) (lean mode: only before a check / the end)
 };
 // A pass's short-row, long-row and row-slice kernels touch disjoint rows and
 // only read the gathered vector, so they may run side by side: with a
@@ -460,7 +473,12 @@ void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_
 // Lane-interleaved copy of the slices' rows: for slice s, lane l, entry k <
 // rlen: col/v32/v64[off + 32 k + l] = the row's k-th entry; padding entries
 // get column 0 and value 0.
-void launch_affine_slices(const RowSlices& S, int2* affine, cudaStream_t s);
+// nnz_affine / nnz_dense: device counters that the kernels add the entries
+// of affine slices / dense rows to
+void launch_affine_slices(const RowSlices& S, int2* affine, unsigned long long* nnz_affine,
+                          cudaStream_t s);
+void launch_dense_rows(const int32_t* ci, const int4* ext, int32_t n_ext, int32_t* dense_off,
+                       unsigned long long* nnz_dense, cudaStream_t s);
 void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,
                         int64_t total, cudaStream_t s);
 void launch_ruiz_sweep(const DevCsr& A, const DevCsr& AT, double* rs, double* cs,

@@ -218,19 +218,56 @@ __device__ __forceinline__ bool warp_segment_finish(const RowItems& L, int idx, 
     return true;
 }
 
-// Long-row dot product: 128-bit loads of values and column indices on the
-// aligned body, scalar head and tail. The matrix is streamed (evict-first,
-// ld.global.cs) so that the gathered vector keeps its L2 lines; gathers go
-// through the read-only path.
+// Vector types of the 128-bit loads (W = 16 / sizeof(T) entries).
 template <class T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+};
+
+// Gathered entries of one 128-bit vector of a row. DENSE: entry k of the row
+// sits in column k + off, so the W entries are consecutive: one vector load
+// when `va` (the gathered vector aligned with the row's values), else W
+// scalar loads at computed addresses. Otherwise the columns come from `c`.
+template <class T>
+__device__ __forceinline__ typename Vec16<T>::type gather16(const T* __restrict__ xg, int k, int off,
+                                                            bool va) {
+    if (va) return __ldg(reinterpret_cast<const typename Vec16<T>::type*>(xg + k + off));
+    typename Vec16<T>::type g;
+    if constexpr (std::is_same<T, float>::value) {
+        g.x = __ldg(xg + k + off);
+        g.y = __ldg(xg + k + off + 1);
+        g.z = __ldg(xg + k + off + 2);
+        g.w = __ldg(xg + k + off + 3);
+    } else {
+        g.x = __ldg(xg + k + off);
+        g.y = __ldg(xg + k + off + 1);
+    }
+    return g;
+}
+
+// Long-row dot product, one CTA: 128-bit loads of values and column indices
+// on the aligned body (four of each in flight per thread), scalar head and
+// tail. The matrix is streamed (evict-first, ld.global.cs) so that the
+// gathered vector keeps its L2 lines; gathers go through the read-only path.
+// DENSE: the columns are k + off (no index loads); the sum order is the same
+// either way.
+template <class T, bool DENSE = false>
 __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
                                           const T* __restrict__ v, const T* __restrict__ xg,
-                                          int b, int e) {
+                                          int b, int e, int off = 0) {
     constexpr int W = 16 / sizeof(T);
     int bA = ((b + W - 1) / W) * W;
     if (bA > e) bA = e;
+    const bool va = DENSE && ((bA + off) & (W - 1)) == 0;
+    auto col = [&](int k) { return DENSE ? k + off : __ldcs(ci + k); };
     T acc = T(0);
-    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
+    for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + col(k));
     const int nvec = (e - bA) / W;
     if constexpr (W == 4) {
         const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
@@ -238,35 +275,57 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
         int q = threadIdx.x;
         // four independent 128-bit loads of each stream in flight per thread
         for (; q + 3 * kBlock < nvec; q += 4 * kBlock) {
-            int4 c[4];
             float4 w[4];
+            if (DENSE) {
+                float4 g[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                c[u] = __ldcs(ci4 + q + u * kBlock);
-                w[u] = __ldcs(v4 + q + u * kBlock);
+                for (int u = 0; u < 4; ++u) {
+                    w[u] = __ldcs(v4 + q + u * kBlock);
+                    g[u] = gather16<T>(xg, bA + 4 * (q + u * kBlock), off, va);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    acc += w[u].x * g[u].x + w[u].y * g[u].y + w[u].z * g[u].z + w[u].w * g[u].w;
+            } else {
+                int4 c[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    c[u] = __ldcs(ci4 + q + u * kBlock);
+                    w[u] = __ldcs(v4 + q + u * kBlock);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    acc += w[u].x * __ldg(xg + c[u].x) + w[u].y * __ldg(xg + c[u].y) +
+                           w[u].z * __ldg(xg + c[u].z) + w[u].w * __ldg(xg + c[u].w);
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                acc += w[u].x * __ldg(xg + c[u].x) + w[u].y * __ldg(xg + c[u].y) +
-                       w[u].z * __ldg(xg + c[u].z) + w[u].w * __ldg(xg + c[u].w);
         }
         for (; q < nvec; q += kBlock) {
-            const int4 c = __ldcs(ci4 + q);
             const float4 w = __ldcs(v4 + q);
-            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
-                   w.w * __ldg(xg + c.w);
+            if (DENSE) {
+                const float4 g = gather16<T>(xg, bA + 4 * q, off, va);
+                acc += w.x * g.x + w.y * g.y + w.z * g.z + w.w * g.w;
+            } else {
+                const int4 c = __ldcs(ci4 + q);
+                acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
+                       w.w * __ldg(xg + c.w);
+            }
         }
     } else {
         const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
         const double2* v2 = reinterpret_cast<const double2*>(v + bA);
         for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const int2 c = __ldcs(ci2 + q);
             const double2 w = __ldcs(v2 + q);
-            acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
+            if (DENSE) {
+                const double2 g = gather16<T>(xg, bA + 2 * q, off, va);
+                acc += w.x * g.x + w.y * g.y;
+            } else {
+                const int2 c = __ldcs(ci2 + q);
+                acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
+            }
         }
     }
     for (int k = bA + nvec * W + threadIdx.x; k < e; k += kBlock)
-        acc += __ldcs(v + k) * __ldg(xg + __ldcs(ci + k));
+        acc += __ldcs(v + k) * __ldg(xg + col(k));
     return block_total(acc);
 }
 
@@ -289,27 +348,33 @@ constexpr int kWarpUnroll = PDHG_WARP_UNROLL;
 template <class T>
 __device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ ci,
                                           const T* __restrict__ v, const T* __restrict__ xg,
-                                          int b, int e) {
+                                          int b, int e, int off = kNotDense) {
     constexpr int W = 16 / sizeof(T);
+    using V = typename Vec16<T>::type;
     const int lane = threadIdx.x & 31;
+    // a dense row (off set, warp-uniform) computes its columns k + off in the
+    // same loop: one register set for both kinds of row
+    const bool dense = off != kNotDense;
     int bA = ((b + W - 1) / W) * W;
     if (bA > e) bA = e;
+    auto col = [&](int k) { return dense ? k + off : __ldcs(ci + k); };
     T acc = T(0);
-    for (int k = b + lane; k < bA; k += 32) acc += __ldcs(v + k) * PDHG_GATHER(xg + __ldcs(ci + k));
+    for (int k = b + lane; k < bA; k += 32) acc += __ldcs(v + k) * PDHG_GATHER(xg + col(k));
     const int nvec = (e - bA) / W;
+    const V* vv = reinterpret_cast<const V*>(v + bA);
     // rounds of up to kWarpUnroll vectors per lane in flight; the last round
     // is predicated instead of falling back to one vector at a time
     if constexpr (W == 4) {
         const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
-        const float4* v4 = reinterpret_cast<const float4*>(v + bA);
         for (int q = lane; q < nvec; q += 32 * kWarpUnroll) {
             int4 c[kWarpUnroll];
             float4 w[kWarpUnroll];
 #pragma unroll
             for (int u = 0; u < kWarpUnroll; ++u) {
                 const bool ok = q + 32 * u < nvec;
-                c[u] = ok ? __ldcs(ci4 + q + 32 * u) : make_int4(0, 0, 0, 0);
-                w[u] = ok ? __ldcs(v4 + q + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const int k = bA + 4 * (q + 32 * u) + off;
+                c[u] = !ok ? make_int4(0, 0, 0, 0) : dense ? make_int4(k, k + 1, k + 2, k + 3) : __ldcs(ci4 + q + 32 * u);
+                w[u] = ok ? __ldcs(vv + q + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int u = 0; u < kWarpUnroll; ++u)
@@ -319,15 +384,15 @@ __device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ ci,
         }
     } else {
         const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
-        const double2* v2 = reinterpret_cast<const double2*>(v + bA);
         for (int q = lane; q < nvec; q += 32 * kWarpUnroll) {
             int2 c[kWarpUnroll];
             double2 w[kWarpUnroll];
 #pragma unroll
             for (int u = 0; u < kWarpUnroll; ++u) {
                 const bool ok = q + 32 * u < nvec;
-                c[u] = ok ? __ldcs(ci2 + q + 32 * u) : make_int2(0, 0);
-                w[u] = ok ? __ldcs(v2 + q + 32 * u) : make_double2(0.0, 0.0);
+                const int k = bA + 2 * (q + 32 * u) + off;
+                c[u] = !ok ? make_int2(0, 0) : dense ? make_int2(k, k + 1) : __ldcs(ci2 + q + 32 * u);
+                w[u] = ok ? __ldcs(vv + q + 32 * u) : make_double2(0.0, 0.0);
             }
 #pragma unroll
             for (int u = 0; u < kWarpUnroll; ++u)
@@ -336,7 +401,7 @@ __device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ ci,
         }
     }
     for (int k = bA + nvec * W + lane; k < e; k += 32)
-        acc += __ldcs(v + k) * PDHG_GATHER(xg + __ldcs(ci + k));
+        acc += __ldcs(v + k) * PDHG_GATHER(xg + col(k));
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
@@ -352,23 +417,61 @@ struct EpiIn {
     T a, b, lo, hi, ps;  // primal: c, x, lo, hi, sum; dual: y, s, row lo, row hi, sum
 };
 
-// The reflected Halpern weight w = (k+1)/(k+2) of an iteration, k the
-// iterations since the last restart (0 without the option).
+// The reflected Halpern weights of an iteration: w = (k+1)/(k+2), k the
+// iterations since the last restart, and the previous iteration's w' =
+// k/(k+1) (0 right after a restart, when z is the anchor). Both zero without
+// the option.
 template <class T>
-__device__ __forceinline__ T halpern_weight(const Iterates<T>& it, long long since_restart, int hk) {
-    if (!it.halpern) return T(0);
+struct Hw {
+    T w, wp;
+};
+
+template <class T>
+__device__ __forceinline__ Hw<T> halpern_weight(const Iterates<T>& it, long long since_restart,
+                                                int hk) {
+    if (!it.halpern) return {T(0), T(0)};
     const double k = static_cast<double>(since_restart + hk);
-    return static_cast<T>((k + 1.0) / (k + 2.0));
+    return {static_cast<T>((k + 1.0) / (k + 2.0)), static_cast<T>(k / (k + 1.0))};
 }
 
-template <class T, bool PRIMAL>
+// The same weights where one k holds for the whole launch and every lane of
+// the warp is converged (the single-LP kernels): lane 0 forms them and the
+// warp shares them by shuffle, so the FP64 divisions run once per warp.
+template <class T>
+__device__ __forceinline__ Hw<T> halpern_weight_warp(const Iterates<T>& it, const DevState* st,
+                                                     int hk) {
+    if (!it.halpern) return {T(0), T(0)};
+    Hw<T> h{T(0), T(0)};
+    if ((threadIdx.x & 31) == 0) h = halpern_weight<T>(it, st->since_restart, hk);
+    h.w = __shfl_sync(0xffffffffu, h.w, 0);
+    h.wp = __shfl_sync(0xffffffffu, h.wp, 0);
+    return h;
+}
+
+// z+ = w (2 T(z) - z) + (1 - w) z_a: the same rounding wherever it is formed
+// (the primal's store, and its rebuild of x in lean mode)
+template <class T>
+__device__ __forceinline__ T halpern_mix(T w, T refl, T anchor) {
+    if constexpr (std::is_same<T, float>::value) return __fmaf_rn(w, refl, (1.0f - w) * anchor);
+    else return __fma_rn(w, refl, (1.0 - w) * anchor);
+}
+
+// LEAN = false compiles the lean Halpern form out (callers that never set it)
+template <class T, bool PRIMAL, bool LEAN = true>
 __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>& pv, int r,
-                                             int first, bool fresh) {
+                                             int first, bool fresh, const Hw<T>& hw) {
     EpiIn<T> in;
     // Halpern: the sums' slot is only written, so `ps` carries the anchor of x
     // (primal) or y (dual) instead; the slack's anchor is read at the store
     if (PRIMAL) {
         in.a = __ldcs(pv.c + r);
+        if (LEAN && it.lean) {  // x = w' x_bar + (1 - w') x_a, x_a right after a restart
+            in.ps = __ldcs(it.xa + r);
+            in.b = hw.wp == T(0) ? in.ps : halpern_mix<T>(hw.wp, it.xbar[r], in.ps);
+            in.lo = pv.ub ? pv.lo_u : __ldcs(pv.lo + r);
+            in.hi = pv.ub ? pv.hi_u : __ldcs(pv.hi + r);
+            return in;
+        }
         in.b = __ldcs(it.x + r);
         in.lo = pv.ub ? pv.lo_u : __ldcs(pv.lo + r);
         in.hi = pv.ub ? pv.hi_u : __ldcs(pv.hi + r);
@@ -392,9 +495,14 @@ __device__ __forceinline__ EpiIn<T> epi_load(const Iterates<T>& it, const PV<T>&
 // With the Halpern option (weight hw = w) the step's output T(z) = (x+, s+, y+)
 // goes to the sums' slot and z moves to w (2 T(z) - z) + (1 - w) z_a (the
 // anchor of x or y arrives in in.ps).
-template <class T, bool PRIMAL>
+template <class T, bool PRIMAL, bool LEAN = true>
 __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, const EpiIn<T>& in,
-                                          T tau, T sigma, T hw) {
+                                          T tau, T sigma, const Hw<T>& hw, int tz) {
+    // tz (lean Halpern): this iteration stores T(z) and z's x part; read from
+    // the launch's parameters at the store so that it holds no register across
+    // the SpMV
+    const bool lean = LEAN && it.lean;
+    const bool store_tz = !lean || tz != 0;
     T* ps = nullptr;
     if constexpr (std::is_same<T, float>::value) ps = PRIMAL ? it.psx : it.psy;
     else ps = PRIMAL ? it.xsum : it.ysum;
@@ -404,8 +512,8 @@ __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, c
         const T xb = T(2) * xn - xo;
         it.xbar[r] = xb;
         if (it.halpern) {
-            __stcs(it.x + r, hw * xb + (T(1) - hw) * in.ps);
-            __stcs(ps + r, xn);
+            if (store_tz) __stcs(it.x + r, halpern_mix<T>(hw.w, xb, in.ps));
+            if (store_tz) __stcs(ps + r, xn);
         } else {
             __stcs(it.x + r, xn);
             __stcs(ps + r, in.ps + xn);
@@ -416,9 +524,9 @@ __device__ __forceinline__ void epi_store(const Iterates<T>& it, int r, T dot, c
         const T sb = T(2) * sn - so;
         const T yn = yo + sigma * (sb - dot);
         if (it.halpern) {
-            it.y[r] = hw * (T(2) * yn - yo) + (T(1) - hw) * in.ps;
-            __stcs(it.s + r, hw * sb + (T(1) - hw) * __ldcs(it.sa + r));
-            __stcs(ps + r, yn);
+            it.y[r] = halpern_mix<T>(hw.w, T(2) * yn - yo, in.ps);
+            __stcs(it.s + r, halpern_mix<T>(hw.w, sb, __ldcs(it.sa + r)));
+            if (store_tz) __stcs(ps + r, yn);
         } else {
             it.y[r] = yn;
             __stcs(it.s + r, sn);
@@ -454,6 +562,9 @@ __device__ __forceinline__ double clipped_inf(double coeff, double lo, double hi
 // of squares of termination rule 2.
 constexpr int kCheckInf = 1;
 constexpr int kCheckL2 = 2;
+// ... measuring one point only (the Halpern iteration's T(z)): the current
+// point's terms are not formed, and its slots carry the measured point's
+constexpr int kCheckOne = 4;
 
 // The part of a multiplier or reduced cost v (internal minimize sense)
 // outside the sign the bounds of its row or column allow: >= 0 with only a
@@ -505,20 +616,23 @@ __device__ __forceinline__ void ray_term(double mult, double lo, double hi, doub
     }
 }
 
-template <class T>
+// H: the caller knows the Halpern form is on (the check's one-point instance)
+template <class T, bool H = false>
 __device__ __forceinline__ double avg_x(const Iterates<T>& it, int j, double inv) {
     if constexpr (std::is_same<T, float>::value) {
-        if (it.halpern) return static_cast<double>(it.psx[j]);  // T(z); the FP64 sums stay 0
+        if (H || it.halpern) return static_cast<double>(it.psx[j]);  // T(z); the FP64 sums stay 0
         return (it.xsum[j] + static_cast<double>(it.psx[j])) * inv;
     }
+    if (H) return it.xsum[j];
     return it.xsum[j] * inv;
 }
-template <class T>
+template <class T, bool H = false>
 __device__ __forceinline__ double avg_y(const Iterates<T>& it, int i, double inv) {
     if constexpr (std::is_same<T, float>::value) {
-        if (it.halpern) return static_cast<double>(it.psy[i]);
+        if (H || it.halpern) return static_cast<double>(it.psy[i]);
         return (it.ysum[i] + static_cast<double>(it.psy[i])) * inv;
     }
+    if (H) return it.ysum[i];
     return it.ysum[i] * inv;
 }
 // The current point's entry for the check's products; the Halpern form

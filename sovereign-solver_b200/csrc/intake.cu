@@ -184,7 +184,7 @@ __global__ void k_fill_slices(const int32_t* rp, const int32_t* ci, const double
 // lane's row length) is column base + l + k * stride, the slice kernel
 // computes the columns instead of loading them. {base, stride}, or {0, 0} for
 // a slice with any other entry; every entry is compared.
-__global__ void k_affine_slices(RowSlices S, int2* affine) {
+__global__ void k_affine_slices(RowSlices S, int2* affine, unsigned long long* nnz_affine) {
     __shared__ int ok;
     for (int sl = blockIdx.x; sl < S.n_slice; sl += gridDim.x) {
         const int4 d = S.slice[sl];
@@ -201,8 +201,40 @@ __global__ void k_affine_slices(RowSlices S, int2* affine) {
         }
         if (bad) ok = 0;  // every writer writes 0
         __syncthreads();
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0) {
             affine[sl] = ok ? make_int2(static_cast<int>(base), static_cast<int>(stride)) : make_int2(0, 0);
+            if (ok) {
+                unsigned long long len = 0;
+                for (int l = 0; l < 32; ++l) len += static_cast<unsigned long long>(S.rlen[32 * sl + l]);
+                atomicAdd(nnz_affine, len);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Dense rows: a long row whose entries k = b..e-1 sit in columns k + off
+// (consecutive columns, a supply row of a transportation LP) gets off in
+// dense_off[row], so the iteration kernels compute the columns instead of
+// loading them and stream the gathered vector. Every entry is compared; the
+// other rows keep kNotDense (set before the launch).
+__global__ void k_dense_rows(const int32_t* ci, const int4* ext, int32_t n_ext, int32_t* dense_off,
+                             unsigned long long* nnz_dense) {
+    __shared__ int ok;
+    for (int q = blockIdx.x; q < n_ext; q += gridDim.x) {
+        const int4 w = ext[q];
+        const int off = ci[w.y] - w.y;
+        if (threadIdx.x == 0) ok = off != kNotDense ? 1 : 0;
+        __syncthreads();
+        bool bad = false;
+        for (int k = w.y + static_cast<int>(threadIdx.x); k < w.z; k += kBlock)
+            if (ci[k] - k != off) bad = true;
+        if (bad) ok = 0;  // every writer writes 0
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            dense_off[w.x] = off;
+            atomicAdd(nnz_dense, static_cast<unsigned long long>(w.z - w.y));
+        }
         __syncthreads();
     }
 }
@@ -521,9 +553,16 @@ void launch_gather_cols(const int32_t* ci, const int64_t* pos, int32_t n, int32_
     if (n > 0) k_gather_cols<<<nblocks(n), kBlock, 0, s>>>(ci, pos, n, out);
 }
 
-void launch_affine_slices(const RowSlices& S, int2* affine, cudaStream_t s) {
+void launch_dense_rows(const int32_t* ci, const int4* ext, int32_t n_ext, int32_t* dense_off,
+                       unsigned long long* nnz_dense, cudaStream_t s) {
+    if (n_ext > 0)
+        k_dense_rows<<<n_ext < 4096 ? n_ext : 4096, kBlock, 0, s>>>(ci, ext, n_ext, dense_off, nnz_dense);
+}
+
+void launch_affine_slices(const RowSlices& S, int2* affine, unsigned long long* nnz_affine,
+                          cudaStream_t s) {
     if (S.n_slice == 0) return;
-    k_affine_slices<<<S.n_slice < 4096 ? S.n_slice : 4096, kBlock, 0, s>>>(S, affine);
+    k_affine_slices<<<S.n_slice < 4096 ? S.n_slice : 4096, kBlock, 0, s>>>(S, affine, nnz_affine);
 }
 
 void launch_fill_slices(const DevCsr& M, RowSlices S, int32_t* col, float* v32, double* v64,

@@ -53,6 +53,12 @@
 #ifndef PDHG_WARPITEM_MIN_CTAS
 #define PDHG_WARPITEM_MIN_CTAS 4
 #endif
+#ifndef PDHG_PAIR_MIN_CTAS
+#define PDHG_PAIR_MIN_CTAS 8
+#endif
+#ifndef PDHG_PAIR_MIN_CTAS_F64
+#define PDHG_PAIR_MIN_CTAS_F64 4
+#endif
 #ifndef PDHG_SLICE_MIN_CTAS
 #define PDHG_SLICE_MIN_CTAS 4
 #endif
@@ -82,6 +88,47 @@ __device__ __forceinline__ void iter_reset(DevState* st, int reset) {
     }
 }
 
+// Two consecutive values of a row, loaded as one vector.
+template <class T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <class T>
+__device__ __forceinline__ bool pair_aligned(const int32_t* ci, const T* v) {
+    return ((reinterpret_cast<uintptr_t>(ci) & 7u) | (reinterpret_cast<uintptr_t>(v) & (2 * sizeof(T) - 1))) == 0;
+}
+template <class T>
+__device__ __forceinline__ T fma_rn(T a, T b, T c) {
+    if constexpr (std::is_same<T, float>::value) return __fmaf_rn(a, b, c);
+    else return __fma_rn(a, b, c);
+}
+template <class T>
+__device__ __forceinline__ T mul_rn(T a, T b) {
+    if constexpr (std::is_same<T, float>::value) return __fmul_rn(a, b);
+    else return __dmul_rn(a, b);
+}
+
+// The dot of long row `row` over entries [b, e), by one CTA (block-uniform)
+// or one warp (warp-uniform); a dense row computes its columns.
+template <class T>
+__device__ __forceinline__ T cta_row_dot(const DevCsr& M, const T* vals, const T* xg, int row, int b,
+                                         int e) {
+    const int off = M.dense_off ? __ldg(M.dense_off + row) : kNotDense;
+    if (off != kNotDense) return long_row_dot<T, true>(M.ci, vals, xg, b, e, off);
+    return long_row_dot<T>(M.ci, vals, xg, b, e);
+}
+template <class T>
+__device__ __forceinline__ T warp_dot(const DevCsr& M, const T* vals, const T* xg, int row, int b,
+                                      int e) {
+    return warp_row_dot<T>(M.ci, vals, xg, b, e, M.dense_off ? __ldg(M.dense_off + row) : kNotDense);
+}
+
 // PRIMAL = true: rows of A^T gather y; false: rows of A gather x_bar.
 template <class T, int VW, bool PRIMAL>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS : PDHG_SHORT_MIN_CTAS_F64)
@@ -95,12 +142,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
+    const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
     const int lane = threadIdx.x & (VW - 1);
     const int r = (blockIdx.x * kBlock + threadIdx.x) / VW;
     if (r >= M.rows) return;
     EpiIn<T> in{};
-    if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
+    if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh, hw);
     int b, e;
     if (M.rp_stride > 0) {  // rows of one length: the extent is computed
         b = r * M.rp_stride;
@@ -110,9 +157,20 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
         e = __ldcs(M.rp + r + 1);
     }
     if (e - b > M.short_max) return;  // fast_iter_long handles it
+    T acc = T(0);
+    if (VW == 1 && M.rp_stride == 2 && pair_aligned<T>(M.ci, vals)) {
+        // two entries per row (the columns of a transportation LP): one
+        // 8-byte index load and one vector value load, the same sum order as
+        // the loop below
+        const int2 c2 = __ldcs(reinterpret_cast<const int2*>(M.ci + b));
+        const typename Pair<T>::type v2 = __ldcs(reinterpret_cast<const typename Pair<T>::type*>(vals + b));
+        const T g0 = __ldg(xg + c2.x), g1 = __ldg(xg + c2.y);
+        acc = fma_rn<T>(v2.y, g1, mul_rn<T>(v2.x, g0));
+        epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw, a.tz);
+        return;
+    }
     // rounds of four entries per lane: the index and value loads of a round
     // are all in flight before its gathers, the gathers before the adds
-    T acc = T(0);
     for (int k0 = b + lane; k0 < e; k0 += 4 * VW) {
         int c[4];
         T v[4];
@@ -127,7 +185,57 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
             if (k0 + u * VW < e) acc += v[u] * __ldg(xg + c[u]);
     }
     if (VW > 1) acc = group_sum(acc, VW);
-    if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw);
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw, a.tz);
+}
+
+// Rows of exactly two entries (rp_stride 2: the columns of a network or
+// transportation LP), a persistent grid (the resident CTAs): each thread walks
+// rows r, r + T, r + 2T, ... (T threads in the grid, so a warp's rows stay
+// consecutive) and pipelines them: the next row's operand, index and value
+// loads are issued before the current row's gathers are consumed, so the
+// streamed arrays stay in flight while the gathers wait. fast_iter (one row
+// per thread) leaves DRAM idle during every thread's gather phase. The
+// arithmetic is fast_iter's two-entry path.
+template <class T, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_PAIR_MIN_CTAS : PDHG_PAIR_MIN_CTAS_F64)
+    fast_iter_pairs(FastIter<T> a, int first, int reset) {
+    using P2 = typename Pair<T>::type;
+    DevState* st = a.st;
+    iter_reset(st, reset);
+    if (st->done) return;
+    const DevCsr& M = PRIMAL ? a.AT : a.A;
+    const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
+    const int2* __restrict__ ci2 = reinterpret_cast<const int2*>(M.ci);
+    const P2* __restrict__ v2 = reinterpret_cast<const P2*>(mvals<T>(M));
+    const PV<T> pv = pvec<T>(a.P);
+    const bool fresh = first && st->fresh;
+    const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
+    const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
+    const int stride = gridDim.x * kBlock;
+    int r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= M.rows) return;
+    EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh, hw);
+    int2 c = __ldcs(ci2 + r);
+    P2 v = __ldcs(v2 + r);
+    for (;;) {
+        const T g0 = __ldg(xg + c.x), g1 = __ldg(xg + c.y);
+        const int rn = r + stride;
+        const bool more = rn < M.rows;
+        EpiIn<T> nin{};
+        int2 nc = make_int2(0, 0);
+        P2 nv{};
+        if (more) {
+            nin = epi_load<T, PRIMAL>(a.it, pv, rn, first, fresh, hw);
+            nc = __ldcs(ci2 + rn);
+            nv = __ldcs(v2 + rn);
+        }
+        epi_store<T, PRIMAL>(a.it, r, fma_rn<T>(v.y, g1, mul_rn<T>(v.x, g0)), in, tau, sigma, hw, a.tz);
+        if (!more) break;
+        r = rn;
+        in = nin;
+        c = nc;
+        v = nv;
+    }
 }
 
 // One CTA work item of L (block-uniform): the dot of its entries, then for a
@@ -135,21 +243,23 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
 // update when this CTA completes the row).
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void cta_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
-                                         int idx, int first, bool fresh, T tau, T sigma, T hw) {
+                                         int idx, int first, bool fresh, T tau, T sigma, Hw<T> hw) {
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     const PV<T> pv = pvec<T>(a.P);
     const int4 w = __ldg(L.item + idx);
-    EpiIn<T> in{};
-    if (threadIdx.x == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
-    T acc = long_row_dot<T>(M.ci, vals, xg, w.y, w.z);
+    T acc = cta_row_dot<T>(M, vals, xg, w.x, w.y, w.z);
     if (w.w >= 0) {  // block-uniform
         double tot, unused;
         if (!segment_finish(L, idx, w.w, static_cast<double>(acc), 0.0, &tot, &unused)) return;
         acc = static_cast<T>(tot);
-        if (threadIdx.x == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
     }
-    if (threadIdx.x == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw);
+    // the row's operands are loaded after its dot (rows here are long: the
+    // load's latency is small beside the dot, and nothing stays live across it)
+    if (threadIdx.x == 0) {
+        const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh, hw);
+        epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw, a.tz);
+    }
 }
 
 // WARPS = true: the first warp_blocks CTAs take the warp rows, one CTA per
@@ -166,7 +276,7 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
+    const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
     const RowItems& L = MODE == 0 ? M.items_long : M.items_huge;
     if (!WARPS) {
         for (;;) {
@@ -186,10 +296,10 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
         const int lane = threadIdx.x & 31;
         const PV<T> pv = pvec<T>(a.P);
         EpiIn<T> in{};
-        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh);
-        const T acc = warp_row_dot<T>(M.ci, mvals<T>(M), PRIMAL ? a.it.y : a.it.xbar,
-                                      __ldg(M.rp + r), __ldg(M.rp + r + 1));
-        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw);
+        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh, hw);
+        const T acc = warp_dot<T>(M, mvals<T>(M), PRIMAL ? a.it.y : a.it.xbar, r, __ldg(M.rp + r),
+                                  __ldg(M.rp + r + 1));
+        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw, a.tz);
     } else {
         // CTA work items: rows above kLongRow (mode 0) or kHugeRow (mode 1),
         // those above the segment length in segments
@@ -202,22 +312,22 @@ __global__ void __launch_bounds__(kBlock, WARPS ? PDHG_WARPROW_MIN_CTAS : PDHG_L
 // of a longer one whose last warp adds the segments in order.
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void warp_item(const FastIter<T>& a, const DevCsr& M, const RowItems& L,
-                                          int idx, int first, bool fresh, T tau, T sigma, T hw) {
+                                          int idx, int first, bool fresh, T tau, T sigma, Hw<T> hw) {
     const T* __restrict__ vals = mvals<T>(M);
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     const PV<T> pv = pvec<T>(a.P);
     const int lane = threadIdx.x & 31;
     const int4 w = __ldg(L.item + idx);
     EpiIn<T> in{};
-    if (lane == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
-    T acc = warp_row_dot<T>(M.ci, vals, xg, w.y, w.z);
+    if (lane == 0 && w.w < 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh, hw);
+    T acc = warp_dot<T>(M, vals, xg, w.x, w.y, w.z);
     if (w.w >= 0) {  // warp-uniform
         double tot;
         if (!warp_segment_finish(L, idx, w.w, static_cast<double>(acc), &tot)) return;
         acc = static_cast<T>(tot);
-        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh);
+        if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, w.x, first, fresh, hw);
     }
-    if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw);
+    if (lane == 0) epi_store<T, PRIMAL>(a.it, w.x, acc, in, tau, sigma, hw, a.tz);
 }
 
 // long_mode 2: every row above short_max as warp work items; no block barrier
@@ -233,7 +343,7 @@ __global__ void __launch_bounds__(kBlock, PDHG_WARPITEM_MIN_CTAS)
     if (idx >= M.items_warp.n_item) return;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
+    const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
     warp_item<T, PRIMAL>(a, M, M.items_warp, idx, first, fresh, tau, sigma, hw);
 }
 
@@ -297,7 +407,7 @@ __device__ __forceinline__ T slice_dot(const RowSlices& S, int off, int k0s, int
 // interleaved sums, fixed) before the 32 rows' updates.
 template <class T, bool PRIMAL>
 __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices& S, int idx,
-                                           int first, bool fresh, T tau, T sigma, T hw) {
+                                           int first, bool fresh, T tau, T sigma, Hw<T> hw) {
     const int lane = threadIdx.x & 31;
     const int4 w = __ldg(S.item + idx);
     const int4 d = __ldg(S.slice + w.x);
@@ -333,8 +443,8 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
     }
     if (row < 0) return;
     const PV<T> pv = pvec<T>(a.P);
-    const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, row, first, fresh);
-    epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma, hw);
+    const EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, row, first, fresh, hw);
+    epi_store<T, PRIMAL>(a.it, row, acc, in, tau, sigma, hw, a.tz);
 }
 
 // The row-slice kernel: a persistent grid (the resident CTAs) whose warps
@@ -351,7 +461,7 @@ __global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
     const RowSlices& S = M.slices;
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
-    const T hw = halpern_weight<T>(a.it, st->since_restart, a.hk);
+    const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
     const int ns = S.n_item;
     const int nt = ns + (WITEMS ? M.items_warp.n_item : 0);
     for (;;) {
@@ -404,6 +514,7 @@ struct PassPlan {
 // capped at these (set by init_fast_kernels from the occupancy calculator).
 int g_cap_long[2] = {148 * PDHG_LONG_MIN_CTAS, 148 * PDHG_LONG_MIN_CTAS};
 int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};
+int g_cap_pair[2] = {148 * PDHG_PAIR_MIN_CTAS, 148 * PDHG_PAIR_MIN_CTAS_F64};
 
 inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
     PassPlan p;
@@ -438,6 +549,16 @@ inline int pass_launches(const DevCsr& M0) {
 }
 
 // Returns the number of kernels launched.
+// Every row of exactly two entries, the arrays aligned for the pair loads
+// (a one-lane pass then runs fast_iter_pairs).
+template <class T>
+bool pairs_ok(const DevCsr& M) {
+    return M.rp_stride == 2 && (reinterpret_cast<uintptr_t>(M.ci) & 7u) == 0 &&
+           (reinterpret_cast<uintptr_t>(sizeof(T) == 4 ? static_cast<const void*>(M.v32)
+                                                       : static_cast<const void*>(M.v64)) &
+            (2 * sizeof(T) - 1)) == 0;
+}
+
 template <class T, bool PRIMAL>
 int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork* f) {
     const DevCsr& M0 = PRIMAL ? a0.AT : a0.A;
@@ -488,7 +609,15 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
     if (p.shrt > 0) {
         const int sb = p.shrt;
         switch (iter_lanes(M)) {
-            case 1: fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
+            case 1:
+                if (pairs_ok<T>(M)) {
+                    const int64_t need = (static_cast<int64_t>(M.rows) + kBlock - 1) / kBlock;
+                    const int pb = static_cast<int>(need < g_cap_pair[pi] ? need : g_cap_pair[pi]);
+                    fast_iter_pairs<T, PRIMAL><<<pb, kBlock, 0, s>>>(a, first, reset_short);
+                } else {
+                    fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short);
+                }
+                break;
             case 2: fast_iter<T, 2, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 4: fast_iter<T, 4, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 8: fast_iter<T, 8, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
@@ -519,33 +648,37 @@ __device__ __forceinline__ void row_terms(const FastCheck<T>& a, int i, double a
                                           double act_a, double inv, Terms& t) {
     constexpr bool INF = (F & kCheckInf) != 0;
     constexpr bool L2 = (F & kCheckL2) != 0;
+    constexpr bool ONE = (F & kCheckOne) != 0;  // the current point's terms are not formed
     const DevProblem& P = a.P;
     a.cs.act_avg[i] = act_a;
     const double lo = P.rlo[i], hi = P.rhi[i];
-    const double yc = static_cast<double>(a.it.y[i]);
-    const double ya = avg_y(a.it, i, inv);
-    t.cp = smax(t.cp, primal_term(act_c, lo, hi));
+    const double yc = ONE ? 0.0 : static_cast<double>(a.it.y[i]);
+    const double ya = avg_y<T, ONE>(a.it, i, inv);
+    if (!ONE) t.cp = smax(t.cp, primal_term(act_c, lo, hi));
     t.ap = smax(t.ap, primal_term(act_a, lo, hi));
-    t.cd = smax(t.cd, cs_term(yc, act_c, lo, hi, a.tol));
+    if (!ONE) t.cd = smax(t.cd, cs_term(yc, act_c, lo, hi, a.tol));
     t.ad = smax(t.ad, cs_term(ya, act_a, lo, hi, a.tol));
     const double rs = P.rs[i];
     const double lo_o = P.rlo_o[i], hi_o = P.rhi_o[i];
     const double aoc = act_c / rs, aoa = act_a / rs;
-    t.ocp = smax(t.ocp, primal_term(aoc, lo_o, hi_o));
+    if (!ONE) t.ocp = smax(t.ocp, primal_term(aoc, lo_o, hi_o));
     t.oap = smax(t.oap, primal_term(aoa, lo_o, hi_o));
-    t.ocd = smax(t.ocd, cs_term(yc * rs, aoc, lo_o, hi_o, a.bound_tol));
+    if (!ONE) t.ocd = smax(t.ocd, cs_term(yc * rs, aoc, lo_o, hi_o, a.bound_tol));
     t.oad = smax(t.oad, cs_term(ya * rs, aoa, lo_o, hi_o, a.bound_tol));
     if (a.termination_rule != 0) {  // internal (minimize) sense: y_int = y_s * rs
-        t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
+        if (!ONE) t.dobj_c += clipped_inf(yc * rs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ya * rs, lo_o, hi_o);
     }
     if (L2) {  // termination rule 2: squares of the row violation and of y's sign violation
-        const double pc = primal_term(aoc, lo_o, hi_o), pa = primal_term(aoa, lo_o, hi_o);
-        const double dc = sign_violation(yc * rs, lo_o, hi_o);
+        const double pa = primal_term(aoa, lo_o, hi_o);
         const double da = sign_violation(ya * rs, lo_o, hi_o);
-        t.ppc += pc * pc;
+        if (!ONE) {
+            const double pc = primal_term(aoc, lo_o, hi_o);
+            const double dc = sign_violation(yc * rs, lo_o, hi_o);
+            t.ppc += pc * pc;
+            t.ddc += dc * dc;
+        }
         t.ppa += pa * pa;
-        t.ddc += dc * dc;
         t.dda += da * da;
     }
     if (INF) {  // the change of y since the previous check, original units
@@ -562,28 +695,33 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
                                           double aty_a, double inv, Terms& t) {
     constexpr bool INF = (F & kCheckInf) != 0;
     constexpr bool L2 = (F & kCheckL2) != 0;
+    constexpr bool ONE = (F & kCheckOne) != 0;  // the current point's terms are not formed
     const DevProblem& P = a.P;
     const double cj = P.c[j];
     const double lo = P.lo[j], hi = P.hi[j];
-    const double xc = static_cast<double>(a.it.x[j]);
-    const double xa = avg_x(a.it, j, inv);
+    const double xc = ONE ? 0.0 : static_cast<double>(a.it.x[j]);
+    const double xa = avg_x<T, ONE>(a.it, j, inv);
     const double rc = cj - aty_c, ra = cj - aty_a;
-    t.cd = smax(t.cd, cs_term(rc, xc, lo, hi, a.tol));
+    if (!ONE) t.cd = smax(t.cd, cs_term(rc, xc, lo, hi, a.tol));
     t.ad = smax(t.ad, cs_term(ra, xa, lo, hi, a.tol));
     const double cs = P.cs[j];
     const double lo_o = P.lo_o[j], hi_o = P.hi_o[j];
-    t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol));
+    if (!ONE) t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol));
     t.oad = smax(t.oad, cs_term(ra / cs, xa * cs, lo_o, hi_o, a.bound_tol));
     if (L2) {  // termination rule 2: squares of the reduced cost's sign violation
-        const double dc = sign_violation(rc / cs, lo_o, hi_o);
+        if (!ONE) {
+            const double dc = sign_violation(rc / cs, lo_o, hi_o);
+            t.ddc += dc * dc;
+        }
         const double da = sign_violation(ra / cs, lo_o, hi_o);
-        t.ddc += dc * dc;
         t.dda += da * da;
     }
     if (a.termination_rule != 0) {  // internal sense: c_int x = sign c_o x, r_int = r_s / cs
-        t.pobj_c += P.obj_sign * P.c_o[j] * (xc * cs);
+        if (!ONE) {
+            t.pobj_c += P.obj_sign * P.c_o[j] * (xc * cs);
+            t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
+        }
         t.pobj_a += P.obj_sign * P.c_o[j] * (xa * cs);
-        t.dobj_c += clipped_inf(rc / cs, lo_o, hi_o);
         t.dobj_a += clipped_inf(ra / cs, lo_o, hi_o);
     }
     if (INF) {  // d = A_o^T dy_o = sign (A_s^T dy_s) / cs, by linearity
@@ -635,18 +773,19 @@ __device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
 
 // Products of entries [k, e) (stride `step`) of a row of A (ROWS: with the
 // current x and the Cesaro average of x) or of A^T (with y and its average).
-template <class T, bool ROWS>
+// ONE: only the average (T(z) of the Halpern iteration) is measured.
+template <class T, bool ROWS, bool ONE>
 __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr& M, int k, int e,
                                              int step, double inv, double& ac, double& aa) {
     for (; k < e; k += step) {
         const int j = M.ci[k];
         const double v = M.v64[k];
         if (ROWS) {
-            ac += v * cur_x(a.it, j);
-            aa += v * avg_x(a.it, j, inv);
+            if (!ONE) ac += v * cur_x(a.it, j);
+            aa += v * avg_x<T, ONE>(a.it, j, inv);
         } else {
-            ac += v * cur_y(a.it, j);
-            aa += v * avg_y(a.it, j, inv);
+            if (!ONE) ac += v * cur_y(a.it, j);
+            aa += v * avg_y<T, ONE>(a.it, j, inv);
         }
     }
 }
@@ -672,7 +811,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         if (r >= M.rows) return;
         const int b = M.rp[r], e = M.rp[r + 1];
         if (e - b > M.short_max) return;
-        row_products<T, ROWS>(a, M, b + lane, e, vw, inv, ac, aa);
+        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, b + lane, e, vw, inv, ac, aa);
         ac = group_sum(ac, vw);
         aa = group_sum(aa, vw);
         if (lane == 0) row_or_col_terms<T, ROWS, F>(a, r, ac, aa, inv, t);
@@ -681,7 +820,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         if (w >= M.n_warp0) return;
         const int r = M.warp_rows0[w];
         const int lane = threadIdx.x & 31;
-        row_products<T, ROWS>(a, M, M.rp[r] + lane, M.rp[r + 1], 32, inv, ac, aa);
+        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, M.rp[r] + lane, M.rp[r + 1], 32, inv, ac, aa);
         for (int o = 16; o > 0; o >>= 1) {
             ac += __shfl_xor_sync(0xffffffffu, ac, o);
             aa += __shfl_xor_sync(0xffffffffu, aa, o);
@@ -690,7 +829,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
     } else {
         const int idx = vb - sb - wb;
         const int4 w = M.items_long.item[idx];
-        row_products<T, ROWS>(a, M, w.y + threadIdx.x, w.z, kBlock, inv, ac, aa);
+        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, w.y + threadIdx.x, w.z, kBlock, inv, ac, aa);
         ac = block_total(ac);
         aa = block_total(aa);
         if (w.w >= 0 && !segment_finish(M.items_long, idx, w.w, ac, aa, &ac, &aa)) return;
@@ -706,6 +845,7 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
 // check's own ticket and partials.
 template <class T, bool ROWS, int F>
 __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, double inv, Terms& t) {
+    constexpr bool ONE = (F & kCheckOne) != 0;
     const RowSlices& S = M.slices;
     const int idx = vb * (kBlock / 32) + (threadIdx.x >> 5);
     if (idx >= S.n_item) return;  // warp-uniform
@@ -729,11 +869,11 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
             if (ROWS) {
-                ac += v[u] * cur_x(a.it, j[u]);
-                aa += v[u] * avg_x(a.it, j[u], inv);
+                if (!ONE) ac += v[u] * cur_x(a.it, j[u]);
+                aa += v[u] * avg_x<T, ONE>(a.it, j[u], inv);
             } else {
-                ac += v[u] * cur_y(a.it, j[u]);
-                aa += v[u] * avg_y(a.it, j[u], inv);
+                if (!ONE) ac += v[u] * cur_y(a.it, j[u]);
+                aa += v[u] * avg_y<T, ONE>(a.it, j[u], inv);
             }
         }
     }
@@ -741,11 +881,11 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
         const int j = __ldcs(col + 32 * static_cast<int64_t>(k));
         const double v = __ldcs(val + 32 * static_cast<int64_t>(k));
         if (ROWS) {
-            ac += v * cur_x(a.it, j);
-            aa += v * avg_x(a.it, j, inv);
+            if (!ONE) ac += v * cur_x(a.it, j);
+            aa += v * avg_x<T, ONE>(a.it, j, inv);
         } else {
-            ac += v * cur_y(a.it, j);
-            aa += v * avg_y(a.it, j, inv);
+            if (!ONE) ac += v * cur_y(a.it, j);
+            aa += v * avg_y<T, ONE>(a.it, j, inv);
         }
     }
     if (w.w >= 0) {  // warp-uniform
@@ -812,10 +952,11 @@ inline DevCsr check_view(const DevCsr& M) {
 // 109-118 registers and two CTAs per SM. The instance with the infeasibility
 // tests (INF) carries 11 more running terms: two CTAs per SM.
 template <class T, int F>
-__global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 ? 4 : 3))
+__global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 || (F & kCheckOne)) ? 4 : 3)
     fast_check(FastCheck<T> a) {
     constexpr bool INF = (F & kCheckInf) != 0;
     constexpr bool L2 = (F & kCheckL2) != 0;
+    constexpr bool ONE = (F & kCheckOne) != 0;
     DevState* st = a.st;
     if (st->done) return;
     const long long k_avg = st->since_restart + a.period_iters;
@@ -832,6 +973,16 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
         else if (bid < nA) check_slices<T, true, F>(a, a.A, bid - pA, inv, t);
         else if (bid < nA + pT) check_part<T, false, F>(a, a.AT, bid - nA, sbT, wbT, inv, t);
         else check_slices<T, false, F>(a, a.AT, bid - nA - pT, inv, t);
+    }
+    if (ONE) {  // the current point's slots carry the measured point's terms
+        t.cp = t.ap;
+        t.cd = t.ad;
+        t.ocp = t.oap;
+        t.ocd = t.oad;
+        t.pobj_c = t.pobj_a;
+        t.dobj_c = t.dobj_a;
+        t.ppc = t.ppa;
+        t.ddc = t.dda;
     }
     block_max_terms<INF>(t, st->acc);
     // per-CTA partial sums, kCheckSums per CTA: the objectives [0..3]
@@ -1169,7 +1320,11 @@ int init_fast_kernels(int device) {
     const int l64 = resident_per_sm(fast_iter_long<double, false, 0, false>);
     const int s32 = resident_per_sm(fast_iter_slices<float, false, false>);
     const int s64 = resident_per_sm(fast_iter_slices<double, false, false>);
-    if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0) return 1;
+    const int p32 = resident_per_sm(fast_iter_pairs<float, true>);
+    const int p64 = resident_per_sm(fast_iter_pairs<double, true>);
+    if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0 || p32 <= 0 || p64 <= 0) return 1;
+    g_cap_pair[0] = p32 * sms;
+    g_cap_pair[1] = p64 * sms;
     g_cap_long[0] = l32 * sms;
     g_cap_long[1] = l64 * sms;
     g_cap_slice[0] = s32 * sms;
@@ -1231,6 +1386,8 @@ void launch_fast_check(const FastCheck<T>& a0, cudaStream_t s) {
         const int rows_grid = (a.A.rows + kBlock / 32 - 1) / (kBlock / 32);
         const int xg = rows_grid < a.grid_cap || a.grid_cap <= 0 ? rows_grid : a.grid_cap;
         fast_xray_rows<T><<<xg > 0 ? xg : 1, kBlock, 0, s>>>(a);
+    } else if (l2 && a.it.halpern) {  // only T(z) is measured
+        fast_check<T, kCheckL2 | kCheckOne><<<grid, kBlock, 0, s>>>(a);
     } else if (l2) {
         fast_check<T, kCheckL2><<<grid, kBlock, 0, s>>>(a);
     } else {

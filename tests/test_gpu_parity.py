@@ -421,6 +421,48 @@ def test_mixed_halpern_reaches_the_fp64_optimum(pkg, orc, engine, name):
     assert abs(o.objective - opt) <= 2e-3 * (1 + abs(opt)), (o.objective, opt)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("max_it", [200_000, 97, 23])
+@pytest.mark.parametrize("name", ["transportation_40x100", "badly_scaled_300x800"])
+def test_lean_halpern_is_the_stored_form(pkg, engine, precision, max_it, name):
+    # Without a trace the Halpern iteration stores no z: the primal pass
+    # rebuilds x from x_bar and the anchor, and T(z) is stored only where a
+    # check or the result reads it (97: a tail after two checks; 23: no check
+    # at all). A trace switches to the stored form. Same kernels' arithmetic,
+    # so the same point bit for bit.
+    fn, args, kw = RULE2_CASES[name]
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    o = dict(precision=precision, termination_rule="relative_kkt_l2", restart_rule="adaptive_l2",
+             primal_weight_update=True, halpern=True, max_iterations=max_it)
+    lean = solve(pkg, engine, p, **o)
+    full = solve(pkg, engine, p, trace_iters=1, **o)
+    assert (lean.status, lean.iterations, lean.restarts) == \
+        (full.status, full.iterations, full.restarts)
+    assert lean.fp64_iterations == full.fp64_iterations
+    np.testing.assert_array_equal(lean.primal, full.primal)
+    np.testing.assert_array_equal(lean.dual, full.dual)
+    assert lean.objective == full.objective
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("demands", [400, 2000])
+def test_dense_rows_match_loaded_columns(pkg, engine, monkeypatch, precision, demands):
+    # The supply rows of a transportation LP sit in consecutive columns: the
+    # long-row paths compute those columns instead of loading them (400
+    # entries: one warp per row; 2,000: CTA items). The sum order is the
+    # same, so the solve matches the one that loads every index bit for bit.
+    p = pkg.lpgen.transportation_lp(40, demands, seed=1000)
+    o = dict(precision=precision, termination_rule="relative_kkt_l2", restart_rule="adaptive_l2",
+             primal_weight_update=True, halpern=True, max_iterations=3000)
+    dense = solve(pkg, engine, p, **o)
+    monkeypatch.setenv("PDHG_B200_DENSE_ROWS", "0")
+    loaded = solve(pkg, engine, p, **o)
+    assert (dense.status, dense.iterations, dense.restarts) == \
+        (loaded.status, loaded.iterations, loaded.restarts)
+    np.testing.assert_array_equal(dense.primal, loaded.primal)
+    np.testing.assert_array_equal(dense.dual, loaded.dual)
+
+
 @pytest.mark.parametrize("halpern", [False, True])
 def test_fp64_warm_start_follows_the_oracle(pkg, orc, engine, halpern):
     # x0 / y0 (original units): x = proj(x0 / col_scale), y = y0 sign / row_scale,
