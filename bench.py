@@ -676,6 +676,7 @@ def main() -> None:
     o.precision, o.tolerance = 1, 1e-12
     o.termination_rule = pkg.pdhg.TERMINATION_RULES[HEADLINE["termination_rule"]]
     o.restart_rule = pkg.pdhg.RESTART_RULES[HEADLINE["restart_rule"]]
+    o.halpern = 1 if HEADLINE["halpern"] else 0
     o.max_iterations = args.iters_per_step
     info = pkg.pdhg._Info()
 

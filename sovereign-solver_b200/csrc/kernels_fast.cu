@@ -53,11 +53,14 @@
 #ifndef PDHG_WARPITEM_MIN_CTAS
 #define PDHG_WARPITEM_MIN_CTAS 4
 #endif
-#ifndef PDHG_PAIR_MIN_CTAS
-#define PDHG_PAIR_MIN_CTAS 8
+#ifndef PDHG_UNIFORM_MIN_CTAS
+#define PDHG_UNIFORM_MIN_CTAS 8
 #endif
-#ifndef PDHG_PAIR_MIN_CTAS_F64
-#define PDHG_PAIR_MIN_CTAS_F64 4
+#ifndef PDHG_UNIFORM_MIN_CTAS_E4
+#define PDHG_UNIFORM_MIN_CTAS_E4 6
+#endif
+#ifndef PDHG_UNIFORM_MIN_CTAS_F64
+#define PDHG_UNIFORM_MIN_CTAS_F64 4
 #endif
 #ifndef PDHG_SLICE_MIN_CTAS
 #define PDHG_SLICE_MIN_CTAS 4
@@ -188,53 +191,112 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_SHORT_MIN_CTAS :
     if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw, a.tz);
 }
 
-// Rows of exactly two entries (rp_stride 2: the columns of a network or
-// transportation LP), a persistent grid (the resident CTAs): each thread walks
-// rows r, r + T, r + 2T, ... (T threads in the grid, so a warp's rows stay
-// consecutive) and pipelines them: the next row's operand, index and value
-// loads are issued before the current row's gathers are consumed, so the
-// streamed arrays stay in flight while the gathers wait. fast_iter (one row
-// per thread) leaves DRAM idle during every thread's gather phase. The
-// arithmetic is fast_iter's two-entry path.
-template <class T, bool PRIMAL>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? PDHG_PAIR_MIN_CTAS : PDHG_PAIR_MIN_CTAS_F64)
-    fast_iter_pairs(FastIter<T> a, int first, int reset) {
-    using P2 = typename Pair<T>::type;
+// E consecutive column indices / values of one lane, as one or two vector loads.
+template <int E>
+__device__ __forceinline__ void load_idx(const int32_t* p, int (&c)[E]) {
+    if constexpr (E == 2) {
+        const int2 q = __ldcs(reinterpret_cast<const int2*>(p));
+        c[0] = q.x;
+        c[1] = q.y;
+    } else {
+        const int4 q = __ldcs(reinterpret_cast<const int4*>(p));
+        c[0] = q.x;
+        c[1] = q.y;
+        c[2] = q.z;
+        c[3] = q.w;
+    }
+}
+template <class T, int E>
+__device__ __forceinline__ void load_vals(const T* p, T (&v)[E]) {
+    if constexpr (std::is_same<T, float>::value) {
+        if constexpr (E == 2) {
+            const float2 q = __ldcs(reinterpret_cast<const float2*>(p));
+            v[0] = q.x;
+            v[1] = q.y;
+        } else {
+            const float4 q = __ldcs(reinterpret_cast<const float4*>(p));
+            v[0] = q.x;
+            v[1] = q.y;
+            v[2] = q.z;
+            v[3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < E / 2; ++h) {
+            const double2 q = __ldcs(reinterpret_cast<const double2*>(p) + h);
+            v[2 * h] = q.x;
+            v[2 * h + 1] = q.y;
+        }
+    }
+}
+
+// Rows of one length S = E * VW (rp_stride 2, 4 or 8: the columns of a
+// network or transportation LP have 2 entries, those of config 2's LP 8), a
+// persistent grid (the resident CTAs): groups of VW lanes, lane l owning the
+// row's entries [l E, (l + 1) E) as one index and one value vector load. Each
+// group walks rows r, r + G, r + 2G, ... (G groups in the grid, so a warp's
+// rows stay consecutive) and pipelines them: the next row's operand, index
+// and value loads are issued before the current row's gathers are used, so
+// the streamed arrays stay in flight while the gathers wait. One row per
+// thread (fast_iter) leaves DRAM idle during every thread's gather phase and
+// while CTAs retire and launch. A lane sums its E products in order, then the
+// group adds its lanes (the two-entry rows' order is fast_iter's).
+template <class T, int E, int VW>
+constexpr int uniform_min_ctas() {
+    return sizeof(T) == 8 ? PDHG_UNIFORM_MIN_CTAS_F64 : (E == 2 ? PDHG_UNIFORM_MIN_CTAS : PDHG_UNIFORM_MIN_CTAS_E4);
+}
+
+template <class T, int E, int VW, bool PRIMAL>
+__global__ void __launch_bounds__(kBlock, (uniform_min_ctas<T, E, VW>()))
+    fast_iter_uniform(FastIter<T> a, int first, int reset) {
+    constexpr int S = E * VW;
     DevState* st = a.st;
     iter_reset(st, reset);
     if (st->done) return;
     const DevCsr& M = PRIMAL ? a.AT : a.A;
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
-    const int2* __restrict__ ci2 = reinterpret_cast<const int2*>(M.ci);
-    const P2* __restrict__ v2 = reinterpret_cast<const P2*>(mvals<T>(M));
+    const T* __restrict__ vals = mvals<T>(M);
     const PV<T> pv = pvec<T>(a.P);
     const bool fresh = first && st->fresh;
     const T tau = static_cast<T>(st->tau), sigma = static_cast<T>(st->sigma);
     const Hw<T> hw = halpern_weight_warp<T>(a.it, st, a.hk);
-    const int stride = gridDim.x * kBlock;
-    int r = blockIdx.x * kBlock + threadIdx.x;
-    if (r >= M.rows) return;
-    EpiIn<T> in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh, hw);
-    int2 c = __ldcs(ci2 + r);
-    P2 v = __ldcs(v2 + r);
+    const int lane = threadIdx.x & (VW - 1);
+    const int groups = gridDim.x * (kBlock / VW);
+    int r = (blockIdx.x * kBlock + static_cast<int>(threadIdx.x)) / VW;
+    if (r >= M.rows) return;  // group-uniform
+    EpiIn<T> in{};
+    if (lane == 0) in = epi_load<T, PRIMAL>(a.it, pv, r, first, fresh, hw);
+    int c[E];
+    T v[E];
+    load_idx<E>(M.ci + static_cast<int64_t>(r) * S + lane * E, c);
+    load_vals<T, E>(vals + static_cast<int64_t>(r) * S + lane * E, v);
     for (;;) {
-        const T g0 = __ldg(xg + c.x), g1 = __ldg(xg + c.y);
-        const int rn = r + stride;
-        const bool more = rn < M.rows;
+        T g[E];
+#pragma unroll
+        for (int q = 0; q < E; ++q) g[q] = __ldg(xg + c[q]);
+        const int rn = r + groups;
+        const bool more = rn < M.rows;  // group-uniform
         EpiIn<T> nin{};
-        int2 nc = make_int2(0, 0);
-        P2 nv{};
+        int nc[E];
+        T nv[E];
         if (more) {
-            nin = epi_load<T, PRIMAL>(a.it, pv, rn, first, fresh, hw);
-            nc = __ldcs(ci2 + rn);
-            nv = __ldcs(v2 + rn);
+            if (lane == 0) nin = epi_load<T, PRIMAL>(a.it, pv, rn, first, fresh, hw);
+            load_idx<E>(M.ci + static_cast<int64_t>(rn) * S + lane * E, nc);
+            load_vals<T, E>(vals + static_cast<int64_t>(rn) * S + lane * E, nv);
         }
-        epi_store<T, PRIMAL>(a.it, r, fma_rn<T>(v.y, g1, mul_rn<T>(v.x, g0)), in, tau, sigma, hw, a.tz);
+        T acc = mul_rn<T>(v[0], g[0]);
+#pragma unroll
+        for (int q = 1; q < E; ++q) acc = fma_rn<T>(v[q], g[q], acc);
+        if (VW > 1) acc = group_sum(acc, VW);
+        if (lane == 0) epi_store<T, PRIMAL>(a.it, r, acc, in, tau, sigma, hw, a.tz);
         if (!more) break;
         r = rn;
         in = nin;
-        c = nc;
-        v = nv;
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            c[q] = nc[q];
+            v[q] = nv[q];
+        }
     }
 }
 
@@ -514,7 +576,10 @@ struct PassPlan {
 // capped at these (set by init_fast_kernels from the occupancy calculator).
 int g_cap_long[2] = {148 * PDHG_LONG_MIN_CTAS, 148 * PDHG_LONG_MIN_CTAS};
 int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};
-int g_cap_pair[2] = {148 * PDHG_PAIR_MIN_CTAS, 148 * PDHG_PAIR_MIN_CTAS_F64};
+// resident CTAs of fast_iter_uniform for rows of 2, 4 and 8 entries, FP32 / FP64
+int g_cap_uni[3][2] = {{148 * PDHG_UNIFORM_MIN_CTAS, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
+                       {148 * PDHG_UNIFORM_MIN_CTAS_E4, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
+                       {148 * PDHG_UNIFORM_MIN_CTAS_E4, 148 * PDHG_UNIFORM_MIN_CTAS_F64}};
 
 inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
     PassPlan p;
@@ -549,14 +614,21 @@ inline int pass_launches(const DevCsr& M0) {
 }
 
 // Returns the number of kernels launched.
-// Every row of exactly two entries, the arrays aligned for the pair loads
-// (a one-lane pass then runs fast_iter_pairs).
+// Every row of 2, 4 or 8 entries, the arrays 16-byte aligned for the vector
+// loads: the pass's short rows run fast_iter_uniform (slot 0, 1, 2), else -1.
 template <class T>
-bool pairs_ok(const DevCsr& M) {
-    return M.rp_stride == 2 && (reinterpret_cast<uintptr_t>(M.ci) & 7u) == 0 &&
-           (reinterpret_cast<uintptr_t>(sizeof(T) == 4 ? static_cast<const void*>(M.v32)
-                                                       : static_cast<const void*>(M.v64)) &
-            (2 * sizeof(T) - 1)) == 0;
+int uniform_slot(const DevCsr& M) {
+    const void* v = sizeof(T) == 4 ? static_cast<const void*>(M.v32) : static_cast<const void*>(M.v64);
+    if (((reinterpret_cast<uintptr_t>(M.ci) | reinterpret_cast<uintptr_t>(v)) & 15u) != 0) return -1;
+    return M.rp_stride == 2 ? 0 : M.rp_stride == 4 ? 1 : M.rp_stride == 8 ? 2 : -1;
+}
+
+template <class T, int E, int VW, bool PRIMAL>
+void launch_uniform(const FastIter<T>& a, const DevCsr& M, int cap, int first, int reset,
+                    cudaStream_t s) {
+    const int64_t need = (static_cast<int64_t>(M.rows) * VW + kBlock - 1) / kBlock;
+    const int grid = static_cast<int>(need < cap ? need : cap);
+    fast_iter_uniform<T, E, VW, PRIMAL><<<grid, kBlock, 0, s>>>(a, first, reset);
 }
 
 template <class T, bool PRIMAL>
@@ -606,18 +678,14 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
         fast_iter_slices<T, PRIMAL, true><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
     else if (p.slc > 0)
         fast_iter_slices<T, PRIMAL, false><<<p.slc, kBlock, 0, ss>>>(a, first, reset_slc);
-    if (p.shrt > 0) {
+    const int us = p.shrt > 0 ? uniform_slot<T>(M) : -1;
+    if (us == 0) launch_uniform<T, 2, 1, PRIMAL>(a, M, g_cap_uni[0][pi], first, reset_short, s);
+    else if (us == 1) launch_uniform<T, 4, 1, PRIMAL>(a, M, g_cap_uni[1][pi], first, reset_short, s);
+    else if (us == 2) launch_uniform<T, 4, 2, PRIMAL>(a, M, g_cap_uni[2][pi], first, reset_short, s);
+    else if (p.shrt > 0) {
         const int sb = p.shrt;
         switch (iter_lanes(M)) {
-            case 1:
-                if (pairs_ok<T>(M)) {
-                    const int64_t need = (static_cast<int64_t>(M.rows) + kBlock - 1) / kBlock;
-                    const int pb = static_cast<int>(need < g_cap_pair[pi] ? need : g_cap_pair[pi]);
-                    fast_iter_pairs<T, PRIMAL><<<pb, kBlock, 0, s>>>(a, first, reset_short);
-                } else {
-                    fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short);
-                }
-                break;
+            case 1: fast_iter<T, 1, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 2: fast_iter<T, 2, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 4: fast_iter<T, 4, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
             case 8: fast_iter<T, 8, PRIMAL><<<sb, kBlock, 0, s>>>(a, first, reset_short); break;
@@ -1320,11 +1388,18 @@ int init_fast_kernels(int device) {
     const int l64 = resident_per_sm(fast_iter_long<double, false, 0, false>);
     const int s32 = resident_per_sm(fast_iter_slices<float, false, false>);
     const int s64 = resident_per_sm(fast_iter_slices<double, false, false>);
-    const int p32 = resident_per_sm(fast_iter_pairs<float, true>);
-    const int p64 = resident_per_sm(fast_iter_pairs<double, true>);
-    if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0 || p32 <= 0 || p64 <= 0) return 1;
-    g_cap_pair[0] = p32 * sms;
-    g_cap_pair[1] = p64 * sms;
+    const int u[3][2] = {{resident_per_sm(fast_iter_uniform<float, 2, 1, true>),
+                          resident_per_sm(fast_iter_uniform<double, 2, 1, true>)},
+                         {resident_per_sm(fast_iter_uniform<float, 4, 1, true>),
+                          resident_per_sm(fast_iter_uniform<double, 4, 1, true>)},
+                         {resident_per_sm(fast_iter_uniform<float, 4, 2, true>),
+                          resident_per_sm(fast_iter_uniform<double, 4, 2, true>)}};
+    for (int q = 0; q < 3; ++q)
+        for (int t = 0; t < 2; ++t) {
+            if (u[q][t] <= 0) return 1;
+            g_cap_uni[q][t] = u[q][t] * sms;
+        }
+    if (l32 <= 0 || l64 <= 0 || s32 <= 0 || s64 <= 0) return 1;
     g_cap_long[0] = l32 * sms;
     g_cap_long[1] = l64 * sms;
     g_cap_slice[0] = s32 * sms;

@@ -444,6 +444,34 @@ def test_lean_halpern_is_the_stored_form(pkg, engine, precision, max_it, name):
     assert lean.objective == full.objective
 
 
+@pytest.mark.parametrize("lp", [("random_equality_lp", (200, 500, 4), dict(seed=31)),
+                                ("badly_scaled_lp", (300, 800, 8), dict(seed=2002)),
+                                ("random_equality_lp", (150, 400, 2), dict(seed=32))])
+def test_uniform_rows_follow_the_oracle(pkg, orc, engine, lp):
+    # every column with 2, 4 or 8 entries: the primal pass runs the persistent
+    # uniform-row kernel (one vector load of indices and of values per lane,
+    # the next row's loads in flight during the current row's gathers)
+    fn, args, kw = lp
+    p = getattr(pkg.lpgen, fn)(*args, **kw)
+    per_col = np.bincount(p.col_idx, minlength=p.n)
+    assert np.all(per_col == args[2])
+    o = orc.oracle_solve(p, termination_rule=2, restart_rule=2, primal_weight_update=1,
+                         halpern=1, max_iterations=200_000)
+    r = solve(pkg, engine, p, precision="fp64", termination_rule="relative_kkt_l2",
+              restart_rule="adaptive_l2", primal_weight_update=True, halpern=True,
+              max_iterations=200_000)
+    assert r.status == o.status == "optimal", (r.status, o.status)
+    assert abs(r.iterations - o.iterations) <= 40, (r.iterations, o.iterations)
+    if r.iterations == o.iterations:
+        assert abs(r.objective - o.objective) <= 1e-8 * max(1.0, abs(o.objective))
+    m = solve(pkg, engine, p, precision="mixed", termination_rule="relative_kkt_l2",
+              restart_rule="adaptive_l2", primal_weight_update=True, halpern=True,
+              max_iterations=200_000)
+    assert m.status == "optimal" and m.relative_kkt < 1e-4
+    opt = highs_optimum(p)
+    assert abs(m.objective - opt) <= 2e-3 * (1 + abs(opt)), (m.objective, opt)
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("demands", [400, 2000])
 def test_dense_rows_match_loaded_columns(pkg, engine, monkeypatch, precision, demands):
