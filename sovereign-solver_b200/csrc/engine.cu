@@ -74,6 +74,8 @@ struct Ctx {
     double bnorm2 = 0, cnorm2 = 0;     // termination rule 2 norms, original space (l2)
     int col_uniform = 0;               // every column has the scaled bounds lo_u, hi_u
     double lo_u = 0, hi_u = 0;
+    int col_uniform_o = 0;             // ... and the original bounds lo_uo, hi_uo
+    double lo_uo = 0, hi_uo = 0;
     double cnorm2_s = 0, bnorm2_s = 0;  // initial primal weight |c|_2 / |b|_2, scaled space
 
     MatDev Ao, ATo, As, ATs;
@@ -162,6 +164,9 @@ struct Ctx {
         P.bnorm2 = bnorm2;
         P.cnorm2 = cnorm2;
         P.col_bounds_uniform = col_uniform;
+        P.col_bounds_uniform_o = col_uniform_o;
+        P.lo_uo = lo_uo;
+        P.hi_uo = hi_uo;
         P.lo_u = lo_u;
         P.hi_u = hi_u;
         return P;
@@ -294,24 +299,32 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
     launch_norms(m, n, c.c_s.p, c.rlo_s.p, c.rhi_s.p, c.c_o.p, c.rlo_o.p, c.rhi_o.p, part.p, is.p, s);
     // columns that all share their scaled bounds (x >= 0 LPs): the iteration
     // kernels then skip the bound loads
+    // (and the check kernels those of the original bounds)
     DBuf<unsigned> uflag;
-    CK(uflag.alloc(1));
-    CK(cudaMemsetAsync(uflag.p, 0, sizeof(unsigned), s));
+    CK(uflag.alloc(2));
+    CK(cudaMemsetAsync(uflag.p, 0, 2 * sizeof(unsigned), s));
     launch_uniform_vec(c.lo_s.p, n, uflag.p, s);
     launch_uniform_vec(c.hi_s.p, n, uflag.p, s);
-    unsigned uh = 1;
-    double b0[2] = {0.0, 0.0};
-    CK(cudaMemcpyAsync(&uh, uflag.p, sizeof uh, cudaMemcpyDeviceToHost, s));
+    launch_uniform_vec(c.lo_o.p, n, uflag.p + 1, s);
+    launch_uniform_vec(c.hi_o.p, n, uflag.p + 1, s);
+    unsigned uh[2] = {1, 1};
+    double b0[4] = {0.0, 0.0, 0.0, 0.0};
+    CK(cudaMemcpyAsync(uh, uflag.p, sizeof uh, cudaMemcpyDeviceToHost, s));
     if (n > 0) {
         CK(cudaMemcpyAsync(&b0[0], c.lo_s.p, sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(&b0[1], c.hi_s.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&b0[2], c.lo_o.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&b0[3], c.hi_o.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
     IntakeState h;
     CK(cudaMemcpyAsync(&h, is.p, sizeof h, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    c.col_uniform = (n > 0 && uh == 0) ? 1 : 0;
+    c.col_uniform = (n > 0 && uh[0] == 0) ? 1 : 0;
     c.lo_u = b0[0];
     c.hi_u = b0[1];
+    c.col_uniform_o = (n > 0 && uh[1] == 0) ? 1 : 0;
+    c.lo_uo = b0[2];
+    c.hi_uo = b0[3];
     pc.mark("scale: bins, vectors");
     c.cnorm2_s = std::sqrt(h.norms[0]);
     c.bnorm2_s = std::sqrt(h.norms[1]);

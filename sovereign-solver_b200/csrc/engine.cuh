@@ -236,6 +236,9 @@ struct DevProblem {
     // the iteration kernels use the two values instead of loading the vectors
     int col_bounds_uniform = 0;
     double lo_u = 0.0, hi_u = 0.0;
+    // ... the original bounds likewise (the check kernels' column terms)
+    int col_bounds_uniform_o = 0;
+    double lo_uo = 0.0, hi_uo = 0.0;
 };
 
 // Iterates. T = double for the FP64 modes, float for the mixed mode; the

@@ -262,6 +262,9 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
                                           const T* __restrict__ v, const T* __restrict__ xg,
                                           int b, int e, int off = 0) {
     constexpr int W = 16 / sizeof(T);
+    constexpr int U = 2;  // vectors of each stream in flight per thread
+    using V = typename Vec16<T>::type;
+    using I = typename std::conditional<W == 4, int4, int2>::type;
     int bA = ((b + W - 1) / W) * W;
     if (bA > e) bA = e;
     const bool va = DENSE && ((bA + off) & (W - 1)) == 0;
@@ -269,58 +272,36 @@ __device__ __forceinline__ T long_row_dot(const int32_t* __restrict__ ci,
     T acc = T(0);
     for (int k = b + threadIdx.x; k < bA; k += kBlock) acc += __ldcs(v + k) * __ldg(xg + col(k));
     const int nvec = (e - bA) / W;
-    if constexpr (W == 4) {
-        const int4* ci4 = reinterpret_cast<const int4*>(ci + bA);
-        const float4* v4 = reinterpret_cast<const float4*>(v + bA);
-        int q = threadIdx.x;
-        // four independent 128-bit loads of each stream in flight per thread
-        for (; q + 3 * kBlock < nvec; q += 4 * kBlock) {
-            float4 w[4];
-            if (DENSE) {
-                float4 g[4];
+    const V* vv = reinterpret_cast<const V*>(v + bA);
+    const I* cc = reinterpret_cast<const I*>(ci + bA);
+    // rounds of up to U vectors per thread, the last round predicated, so a
+    // segment of a few thousand entries takes one or two rounds with all of a
+    // round's loads in flight together (a one-vector remainder loop
+    // serialised them); U = 2 keeps the 40-register kernels free of spills
+    for (int q = threadIdx.x; q < nvec; q += U * kBlock) {
+        V w[U], g[U];
+        I c[U];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    w[u] = __ldcs(v4 + q + u * kBlock);
-                    g[u] = gather16<T>(xg, bA + 4 * (q + u * kBlock), off, va);
-                }
+        for (int u = 0; u < U; ++u) {
+            const bool ok = q + u * kBlock < nvec;
+            const int qq = ok ? q + u * kBlock : 0;
+            w[u] = ok ? __ldcs(vv + qq) : V{};
+            if (DENSE) g[u] = ok ? gather16<T>(xg, bA + W * qq, off, va) : V{};
+            else c[u] = ok ? __ldcs(cc + qq) : I{};
+        }
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < U; ++u) {
+            if (q + u * kBlock >= nvec) continue;
+            if constexpr (W == 4) {
+                if (DENSE) {
                     acc += w[u].x * g[u].x + w[u].y * g[u].y + w[u].z * g[u].z + w[u].w * g[u].w;
-            } else {
-                int4 c[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    c[u] = __ldcs(ci4 + q + u * kBlock);
-                    w[u] = __ldcs(v4 + q + u * kBlock);
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
+                } else {
                     acc += w[u].x * __ldg(xg + c[u].x) + w[u].y * __ldg(xg + c[u].y) +
                            w[u].z * __ldg(xg + c[u].z) + w[u].w * __ldg(xg + c[u].w);
-            }
-        }
-        for (; q < nvec; q += kBlock) {
-            const float4 w = __ldcs(v4 + q);
-            if (DENSE) {
-                const float4 g = gather16<T>(xg, bA + 4 * q, off, va);
-                acc += w.x * g.x + w.y * g.y + w.z * g.z + w.w * g.w;
+                }
             } else {
-                const int4 c = __ldcs(ci4 + q);
-                acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y) + w.z * __ldg(xg + c.z) +
-                       w.w * __ldg(xg + c.w);
-            }
-        }
-    } else {
-        const int2* ci2 = reinterpret_cast<const int2*>(ci + bA);
-        const double2* v2 = reinterpret_cast<const double2*>(v + bA);
-        for (int q = threadIdx.x; q < nvec; q += kBlock) {
-            const double2 w = __ldcs(v2 + q);
-            if (DENSE) {
-                const double2 g = gather16<T>(xg, bA + 2 * q, off, va);
-                acc += w.x * g.x + w.y * g.y;
-            } else {
-                const int2 c = __ldcs(ci2 + q);
-                acc += w.x * __ldg(xg + c.x) + w.y * __ldg(xg + c.y);
+                if (DENSE) acc += w[u].x * g[u].x + w[u].y * g[u].y;
+                else acc += w[u].x * __ldg(xg + c[u].x) + w[u].y * __ldg(xg + c[u].y);
             }
         }
     }

@@ -766,14 +766,16 @@ __device__ __forceinline__ void col_terms(const FastCheck<T>& a, int j, double a
     constexpr bool ONE = (F & kCheckOne) != 0;  // the current point's terms are not formed
     const DevProblem& P = a.P;
     const double cj = P.c[j];
-    const double lo = P.lo[j], hi = P.hi[j];
+    const double lo = P.col_bounds_uniform ? P.lo_u : P.lo[j];
+    const double hi = P.col_bounds_uniform ? P.hi_u : P.hi[j];
     const double xc = ONE ? 0.0 : static_cast<double>(a.it.x[j]);
     const double xa = avg_x<T, ONE>(a.it, j, inv);
     const double rc = cj - aty_c, ra = cj - aty_a;
     if (!ONE) t.cd = smax(t.cd, cs_term(rc, xc, lo, hi, a.tol));
     t.ad = smax(t.ad, cs_term(ra, xa, lo, hi, a.tol));
     const double cs = P.cs[j];
-    const double lo_o = P.lo_o[j], hi_o = P.hi_o[j];
+    const double lo_o = P.col_bounds_uniform_o ? P.lo_uo : P.lo_o[j];
+    const double hi_o = P.col_bounds_uniform_o ? P.hi_uo : P.hi_o[j];
     if (!ONE) t.ocd = smax(t.ocd, cs_term(rc / cs, xc * cs, lo_o, hi_o, a.bound_tol));
     t.oad = smax(t.oad, cs_term(ra / cs, xa * cs, lo_o, hi_o, a.bound_tol));
     if (L2) {  // termination rule 2: squares of the reduced cost's sign violation
@@ -841,12 +843,14 @@ __device__ void block_max_terms(const Terms& t, unsigned long long* acc) {
 
 // Products of entries [k, e) (stride `step`) of a row of A (ROWS: with the
 // current x and the Cesaro average of x) or of A^T (with y and its average).
-// ONE: only the average (T(z) of the Halpern iteration) is measured.
+// ONE: only the average (T(z) of the Halpern iteration) is measured. A dense
+// row (off set) computes its columns k + off.
 template <class T, bool ROWS, bool ONE>
 __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr& M, int k, int e,
-                                             int step, double inv, double& ac, double& aa) {
+                                             int step, double inv, double& ac, double& aa,
+                                             int off = kNotDense) {
     for (; k < e; k += step) {
-        const int j = M.ci[k];
+        const int j = off != kNotDense ? k + off : M.ci[k];
         const double v = M.v64[k];
         if (ROWS) {
             if (!ONE) ac += v * cur_x(a.it, j);
@@ -871,13 +875,19 @@ __device__ __forceinline__ void row_or_col_terms(const FastCheck<T>& a, int r, d
 template <class T, bool ROWS, int F>
 __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int sb, int wb,
                            double inv, Terms& t) {
+    constexpr bool ONE = (F & kCheckOne) != 0;
     double ac = 0.0, aa = 0.0;
     if (vb < sb) {
         const int vw = M.vw;
         const int lane = threadIdx.x & (vw - 1);
         const int r = (vb * kBlock + threadIdx.x) / vw;
         if (r >= M.rows) return;
-        const int b = M.rp[r], e = M.rp[r + 1];
+        // the one-point instance also skips what the LP's structure makes
+        // constant (row extents of equal-length rows, dense rows' columns);
+        // in the others the extra registers would spill
+        const bool st = ONE && M.rp_stride > 0;
+        const int b = st ? r * M.rp_stride : M.rp[r];
+        const int e = st ? b + M.rp_stride : M.rp[r + 1];
         if (e - b > M.short_max) return;
         row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, b + lane, e, vw, inv, ac, aa);
         ac = group_sum(ac, vw);
@@ -888,7 +898,8 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
         if (w >= M.n_warp0) return;
         const int r = M.warp_rows0[w];
         const int lane = threadIdx.x & 31;
-        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, M.rp[r] + lane, M.rp[r + 1], 32, inv, ac, aa);
+        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, M.rp[r] + lane, M.rp[r + 1], 32, inv, ac, aa,
+                                                    ONE && M.dense_off ? M.dense_off[r] : kNotDense);
         for (int o = 16; o > 0; o >>= 1) {
             ac += __shfl_xor_sync(0xffffffffu, ac, o);
             aa += __shfl_xor_sync(0xffffffffu, aa, o);
@@ -897,7 +908,8 @@ __device__ void check_part(const FastCheck<T>& a, const DevCsr& M, int vb, int s
     } else {
         const int idx = vb - sb - wb;
         const int4 w = M.items_long.item[idx];
-        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, w.y + threadIdx.x, w.z, kBlock, inv, ac, aa);
+        row_products<T, ROWS, (F & kCheckOne) != 0>(a, M, w.y + threadIdx.x, w.z, kBlock, inv, ac, aa,
+                                                    ONE && M.dense_off ? M.dense_off[w.x] : kNotDense);
         ac = block_total(ac);
         aa = block_total(aa);
         if (w.w >= 0 && !segment_finish(M.items_long, idx, w.w, ac, aa, &ac, &aa)) return;
