@@ -94,6 +94,7 @@ struct Ctx {
     DBuf<float> xa32, sa32, ya32;
     DBuf<double> act_avg, cand_xo, cand_yo, part, bx, by, xo, yo, rc, trow, tcol;
     DBuf<double> pw_u, pw_v, pw_w, pw_part, pw_out, x0s, y0s;
+    DBuf<int> pw_stop;
     DBuf<double> x_last, y_last;  // restart points (primal-weight update)
     DBuf<double> ray_yp, ray_atyp, ray_y;  // infeasibility test: previous y, A^T y; dy (original)
     DBuf<double> xray_xp, xray_d0, xray_d1;  // ray test: previous x; two projected rays (scaled)
@@ -346,6 +347,11 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
 
 // estimate_operator_norm (pdhg.cpp:48-79) with the exact kernels; the scalar
 // tail (sqrt, 1/x) runs on the host exactly as in the reference.
+// The power iteration of pdhg.cpp:50-78 with the reference's arithmetic
+// (ordered sums, pairwise norms, IEEE square roots and divisions). Its scalar
+// steps run on the device (k_pw_norm_w / _e), so the loop issues every
+// iteration without waiting on the host; a device flag stands in for the
+// loop's two early exits and turns the remaining launches into no-ops.
 int operator_norm(Ctx& c, int iterations, double* out) {
     cudaStream_t s = c.stream;
     const int32_t n = c.lp.n, m = c.lp.m;
@@ -354,36 +360,34 @@ int operator_norm(Ctx& c, int iterations, double* out) {
     CK(c.pw_w.alloc(static_cast<size_t>(m) + 1));
     const int64_t ps = std::max(pairwise_partial_size(n), pairwise_partial_size(m));
     CK(c.pw_part.alloc(static_cast<size_t>(ps)));
-    CK(c.pw_out.alloc(4));
+    CK(c.pw_out.alloc(8));  // [0..1] norms' squares, [4..6] the scalar state
+    CK(c.pw_stop.alloc(1));
     launch_fill(c.pw_u.p, n, 1.0, s);
     launch_fill(c.pw_v.p, m, 1.0, s);
     launch_fill(c.pw_w.p, m, 0.0, s);
+    launch_fill(c.pw_out.p, 8, 0.0, s);
+    CK(cudaMemsetAsync(c.pw_stop.p, 0, sizeof(int), s));
     const DevCsr A = c.As.view(), AT = c.ATs.view();
-    double estimate = 0.0;
-    double h[2];
+    double* dots = c.pw_out.p;
+    double* st = c.pw_out.p + 4;
+    int* stop = c.pw_stop.p;
     for (int it = 0; it < iterations; ++it) {
-        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s);
-        launch_pairwise_dot(c.pw_w.p, c.pw_w.p, m, c.pw_part.p, c.pw_out.p, s);
-        CK(cudaMemcpyAsync(h, c.pw_out.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        const double wn = std::sqrt(h[0]);
-        if (wn < 1e-300) break;
-        launch_scale(c.pw_w.p, m, 1.0 / wn, s);
-        launch_pw_u(AT, c.pw_w.p, c.pw_u.p, s);
-        if (m > 0)
-            CK(cudaMemcpyAsync(c.pw_v.p, c.pw_w.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
-        launch_pairwise_dot(c.pw_u.p, c.pw_u.p, n, c.pw_part.p, c.pw_out.p, s);
-        launch_pairwise_dot(c.pw_v.p, c.pw_v.p, m, c.pw_part.p, c.pw_out.p + 1, s);
-        CK(cudaMemcpyAsync(h, c.pw_out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        const double un = std::sqrt(h[0]);
-        const double vn = std::sqrt(h[1]);
-        estimate = std::sqrt(un * un + vn * vn);
-        if (estimate < 1e-300) break;
-        launch_scale(c.pw_u.p, n, 1.0 / estimate, s);
-        launch_scale(c.pw_v.p, m, 1.0 / estimate, s);
+        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s, stop);
+        launch_pairwise_dot(c.pw_w.p, c.pw_w.p, m, c.pw_part.p, dots, s);
+        launch_pw_norm_w(dots, st, stop, s);
+        launch_scale_by(c.pw_w.p, m, st, stop, s);
+        launch_pw_u(AT, c.pw_w.p, c.pw_u.p, s, stop);
+        launch_copy_unless(c.pw_v.p, c.pw_w.p, m, stop, s);
+        launch_pairwise_dot(c.pw_u.p, c.pw_u.p, n, c.pw_part.p, dots, s);
+        launch_pairwise_dot(c.pw_v.p, c.pw_v.p, m, c.pw_part.p, dots + 1, s);
+        launch_pw_norm_e(dots, st, stop, s);
+        launch_scale_by(c.pw_u.p, n, st + 2, stop, s);
+        launch_scale_by(c.pw_v.p, m, st + 2, stop, s);
     }
     CK(cudaGetLastError());
+    double estimate = 0.0;
+    CK(cudaMemcpyAsync(&estimate, st + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     *out = estimate;
     return PDHG_OK;
 }

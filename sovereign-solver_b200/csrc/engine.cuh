@@ -380,9 +380,17 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
                          double* out, cudaStream_t s);
 int64_t pairwise_partial_size(int64_t n);
 // Power-iteration pieces (estimate_operator_norm, pdhg.cpp:48-79).
-void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s);
-void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s);
+// stop: a device flag that turns the launch into a no-op (null: always run)
+void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s,
+                 const int* stop = nullptr);
+void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s,
+                 const int* stop = nullptr);
 void launch_scale(double* x, int64_t n, double alpha, cudaStream_t s);
+// the power iteration's scalar steps on the device (k_pw_norm_w / _e)
+void launch_pw_norm_w(const double* dot, double* st, int* stop, cudaStream_t s);
+void launch_pw_norm_e(const double* dots, double* st, int* stop, cudaStream_t s);
+void launch_scale_by(double* x, int64_t n, const double* alpha, const int* stop, cudaStream_t s);
+void launch_copy_unless(double* dst, const double* src, int64_t n, const int* stop, cudaStream_t s);
 void launch_fill(double* x, int64_t n, double v, cudaStream_t s);
 
 struct FinalArgs {

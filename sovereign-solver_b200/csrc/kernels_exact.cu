@@ -394,7 +394,8 @@ __global__ void __launch_bounds__(kBlock) ex_restart(ExactCheck a) {
 
 // w = -(A u) + v  (spmv(A, -1, u, 0, w) then axpy(1, v, w), pdhg.cpp:59-60)
 __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, const double* v,
-                                                 double* w) {
+                                                 double* w, const int* stop) {
+    if (stop != nullptr && *stop) return;
     const RowTask t = row_task(A, blockIdx.x);
     if (t.row < 0) return;
     const double sum = row_dot(t, A, [u](int j) { return u[j]; }, 0.0);
@@ -403,11 +404,50 @@ __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, cons
 
 // u = A^T (-w) via spmv_transpose(A, -1, w, 0, u) (pdhg.cpp:67): u starts at
 // 0 and adds val * (-w_r) in row order.
-__global__ void __launch_bounds__(kBlock) k_pw_u(DevCsr AT, const double* w, double* u) {
+__global__ void __launch_bounds__(kBlock) k_pw_u(DevCsr AT, const double* w, double* u,
+                                                 const int* stop) {
+    if (stop != nullptr && *stop) return;
     const RowTask t = row_task(AT, blockIdx.x);
     if (t.row < 0) return;
     const double sum = row_dot(t, AT, [w](int i) { return -w[i]; }, 0.0);
     if (t.lead) u[t.row] = sum;
+}
+
+// The power iteration's scalar steps on the device (pdhg.cpp:58-75, the
+// host's arithmetic: IEEE square roots and divisions, no contraction), so the
+// loop runs without a host round trip. st[0] = 1 / ||w||, st[1] = the
+// estimate, st[2] = 1 / estimate; *stop = 1 where the host loop breaks
+// (||w|| or the estimate below 1e-300), after which every step is a no-op.
+__global__ void k_pw_norm_w(const double* dot, double* st, int* stop) {
+    if (*stop) return;
+    const double wn = sqrt(dot[0]);
+    if (wn < 1e-300) {
+        *stop = 1;
+        return;
+    }
+    st[0] = 1.0 / wn;
+}
+__global__ void k_pw_norm_e(const double* dots, double* st, int* stop) {
+    if (*stop) return;
+    const double un = sqrt(dots[0]), vn = sqrt(dots[1]);
+    const double est = sqrt(__dadd_rn(__dmul_rn(un, un), __dmul_rn(vn, vn)));
+    st[1] = est;
+    if (est < 1e-300) {
+        *stop = 1;
+        return;
+    }
+    st[2] = 1.0 / est;
+}
+__global__ void k_scale_by(double* x, int64_t n, const double* alpha, const int* stop) {
+    if (*stop) return;
+    const double a = *alpha;
+    const int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    if (t < n) x[t] = __dmul_rn(x[t], a);
+}
+__global__ void k_copy_unless(double* dst, const double* src, int64_t n, const int* stop) {
+    if (*stop) return;
+    const int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
+    if (t < n) dst[t] = src[t];
 }
 
 __global__ void k_scale(double* x, int64_t n, double alpha) {
@@ -425,8 +465,8 @@ __global__ void k_fill(double* x, int64_t n, double v) {
 // At depth d every node has size floor or ceil of n / 2^d, so the nodes of
 // depth D-1 (D = first depth whose sizes are all <= 128) are either leaves
 // (size <= 128) or parents of two leaves, and every node above is internal.
-// Kernel 1 evaluates depth D-1 (one thread per node); kernel 2 folds the
-// levels pairwise, left + right, exactly like the recursion.
+// Kernel 1 evaluates depth D-1 (k_pw_level_staged); kernel 2 folds the levels
+// pairwise, left + right, exactly like the recursion.
 __host__ __device__ inline void pw_node(int64_t n, int depth, int64_t idx, int64_t* off,
                                         int64_t* size) {
     int64_t o = 0, s = n;
@@ -443,25 +483,44 @@ __host__ __device__ inline void pw_node(int64_t n, int depth, int64_t idx, int64
     *size = s;
 }
 
-__device__ __forceinline__ double pw_leaf(const double* x, const double* y, int64_t o,
-                                          int64_t s) {
-    double acc = 0.0;
-    for (int64_t i = 0; i < s; ++i) acc = __dadd_rn(acc, __dmul_rn(x[o + i], y[o + i]));
-    return acc;
-}
-
-__global__ void k_pw_level(const double* x, const double* y, int64_t n, int depth,
-                           double* out) {
-    const int64_t t = blockIdx.x * static_cast<int64_t>(kBlock) + threadIdx.x;
-    if (t >= (int64_t{1} << depth)) return;
-    int64_t o, s;
-    pw_node(n, depth, t, &o, &s);
-    if (s <= 128) {
-        out[t] = pw_leaf(x, y, o, s);
-    } else {
-        const int64_t h = s / 2;
-        out[t] = __dadd_rn(pw_leaf(x, y, o, h), pw_leaf(x, y, o + h, s - h));
+// The nodes of depth D-1, 32 consecutive nodes per CTA: their entries form
+// one contiguous range of at most 32 x 256 products, which all 256 threads
+// load with coalesced reads into shared memory; then thread l adds the
+// products of node l in index order (its left and right leaf sums, then
+// their sum), the recursion's sequence of additions for that node, so the
+// result is identical. (One thread per node reading its ~150 consecutive
+// entries from global memory alone made every warp-wide load touch 32 lines;
+// one warp per 32 nodes streaming the range in chunks left most lanes idle
+// while the others added.)
+constexpr int kPwNodes = 32;
+constexpr int kPwMaxNode = 256;  // a depth D-1 node: at most two leaves of 128
+__global__ void __launch_bounds__(kBlock) k_pw_level_staged(const double* x, const double* y,
+                                                            int64_t n, int depth, double* out) {
+    extern __shared__ double prod[];
+    __shared__ int64_t off[kPwNodes + 1];
+    const int64_t nodes = int64_t{1} << depth;
+    const int64_t t0 = static_cast<int64_t>(blockIdx.x) * kPwNodes;
+    const int cnt = nodes - t0 < kPwNodes ? static_cast<int>(nodes - t0) : kPwNodes;
+    int64_t o = 0, sz = 0;
+    if (threadIdx.x < cnt) {
+        pw_node(n, depth, t0 + threadIdx.x, &o, &sz);
+        off[threadIdx.x] = o;
+        if (threadIdx.x == cnt - 1) off[cnt] = o + sz;
     }
+    __syncthreads();
+    const int64_t r0 = off[0], len = off[cnt] - r0;
+#pragma unroll 4
+    for (int64_t i = threadIdx.x; i < len; i += kBlock) prod[i] = __dmul_rn(x[r0 + i], y[r0 + i]);
+    __syncthreads();
+    if (threadIdx.x >= cnt) return;
+    const double* p = prod + (o - r0);
+    const int h = sz <= 128 ? static_cast<int>(sz) : static_cast<int>(sz / 2);
+    double accl = 0.0, accr = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < h; ++i) accl = __dadd_rn(accl, p[i]);
+#pragma unroll 8
+    for (int i = h; i < static_cast<int>(sz); ++i) accr = __dadd_rn(accr, p[i]);
+    out[t0 + threadIdx.x] = sz <= 128 ? accl : __dadd_rn(accl, accr);
 }
 
 int pw_depth(int64_t n) {
@@ -809,7 +868,14 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
     const int64_t count = int64_t{1} << d;
     double* a = partial;
     double* b = partial + count;
-    k_pw_level<<<grid64(count), kBlock, 0, s>>>(x, y, n, d, a);
+    // the CTA's range: 32 nodes of at most ceil(n / 2^d) <= 256 entries
+    const int64_t per = (n + count - 1) / count;
+    const size_t smem = sizeof(double) * static_cast<size_t>(kPwNodes * per);
+    if (smem > 48 * 1024)  // up to 64 KB: above the default dynamic limit
+        cudaFuncSetAttribute(k_pw_level_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(sizeof(double) * kPwNodes * kPwMaxNode));
+    k_pw_level_staged<<<static_cast<unsigned>((count + kPwNodes - 1) / kPwNodes), kBlock, smem, s>>>(
+        x, y, n, d, a);
     int lvl = d;
     for (; lvl > 10; --lvl) {  // wide levels: one launch each
         const int64_t half = int64_t{1} << (lvl - 1);
@@ -821,14 +887,27 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
     k_pw_fold_tail<<<1, 512, 0, s>>>(a, b, lvl, out);  // the last <= 1024 values in one CTA
 }
 
-void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s) {
-    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w);
+void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s,
+                 const int* stop) {
+    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop);
 }
-void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s) {
-    if (AT.rows > 0) k_pw_u<<<mat_blocks(AT), kBlock, 0, s>>>(AT, w, u);
+void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s, const int* stop) {
+    if (AT.rows > 0) k_pw_u<<<mat_blocks(AT), kBlock, 0, s>>>(AT, w, u, stop);
 }
 void launch_scale(double* x, int64_t n, double alpha, cudaStream_t s) {
     if (n > 0) k_scale<<<grid64(n), kBlock, 0, s>>>(x, n, alpha);
+}
+void launch_pw_norm_w(const double* dot, double* st, int* stop, cudaStream_t s) {
+    k_pw_norm_w<<<1, 1, 0, s>>>(dot, st, stop);
+}
+void launch_pw_norm_e(const double* dots, double* st, int* stop, cudaStream_t s) {
+    k_pw_norm_e<<<1, 1, 0, s>>>(dots, st, stop);
+}
+void launch_scale_by(double* x, int64_t n, const double* alpha, const int* stop, cudaStream_t s) {
+    if (n > 0) k_scale_by<<<grid64(n), kBlock, 0, s>>>(x, n, alpha, stop);
+}
+void launch_copy_unless(double* dst, const double* src, int64_t n, const int* stop, cudaStream_t s) {
+    if (n > 0) k_copy_unless<<<grid64(n), kBlock, 0, s>>>(dst, src, n, stop);
 }
 void launch_fill(double* x, int64_t n, double v, cudaStream_t s) {
     if (n > 0) k_fill<<<grid64(n), kBlock, 0, s>>>(x, n, v);
