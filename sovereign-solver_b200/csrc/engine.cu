@@ -366,13 +366,14 @@ int operator_norm(Ctx& c, int iterations, double* out) {
     launch_fill(c.pw_v.p, m, 1.0, s);
     launch_fill(c.pw_w.p, m, 0.0, s);
     launch_fill(c.pw_out.p, 8, 0.0, s);
+    launch_fill(c.pw_out.p + 6, 1, 1.0, s);  // u's scale before the first iteration
     CK(cudaMemsetAsync(c.pw_stop.p, 0, sizeof(int), s));
     const DevCsr A = c.As.view(), AT = c.ATs.view();
     double* dots = c.pw_out.p;
     double* st = c.pw_out.p + 4;
     int* stop = c.pw_stop.p;
     for (int it = 0; it < iterations; ++it) {
-        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s, stop);
+        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s, stop, st + 2);  // u scaled where gathered
         launch_pairwise_dot(c.pw_w.p, c.pw_w.p, m, c.pw_part.p, dots, s);
         launch_pw_norm_w(dots, st, stop, s);
         launch_scale_by(c.pw_w.p, m, st, stop, s);
@@ -381,7 +382,6 @@ int operator_norm(Ctx& c, int iterations, double* out) {
         launch_pairwise_dot(c.pw_u.p, c.pw_u.p, n, c.pw_part.p, dots, s);
         launch_pairwise_dot(c.pw_v.p, c.pw_v.p, m, c.pw_part.p, dots + 1, s);
         launch_pw_norm_e(dots, st, stop, s);
-        launch_scale_by(c.pw_u.p, n, st + 2, stop, s);
         launch_scale_by(c.pw_v.p, m, st + 2, stop, s);
     }
     CK(cudaGetLastError());

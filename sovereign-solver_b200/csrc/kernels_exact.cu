@@ -392,13 +392,20 @@ __global__ void __launch_bounds__(kBlock) ex_restart(ExactCheck a) {
 // Setup: power iteration pieces and the exact pairwise norm
 // ---------------------------------------------------------------------------
 
-// w = -(A u) + v  (spmv(A, -1, u, 0, w) then axpy(1, v, w), pdhg.cpp:59-60)
+// w = -(A u) + v  (spmv(A, -1, u, 0, w) then axpy(1, v, w), pdhg.cpp:59-60).
+// uscale (null: 1): u is read as u * uscale, the previous iteration's scaling
+// of u by 1 / estimate (pdhg.cpp:75) applied where u is gathered -- the same
+// rounded value as the scaled vector, without a pass over u.
 __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, const double* v,
-                                                 double* w, const int* stop) {
+                                                 double* w, const int* stop, const double* uscale) {
     if (stop != nullptr && *stop) return;
     const RowTask t = row_task(A, blockIdx.x);
     if (t.row < 0) return;
-    const double sum = row_dot(t, A, [u](int j) { return u[j]; }, 0.0);
+    const double us = uscale != nullptr ? *uscale : 1.0;
+    const auto g = [u, us](int j) { return __dmul_rn(u[j], us); };
+    const double sum = t.warp ? ordered_dot_warp_pipelined(A.rp[t.row], A.rp[t.row + 1], A.ci, A.v64, g,
+                                                           0.0, warp_stage2())
+                              : row_dot(t, A, g, 0.0);
     if (t.lead) w[t.row] = __dadd_rn(-sum, v[t.row]);
 }
 
@@ -888,8 +895,8 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
 }
 
 void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s,
-                 const int* stop) {
-    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop);
+                 const int* stop, const double* uscale) {
+    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop, uscale);
 }
 void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s, const int* stop) {
     if (AT.rows > 0) k_pw_u<<<mat_blocks(AT), kBlock, 0, s>>>(AT, w, u, stop);

@@ -88,6 +88,92 @@ __device__ __forceinline__ double ordered_sum_warp(int b, int e, Term term, doub
     return acc;
 }
 
+// The ordered dot of a long row by one warp with the loads pipelined
+// ahead of the additions: acc = init, then acc = acc + v[k] * g(ci[k]) in k
+// order, each product and sum rounded -- the sequence of ordered_dot, so the
+// result is bit for bit the same. Rounds of kStage terms (four per lane): the
+// indices and values of round r + 2 and the gathers of round r + 1 are in
+// flight while the lanes add round r from shared memory (two buffers of
+// kStage doubles per warp), so only the chain of additions is exposed.
+// ordered_sum_warp evaluates a round's terms (index load, then gather) and
+// only then adds it.
+template <class G>
+__device__ __forceinline__ double ordered_dot_warp_pipelined(int b, int e,
+                                                             const int32_t* __restrict__ ci,
+                                                             const double* __restrict__ v, G g,
+                                                             double init, double* stage2) {
+    constexpr int Q = kStage / 32;
+    const int lane = threadIdx.x & 31;
+    double acc = init;
+    if (b >= e) return acc;
+    auto load_cv = [&](int k0, int (&c)[Q], double (&w)[Q]) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int k = k0 + 32 * q + lane;
+            c[q] = k < e ? ci[k] : 0;
+            w[q] = k < e ? v[k] : 0.0;
+        }
+    };
+    // round 0's terms into buffer 0; round 1's indices and values in registers
+    int c1[Q];
+    double w1[Q];
+    {
+        int c0[Q];
+        double w0[Q], t0[Q];
+        load_cv(b, c0, w0);
+        load_cv(b + kStage, c1, w1);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) t0[q] = b + 32 * q + lane < e ? __dmul_rn(w0[q], g(c0[q])) : 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) stage2[32 * q + lane] = t0[q];
+    }
+    __syncwarp();
+    int buf = 0;
+    for (int k0 = b; k0 < e; k0 += kStage) {
+        const int cnt = min(kStage, e - k0);
+        const int ka = k0 + kStage;  // round r + 1
+        // round r + 1's gathers and round r + 2's indices and values
+        double g1[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g1[q] = ka + 32 * q + lane < e ? g(c1[q]) : 0.0;
+        int c2[Q];
+        double w2[Q];
+        load_cv(ka + kStage, c2, w2);
+        // add round r
+        const double* cur = stage2 + buf * kStage;
+        if (cnt == kStage) {
+            const double2* s2 = reinterpret_cast<const double2*>(cur);
+#pragma unroll 8
+            for (int i = 0; i < kStage / 2; ++i) {
+                const double2 p = s2[i];
+                acc = __dadd_rn(acc, p.x);
+                acc = __dadd_rn(acc, p.y);
+            }
+        } else {
+            for (int i = 0; i < cnt; ++i) acc = __dadd_rn(acc, cur[i]);
+        }
+        // round r + 1's terms into the other buffer
+        double* nxt = stage2 + (buf ^ 1) * kStage;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            nxt[32 * q + lane] = ka + 32 * q + lane < e ? __dmul_rn(w1[q], g1[q]) : 0.0;
+        __syncwarp();  // every lane has added `cur` and written `nxt`
+        buf ^= 1;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            c1[q] = c2[q];
+            w1[q] = w2[q];
+        }
+    }
+    return acc;
+}
+
+// Two rounds of kStage doubles per warp for ordered_dot_warp_pipelined.
+__device__ __forceinline__ double* warp_stage2() {
+    __shared__ __align__(16) double stage2[kWarps][2 * kStage];
+    return stage2[threadIdx.x >> 5];
+}
+
 // Row assignment of the ordered kernels over one matrix: rows of at most
 // kWarpRow entries take one thread each (blocks [0, ordered_blocks(rows))); the
 // longer rows listed in M.wrows take one warp each (the next warp_blocks(M)
