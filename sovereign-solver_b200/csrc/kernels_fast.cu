@@ -418,17 +418,13 @@ __device__ __forceinline__ const double* slice_vals<double>(const RowSlices& S) 
 
 // Lane l's dot product over steps [k0, k1) of a slice (k below kend), in
 // rounds of eight: the next round's index and value loads are issued before
-// this round's gathers. AFF: the slice's columns are base + l + k * stride
-// (checked entry by entry at load), computed instead of loaded.
-template <class T, bool AFF>
+// this round's gathers.
+template <class T>
 __device__ __forceinline__ T slice_dot(const RowSlices& S, int off, int k0s, int k1, int kend, int lane,
-                                       const T* __restrict__ xg, int2 af) {
+                                       const T* __restrict__ xg) {
     const int32_t* __restrict__ col = S.col + off + lane;
     const T* __restrict__ val = slice_vals<T>(S) + off + lane;
-    const int abase = af.x + lane;
-    auto colk = [&](int k) -> int {
-        return AFF ? abase + k * af.y : __ldcs(col + 32 * static_cast<int64_t>(k));
-    };
+    auto colk = [&](int k) -> int { return __ldcs(col + 32 * static_cast<int64_t>(k)); };
     T acc = T(0);
     int c[8];
     T v[8];
@@ -459,6 +455,33 @@ __device__ __forceinline__ T slice_dot(const RowSlices& S, int off, int k0s, int
     return acc;
 }
 
+// The same dot over an affine slice (columns base + l + k stride, checked
+// entry by entry at load): both streams, the lane-interleaved values and
+// x_bar, have computed addresses, so a lane keeps 16 (FP64: 8) steps of both
+// in flight per round; the sum runs in k order like slice_dot's.
+template <class T>
+__device__ __forceinline__ T slice_dot_affine(const RowSlices& S, int off, int k0s, int k1, int kend,
+                                              int lane, const T* __restrict__ xg, int2 af) {
+    constexpr int U = sizeof(T) == 4 ? 16 : 8;
+    const T* __restrict__ val = slice_vals<T>(S) + off + lane;
+    const T* __restrict__ g = xg + af.x + lane;
+    T acc = T(0);
+    for (int k0 = k0s; k0 < k1; k0 += U) {
+        T v[U], x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            const bool ok = k < kend;
+            v[u] = ok ? __ldcs(val + 32 * static_cast<int64_t>(k)) : T(0);
+            x[u] = ok ? __ldg(g + static_cast<int64_t>(k) * af.y) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < kend) acc += v[u] * x[u];
+    }
+    return acc;
+}
+
 // One warp item of the row slices (warp-uniform): entries [k0, k1) of one
 // slice, lane l on the slice's row l, in rounds of eight steps; each step is
 // one coalesced index load, one coalesced value load and one gather per lane.
@@ -478,8 +501,8 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
     const T* __restrict__ xg = PRIMAL ? a.it.y : a.it.xbar;
     // an affine slice's columns are computed, not loaded (warp-uniform)
     const int2 af = __ldg(S.affine + w.x);
-    T acc = af.y > 0 ? slice_dot<T, true>(S, d.y, w.y, w.z, kend, lane, xg, af)
-                     : slice_dot<T, false>(S, d.y, w.y, w.z, kend, lane, xg, af);
+    T acc = af.y > 0 ? slice_dot_affine<T>(S, d.y, w.y, w.z, kend, lane, xg, af)
+                     : slice_dot<T>(S, d.y, w.y, w.z, kend, lane, xg);
     if (w.w >= 0) {
         S.part[32 * static_cast<int64_t>(idx) + lane] = static_cast<double>(acc);
         __threadfence();
@@ -936,6 +959,11 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
     const int kend = min(w.z, __ldg(S.rlen + 32 * w.x + lane));
     const int32_t* __restrict__ col = S.col + d.y + lane;
     const double* __restrict__ val = S.v64 + d.y + lane;
+    // the one-point instance computes an affine slice's columns (warp-uniform)
+    const int2 af = ONE ? __ldg(S.affine + w.x) : make_int2(0, 0);
+    auto colk = [&](int kk) -> int {
+        return af.y > 0 ? af.x + lane + kk * af.y : __ldcs(col + 32 * static_cast<int64_t>(kk));
+    };
     double ac = 0.0, aa = 0.0;
     int k = w.y;
     for (; k + 2 <= kend; k += 2) {
@@ -943,7 +971,7 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
         double v[2];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-            j[u] = __ldcs(col + 32 * static_cast<int64_t>(k + u));
+            j[u] = colk(k + u);
             v[u] = __ldcs(val + 32 * static_cast<int64_t>(k + u));
         }
 #pragma unroll
@@ -958,7 +986,7 @@ __device__ void check_slices(const FastCheck<T>& a, const DevCsr& M, int vb, dou
         }
     }
     for (; k < kend; ++k) {
-        const int j = __ldcs(col + 32 * static_cast<int64_t>(k));
+        const int j = colk(k);
         const double v = __ldcs(val + 32 * static_cast<int64_t>(k));
         if (ROWS) {
             if (!ONE) ac += v * cur_x(a.it, j);
