@@ -62,6 +62,10 @@
 #ifndef PDHG_UNIFORM_MIN_CTAS_F64
 #define PDHG_UNIFORM_MIN_CTAS_F64 4
 #endif
+// FP32 slice kernel without the warp items: 40 registers, no spill
+#ifndef PDHG_SLICE_MIN_CTAS_NW
+#define PDHG_SLICE_MIN_CTAS_NW 6
+#endif
 #ifndef PDHG_SLICE_MIN_CTAS
 #define PDHG_SLICE_MIN_CTAS 4
 #endif
@@ -537,7 +541,8 @@ __device__ __forceinline__ void slice_item(const FastIter<T>& a, const RowSlices
 // goes on past the slice items into the warp items of the other long rows, so
 // one kernel and one tail cover every long row of the pass.
 template <class T, bool PRIMAL, bool WITEMS>
-__global__ void __launch_bounds__(kBlock, PDHG_SLICE_MIN_CTAS)
+__global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && !WITEMS) ? PDHG_SLICE_MIN_CTAS_NW
+                                                                      : PDHG_SLICE_MIN_CTAS)
     fast_iter_slices(FastIter<T> a, int first, int reset) {
     DevState* st = a.st;
     iter_reset(st, reset);
@@ -598,13 +603,14 @@ struct PassPlan {
 // CTA-item kernel without warp rows and the row-slice kernel. Their grids are
 // capped at these (set by init_fast_kernels from the occupancy calculator).
 int g_cap_long[2] = {148 * PDHG_LONG_MIN_CTAS, 148 * PDHG_LONG_MIN_CTAS};
-int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};
+int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS_NW, 148 * PDHG_SLICE_MIN_CTAS};
+int g_cap_slice_w[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};  // with warp items
 // resident CTAs of fast_iter_uniform for rows of 2, 4 and 8 entries, FP32 / FP64
 int g_cap_uni[3][2] = {{148 * PDHG_UNIFORM_MIN_CTAS, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
                        {148 * PDHG_UNIFORM_MIN_CTAS_E4, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
                        {148 * PDHG_UNIFORM_MIN_CTAS_E4, 148 * PDHG_UNIFORM_MIN_CTAS_F64}};
 
-inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
+inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice, int cap_slice_w) {
     PassPlan p;
     if (M.rows == 0) return p;
     p.shrt = short_blocks_for(M);
@@ -615,7 +621,7 @@ inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
     if (mode == 2 && sliced) {
         // the slice kernel takes the warp items too (fast_iter_slices)
         p.warp = 0;
-        p.slc = std::min((M.slices.n_item + nw + kBlock / 32 - 1) / (kBlock / 32), std::max(cap_slice, 1));
+        p.slc = std::min((M.slices.n_item + nw + kBlock / 32 - 1) / (kBlock / 32), std::max(cap_slice_w, 1));
         return p;
     }
     if (mode == 2) {
@@ -632,7 +638,7 @@ inline PassPlan pass_plan(const DevCsr& M, int cap_long, int cap_slice) {
 
 // Kernels one pass over M launches besides the flag reset.
 inline int pass_launches(const DevCsr& M0) {
-    const PassPlan p = pass_plan(pass_matrix(M0), 1, 1);
+    const PassPlan p = pass_plan(pass_matrix(M0), 1, 1, 1);
     return (p.shrt > 0 ? 1 : 0) + (p.lng > 0 ? 1 : 0) + (p.slc > 0 ? 1 : 0);
 }
 
@@ -668,7 +674,7 @@ int launch_iter(const FastIter<T>& a0, int first, cudaStream_t s, const PassFork
     DevCsr& M = PRIMAL ? a.AT : a.A;
     M = pass_matrix(M0);
     const int pi = sizeof(T) == 4 ? 0 : 1;
-    const PassPlan p = pass_plan(M, g_cap_long[pi], g_cap_slice[pi]);
+    const PassPlan p = pass_plan(M, g_cap_long[pi], g_cap_slice[pi], g_cap_slice_w[pi]);
     const int mode = M.long_mode;
     // the flag reset rides on the first kernel of the period's first pass
     const int rs = PRIMAL && first ? 1 : 0;
@@ -1444,6 +1450,11 @@ int init_fast_kernels(int device) {
     g_cap_long[1] = l64 * sms;
     g_cap_slice[0] = s32 * sms;
     g_cap_slice[1] = s64 * sms;
+    const int w32 = resident_per_sm(fast_iter_slices<float, false, true>);
+    const int w64 = resident_per_sm(fast_iter_slices<double, false, true>);
+    if (w32 <= 0 || w64 <= 0) return 1;
+    g_cap_slice_w[0] = w32 * sms;
+    g_cap_slice_w[1] = w64 * sms;
     return 0;
 }
 

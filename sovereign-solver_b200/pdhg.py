@@ -12,6 +12,7 @@ compiled library and a CUDA device, and fails loudly without them.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import ctypes as C
 import os
 from dataclasses import dataclass, field, fields
@@ -299,18 +300,31 @@ def stack_batch(problems: list[Problem]) -> dict:
     col_idx = np.empty(nnz, dtype=np.int32)
     vec = {name: np.empty(size, dtype=np.float64) for name, size in
            (("val", nnz), ("c", n), ("col_lo", n), ("col_hi", n), ("row_lo", m), ("row_hi", m))}
-    for k, p in enumerate(problems):
-        r0, r1 = int(row_off64[k]), int(row_off64[k + 1])
-        c0, c1 = int(col_off64[k]), int(col_off64[k + 1])
-        z0, z1 = int(nz_off[k]), int(nz_off[k + 1])
-        np.add(p.row_ptr[:-1], z0, out=row_ptr[r0:r1], casting="unsafe")
-        np.add(p.col_idx, c0, out=col_idx[z0:z1], casting="unsafe")
-        vec["val"][z0:z1] = p.val
-        vec["c"][c0:c1] = p.c
-        vec["col_lo"][c0:c1] = p.col_lo
-        vec["col_hi"][c0:c1] = p.col_hi
-        vec["row_lo"][r0:r1] = p.row_lo
-        vec["row_hi"][r0:r1] = p.row_hi
+    def fill(ks: range) -> None:
+        for k in ks:
+            p = problems[k]
+            r0, r1 = int(row_off64[k]), int(row_off64[k + 1])
+            c0, c1 = int(col_off64[k]), int(col_off64[k + 1])
+            z0, z1 = int(nz_off[k]), int(nz_off[k + 1])
+            np.add(p.row_ptr[:-1], z0, out=row_ptr[r0:r1], casting="unsafe")
+            np.add(p.col_idx, c0, out=col_idx[z0:z1], casting="unsafe")
+            vec["val"][z0:z1] = p.val
+            vec["c"][c0:c1] = p.c
+            vec["col_lo"][c0:c1] = p.col_lo
+            vec["col_hi"][c0:c1] = p.col_hi
+            vec["row_lo"][r0:r1] = p.row_lo
+            vec["row_hi"][r0:r1] = p.row_hi
+
+    # the copies are memory-bound and numpy releases the GIL for them: the
+    # instances are filled by a few threads in contiguous runs
+    workers = max(1, min(16, os.cpu_count() or 1, len(problems) // 64))
+    if workers == 1:
+        fill(range(len(problems)))
+    else:
+        bounds = np.searchsorted(nz_off, np.linspace(0, nnz, workers + 1)).tolist()
+        bounds[0], bounds[-1] = 0, len(problems)
+        with concurrent.futures.ThreadPoolExecutor(workers) as pool:
+            list(pool.map(fill, [range(bounds[i], bounds[i + 1]) for i in range(workers)]))
     row_ptr[m] = nnz
     return {"row_off": row_off64.astype(np.int32), "col_off": col_off64.astype(np.int32),
             "nnz": nnz, "row_ptr": row_ptr, "col_idx": col_idx, **vec,
