@@ -605,6 +605,8 @@ struct PassPlan {
 int g_cap_long[2] = {148 * PDHG_LONG_MIN_CTAS, 148 * PDHG_LONG_MIN_CTAS};
 int g_cap_slice[2] = {148 * PDHG_SLICE_MIN_CTAS_NW, 148 * PDHG_SLICE_MIN_CTAS};
 int g_cap_slice_w[2] = {148 * PDHG_SLICE_MIN_CTAS, 148 * PDHG_SLICE_MIN_CTAS};  // with warp items
+// resident CTAs of the one-point check kernel, FP32 / FP64
+int g_cap_check1[2] = {148 * 4, 148 * 4};
 // resident CTAs of fast_iter_uniform for rows of 2, 4 and 8 entries, FP32 / FP64
 int g_cap_uni[3][2] = {{148 * PDHG_UNIFORM_MIN_CTAS, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
                        {148 * PDHG_UNIFORM_MIN_CTAS_E4, 148 * PDHG_UNIFORM_MIN_CTAS_F64},
@@ -1056,6 +1058,77 @@ inline DevCsr check_view(const DevCsr& M) {
     return X;
 }
 
+// The one-point check over the rows of A^T (the columns of A) when every
+// row has S = 2 or 4 entries: each thread walks rows j, j + T, j + 2T, ...
+// (T threads in the grid) and issues the next row's index and value loads
+// (vector loads) before it gathers the current row's y and forms its column
+// terms, so the streamed arrays stay in flight while the gathers wait. The
+// products are added in k order, as row_products does with one lane per row.
+template <int S>
+__device__ __forceinline__ void load_col_row(const DevCsr& M, int j, int (&c)[S], double (&v)[S]) {
+    const int64_t b = static_cast<int64_t>(j) * S;
+    if constexpr (S == 2) {
+        const int2 q = __ldcs(reinterpret_cast<const int2*>(M.ci + b));
+        const double2 w = __ldcs(reinterpret_cast<const double2*>(M.v64 + b));
+        c[0] = q.x;
+        c[1] = q.y;
+        v[0] = w.x;
+        v[1] = w.y;
+    } else {
+        const int4 q = __ldcs(reinterpret_cast<const int4*>(M.ci + b));
+        const double2 w0 = __ldcs(reinterpret_cast<const double2*>(M.v64 + b));
+        const double2 w1 = __ldcs(reinterpret_cast<const double2*>(M.v64 + b) + 1);
+        c[0] = q.x;
+        c[1] = q.y;
+        c[2] = q.z;
+        c[3] = q.w;
+        v[0] = w0.x;
+        v[1] = w0.y;
+        v[2] = w1.x;
+        v[3] = w1.y;
+    }
+}
+
+template <class T, int F, int S>
+__device__ void check_uniform_cols(const FastCheck<T>& a, double inv, Terms& t) {
+    const DevCsr& M = a.AT;
+    const int stride = gridDim.x * kBlock;
+    int j = blockIdx.x * kBlock + threadIdx.x;
+    if (j >= M.rows) return;
+    int c[S];
+    double v[S];
+    load_col_row<S>(M, j, c, v);
+    for (;;) {
+        double g[S];
+#pragma unroll
+        for (int q = 0; q < S; ++q) g[q] = avg_y<T, true>(a.it, c[q], inv);
+        const int jn = j + stride;
+        const bool more = jn < M.rows;
+        int nc[S] = {};
+        double nv[S] = {};
+        if (more) load_col_row<S>(M, jn, nc, nv);
+        double aa = 0.0;
+#pragma unroll
+        for (int q = 0; q < S; ++q) aa += v[q] * g[q];
+        col_terms<T, F>(a, j, 0.0, aa, inv, t);
+        if (!more) break;
+        j = jn;
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            c[q] = nc[q];
+            v[q] = nv[q];
+        }
+    }
+}
+
+// A^T rows the one-point check walks with check_uniform_cols: 2 or 4
+// entries each (0: the virtual blocks take them), the arrays aligned.
+__host__ __device__ inline int check_uniform_stride(const DevCsr& M) {
+    if (M.rp_stride != 2 && M.rp_stride != 4) return 0;
+    if (((reinterpret_cast<uintptr_t>(M.ci) | reinterpret_cast<uintptr_t>(M.v64)) & 15u) != 0) return 0;
+    return M.rp_stride;
+}
+
 // Grid-stride over the virtual blocks of A (act = A x, current and average)
 // then of A^T (aty = A^T y); the grid itself is capped (a few CTAs per SM),
 // so each CTA sums its rows into per-thread running terms and takes part in
@@ -1077,8 +1150,11 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
     // Halpern: the sums' slots hold T(z) itself
     const double inv = a.it.halpern ? 1.0 : 1.0 / static_cast<double>(k_avg);
     Terms t;
+    // the one-point instance walks equal-length rows of A^T with the
+    // pipelined loop after the virtual blocks (their short blocks dropped)
+    const int uni = ONE ? check_uniform_stride(a.AT) : 0;
     const int sbA = check_short_blocks(a.A), wbA = check_warp_blocks(a.A);
-    const int sbT = check_short_blocks(a.AT), wbT = check_warp_blocks(a.AT);
+    const int sbT = uni ? 0 : check_short_blocks(a.AT), wbT = check_warp_blocks(a.AT);
     const int pA = sbA + wbA + a.A.items_long.n_item, pT = sbT + wbT + a.AT.items_long.n_item;
     const int nA = pA + check_slice_blocks(a.A);
     const int nT = pT + check_slice_blocks(a.AT);
@@ -1088,6 +1164,8 @@ __global__ void __launch_bounds__(kBlock, (F & kCheckInf) ? 2 : (sizeof(T) == 4 
         else if (bid < nA + pT) check_part<T, false, F>(a, a.AT, bid - nA, sbT, wbT, inv, t);
         else check_slices<T, false, F>(a, a.AT, bid - nA - pT, inv, t);
     }
+    if (uni == 2) check_uniform_cols<T, F, 2>(a, inv, t);
+    else if (uni == 4) check_uniform_cols<T, F, 4>(a, inv, t);
     if (ONE) {  // the current point's slots carry the measured point's terms
         t.cp = t.ap;
         t.cd = t.ad;
@@ -1450,6 +1528,11 @@ int init_fast_kernels(int device) {
     g_cap_long[1] = l64 * sms;
     g_cap_slice[0] = s32 * sms;
     g_cap_slice[1] = s64 * sms;
+    const int k32 = resident_per_sm(fast_check<float, kCheckL2 | kCheckOne>);
+    const int k64 = resident_per_sm(fast_check<double, kCheckL2 | kCheckOne>);
+    if (k32 <= 0 || k64 <= 0) return 1;
+    g_cap_check1[0] = k32 * sms;
+    g_cap_check1[1] = k64 * sms;
     const int w32 = resident_per_sm(fast_iter_slices<float, false, true>);
     const int w64 = resident_per_sm(fast_iter_slices<double, false, true>);
     if (w32 <= 0 || w64 <= 0) return 1;
@@ -1504,8 +1587,14 @@ void launch_fast_check(const FastCheck<T>& a0, cudaStream_t s) {
     a.AT = check_view(a0.AT);
     int grid = check_blocks(a.A) + check_blocks(a.AT);
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
-    if (grid == 0) grid = 1;
     const bool l2 = a.termination_rule == 2;
+    // the one-point instance's pipelined column walk: at most one wave of
+    // resident CTAs (only ever fewer CTAs than the grid the per-CTA partial
+    // sums are allocated for, fast_check_grid)
+    const int pi = sizeof(T) == 4 ? 0 : 1;
+    if (l2 && a.it.halpern && !a.infeas && check_uniform_stride(a.AT) && grid > g_cap_check1[pi])
+        grid = g_cap_check1[pi];
+    if (grid == 0) grid = 1;
     if (a.infeas) {
         if (l2) fast_check<T, kCheckInf | kCheckL2><<<grid, kBlock, 0, s>>>(a);
         else fast_check<T, kCheckInf><<<grid, kBlock, 0, s>>>(a);
