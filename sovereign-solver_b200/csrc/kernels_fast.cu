@@ -880,6 +880,23 @@ template <class T, bool ROWS, bool ONE>
 __device__ __forceinline__ void row_products(const FastCheck<T>& a, const DevCsr& M, int k, int e,
                                              int step, double inv, double& ac, double& aa,
                                              int off = kNotDense) {
+    if constexpr (ONE) {  // rounds of four terms: their loads in flight together, same order
+        for (; k + 3 * step < e; k += 4 * step) {
+            int j[4];
+            double v[4], g[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int kk = k + u * step;
+                j[u] = off != kNotDense ? kk + off : M.ci[kk];
+                v[u] = M.v64[kk];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                g[u] = ROWS ? avg_x<T, true>(a.it, j[u], inv) : avg_y<T, true>(a.it, j[u], inv);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) aa += v[u] * g[u];
+        }
+    }
     for (; k < e; k += step) {
         const int j = off != kNotDense ? k + off : M.ci[k];
         const double v = M.v64[k];
