@@ -36,3 +36,20 @@ def test_stacking_keeps_empty_instances(pkg):
     b = pkg.pdhg.stack_batch([p, empty, p])
     assert list(b["row_off"]) == [0, 5, 5, 10] and list(b["col_off"]) == [0, 12, 12, 24]
     assert np.all(np.diff(b["row_ptr"]) >= 0)
+
+
+def test_threaded_stacking_matches_concatenation(pkg):
+    # enough instances for several filling threads: the result must be the
+    # plain concatenation with rows, columns and entries offset per instance
+    ps = [pkg.lpgen.random_equality_lp(5 + s % 7, 11 + s % 13, 2, seed=s) for s in range(400)]
+    b = pkg.pdhg.stack_batch(ps)
+    roff = np.concatenate([[0], np.cumsum([p.m for p in ps])])
+    coff = np.concatenate([[0], np.cumsum([p.n for p in ps])])
+    zoff = np.concatenate([[0], np.cumsum([p.nnz for p in ps])])
+    rp = np.concatenate([p.row_ptr[:-1] + z for p, z in zip(ps, zoff)] + [[zoff[-1]]])
+    assert np.array_equal(b["row_ptr"], rp)
+    assert np.array_equal(b["col_idx"], np.concatenate([p.col_idx + c for p, c in zip(ps, coff)]))
+    assert np.array_equal(b["val"], np.concatenate([p.val for p in ps]))
+    for f in ("c", "col_lo", "col_hi", "row_lo", "row_hi"):
+        assert np.array_equal(b[f], np.concatenate([getattr(p, f) for p in ps])), f
+    assert np.array_equal(b["row_off"], roff) and np.array_equal(b["col_off"], coff)
