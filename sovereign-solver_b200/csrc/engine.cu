@@ -84,6 +84,7 @@ struct Ctx {
 
     bool have_opnorm = false;
     int opnorm_iters = -1;
+    bool opnorm_fast = false;  // the estimate's rows were summed in parallel (non-exact modes)
     double opnorm = 0;
 
     DBuf<double> x64, xbar64, s64, y64, xsum, ysum;
@@ -352,7 +353,7 @@ int ensure_scaled(Ctx& c, const ScalingParams& sp) {
 // steps run on the device (k_pw_norm_w / _e), so the loop issues every
 // iteration without waiting on the host; a device flag stands in for the
 // loop's two early exits and turns the remaining launches into no-ops.
-int operator_norm(Ctx& c, int iterations, double* out) {
+int operator_norm(Ctx& c, int iterations, bool fast, double* out) {
     cudaStream_t s = c.stream;
     const int32_t n = c.lp.n, m = c.lp.m;
     CK(c.pw_u.alloc(static_cast<size_t>(n) + 1));
@@ -373,7 +374,7 @@ int operator_norm(Ctx& c, int iterations, double* out) {
     double* st = c.pw_out.p + 4;
     int* stop = c.pw_stop.p;
     for (int it = 0; it < iterations; ++it) {
-        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s, stop, st + 2);  // u scaled where gathered
+        launch_pw_w(A, c.pw_u.p, c.pw_v.p, c.pw_w.p, s, stop, st + 2, fast);  // u scaled where gathered
         launch_pairwise_dot(c.pw_w.p, c.pw_w.p, m, c.pw_part.p, dots, s);
         launch_pw_norm_w(dots, st, stop, s);
         launch_scale_by(c.pw_w.p, m, st, stop, s);
@@ -1157,11 +1158,15 @@ int solve(Ctx& c, const pdhg_options& o, pdhg_info* info, double* x, double* y, 
     int rc = ensure_scaled(c, sp);
     if (rc != PDHG_OK) return rc;
     pc.mark("solve: scaling");
-    if (!c.have_opnorm || c.opnorm_iters != o.power_iterations) {
-        rc = operator_norm(c, o.power_iterations, &c.opnorm);
+    // FP64-exact reproduces the reference's estimate bit for bit; the other
+    // modes sum A u's long rows in parallel (the same estimate up to rounding)
+    const bool fast_norm = o.precision != PDHG_PREC_FP64_EXACT;
+    if (!c.have_opnorm || c.opnorm_iters != o.power_iterations || c.opnorm_fast != fast_norm) {
+        rc = operator_norm(c, o.power_iterations, fast_norm, &c.opnorm);
         if (rc != PDHG_OK) return rc;
         c.have_opnorm = true;
         c.opnorm_iters = o.power_iterations;
+        c.opnorm_fast = fast_norm;
     }
     pc.mark("solve: operator norm");
     const double op = c.opnorm;

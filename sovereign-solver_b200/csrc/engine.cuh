@@ -381,8 +381,9 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
 int64_t pairwise_partial_size(int64_t n);
 // Power-iteration pieces (estimate_operator_norm, pdhg.cpp:48-79).
 // stop: a device flag that turns the launch into a no-op (null: always run)
+// fast: the rows' products added in parallel (not the reference's order)
 void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s,
-                 const int* stop = nullptr, const double* uscale = nullptr);
+                 const int* stop = nullptr, const double* uscale = nullptr, bool fast = false);
 void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s,
                  const int* stop = nullptr);
 void launch_scale(double* x, int64_t n, double alpha, cudaStream_t s);

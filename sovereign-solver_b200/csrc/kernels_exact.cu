@@ -396,6 +396,12 @@ __global__ void __launch_bounds__(kBlock) ex_restart(ExactCheck a) {
 // uscale (null: 1): u is read as u * uscale, the previous iteration's scaling
 // of u by 1 / estimate (pdhg.cpp:75) applied where u is gathered -- the same
 // rounded value as the scaled vector, without a pass over u.
+// FAST (the mixed and FP64 modes, whose estimate need not be the
+// reference's bit for bit): a warp row's products are added by its lanes in
+// parallel (four strided partial sums per lane, then a shuffle tree) instead
+// of in the row's order, which takes a long row from a chain of dependent
+// additions to a streaming pass.
+template <bool FAST>
 __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, const double* v,
                                                  double* w, const int* stop, const double* uscale) {
     if (stop != nullptr && *stop) return;
@@ -403,9 +409,27 @@ __global__ void __launch_bounds__(kBlock) k_pw_w(DevCsr A, const double* u, cons
     if (t.row < 0) return;
     const double us = uscale != nullptr ? *uscale : 1.0;
     const auto g = [u, us](int j) { return __dmul_rn(u[j], us); };
-    const double sum = t.warp ? ordered_dot_warp_pipelined(A.rp[t.row], A.rp[t.row + 1], A.ci, A.v64, g,
-                                                           0.0, warp_stage2())
-                              : row_dot(t, A, g, 0.0);
+    double sum;
+    if (FAST && t.warp) {
+        const int lane = threadIdx.x & 31;
+        const int b = A.rp[t.row], e = A.rp[t.row + 1];
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+        int k = b + lane;
+        for (; k + 96 < e; k += 128) {
+            p0 += A.v64[k] * g(A.ci[k]);
+            p1 += A.v64[k + 32] * g(A.ci[k + 32]);
+            p2 += A.v64[k + 64] * g(A.ci[k + 64]);
+            p3 += A.v64[k + 96] * g(A.ci[k + 96]);
+        }
+        for (; k < e; k += 32) p0 += A.v64[k] * g(A.ci[k]);
+        sum = (p0 + p1) + (p2 + p3);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    } else if (t.warp) {
+        sum = ordered_dot_warp_pipelined(A.rp[t.row], A.rp[t.row + 1], A.ci, A.v64, g, 0.0,
+                                         warp_stage2());
+    } else {
+        sum = row_dot(t, A, g, 0.0);
+    }
     if (t.lead) w[t.row] = __dadd_rn(-sum, v[t.row]);
 }
 
@@ -895,8 +919,10 @@ void launch_pairwise_dot(const double* x, const double* y, int64_t n, double* pa
 }
 
 void launch_pw_w(const DevCsr& A, const double* u, const double* v, double* w, cudaStream_t s,
-                 const int* stop, const double* uscale) {
-    if (A.rows > 0) k_pw_w<<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop, uscale);
+                 const int* stop, const double* uscale, bool fast) {
+    if (A.rows == 0) return;
+    if (fast) k_pw_w<true><<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop, uscale);
+    else k_pw_w<false><<<mat_blocks(A), kBlock, 0, s>>>(A, u, v, w, stop, uscale);
 }
 void launch_pw_u(const DevCsr& AT, const double* w, double* u, cudaStream_t s, const int* stop) {
     if (AT.rows > 0) k_pw_u<<<mat_blocks(AT), kBlock, 0, s>>>(AT, w, u, stop);

@@ -208,6 +208,39 @@ def test_edge_sizes(pkg, orc, engine):
     assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
 
 
+def test_power_iteration_early_exit_matches_the_oracle(pkg, orc, engine):
+    # every row of A sums to 1 and nothing is scaled: the power iteration's
+    # first w = -A u + v (u = v = 1) is zero, so the loop stops at once with
+    # the estimate 0 and the step falls back (pdhg.cpp:261-265). The device
+    # loop's early-exit flag must give the oracle's run bit for bit, in every
+    # precision's setup.
+    q = pkg.Problem.from_coo(2, 4, [0, 0, 1, 1], [0, 1, 2, 3], [0.5, 0.5, 0.25, 0.75],
+                             c=np.array([1.0, 2.0, 3.0, 4.0]), col_lo=np.zeros(4),
+                             col_hi=np.ones(4), row_lo=np.array([0.5, 0.5]),
+                             row_hi=np.array([0.5, 0.5]))
+    kw = dict(apply_ruiz=False, apply_pock_chambolle=False, max_iterations=200)
+    o = orc.oracle_solve(q, **kw)
+    r = solve(pkg, engine, q, **kw)
+    assert r.operator_norm_estimate == o.operator_norm_estimate == 0.0
+    assert (r.status, r.iterations, r.objective) == (o.status, o.iterations, o.objective)
+    assert np.array_equal(r.primal, o.primal) and np.array_equal(r.dual, o.dual)
+    for precision in ("mixed", "fp64"):
+        assert solve(pkg, engine, q, precision=precision, **kw).operator_norm_estimate == 0.0
+
+
+def test_parallel_power_iteration_is_the_estimate_up_to_rounding(pkg, orc, engine):
+    # supply rows of 700 entries take the warp rows of A u; FP64-exact sums them
+    # in the reference's order (bit-identical), the mixed and FP64 modes in
+    # parallel partial sums, which may move the estimate by rounding only
+    p = pkg.lpgen.transportation_lp(40, 700, seed=17)
+    o = orc.oracle_solve(p, max_iterations=1)
+    assert solve(pkg, engine, p, max_iterations=1).operator_norm_estimate == \
+        o.operator_norm_estimate
+    for precision in ("mixed", "fp64"):
+        est = solve(pkg, engine, p, precision=precision, max_iterations=1).operator_norm_estimate
+        assert abs(est - o.operator_norm_estimate) <= 1e-12 * o.operator_norm_estimate
+
+
 def test_backend_known_answers(pkg):
     g = load_golden("backend_known_answers")
     A = golden_problem(pkg, g)
