@@ -148,6 +148,68 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlClockSampler:
+    """The same fields read in this process through NVML (a thread polling
+    every 200 ms), without a second process querying the GPU. The device is
+    found by its PCI bus id, so the index under CUDA_VISIBLE_DEVICES does not
+    matter."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples: list[tuple[float, float, int]] = []
+        self.max_mhz = None
+        self.handle = None
+        self.nvml = None
+        self.halt = threading.Event()
+        self.thread = None
+
+    def start(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(self.device)
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+        except Exception:
+            self.handle = None
+            return
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+
+    def _poll(self):
+        n = self.nvml
+        while not self.halt.is_set():
+            try:
+                self.samples.append((n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM),
+                                     n.nvmlDeviceGetPowerUsage(self.handle) / 1e3,
+                                     n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)))
+            except Exception:
+                pass
+            self.halt.wait(0.2)
+
+    def stop(self) -> dict:
+        if self.handle is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable"]}
+        self.halt.set()
+        self.thread.join(timeout=5)
+        n = self.nvml
+        bits = {"hw_slowdown": n.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": n.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": n.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": n.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted(k for k, b in bits.items() if any(s[2] & b for s in self.samples))
+        sm = [s[0] for s in self.samples]
+        try:
+            n.nvmlShutdown()
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sm), "source": "nvml"}
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -577,6 +639,9 @@ def main() -> None:
                          "iterations, nothing else")
     ap.add_argument("--supplies", type=int, default=SUPPLIES)
     ap.add_argument("--demands", type=int, default=DEMANDS)
+    ap.add_argument("--clock-sampler", default="nvidia-smi", choices=["nvidia-smi", "nvml"],
+                    help="how clocks are sampled during the timed region: an nvidia-smi "
+                         "process (-lms 200) or NVML read in this process every 200 ms")
     ap.add_argument("--mps-reader", action="store_true",
                     help="measure the MPS reader instead (host only, one JSON line)")
     ap.add_argument("--mps-ref-supplies", type=int, default=200,
@@ -616,7 +681,7 @@ def main() -> None:
         eng.solve(opts, want_point=False)
     torch.cuda.synchronize()
     barrier(world)
-    sampler = ClockSampler(local)
+    sampler = (NvmlClockSampler if args.clock_sampler == "nvml" else ClockSampler)(local)
     sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
