@@ -264,15 +264,19 @@ def _c_start(o: _Options, keep: list, cancel, x0, y0) -> None:
         o.y0 = _d(y0a)
 
 
-def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray) -> PdhgResult:
-    hp = bool(info.has_point)
-    farkas = STATUS[info.status] == "primal_infeasible"
-    ray = STATUS[info.status] == "dual_infeasible"
+def _result(info: _Info, x: np.ndarray, y: np.ndarray, rc: np.ndarray,
+            want_point: bool = True) -> PdhgResult:
+    """The result of one solve; x, y, rc are the arrays the engine wrote (views
+    into the call's own buffers, handed over without a copy). Without
+    want_point nothing was written and the point fields stay empty."""
+    hp = bool(info.has_point) and want_point
+    farkas = want_point and STATUS[info.status] == "primal_infeasible"
+    ray = want_point and STATUS[info.status] == "dual_infeasible"
     return PdhgResult(
-        farkas=y.copy() if farkas else None, ray=x.copy() if ray else None,
+        farkas=y if farkas else None, ray=x if ray else None,
         status=STATUS[info.status], objective=info.objective,
-        primal=x.copy() if hp else np.zeros(0), dual=y.copy() if hp else np.zeros(0),
-        reduced_costs=rc.copy() if hp else np.zeros(0),
+        primal=x if hp else np.zeros(0), dual=y if hp else np.zeros(0),
+        reduced_costs=rc if hp else np.zeros(0),
         primal_infeasibility=info.primal_infeasibility,
         dual_infeasibility=info.dual_infeasibility, duality_gap=info.duality_gap,
         iterations=info.iterations, restarts=info.restarts, seconds=info.seconds,
@@ -405,14 +409,14 @@ class Engine:
             o.trace_x = _d(tx)
             o.trace_y = _d(ty)
         info = _Info()
-        x = np.zeros(max(p.n, 1))
-        y = np.zeros(max(p.m, 1))
-        rc = np.zeros(max(p.n, 1))
+        # without want_point the engine writes no point: no host buffers of n
+        k_n, k_m = (max(p.n, 1), max(p.m, 1)) if want_point else (1, 1)
+        x, y, rc = np.zeros(k_n), np.zeros(k_m), np.zeros(k_n)
         null = C.cast(None, _dp)
         _check(lib().pdhg_solve(self._h, C.byref(o), C.byref(info),
                                 _d(x) if want_point else null, _d(y) if want_point else null,
                                 _d(rc) if want_point else null), "pdhg_solve", self._h)
-        r = _result(info, x[: p.n], y[: p.m], rc[: p.n])
+        r = _result(info, x[: p.n], y[: p.m], rc[: p.n], want_point)
         if tx is not None:
             r.trace_x = tx[:, : p.n]
             r.trace_y = ty[:, : p.m]
@@ -450,7 +454,8 @@ class Engine:
         count = len(shapes)
         infos = (_Info * count)()
         m, n = int(b["row_off"][-1]), int(b["col_off"][-1])
-        x, y, rc = np.zeros(max(n, 1)), np.zeros(max(m, 1)), np.zeros(max(n, 1))
+        k_n, k_m = (max(n, 1), max(m, 1)) if want_point else (1, 1)
+        x, y, rc = np.zeros(k_n), np.zeros(k_m), np.zeros(k_n)
         null = C.cast(None, _dp)
         _check(lib().pdhg_solve_batch(self._h, C.byref(o), infos,
                                       _d(x) if want_point else null,
@@ -461,7 +466,7 @@ class Engine:
         for k in range(count):
             r0, r1 = int(b["row_off"][k]), int(b["row_off"][k + 1])
             c0, c1 = int(b["col_off"][k]), int(b["col_off"][k + 1])
-            out.append(_result(infos[k], x[c0:c1], y[r0:r1], rc[c0:c1]))
+            out.append(_result(infos[k], x[c0:c1], y[r0:r1], rc[c0:c1], want_point))
         return out
 
     def start_kkt(self, x0: list[np.ndarray] | None = None,

@@ -101,3 +101,26 @@ def test_header_documents_each_entry_with_a_reference_citation():
             "pdhg_csr_spmv_noalloc", "pdhg_get_tuning", "pdhg_get_batch_tuning",
             "pdhg_gemm_bf16") or \
             n.startswith("pdhg_mlp_"), n  # the warm start's network: no reference counterpart
+
+
+def test_results_hand_over_the_written_point_and_nothing_else(pkg):
+    # the result owns views of the buffers the engine wrote (no second copy of
+    # a 10M-column point); without want_point the engine wrote nothing and the
+    # point fields stay empty, whatever has_point says
+    P = pkg.pdhg
+    info = P._Info()
+    info.status = P.STATUS.index("iteration_limit")
+    info.has_point = 1
+    x, y, rc = np.arange(6.0), np.arange(3.0), -np.arange(6.0)
+    r = P._result(info, x[:5], y[:2], rc[:5])
+    assert r.primal.base is x and r.dual.base is y and r.reduced_costs.base is rc
+    assert np.array_equal(r.primal, x[:5]) and r.farkas is None and r.ray is None
+    r = P._result(info, x[:5], y[:2], rc[:5], want_point=False)
+    assert r.primal.size == r.dual.size == r.reduced_costs.size == 0
+    info.status = P.STATUS.index("primal_infeasible")
+    info.has_point = 0
+    assert np.array_equal(P._result(info, x, y, rc).farkas, y)
+    assert P._result(info, x, y, rc, want_point=False).farkas is None
+    info.status = P.STATUS.index("dual_infeasible")
+    assert np.array_equal(P._result(info, x, y, rc).ray, x)
+    assert P._result(info, x, y, rc, want_point=False).ray is None
