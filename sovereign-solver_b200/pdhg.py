@@ -384,6 +384,10 @@ class Engine:
     def solve(self, opt: PdhgOptions | None = None, cancel: CancellationToken | None = None,
               x0: np.ndarray | None = None, y0: np.ndarray | None = None,
               want_point: bool = True) -> PdhgResult:
+        """``sov::Pdhg::solve`` (pdhg.cpp:218-502) on the loaded problem. With
+        ``want_point`` False the engine downloads no point: ``primal``,
+        ``dual``, ``reduced_costs``, ``farkas`` and ``ray`` stay empty and
+        only the scalar fields are filled (the form timed loops use)."""
         if self.problem is None:
             raise PdhgError(3, "Engine.solve: no problem loaded")
         p = self.problem
