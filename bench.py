@@ -485,7 +485,9 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
     c by ~10%). Training solves from the batched engine, basis + network
     (tensor-core training), then on held-out parameters: plain single-LP GPU
     PDHG from the cold start, batched cold, and batched with the gated learned
-    warm start. Solves/s include, for the warm line, prediction and gating."""
+    warm start and the cold fallback past the family's iteration budget.
+    Solves/s include, for the warm line, prediction, gating and the fallback's
+    cold solves."""
     W = pkg.warmstart
     fam = pkg.lpgen.parametric_family(500, 1200, 5, seed=4001)
     opt = pkg.PdhgOptions(precision="mixed", primal_weight_update=True, tolerance=1e-4,
@@ -508,7 +510,7 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
         t_cold = time.perf_counter() - t0
         t0 = time.perf_counter()
         x0s, y0s, used, kw, kc = ws.starts(e, te, te_th, opt)
-        warm = W.solve_family(e, te, opt, x0s, y0s)
+        warm = W.solve_family_with_fallback(e, te, opt, x0s, y0s, ws.budget)
         t_warm = time.perf_counter() - t0
         t0 = time.perf_counter()
         plain = []
@@ -549,6 +551,13 @@ def warmstart_line(pkg, eng, args, rank: int) -> dict:
                                      "iterations_median": float(np.median(it_w)),
                                      "iterations_max": int(it_w.max()),
                                      "at_cap": int((it_w >= cap).sum()),
+                                     "fallback": {"budget": int(ws.budget),
+                                                  "solved_again_cold": int((it_w > ws.budget).sum()),
+                                                  "rule": "a warm solve gets the most iterations "
+                                                          "any training solve needed; one not "
+                                                          "optimal by then is solved again from "
+                                                          "the cold start (iterations of both "
+                                                          "attempts counted)"},
                                      "max_relative_kkt": float(max(r.relative_kkt for r in warm
                                                                    if r.status == "optimal"))},
             "warm_over_cold_iterations": {"median": float(np.median(ratio)),

@@ -14,11 +14,16 @@ c = c0 + B_c theta over one matrix).
    starts cold. Plain PDHG is
    therefore both the fallback and the gate, and every solve is held to the
    same termination tolerance.
+5. Fallback at run time (``solve_family_with_fallback``): a warm-started
+   solve gets as many iterations as the most any training solve of the family
+   needed from the cold start (``LearnedWarmStart.budget``); an instance that
+   is not optimal by then is solved again from the cold start with the full
+   cap, and its result counts the iterations of both attempts.
 """
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -49,6 +54,25 @@ def solve_family(engine: Engine, problems: list, opt: PdhgOptions, x0s=None, y0s
     return out
 
 
+def solve_family_with_fallback(engine: Engine, problems: list, opt: PdhgOptions, x0s, y0s,
+                               budget: int, chunk: int = 256) -> list[PdhgResult]:
+    """Batched solves from the starts (x0s, y0s) with at most `budget`
+    iterations each; the instances that end without an optimal status are
+    solved again, batched, from the cold start with `opt`'s own cap. Their
+    results report the iterations of both attempts. Returns one result per
+    problem, in order."""
+    if x0s is None or budget <= 0 or budget >= opt.max_iterations:
+        return solve_family(engine, problems, opt, x0s, y0s, chunk)
+    warm = solve_family(engine, problems, replace(opt, max_iterations=budget), x0s, y0s, chunk)
+    redo = [i for i, r in enumerate(warm) if r.status != "optimal"]
+    if redo:
+        cold = solve_family(engine, [problems[i] for i in redo], opt, chunk=chunk)
+        for i, r in zip(redo, cold):
+            r.iterations += warm[i].iterations
+            warm[i] = r
+    return warm
+
+
 @dataclass
 class FitReport:
     samples: int
@@ -66,6 +90,7 @@ class LearnedWarmStart:
         self.hidden = hidden
         self.device = device
         self.net: Mlp | None = None
+        self.budget = 0  # iteration budget of a warm solve, set by fit()
 
     # ---- basis and network ----------------------------------------------------
 
@@ -84,6 +109,9 @@ class LearnedWarmStart:
         epochs / rounds epochs and keeps the parameters of the round with the
         lowest validation loss."""
         keep = [i for i, r in enumerate(results) if r.status == "optimal"]
+        # the warm solves' iteration budget: the most any optimal training
+        # solve of the family took from the cold start
+        self.budget = max((results[i].iterations for i in keep), default=0)
         th = np.asarray(thetas)[keep]
         xs = np.stack([results[i].primal for i in keep])
         ys = np.stack([results[i].dual for i in keep])
